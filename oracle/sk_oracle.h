@@ -1,0 +1,120 @@
+/*
+ * sk_oracle.h -- CPU oracle for the sparkit preconditioned-Krylov hot path.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This is a plain-C restatement of the sparkit
+ * reference's sequential algorithms (SpMV over CSR / ELLPACK / jagged
+ * diagonal / BSR, Jacobi and Chebyshev preconditioners, CG, BiCGSTAB and
+ * FGMRES), used by the tests, the smoke check and the CPU-baseline leg of
+ * the benchmark to check the CUDA library.  The product never links it.
+ *
+ * Parity pinning: tests/test_oracle.py checks every routine here against
+ * the known-answer vectors of the reference's own Catch2 tests
+ * (tests/golden/) and, bit for bit, against the reference itself compiled
+ * from its sources into oracle/_ref (see oracle/build_ref.sh).
+ */
+#ifndef SK_ORACLE_H
+#define SK_ORACLE_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum { SKO_CSR = 0, SKO_ELL = 1, SKO_JAD = 2, SKO_BSR = 3 };
+enum { SKO_PREC_IDENTITY = 0, SKO_PREC_JACOBI = 1, SKO_PREC_CHEBYSHEV = 2 };
+enum { SKO_BREAKDOWN = 4 };
+
+/* A matrix in one of the reference's storage layouts (int64 indices, as
+ * sparkit's size_type = std::ptrdiff_t).
+ *   CSR: row_ptr[nrow+1], col_ind[nnz]
+ *   ELL: col_ind[nrow*width] row-major, -1 padding; width = max nnz/row
+ *   JAD: perm[nrow], row_ptr = jdiag[width+1], width = number of jagged
+ *        diagonals, col_ind in jagged-diagonal order
+ *   BSR: row_ptr[nbr+1] over block rows, col_ind[nblocks] block columns,
+ *        vals = nblocks dense row-major block_rows x block_cols blocks */
+typedef struct {
+  int32_t format;
+  int64_t nrow, ncol;
+  int64_t width;
+  int64_t block_rows, block_cols;
+  const int64_t* row_ptr;
+  const int64_t* col_ind;
+  const int64_t* perm;
+  const void* vals;
+} sko_operator;
+
+typedef struct {
+  int32_t kind;
+  const void* inv_diag;          /* Jacobi: inverse diagonal */
+  const void* coeffs;            /* Chebyshev: degree+1 coefficients */
+  double lambda_min, lambda_max; /* Chebyshev interval */
+  int64_t degree;
+  const sko_operator* op;        /* Chebyshev: matrix (NULL = solver's A) */
+} sko_precond;
+
+/* CGConfig, sparkit/data/conjugate_gradient.hpp:48-74 */
+typedef struct {
+  double tolerance;
+  int64_t restart_iterations;
+  int64_t max_iterations;
+  int32_t collect_residuals;
+} sko_cg_config;
+
+/* Bicgstab_config, sparkit/data/bicgstab.hpp:25-42 */
+typedef struct {
+  double tolerance;
+  int64_t max_iterations;
+  int32_t collect_residuals;
+} sko_krylov_config;
+
+/* Fgmres_config, sparkit/data/fgmres.hpp:25-47 */
+typedef struct {
+  double tolerance;
+  int64_t restart_dimension;
+  int64_t max_iterations;
+  int32_t collect_residuals;
+} sko_fgmres_config;
+
+/* CGSummary / Bicgstab_summary / Fgmres_summary, minus the vector (which
+ * goes to the caller's history buffer). */
+typedef struct {
+  double residual_norm;
+  int64_t computed_iterations;
+  int32_t converged;
+  int32_t status;
+  int64_t history_length;
+} sko_summary;
+
+#define SKO_DECLARE(T, S)                                                     \
+  void sko_csr_spmv_##S(int64_t, const int64_t*, const int64_t*, const T*,    \
+                        const T*, T*);                                        \
+  void sko_ell_spmv_##S(int64_t, int64_t, const int64_t*, const T*, const T*, \
+                        T*);                                                  \
+  void sko_jad_spmv_##S(int64_t, int64_t, const int64_t*, const int64_t*,     \
+                        const int64_t*, const T*, const T*, T*);              \
+  void sko_bsr_spmv_##S(int64_t, int64_t, int64_t, const int64_t*,            \
+                        const int64_t*, const T*, const T*, T*);              \
+  void sko_extract_diagonal_##S(int64_t, int64_t, const int64_t*,             \
+                                const int64_t*, const T*, T*);                \
+  int sko_jacobi_##S(int64_t, int64_t, const int64_t*, const int64_t*,        \
+                     const T*, T*);                                           \
+  void sko_chebyshev_coeffs_##S(T, T, int64_t, T*);                           \
+  void sko_chebyshev_apply_##S(const sko_operator*, const T*, T, T, int64_t,  \
+                               const T*, T*);                                 \
+  void sko_cg_##S(const sko_operator*, const sko_precond*,                    \
+                  const sko_precond*, const T*, T*, const sko_cg_config*,     \
+                  sko_summary*, double*);                                     \
+  void sko_bicgstab_##S(const sko_operator*, const sko_precond*,              \
+                        const sko_precond*, const T*, T*,                     \
+                        const sko_krylov_config*, sko_summary*, double*);     \
+  void sko_fgmres_##S(const sko_operator*, const sko_precond*, const T*, T*,  \
+                      const sko_fgmres_config*, sko_summary*, double*);
+
+SKO_DECLARE(double, f64)
+SKO_DECLARE(float, f32)
+
+#ifdef __cplusplus
+}
+#endif
+#endif

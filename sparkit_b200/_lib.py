@@ -1,0 +1,135 @@
+"""ctypes binding of the C ABI in include/sparkit_b200.h.
+
+Loads the in-tree ``libsparkit_b200.so``.  There is no fallback: if the
+library is missing or cannot load, every entry point raises.
+"""
+import ctypes
+import os
+import threading
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libsparkit_b200.so")
+
+c_i64 = ctypes.c_int64
+c_i32 = ctypes.c_int32
+c_dbl = ctypes.c_double
+c_vp = ctypes.c_void_p
+P_i64 = ctypes.POINTER(ctypes.c_int64)
+
+SK_OK = 0
+STATUS_NAMES = {
+    0: "SK_OK", 1: "SK_INVALID_ARG", 2: "SK_INDEX_OVERFLOW", 3: "SK_OUT_OF_MEMORY",
+    4: "SK_BREAKDOWN", 5: "SK_NOT_CONVERGED", 6: "SK_TIMEOUT", 7: "SK_CUDA_ERROR",
+    8: "SK_ZERO_DIAGONAL", 9: "SK_NOT_SUPPORTED", 10: "SK_NO_DEVICE",
+}
+SK_F64, SK_F32 = 0, 1
+SK_CSR, SK_ELL, SK_JAD, SK_BSR = 0, 1, 2, 3
+
+
+class SkError(RuntimeError):
+    """A failed C-ABI call: .status holds the sk_status code."""
+
+    def __init__(self, status, message):
+        super().__init__(f"{STATUS_NAMES.get(status, status)}: {message}")
+        self.status = status
+
+
+class CgConfig(ctypes.Structure):
+    _fields_ = [("tolerance", c_dbl), ("restart_iterations", c_i64),
+                ("max_iterations", c_i64), ("collect_residuals", c_i32)]
+
+
+class BicgstabConfig(ctypes.Structure):
+    _fields_ = [("tolerance", c_dbl), ("max_iterations", c_i64), ("collect_residuals", c_i32)]
+
+
+class FgmresConfig(ctypes.Structure):
+    _fields_ = [("tolerance", c_dbl), ("restart_dimension", c_i64),
+                ("max_iterations", c_i64), ("collect_residuals", c_i32)]
+
+
+class Summary(ctypes.Structure):
+    _fields_ = [("residual_norm", c_dbl), ("computed_iterations", c_i64),
+                ("converged", c_i32), ("status", c_i32), ("history_length", c_i64)]
+
+
+# (name, argtypes) of every exported function, in header order.
+SIGNATURES = [
+    ("sk_version", []),
+    ("sk_last_error", []),
+    ("sk_device_count", [ctypes.POINTER(ctypes.c_int)]),
+    ("sk_launch_count", [P_i64]),
+    ("sk_device_alloc", [ctypes.POINTER(c_vp), ctypes.c_size_t]),
+    ("sk_device_free", [c_vp]),
+    ("sk_memcpy_h2d", [c_vp, c_vp, ctypes.c_size_t, c_vp]),
+    ("sk_memcpy_d2h", [c_vp, c_vp, ctypes.c_size_t, c_vp]),
+    ("sk_stream_synchronize", [c_vp]),
+    ("sk_csr_create", [ctypes.POINTER(c_vp), c_i64, c_i64, c_vp, c_vp, c_vp, ctypes.c_int]),
+    ("sk_ell_create", [ctypes.POINTER(c_vp), c_i64, c_i64, c_i64, c_vp, c_vp, ctypes.c_int]),
+    ("sk_jad_create", [ctypes.POINTER(c_vp), c_i64, c_i64, c_i64, c_vp, c_vp, c_vp, c_vp, ctypes.c_int]),
+    ("sk_bsr_create", [ctypes.POINTER(c_vp), c_i64, c_i64, c_i64, c_i64, c_vp, c_vp, c_vp, ctypes.c_int]),
+    ("sk_matrix_destroy", [c_vp]),
+    ("sk_matrix_info", [c_vp, P_i64]),
+    ("sk_matrix_add_f32_values", [c_vp]),
+    ("sk_spmv", [c_vp, c_vp, c_vp, c_vp]),
+    ("sk_spmv_f32", [c_vp, c_vp, c_vp, c_vp]),
+    ("sk_spmv_host", [c_vp, c_vp, c_vp]),
+    ("sk_dot", [ctypes.c_int, c_i64, c_vp, c_vp, ctypes.POINTER(c_dbl), c_vp]),
+    ("sk_nrm2", [ctypes.c_int, c_i64, c_vp, ctypes.POINTER(c_dbl), c_vp]),
+    ("sk_axpy", [ctypes.c_int, c_i64, c_dbl, c_vp, c_vp, c_vp]),
+    ("sk_xpay", [ctypes.c_int, c_i64, c_vp, c_dbl, c_vp, c_vp]),
+    ("sk_jacobi_create", [ctypes.POINTER(c_vp), c_vp]),
+    ("sk_chebyshev_create", [ctypes.POINTER(c_vp), c_vp, c_dbl, c_dbl, c_i64]),
+    ("sk_precond_apply", [c_vp, c_i64, c_vp, c_vp, c_vp]),
+    ("sk_precond_values", [c_vp, c_vp, c_i64, P_i64]),
+    ("sk_precond_destroy", [c_vp]),
+    ("sk_cg_solve", [c_vp, c_vp, c_vp, c_vp, c_vp, ctypes.POINTER(CgConfig), ctypes.POINTER(Summary),
+                     c_vp, c_vp]),
+    ("sk_bicgstab_solve", [c_vp, c_vp, c_vp, c_vp, c_vp, ctypes.POINTER(BicgstabConfig),
+                           ctypes.POINTER(Summary), c_vp, c_vp]),
+    ("sk_fgmres_solve", [c_vp, c_vp, c_vp, c_vp, ctypes.POINTER(FgmresConfig), ctypes.POINTER(Summary),
+                         c_vp, c_vp]),
+    ("sk_cg_solve_host", [c_vp, c_vp, c_vp, c_vp, c_vp, ctypes.POINTER(CgConfig), ctypes.POINTER(Summary),
+                          c_vp]),
+    ("sk_bicgstab_solve_host", [c_vp, c_vp, c_vp, c_vp, c_vp, ctypes.POINTER(BicgstabConfig),
+                                ctypes.POINTER(Summary), c_vp]),
+    ("sk_fgmres_solve_host", [c_vp, c_vp, c_vp, c_vp, ctypes.POINTER(FgmresConfig), ctypes.POINTER(Summary),
+                              c_vp]),
+]
+
+_lock = threading.Lock()
+_lib = None
+
+
+def lib():
+    """The loaded library; raises OSError when the .so is absent."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    with _lock:
+        if _lib is None:
+            if not os.path.exists(LIB_PATH):
+                raise OSError(
+                    f"{LIB_PATH} is missing: build it with `python -m sparkit_b200.build` "
+                    "(there is no CPU fallback)")
+            L = ctypes.CDLL(LIB_PATH)
+            for name, args in SIGNATURES:
+                fn = getattr(L, name)
+                fn.argtypes = args
+                fn.restype = ctypes.c_char_p if name in ("sk_version", "sk_last_error") else ctypes.c_int
+            _lib = L
+    return _lib
+
+
+def check(status):
+    """Raises SkError for a non-zero sk_status."""
+    if status != SK_OK:
+        msg = lib().sk_last_error()
+        raise SkError(status, msg.decode() if msg else "")
+    return status
+
+
+def launch_count():
+    n = c_i64(0)
+    check(lib().sk_launch_count(ctypes.byref(n)))
+    return n.value

@@ -1,0 +1,178 @@
+// sk_internal.cuh -- shared definitions of the sm_100a library: device
+// matrix layouts, status plumbing, launch accounting and the deterministic
+// grid-wide reduction used by every fused kernel.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <cstdint>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/sparkit_b200.h"
+
+namespace sk {
+
+using i64 = std::int64_t;
+
+constexpr int kThreads = 256;    // CTA size of the streaming kernels
+constexpr int kTileNnz = 2048;   // CSR: stored entries staged per CTA
+constexpr int kRowsMax = 256;    // CSR: rows per CTA (one per thread)
+constexpr int kBsrTileVals = 4096;  // BSR: block values staged per CTA
+constexpr int kMaxRed = 4;       // fused reductions carried per kernel
+
+// ------------------------------------------------------------------
+// Status plumbing
+// ------------------------------------------------------------------
+void set_error(std::string const& msg);
+sk_status fail(sk_status st, std::string const& msg);
+sk_status cuda_fail(cudaError_t e, char const* what);
+
+#define SK_CUDA(call)                                                    \
+  do {                                                                   \
+    cudaError_t e_ = (call);                                             \
+    if (e_ != cudaSuccess) return ::sk::cuda_fail(e_, #call);            \
+  } while (0)
+
+#define SK_CHECK(cond, st, msg)                                          \
+  do {                                                                   \
+    if (!(cond)) return ::sk::fail((st), (msg));                         \
+  } while (0)
+
+// Every kernel launch of the library goes through SK_LAUNCH so that
+// sk_launch_count() can account for them.
+extern std::atomic<i64> g_launches;
+#define SK_LAUNCH(kernel, grid, block, smem, stream, ...)                \
+  do {                                                                   \
+    ::sk::g_launches.fetch_add(1, std::memory_order_relaxed);            \
+    kernel<<<(grid), (block), (smem), (stream)>>>(__VA_ARGS__);          \
+  } while (0)
+
+// ------------------------------------------------------------------
+// Device layouts
+// ------------------------------------------------------------------
+
+// CSR: int32 indices; arrays padded by 4 entries so that the 16-byte
+// vector loads of a tile's last group stay inside the allocation.
+// part[nparts+1] are the first rows of the row blocks one CTA handles.
+struct Csr {
+  int* row_ptr = nullptr;
+  int* col_ind = nullptr;
+  void* vals = nullptr;
+  float* vals32 = nullptr;  // optional FP32 copy of FP64 values
+  int* part = nullptr;
+  unsigned char* lanes = nullptr;  // per row block: 1 = one thread per row
+  int nparts = 0;
+};
+
+// ELLPACK: slot-major (column-major) copy of the reference's row-major
+// layout: entry k of row i at k * nrow + i; rowlen[i] = entries before the
+// first -1 sentinel.
+struct Ell {
+  int* col = nullptr;
+  void* vals = nullptr;
+  int* rowlen = nullptr;
+  i64 width = 0;
+};
+
+// Jagged diagonal: the reference layout with int32 indices; plen[i] is the
+// number of diagonals that reach permuted position i.
+struct Jad {
+  int* perm = nullptr;
+  int* jdiag = nullptr;
+  int* col = nullptr;
+  void* vals = nullptr;
+  int* plen = nullptr;
+  i64 njd = 0;
+};
+
+// BSR: block CSR; part[] as for CSR but over block rows.
+struct Bsr {
+  int* row_ptr = nullptr;
+  int* col = nullptr;
+  void* vals = nullptr;
+  int* part = nullptr;
+  int nparts = 0;
+  i64 br = 0, bc = 0, nbr = 0, nbr_mult = 0, nblocks = 0;
+};
+
+}  // namespace sk
+
+struct sk_matrix_s {
+  sk_format format;
+  sk_dtype dtype;
+  int device = 0;
+  sk::i64 nrow = 0, ncol = 0, nnz = 0;
+  sk::Csr csr;
+  sk::Ell ell;
+  sk::Jad jad;
+  sk::Bsr bsr;
+  cudaStream_t stream = nullptr;
+  std::vector<void*> allocations;
+  sk::i64 device_bytes = 0;
+  void* io = nullptr;  // x and y buffers of the host-pointer calls
+  // Grow-only workspace of the solver calls on this handle.
+  void* ws = nullptr;
+  size_t ws_bytes = 0;
+  sk::i64 spmv_bytes() const;
+};
+
+struct sk_precond_s {
+  int kind;  // 1 = Jacobi, 2 = Chebyshev
+  sk_matrix A;
+  sk_dtype dtype;
+  sk::i64 n;
+  void* inv_diag = nullptr;  // Jacobi (dtype)
+  std::vector<double> coeffs;  // Chebyshev, host copy (double)
+  double lambda_min = 0, lambda_max = 0;
+  sk::i64 degree = 0;
+  void* work = nullptr;  // Chebyshev: 3 n-vectors
+  float* inv_diag32 = nullptr;  // FP32 copy for mixed precision
+};
+
+namespace sk {
+
+cudaStream_t pick_stream(sk_matrix A, sk_stream s);
+sk_status dev_alloc(sk_matrix A, void** p, size_t bytes);
+
+// Grid-wide deterministic reduction workspace: one slot of kMaxRed doubles
+// per CTA plus an arrival counter.  The last CTA to arrive sums the slots in
+// CTA order, so the result does not depend on scheduling.
+struct RedWs {
+  double* partials = nullptr;
+  unsigned* counter = nullptr;
+  int capacity = 0;  // CTAs
+};
+
+// Solver scalars resident on the device for a whole solve.  Written only
+// by the finalize step of a fused kernel (one thread of the last CTA) or by
+// a single-thread kernel; read by every later kernel of the solve.
+struct Scalars {
+  double bnorm;     // ||b||
+  double rz;        // CG: <r, z>
+  double alpha;
+  double beta;
+  double omega;
+  double rho;       // BiCGSTAB: rho of the last full step
+  double rho_new;   // BiCGSTAB: <r_hat, r> for the next step
+  double rnorm;     // last residual norm recorded
+  double tol;
+  double aux;       // FGMRES: 1 / beta or 1 / h_{j+1,j}
+  long long iters;
+  long long hist_len;
+  long long max_iters;
+  long long jfinal; // FGMRES: last Arnoldi step of the cycle
+  int converged;
+  int done;         // later kernels of the solve (or cycle) are no-ops
+  int status;
+  int half;         // BiCGSTAB: half-step convergence, x update pending
+  int skip;         // BiCGSTAB: omega == 0, skip the full-step update
+  int beta0;        // FGMRES: initial residual exactly zero
+  int hist_on;
+  int pad;
+};
+inline int ceil_div(i64 a, i64 b) { return static_cast<int>((a + b - 1) / b); }
+
+}  // namespace sk

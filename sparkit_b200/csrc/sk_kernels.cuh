@@ -1,0 +1,444 @@
+// sk_kernels.cuh -- device code shared by the SpMV, BLAS-1, preconditioner
+// and solver translation units.
+//
+// Arithmetic policy: products and sums are written with the _rn
+// intrinsics, so nvcc never contracts a multiply and an add into an FMA.
+// With the sequential per-row order used below this reproduces the
+// reference's rounding bit for bit wherever a row is summed by one thread
+// (CSR rows in blocks of short rows, every ELL, JAD and BSR row), and every
+// element-wise update of the solvers.  Only the dot products (grid
+// reductions in a fixed tree) round differently from the reference's
+// sequential std::inner_product.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "sk_internal.cuh"
+
+namespace sk {
+
+// ------------------------------------------------------------------
+// Rounding-explicit arithmetic
+// ------------------------------------------------------------------
+__device__ __forceinline__ double mul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ float mul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double add(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ float add(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ double sub(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ float sub(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ double dvd(double a, double b) { return __ddiv_rn(a, b); }
+__device__ __forceinline__ float dvd(float a, float b) { return __fdiv_rn(a, b); }
+
+// Streaming (evict-first) loads for matrix data that is read once per
+// product, so that the vectors stay in L2.
+__device__ __forceinline__ void load4_stream(const double* p, double (&o)[4]) {
+  double2 a = __ldcs(reinterpret_cast<const double2*>(p));
+  double2 b = __ldcs(reinterpret_cast<const double2*>(p) + 1);
+  o[0] = a.x; o[1] = a.y; o[2] = b.x; o[3] = b.y;
+}
+__device__ __forceinline__ void load4_stream(const float* p, float (&o)[4]) {
+  float4 a = __ldcs(reinterpret_cast<const float4*>(p));
+  o[0] = a.x; o[1] = a.y; o[2] = a.z; o[3] = a.w;
+}
+__device__ __forceinline__ void load4_stream(const int* p, int (&o)[4]) {
+  int4 a = __ldcs(reinterpret_cast<const int4*>(p));
+  o[0] = a.x; o[1] = a.y; o[2] = a.z; o[3] = a.w;
+}
+
+// ------------------------------------------------------------------
+// Deterministic block and grid reductions of NR doubles
+// ------------------------------------------------------------------
+template <int NR>
+__device__ __forceinline__ void warp_reduce(double (&v)[NR]) {
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1)
+#pragma unroll
+    for (int j = 0; j < NR; ++j) v[j] += __shfl_xor_sync(0xffffffffu, v[j], off);
+}
+
+// Result valid in thread 0.  Requires blockDim.x == kThreads.
+template <int NR>
+__device__ __forceinline__ void block_reduce(double (&v)[NR]) {
+  __shared__ double red_smem[kThreads / 32][NR > 0 ? NR : 1];
+  warp_reduce<NR>(v);
+  int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  __syncthreads();
+  if (lane == 0)
+#pragma unroll
+    for (int j = 0; j < NR; ++j) red_smem[warp][j] = v[j];
+  __syncthreads();
+  if (warp == 0) {
+#pragma unroll
+    for (int j = 0; j < NR; ++j) v[j] = lane < kThreads / 32 ? red_smem[lane][j] : 0.0;
+    warp_reduce<NR>(v);
+  }
+}
+
+// Sums v over the whole grid; the last CTA to arrive calls fin(total) on
+// thread 0.  Deterministic: CTA partials are summed in CTA order.
+template <int NR, class Fin>
+__device__ __forceinline__ void grid_reduce(double (&v)[NR], RedWs ws, Fin const& fin) {
+  __shared__ bool am_last;
+  block_reduce<NR>(v);
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int j = 0; j < NR; ++j) ws.partials[static_cast<size_t>(blockIdx.x) * kMaxRed + j] = v[j];
+    __threadfence();
+    unsigned prev = atomicAdd(ws.counter, 1u);
+    am_last = (prev == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (!am_last) return;
+  __threadfence();
+  double t[NR];
+#pragma unroll
+  for (int j = 0; j < NR; ++j) t[j] = 0.0;
+  for (unsigned b = threadIdx.x; b < gridDim.x; b += blockDim.x)
+#pragma unroll
+    for (int j = 0; j < NR; ++j) t[j] += __ldcg(ws.partials + static_cast<size_t>(b) * kMaxRed + j);
+  block_reduce<NR>(t);
+  if (threadIdx.x == 0) {
+    fin(t);
+    *ws.counter = 0u;
+  }
+}
+
+__device__ __forceinline__ bool solve_done(const Scalars* sc) {
+  return sc != nullptr && *reinterpret_cast<const volatile int*>(&sc->done) != 0;
+}
+
+// ------------------------------------------------------------------
+// SpMV epilogues.  operator()(row, value, red) receives each finished row
+// exactly once; red[] accumulates the fused reductions (kNR of them);
+// finalize(total) runs once, on the last CTA, with the grid totals.
+// ------------------------------------------------------------------
+template <typename T>
+struct EpiStore {
+  static constexpr int kNR = 0;
+  T* y;
+  __device__ void operator()(int row, T v, double*) const { y[row] = v; }
+  __device__ void finalize(const double*) const {}
+};
+
+// ------------------------------------------------------------------
+// CSR: one CTA per row block (part[]), entries staged through shared
+// memory with 16-byte streaming loads; rows of a short-row block summed
+// sequentially by one thread each (bit-exact), longer rows by L lanes.
+// ------------------------------------------------------------------
+template <typename T, class Epi>
+__global__ void __launch_bounds__(kThreads)
+csr_spmv_kernel(const int* __restrict__ rp, const int* __restrict__ ci,
+                const T* __restrict__ va, const T* __restrict__ x,
+                const int* __restrict__ part,
+                const unsigned char* __restrict__ lanes, Epi epi, RedWs ws,
+                const Scalars* sc) {
+  constexpr int NR = Epi::kNR;
+  __shared__ T prod[kTileNnz];
+  __shared__ int srp[kRowsMax + 1];
+  if (solve_done(sc)) return;
+  const int tid = threadIdx.x;
+  const int r0 = part[blockIdx.x];
+  const int nr = part[blockIdx.x + 1] - r0;
+  for (int t = tid; t <= nr; t += kThreads) srp[t] = rp[r0 + t];
+  __syncthreads();
+  const int s = srp[0], e = srp[nr];
+  double red[NR > 0 ? NR : 1];
+#pragma unroll
+  for (int j = 0; j < (NR > 0 ? NR : 1); ++j) red[j] = 0.0;
+
+  if (e - s > kTileNnz) {
+    // A single row longer than a tile: strided partial sums + tree.
+    double acc[1] = {0.0};
+    T part_sum = T(0);
+    for (int k = s + tid; k < e; k += kThreads)
+      part_sum = add(part_sum, mul(__ldcs(va + k), __ldg(x + __ldcs(ci + k))));
+    acc[0] = static_cast<double>(part_sum);
+    block_reduce<1>(acc);
+    if (tid == 0) epi(r0, static_cast<T>(acc[0]), red);
+  } else {
+    const int as = s & ~3;
+    const int ngroups = (((e + 3) & ~3) - as) >> 2;
+    for (int g = tid; g < ngroups; g += kThreads) {
+      const int k0 = as + 4 * g;
+      int c[4];
+      T v[4];
+      load4_stream(ci + k0, c);
+      load4_stream(va + k0, v);
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const int k = k0 + j;
+        if (k >= s && k < e) prod[k - s] = mul(v[j], __ldg(x + c[j]));
+      }
+    }
+    __syncthreads();
+    const int L = lanes[blockIdx.x];
+    if (L == 1) {
+      if (tid < nr) {
+        T sum = T(0);
+        const int a = srp[tid] - s, b = srp[tid + 1] - s;
+        for (int k = a; k < b; ++k) sum = add(sum, prod[k]);
+        epi(r0 + tid, sum, red);
+      }
+    } else {
+      // L lanes per row (a power of two chosen at upload from the block's
+      // longest row), strided partial sums then a shuffle tree.
+      const int rows_per_pass = kThreads / L;
+      const int npass = (nr + rows_per_pass - 1) / rows_per_pass;
+      const int lane = tid & (L - 1);
+      for (int pass = 0; pass < npass; ++pass) {
+        const int row = pass * rows_per_pass + tid / L;
+        T sum = T(0);
+        if (row < nr) {
+          const int a = srp[row] - s, b = srp[row + 1] - s;
+          for (int k = a + lane; k < b; k += L) sum = add(sum, prod[k]);
+        }
+        for (int off = L >> 1; off > 0; off >>= 1)
+          sum = add(sum, __shfl_xor_sync(0xffffffffu, sum, off));
+        if (row < nr && lane == 0) epi(r0 + row, sum, red);
+      }
+    }
+  }
+  if constexpr (NR > 0) {
+    grid_reduce<NR>(red, ws, [&](const double* t) { epi.finalize(t); });
+  }
+}
+
+// ------------------------------------------------------------------
+// ELLPACK (slot-major): one thread per row, sequential over its slots,
+// stopping at the row's length (the reference stops at the first -1).
+// ------------------------------------------------------------------
+template <typename T, class Epi>
+__global__ void __launch_bounds__(kThreads)
+ell_spmv_kernel(int nrow, const int* __restrict__ col, const T* __restrict__ va,
+                const int* __restrict__ rowlen, const T* __restrict__ x,
+                Epi epi, RedWs ws, const Scalars* sc) {
+  constexpr int NR = Epi::kNR;
+  if (solve_done(sc)) return;
+  double red[NR > 0 ? NR : 1];
+#pragma unroll
+  for (int j = 0; j < (NR > 0 ? NR : 1); ++j) red[j] = 0.0;
+  const int i = blockIdx.x * kThreads + threadIdx.x;
+  if (i < nrow) {
+    const int len = rowlen[i];
+    const size_t stride = static_cast<size_t>(nrow);
+    size_t idx = static_cast<size_t>(i);
+    T sum = T(0);
+    int k = 0;
+    for (; k + 4 <= len; k += 4) {
+      int c[4];
+      T v[4];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        c[j] = __ldcs(col + idx + j * stride);
+        v[j] = __ldcs(va + idx + j * stride);
+      }
+      T p[4];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) p[j] = mul(v[j], __ldg(x + c[j]));
+#pragma unroll
+      for (int j = 0; j < 4; ++j) sum = add(sum, p[j]);
+      idx += 4 * stride;
+    }
+    for (; k < len; ++k) {
+      sum = add(sum, mul(__ldcs(va + idx), __ldg(x + __ldcs(col + idx))));
+      idx += stride;
+    }
+    epi(i, sum, red);
+  }
+  if constexpr (NR > 0) {
+    grid_reduce<NR>(red, ws, [&](const double* t) { epi.finalize(t); });
+  }
+}
+
+// ------------------------------------------------------------------
+// Jagged diagonal: one thread per permuted position i, sweeping the
+// diagonals that reach it (coalesced across i), then y[perm[i]] = sum.
+// ------------------------------------------------------------------
+template <typename T, class Epi>
+__global__ void __launch_bounds__(kThreads)
+jad_spmv_kernel(int nrow, const int* __restrict__ perm, const int* __restrict__ jd,
+                const int* __restrict__ col, const T* __restrict__ va,
+                const int* __restrict__ plen, const T* __restrict__ x,
+                Epi epi, RedWs ws, const Scalars* sc) {
+  constexpr int NR = Epi::kNR;
+  if (solve_done(sc)) return;
+  double red[NR > 0 ? NR : 1];
+#pragma unroll
+  for (int j = 0; j < (NR > 0 ? NR : 1); ++j) red[j] = 0.0;
+  const int i = blockIdx.x * kThreads + threadIdx.x;
+  if (i < nrow) {
+    const int len = plen[i];
+    T sum = T(0);
+    int k = 0;
+    for (; k + 4 <= len; k += 4) {
+      int c[4];
+      T v[4];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const int idx = __ldg(jd + k + j) + i;
+        c[j] = __ldcs(col + idx);
+        v[j] = __ldcs(va + idx);
+      }
+      T p[4];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) p[j] = mul(v[j], __ldg(x + c[j]));
+#pragma unroll
+      for (int j = 0; j < 4; ++j) sum = add(sum, p[j]);
+    }
+    for (; k < len; ++k) {
+      const int idx = __ldg(jd + k) + i;
+      sum = add(sum, mul(__ldcs(va + idx), __ldg(x + __ldcs(col + idx))));
+    }
+    epi(perm[i], sum, red);
+  }
+  if constexpr (NR > 0) {
+    grid_reduce<NR>(red, ws, [&](const double* t) { epi.finalize(t); });
+  }
+}
+
+// ------------------------------------------------------------------
+// BSR: one CTA per block-row range; block values staged through shared
+// memory (16-byte streaming loads) as products with x, then one thread per
+// scalar row sums its block row in the reference's order:
+// y = ((0 + s_0) + s_1) + ..., s_b = sequential sum over the block's row.
+// Block rows at or past nrow / br (a partial last block row) give 0, as the
+// reference's truncating loop bound does.  BR/BC > 0 fixes the block shape
+// at compile time; 0 reads it at run time.
+// ------------------------------------------------------------------
+template <typename T, int BR, int BC, class Epi>
+__global__ void __launch_bounds__(kThreads)
+bsr_spmv_kernel(int nrow, int ncol, int br_rt, int bc_rt, int nbr_trunc,
+                const int* __restrict__ rp, const int* __restrict__ bcol,
+                const T* __restrict__ va, const T* __restrict__ x,
+                const int* __restrict__ part, Epi epi, RedWs ws,
+                const Scalars* sc) {
+  constexpr int NR = Epi::kNR;
+  constexpr int kMaxTileBlocks = 1024;
+  __shared__ T prod[kBsrTileVals];
+  __shared__ int srp[kThreads + 1];
+  __shared__ int scol[kMaxTileBlocks];
+  if (solve_done(sc)) return;
+  const int br = BR > 0 ? BR : br_rt;
+  const int bc = BC > 0 ? BC : bc_rt;
+  const int bsz = br * bc;
+  const int tid = threadIdx.x;
+  const int I0 = part[blockIdx.x];
+  const int nb = part[blockIdx.x + 1] - I0;  // block rows of this CTA
+  for (int t = tid; t <= nb; t += kThreads) srp[t] = rp[I0 + t];
+  __syncthreads();
+  const int bs = srp[0], be = srp[nb];
+  int tile_blocks = kBsrTileVals / bsz;
+  if (tile_blocks > kMaxTileBlocks) tile_blocks = kMaxTileBlocks;
+
+  // thread -> (block row, row within block)
+  const int my_I = tid / br;
+  const int my_r = tid - my_I * br;
+  const bool active = my_I < nb;
+  T acc = T(0);
+  int my_b = active ? srp[my_I] : 0;
+  const int my_e = active ? srp[my_I + 1] : 0;
+
+  for (int cb = bs; cb < be; cb += tile_blocks) {
+    const int ce = cb + tile_blocks < be ? cb + tile_blocks : be;
+    __syncthreads();
+    for (int t = tid; t < ce - cb; t += kThreads) scol[t] = bcol[cb + t];
+    __syncthreads();
+    const size_t vs = static_cast<size_t>(cb) * bsz, ve = static_cast<size_t>(ce) * bsz;
+    const size_t as = vs & ~static_cast<size_t>(3);
+    const int ngroups = static_cast<int>((((ve + 3) & ~static_cast<size_t>(3)) - as) >> 2);
+    for (int g = tid; g < ngroups; g += kThreads) {
+      const size_t e0 = as + 4 * static_cast<size_t>(g);
+      T v[4];
+      load4_stream(va + e0, v);
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const size_t e = e0 + j;
+        if (e >= vs && e < ve) {
+          const int local = static_cast<int>(e - vs);
+          const int lb = local / bsz;
+          const int rem = local - lb * bsz;
+          const int c = rem % bc;
+          const int xc = scol[lb] * bc + c;
+          prod[local] = xc < ncol ? mul(v[j], __ldg(x + xc)) : T(0);
+        }
+      }
+    }
+    __syncthreads();
+    if (active) {
+      for (; my_b < my_e && my_b < ce; ++my_b) {
+        const int base = (my_b - cb) * bsz + my_r * bc;
+        T s = T(0);
+        for (int c = 0; c < bc; ++c) s = add(s, prod[base + c]);
+        acc = add(acc, s);
+      }
+    }
+  }
+  double red[NR > 0 ? NR : 1];
+#pragma unroll
+  for (int j = 0; j < (NR > 0 ? NR : 1); ++j) red[j] = 0.0;
+  if (active) {
+    const int I = I0 + my_I;
+    const int row = I * br + my_r;
+    if (row < nrow) epi(row, I < nbr_trunc ? acc : T(0), red);
+  }
+  if constexpr (NR > 0) {
+    grid_reduce<NR>(red, ws, [&](const double* t) { epi.finalize(t); });
+  }
+}
+
+// Grid size of the SpMV launch for a handle (for sizing RedWs).
+inline int spmv_grid(const sk_matrix_s* A) {
+  switch (A->format) {
+    case SK_CSR: return A->csr.nparts;
+    case SK_BSR: return A->bsr.nparts;
+    default: return ceil_div(A->nrow, kThreads);
+  }
+}
+
+// Launches y-epilogue SpMV on any format.  vals_override lets the
+// mixed-precision path run the FP32 copy of an FP64 CSR handle.
+template <typename T, class Epi>
+void launch_spmv(const sk_matrix_s* A, const T* x, Epi const& epi, RedWs ws,
+                 const Scalars* sc, cudaStream_t st,
+                 const T* vals_override = nullptr) {
+  if (A->nrow == 0) return;
+  switch (A->format) {
+    case SK_CSR: {
+      const T* v = vals_override ? vals_override : static_cast<const T*>(A->csr.vals);
+      SK_LAUNCH((csr_spmv_kernel<T, Epi>), A->csr.nparts, kThreads, 0, st,
+                A->csr.row_ptr, A->csr.col_ind, v, x, A->csr.part, A->csr.lanes, epi,
+                ws, sc);
+      break;
+    }
+    case SK_ELL:
+      SK_LAUNCH((ell_spmv_kernel<T, Epi>), ceil_div(A->nrow, kThreads), kThreads, 0, st,
+                static_cast<int>(A->nrow), A->ell.col, static_cast<const T*>(A->ell.vals),
+                A->ell.rowlen, x, epi, ws, sc);
+      break;
+    case SK_JAD:
+      SK_LAUNCH((jad_spmv_kernel<T, Epi>), ceil_div(A->nrow, kThreads), kThreads, 0, st,
+                static_cast<int>(A->nrow), A->jad.perm, A->jad.jdiag, A->jad.col,
+                static_cast<const T*>(A->jad.vals), A->jad.plen, x, epi, ws, sc);
+      break;
+    case SK_BSR: {
+      const auto& b = A->bsr;
+      const T* v = static_cast<const T*>(b.vals);
+      if (b.br == 3 && b.bc == 3)
+        SK_LAUNCH((bsr_spmv_kernel<T, 3, 3, Epi>), b.nparts, kThreads, 0, st,
+                  static_cast<int>(A->nrow), static_cast<int>(A->ncol), 3, 3,
+                  static_cast<int>(b.nbr_mult), b.row_ptr, b.col, v, x, b.part, epi, ws, sc);
+      else if (b.br == 2 && b.bc == 2)
+        SK_LAUNCH((bsr_spmv_kernel<T, 2, 2, Epi>), b.nparts, kThreads, 0, st,
+                  static_cast<int>(A->nrow), static_cast<int>(A->ncol), 2, 2,
+                  static_cast<int>(b.nbr_mult), b.row_ptr, b.col, v, x, b.part, epi, ws, sc);
+      else
+        SK_LAUNCH((bsr_spmv_kernel<T, 0, 0, Epi>), b.nparts, kThreads, 0, st,
+                  static_cast<int>(A->nrow), static_cast<int>(A->ncol),
+                  static_cast<int>(b.br), static_cast<int>(b.bc),
+                  static_cast<int>(b.nbr_mult), b.row_ptr, b.col, v, x, b.part, epi, ws, sc);
+      break;
+    }
+  }
+}
+
+}  // namespace sk

@@ -1,0 +1,329 @@
+// sk_ops.cu -- C ABI of the SpMV, BLAS-1 and preconditioner operations.
+#include <cmath>
+#include <mutex>
+#include <vector>
+
+#include "sk_vec.cuh"
+
+namespace sk {
+
+// Reduction workspace of the standalone BLAS-1 calls: one per process,
+// grown on demand, serialized by a mutex (those calls synchronize).
+static std::mutex g_red_mutex;
+static RedWs g_red;
+static double* g_red_out = nullptr;
+
+static sk_status global_red(int ctas, RedWs* ws, double** out) {
+  if (g_red.capacity < ctas) {
+    if (g_red.partials) cudaFree(g_red.partials);
+    if (g_red.counter) cudaFree(g_red.counter);
+    g_red = RedWs{};
+    SK_CUDA(cudaMalloc(&g_red.partials, static_cast<size_t>(ctas) * kMaxRed * sizeof(double)));
+    SK_CUDA(cudaMalloc(&g_red.counter, sizeof(unsigned)));
+    SK_CUDA(cudaMemset(g_red.counter, 0, sizeof(unsigned)));
+    g_red.capacity = ctas;
+  }
+  if (!g_red_out) SK_CUDA(cudaMalloc(&g_red_out, 8 * sizeof(double)));
+  *ws = g_red;
+  *out = g_red_out;
+  return SK_OK;
+}
+
+__global__ void extract_inv_diag_kernel(i64 len, const int* __restrict__ rp,
+                                        const int* __restrict__ ci, const double* __restrict__ v64,
+                                        const float* __restrict__ v32, int f32, void* out,
+                                        unsigned long long* zeros) {
+  i64 i = blockIdx.x * static_cast<i64>(blockDim.x) + threadIdx.x;
+  if (i >= len) return;
+  int lo = rp[i], hi = rp[i + 1];
+  const int end = hi;
+  while (lo < hi) {  // lower_bound of column i, unary.hpp:30-32
+    int mid = lo + (hi - lo) / 2;
+    if (ci[mid] < i) lo = mid + 1; else hi = mid;
+  }
+  const bool found = lo < end && ci[lo] == i;
+  if (f32) {
+    float d = found ? v32[lo] : 0.0f;
+    if (d == 0.0f) atomicAdd(zeros, 1ull);
+    static_cast<float*>(out)[i] = d == 0.0f ? 0.0f : __fdiv_rn(1.0f, d);
+  } else {
+    double d = found ? v64[lo] : 0.0;
+    if (d == 0.0) atomicAdd(zeros, 1ull);
+    static_cast<double*>(out)[i] = d == 0.0 ? 0.0 : __ddiv_rn(1.0, d);
+  }
+}
+
+// Chebyshev coefficients of 1/lambda on [lmin, lmax]: the discrete cosine
+// sampling of chebyshev_preconditioner.hpp:53-73, evaluated on the host in
+// the value type T with the C library's cos.
+template <typename T>
+static std::vector<double> cheb_coeffs(T lmin, T lmax, i64 degree) {
+  const i64 d = degree;
+  const i64 N = std::max<i64>(d + 1, 64);
+  const T pi = static_cast<T>(3.141592653589793238462643383279502884L);
+  const T center = (lmax + lmin) / T(2);
+  const T half_width = (lmax - lmin) / T(2);
+  std::vector<double> out(static_cast<size_t>(d + 1));
+  for (i64 k = 0; k <= d; ++k) {
+    T ck = T(0);
+    for (i64 j = 0; j < N; ++j) {
+      T tj = std::cos(pi * (T(j) + T(0.5)) / T(N));
+      T lj = center + half_width * tj;
+      T fj = T(1) / lj;
+      T cos_k = std::cos(pi * T(k) * (T(j) + T(0.5)) / T(N));
+      ck += fj * cos_k;
+    }
+    out[static_cast<size_t>(k)] = static_cast<double>(T(2) * ck / T(N));
+  }
+  out[0] = static_cast<double>(static_cast<T>(out[0]) * T(0.5));
+  return out;
+}
+
+template <typename T>
+static void precond_apply_t(const sk_precond_s* M, i64 n, const T* r, T* z, RedWs ws,
+                            const Scalars* sc, cudaStream_t st) {
+  if (!M) {
+    launch_vec(n, OpCopy<T>{r, z}, ws, sc, st);
+  } else if (M->kind == 1) {
+    launch_vec(n, OpJacobi<T>{static_cast<const T*>(M->inv_diag), r, z}, ws, sc, st);
+  } else {
+    chebyshev_apply_device<T>(M, r, z, static_cast<T*>(M->work), ws, sc, st);
+  }
+}
+
+void precond_apply_dispatch(const sk_precond_s* M, sk_dtype dt, i64 n, const void* r, void* z,
+                            RedWs ws, const Scalars* sc, cudaStream_t st) {
+  if (dt == SK_F64)
+    precond_apply_t<double>(M, n, static_cast<const double*>(r), static_cast<double*>(z), ws, sc, st);
+  else
+    precond_apply_t<float>(M, n, static_cast<const float*>(r), static_cast<float*>(z), ws, sc, st);
+}
+
+}  // namespace sk
+
+using namespace sk;
+
+extern "C" {
+
+sk_status sk_spmv(sk_matrix A, const void* x_dev, void* y_dev, sk_stream s) {
+  SK_CHECK(A, SK_INVALID_ARG, "null handle");
+  SK_CHECK((x_dev || A->ncol == 0) && (y_dev || A->nrow == 0), SK_INVALID_ARG, "null vector");
+  cudaStream_t st = pick_stream(A, s);
+  if (A->dtype == SK_F64)
+    launch_spmv<double>(A, static_cast<const double*>(x_dev),
+                        EpiStore<double>{static_cast<double*>(y_dev)}, RedWs{}, nullptr, st);
+  else
+    launch_spmv<float>(A, static_cast<const float*>(x_dev),
+                       EpiStore<float>{static_cast<float*>(y_dev)}, RedWs{}, nullptr, st);
+  SK_CUDA(cudaGetLastError());
+  return SK_OK;
+}
+
+sk_status sk_spmv_f32(sk_matrix A, const float* x_dev, float* y_dev, sk_stream s) {
+  SK_CHECK(A, SK_INVALID_ARG, "null handle");
+  cudaStream_t st = pick_stream(A, s);
+  if (A->dtype == SK_F32) return sk_spmv(A, x_dev, y_dev, s);
+  SK_CHECK(A->format == SK_CSR && A->csr.vals32, SK_INVALID_ARG,
+           "no FP32 value copy: call sk_matrix_add_f32_values first");
+  launch_spmv<float>(A, x_dev, EpiStore<float>{y_dev}, RedWs{}, nullptr, st, A->csr.vals32);
+  SK_CUDA(cudaGetLastError());
+  return SK_OK;
+}
+
+sk_status sk_spmv_host(sk_matrix A, const void* x_host, void* y_host) {
+  SK_CHECK(A, SK_INVALID_ARG, "null handle");
+  SK_CHECK((x_host || A->ncol == 0) && (y_host || A->nrow == 0), SK_INVALID_ARG, "null vector");
+  const size_t V = A->dtype == SK_F64 ? 8 : 4;
+  if (!A->io) SK_CUDA(cudaMalloc(&A->io, (A->ncol + A->nrow + 16) * V));
+  char* xd = static_cast<char*>(A->io);
+  char* yd = xd + ((A->ncol + 8) * V);
+  if (A->ncol) SK_CUDA(cudaMemcpyAsync(xd, x_host, A->ncol * V, cudaMemcpyHostToDevice, A->stream));
+  sk_status st = sk_spmv(A, xd, yd, A->stream);
+  if (st != SK_OK) return st;
+  if (A->nrow) SK_CUDA(cudaMemcpyAsync(y_host, yd, A->nrow * V, cudaMemcpyDeviceToHost, A->stream));
+  SK_CUDA(cudaStreamSynchronize(A->stream));
+  return SK_OK;
+}
+
+sk_status sk_dot(sk_dtype dtype, int64_t n, const void* a_dev, const void* b_dev, double* result,
+                 sk_stream s) {
+  SK_CHECK(result && n >= 0, SK_INVALID_ARG, "bad arguments");
+  SK_CHECK(n == 0 || (a_dev && b_dev), SK_INVALID_ARG, "null vector");
+  if (n == 0) {
+    *result = 0.0;
+    return SK_OK;
+  }
+  std::lock_guard<std::mutex> lock(g_red_mutex);
+  RedWs ws;
+  double* out = nullptr;
+  sk_status st = global_red(vec_grid(n), &ws, &out);
+  if (st != SK_OK) return st;
+  cudaStream_t cs = static_cast<cudaStream_t>(s);
+  if (dtype == SK_F64)
+    launch_vec(n, OpDot<double>{static_cast<const double*>(a_dev), static_cast<const double*>(b_dev), out},
+               ws, nullptr, cs);
+  else
+    launch_vec(n, OpDot<float>{static_cast<const float*>(a_dev), static_cast<const float*>(b_dev), out},
+               ws, nullptr, cs);
+  SK_CUDA(cudaGetLastError());
+  SK_CUDA(cudaMemcpyAsync(result, out, sizeof(double), cudaMemcpyDeviceToHost, cs));
+  SK_CUDA(cudaStreamSynchronize(cs));
+  return SK_OK;
+}
+
+sk_status sk_nrm2(sk_dtype dtype, int64_t n, const void* a_dev, double* result, sk_stream s) {
+  sk_status st = sk_dot(dtype, n, a_dev, a_dev, result, s);
+  if (st == SK_OK) *result = std::sqrt(*result);
+  return st;
+}
+
+sk_status sk_axpy(sk_dtype dtype, int64_t n, double alpha, const void* x_dev, void* y_dev,
+                  sk_stream s) {
+  SK_CHECK(n >= 0 && (n == 0 || (x_dev && y_dev)), SK_INVALID_ARG, "bad arguments");
+  if (n == 0) return SK_OK;
+  cudaStream_t cs = static_cast<cudaStream_t>(s);
+  if (dtype == SK_F64)
+    launch_vec(n, OpAxpy<double>{alpha, static_cast<const double*>(x_dev), static_cast<double*>(y_dev)},
+               RedWs{}, nullptr, cs);
+  else
+    launch_vec(n, OpAxpy<float>{static_cast<float>(alpha), static_cast<const float*>(x_dev),
+                                static_cast<float*>(y_dev)},
+               RedWs{}, nullptr, cs);
+  SK_CUDA(cudaGetLastError());
+  return SK_OK;
+}
+
+sk_status sk_xpay(sk_dtype dtype, int64_t n, const void* x_dev, double beta, void* y_dev,
+                  sk_stream s) {
+  SK_CHECK(n >= 0 && (n == 0 || (x_dev && y_dev)), SK_INVALID_ARG, "bad arguments");
+  if (n == 0) return SK_OK;
+  cudaStream_t cs = static_cast<cudaStream_t>(s);
+  if (dtype == SK_F64)
+    launch_vec(n, OpXpay<double>{beta, static_cast<const double*>(x_dev), static_cast<double*>(y_dev)},
+               RedWs{}, nullptr, cs);
+  else
+    launch_vec(n, OpXpay<float>{static_cast<float>(beta), static_cast<const float*>(x_dev),
+                                static_cast<float*>(y_dev)},
+               RedWs{}, nullptr, cs);
+  SK_CUDA(cudaGetLastError());
+  return SK_OK;
+}
+
+sk_status sk_jacobi_create(sk_precond* out, sk_matrix A) {
+  SK_CHECK(out && A, SK_INVALID_ARG, "null argument");
+  *out = nullptr;
+  SK_CHECK(A->format == SK_CSR, SK_INVALID_ARG, "jacobi needs a CSR handle (jacobi.hpp:27)");
+  const i64 len = std::min(A->nrow, A->ncol);
+  const size_t V = A->dtype == SK_F64 ? 8 : 4;
+  auto* M = new sk_precond_s;
+  M->kind = 1;
+  M->A = A;
+  M->dtype = A->dtype;
+  M->n = len;
+  unsigned long long* zeros = nullptr;
+  cudaError_t e = cudaMalloc(&M->inv_diag, (len + 8) * V);
+  if (e == cudaSuccess) e = cudaMalloc(&zeros, 8);
+  if (e != cudaSuccess) {
+    cudaFree(M->inv_diag);
+    delete M;
+    return cuda_fail(e, "cudaMalloc");
+  }
+  cudaMemsetAsync(zeros, 0, 8, A->stream);
+  if (len > 0)
+    SK_LAUNCH(extract_inv_diag_kernel, ceil_div(len, kThreads), kThreads, 0, A->stream, len,
+              A->csr.row_ptr, A->csr.col_ind, static_cast<const double*>(A->csr.vals),
+              static_cast<const float*>(A->csr.vals), A->dtype == SK_F32 ? 1 : 0, M->inv_diag, zeros);
+  unsigned long long nz = 0;
+  cudaMemcpyAsync(&nz, zeros, 8, cudaMemcpyDeviceToHost, A->stream);
+  e = cudaStreamSynchronize(A->stream);
+  cudaFree(zeros);
+  if (e != cudaSuccess) {
+    cudaFree(M->inv_diag);
+    delete M;
+    return cuda_fail(e, "jacobi set-up");
+  }
+  if (nz) {
+    cudaFree(M->inv_diag);
+    delete M;
+    return fail(SK_ZERO_DIAGONAL, "jacobi: zero diagonal entry");
+  }
+  *out = M;
+  return SK_OK;
+}
+
+sk_status sk_chebyshev_create(sk_precond* out, sk_matrix A, double lambda_min, double lambda_max,
+                              int64_t degree) {
+  SK_CHECK(out && A, SK_INVALID_ARG, "null argument");
+  *out = nullptr;
+  SK_CHECK(A->format == SK_CSR, SK_INVALID_ARG,
+           "chebyshev preconditioner needs a CSR handle (chebyshev_preconditioner.hpp:29)");
+  SK_CHECK(degree >= 0, SK_INVALID_ARG, "negative degree");
+  SK_CHECK(A->nrow == A->ncol, SK_INVALID_ARG, "chebyshev preconditioner needs a square matrix");
+  auto* M = new sk_precond_s;
+  M->kind = 2;
+  M->A = A;
+  M->dtype = A->dtype;
+  M->n = A->nrow;
+  M->lambda_min = lambda_min;
+  M->lambda_max = lambda_max;
+  M->degree = degree;
+  if (A->dtype == SK_F64)
+    M->coeffs = cheb_coeffs<double>(lambda_min, lambda_max, degree);
+  else
+    M->coeffs = cheb_coeffs<float>(static_cast<float>(lambda_min), static_cast<float>(lambda_max), degree);
+  const size_t V = A->dtype == SK_F64 ? 8 : 4;
+  cudaError_t e = cudaMalloc(&M->work, (2 * A->nrow + 16) * V);
+  if (e != cudaSuccess) {
+    delete M;
+    return cuda_fail(e, "cudaMalloc");
+  }
+  *out = M;
+  return SK_OK;
+}
+
+sk_status sk_precond_apply(sk_precond M, int64_t n, const void* r_dev, void* z_dev, sk_stream s) {
+  SK_CHECK(n >= 0 && (n == 0 || (r_dev && z_dev)), SK_INVALID_ARG, "bad arguments");
+  if (n == 0) return SK_OK;
+  if (M) SK_CHECK(n == M->n, SK_INVALID_ARG, "vector length differs from the preconditioner's");
+  cudaStream_t cs = M ? pick_stream(M->A, s) : static_cast<cudaStream_t>(s);
+  // NULL preconditioner: identity on the FP64 path unless told otherwise.
+  sk_dtype dt = M ? M->dtype : SK_F64;
+  precond_apply_dispatch(M, dt, n, r_dev, z_dev, RedWs{}, nullptr, cs);
+  SK_CUDA(cudaGetLastError());
+  return SK_OK;
+}
+
+sk_status sk_precond_values(sk_precond M, void* host_out, int64_t capacity, int64_t* count) {
+  SK_CHECK(M && count, SK_INVALID_ARG, "null argument");
+  const size_t V = M->dtype == SK_F64 ? 8 : 4;
+  if (M->kind == 1) {
+    *count = M->n;
+    if (host_out && capacity >= M->n && M->n > 0) {
+      SK_CUDA(cudaStreamSynchronize(M->A->stream));
+      SK_CUDA(cudaMemcpy(host_out, M->inv_diag, M->n * V, cudaMemcpyDeviceToHost));
+    }
+  } else {
+    *count = static_cast<int64_t>(M->coeffs.size());
+    if (host_out && capacity >= *count) {
+      for (size_t k = 0; k < M->coeffs.size(); ++k) {
+        if (M->dtype == SK_F64)
+          static_cast<double*>(host_out)[k] = M->coeffs[k];
+        else
+          static_cast<float*>(host_out)[k] = static_cast<float>(M->coeffs[k]);
+      }
+    }
+  }
+  return SK_OK;
+}
+
+sk_status sk_precond_destroy(sk_precond M) {
+  if (!M) return SK_OK;
+  if (M->A && M->A->stream) cudaStreamSynchronize(M->A->stream);
+  if (M->inv_diag) cudaFree(M->inv_diag);
+  if (M->inv_diag32) cudaFree(M->inv_diag32);
+  if (M->work) cudaFree(M->work);
+  delete M;
+  return SK_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,1066 @@
+// sk_solvers.cu -- conjugate gradient, BiCGSTAB and FGMRES(m) on the
+// device.  The whole iteration stays on the GPU: scalars (alpha, beta,
+// rho, ...) live in device memory and are produced by the finalize step of
+// the fused kernel that computes them; a converged or exhausted solve sets
+// a `done` flag that turns every later kernel into a no-op.  The host
+// enqueues iterations in chunks and reads the flag back once per chunk
+// (CG, BiCGSTAB) or once per restart cycle (FGMRES).
+//
+// Each solver follows its reference template step for step (cited per
+// kernel), with the reference's element-wise arithmetic order; only the
+// dot products are summed in a different (fixed, deterministic) order.
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "sk_vec.cuh"
+
+namespace sk {
+
+void precond_apply_dispatch(const sk_precond_s* M, sk_dtype dt, i64 n, const void* r, void* z,
+                            RedWs ws, const Scalars* sc, cudaStream_t st);
+
+enum { PK_IDENTITY = 0, PK_JACOBI = 1, PK_OTHER = 2 };
+
+inline int prec_kind(const sk_precond_s* M) {
+  if (!M) return PK_IDENTITY;
+  return M->kind == 1 ? PK_JACOBI : PK_OTHER;
+}
+
+// ------------------------------------------------------------------
+// Workspace carved out of the handle's grow-only buffer.
+// ------------------------------------------------------------------
+struct Carver {
+  char* base;
+  size_t off = 0;
+  template <typename P>
+  P* take(size_t bytes) {
+    off = (off + 255) & ~size_t(255);
+    P* p = reinterpret_cast<P*>(base + off);
+    off += bytes;
+    return p;
+  }
+};
+
+static sk_status ensure_ws(sk_matrix A, size_t bytes) {
+  if (A->ws_bytes >= bytes) return SK_OK;
+  if (A->ws) {
+    cudaStreamSynchronize(A->stream);
+    cudaFree(A->ws);
+    A->ws = nullptr;
+    A->ws_bytes = 0;
+  }
+  SK_CUDA(cudaMalloc(&A->ws, bytes));
+  A->ws_bytes = bytes;
+  return SK_OK;
+}
+
+struct SolveCommon {
+  Scalars* sc;
+  RedWs ws;
+  double* hist;
+  size_t used;
+};
+
+// Reserves scalars, the reduction slots and the history buffer, then
+// `nvec` n-vectors of `vb` bytes each plus `extra` bytes.
+static sk_status carve_common(sk_matrix A, cudaStream_t st, i64 nvec, size_t vb, size_t extra,
+                              i64 hist_cap, SolveCommon* c, std::vector<char*>* vecs,
+                              char** extra_ptr) {
+  int cap = std::max(spmv_grid(A), vec_grid(A->nrow));
+  size_t need = 4096 + sizeof(Scalars) + 256 + static_cast<size_t>(cap) * kMaxRed * 8 +
+                static_cast<size_t>(hist_cap + 8) * 8 + static_cast<size_t>(nvec) * (vb + 256) +
+                extra + 1024;
+  sk_status s = ensure_ws(A, need);
+  if (s != SK_OK) return s;
+  Carver cv{static_cast<char*>(A->ws)};
+  c->sc = cv.take<Scalars>(sizeof(Scalars));
+  c->ws.counter = cv.take<unsigned>(sizeof(unsigned) * 4);
+  c->ws.partials = cv.take<double>(static_cast<size_t>(cap) * kMaxRed * 8);
+  c->ws.capacity = cap;
+  c->hist = cv.take<double>(static_cast<size_t>(hist_cap + 8) * 8);
+  for (i64 k = 0; k < nvec; ++k) vecs->push_back(cv.take<char>(vb));
+  if (extra_ptr) *extra_ptr = cv.take<char>(extra);
+  c->used = cv.off;
+  SK_CUDA(cudaMemsetAsync(c->sc, 0, sizeof(Scalars), st));
+  SK_CUDA(cudaMemsetAsync(c->ws.counter, 0, sizeof(unsigned) * 4, st));
+  return SK_OK;
+}
+
+static sk_status finish_summary(SolveCommon const& c, cudaStream_t st, sk_summary* out,
+                                double* history_host) {
+  Scalars h;
+  SK_CUDA(cudaMemcpyAsync(&h, c.sc, sizeof(Scalars), cudaMemcpyDeviceToHost, st));
+  SK_CUDA(cudaStreamSynchronize(st));
+  out->residual_norm = h.rnorm;
+  out->computed_iterations = h.iters;
+  out->converged = h.converged;
+  out->status = h.status;
+  out->history_length = h.hist_on ? h.hist_len : 0;
+  if (history_host && h.hist_on && h.hist_len > 0)
+    SK_CUDA(cudaMemcpy(history_host, c.hist, h.hist_len * sizeof(double), cudaMemcpyDeviceToHost));
+  return SK_OK;
+}
+
+static sk_status read_scalars(Scalars const* d, Scalars* h, cudaStream_t st) {
+  SK_CUDA(cudaMemcpyAsync(h, d, sizeof(Scalars), cudaMemcpyDeviceToHost, st));
+  SK_CUDA(cudaStreamSynchronize(st));
+  return SK_OK;
+}
+
+// Writes initial scalars from the host.
+static sk_status put_scalars(Scalars* d, Scalars const& h, cudaStream_t st) {
+  SK_CUDA(cudaMemcpyAsync(d, &h, sizeof(Scalars), cudaMemcpyHostToDevice, st));
+  return SK_OK;
+}
+
+__device__ __forceinline__ void record(Scalars* sc, double* hist, double v) {
+  sc->rnorm = v;
+  if (sc->hist_on) hist[sc->hist_len++] = v;
+}
+
+// ||b|| (conjugate_gradient.hpp:194, bicgstab.hpp:160, fgmres.hpp:168)
+template <typename T>
+struct OpNormB {
+  static constexpr int kNR = 1;
+  const T* b;
+  Scalars* sc;
+  __device__ bool prepare(const Scalars*) { return true; }
+  __device__ void operator()(i64 i, double* red) const { red[0] += static_cast<double>(mul(b[i], b[i])); }
+  __device__ void finalize(const double* t) const {
+    sc->bnorm = static_cast<double>(sqrt(static_cast<T>(t[0])));
+  }
+};
+
+template <typename T>
+static sk_status norm_b(const T* b, i64 n, SolveCommon const& c, cudaStream_t st, double* bnorm) {
+  launch_vec(n, OpNormB<T>{b, c.sc}, c.ws, nullptr, st);
+  SK_CUDA(cudaGetLastError());
+  Scalars h;
+  sk_status s = read_scalars(c.sc, &h, st);
+  if (s != SK_OK) return s;
+  *bnorm = h.bnorm;
+  return SK_OK;
+}
+
+// ==================================================================
+// Conjugate gradient, conjugate_gradient.hpp:122-312
+// ==================================================================
+
+// reorthogonalize (:217-230): r = b - A x; z = M_L r; rz = <r, z>; p = z.
+// The identity and Jacobi left preconditioners are fused into the epilogue.
+template <typename T, int LK>
+struct EpiCgResid {
+  static constexpr int kNR = LK == PK_OTHER ? 0 : 1;
+  const T* b;
+  T* r;
+  T* p;
+  const T* inv_d;
+  Scalars* sc;
+  __device__ void operator()(int row, T ax, double* red) const {
+    const T ri = sub(b[row], ax);
+    r[row] = ri;
+    if constexpr (LK == PK_IDENTITY) {
+      p[row] = ri;
+      red[0] += static_cast<double>(mul(ri, ri));
+    } else if constexpr (LK == PK_JACOBI) {
+      const T zi = mul(inv_d[row], ri);
+      p[row] = zi;
+      red[0] += static_cast<double>(mul(ri, zi));
+    }
+  }
+  __device__ void finalize(const double* t) const {
+    if constexpr (kNR > 0) sc->rz = static_cast<double>(static_cast<T>(t[0]));
+  }
+};
+
+// rz = <r, z>; p = z  (left preconditioner applied separately)
+template <typename T>
+struct OpCgReorthDot {
+  static constexpr int kNR = 1;
+  const T* r;
+  const T* z;
+  T* p;
+  Scalars* sc;
+  __device__ bool prepare(const Scalars* s) { return !solve_done(s); }
+  __device__ void operator()(i64 i, double* red) const {
+    const T zi = z[i];
+    p[i] = zi;
+    red[0] += static_cast<double>(mul(r[i], zi));
+  }
+  __device__ void finalize(const double* t) const { sc->rz = static_cast<double>(static_cast<T>(t[0])); }
+};
+
+// compute_step_size (:233-239): q = A p_hat; alpha = rz / <p, q>.
+template <typename T>
+struct EpiCgPq {
+  static constexpr int kNR = 1;
+  T* q;
+  const T* p;
+  Scalars* sc;
+  __device__ void operator()(int row, T v, double* red) const {
+    q[row] = v;
+    red[0] += static_cast<double>(mul(p[row], v));
+  }
+  __device__ void finalize(const double* t) const {
+    sc->alpha = static_cast<double>(static_cast<T>(sc->rz) / static_cast<T>(t[0]));
+  }
+};
+
+// compute_new_solution (:242-249), compute_new_residual (:252-259),
+// is_converged (:262-276), and for identity / Jacobi left preconditioners
+// the <r, z> of update_direction (:279-284).
+template <typename T, int LK>
+struct OpCgUpdate {
+  static constexpr int kNR = LK == PK_JACOBI ? 2 : 1;
+  T* x;
+  T* r;
+  const T* hatp;
+  const T* q;
+  const T* inv_d;
+  Scalars* sc;
+  double* hist;
+  T alpha;
+  __device__ bool prepare(const Scalars* s) {
+    if (solve_done(s)) return false;
+    alpha = static_cast<T>(s->alpha);
+    return true;
+  }
+  __device__ void operator()(i64 i, double* red) const {
+    x[i] = add(mul(alpha, hatp[i]), x[i]);
+    const T ri = sub(r[i], mul(alpha, q[i]));
+    r[i] = ri;
+    red[0] += static_cast<double>(mul(ri, ri));
+    if constexpr (LK == PK_JACOBI) red[1] += static_cast<double>(mul(ri, mul(inv_d[i], ri)));
+  }
+  __device__ void finalize(const double* t) const {
+    sc->iters += 1;
+    const T rn = sqrt(static_cast<T>(t[0]));
+    record(sc, hist, static_cast<double>(rn));
+    const bool conv = rn / static_cast<T>(sc->bnorm) < static_cast<T>(sc->tol);
+    sc->converged = conv ? 1 : 0;
+    if (conv || sc->iters >= sc->max_iters) sc->done = 1;
+    if (LK != PK_OTHER && !conv) {
+      const T rz_new = static_cast<T>(LK == PK_JACOBI ? t[1] : t[0]);
+      sc->beta = static_cast<double>(rz_new / static_cast<T>(sc->rz));
+      sc->rz = static_cast<double>(rz_new);
+    }
+  }
+};
+
+// update_direction with a separately applied left preconditioner:
+// beta = <r, z>_new / rz.
+template <typename T>
+struct OpCgBeta {
+  static constexpr int kNR = 1;
+  const T* r;
+  const T* z;
+  Scalars* sc;
+  __device__ bool prepare(const Scalars* s) { return !solve_done(s); }
+  __device__ void operator()(i64 i, double* red) const { red[0] += static_cast<double>(mul(r[i], z[i])); }
+  __device__ void finalize(const double* t) const {
+    const T rz_new = static_cast<T>(t[0]);
+    sc->beta = static_cast<double>(rz_new / static_cast<T>(sc->rz));
+    sc->rz = static_cast<double>(rz_new);
+  }
+};
+
+// p = z + beta p (:285-290), z recomputed in registers for identity/Jacobi.
+template <typename T, int LK>
+struct OpCgDirection {
+  static constexpr int kNR = 0;
+  T* p;
+  const T* r;
+  const T* z;
+  const T* inv_d;
+  T beta;
+  __device__ bool prepare(const Scalars* s) {
+    if (solve_done(s)) return false;
+    beta = static_cast<T>(s->beta);
+    return true;
+  }
+  __device__ void operator()(i64 i, double*) const {
+    T zi;
+    if constexpr (LK == PK_IDENTITY) zi = r[i];
+    else if constexpr (LK == PK_JACOBI) zi = mul(inv_d[i], r[i]);
+    else zi = z[i];
+    p[i] = add(zi, mul(beta, p[i]));
+  }
+  __device__ void finalize(const double*) const {}
+};
+
+template <typename T, int LK>
+static void cg_iteration(sk_matrix A, const sk_precond_s* L, const sk_precond_s* R, bool reorth,
+                         const T* b, T* x, T* r, T* z, T* p, T* hatp, T* q, SolveCommon const& c,
+                         cudaStream_t st) {
+  const i64 n = A->nrow;
+  const T* invL = L && L->kind == 1 ? static_cast<const T*>(L->inv_diag) : nullptr;
+  if (reorth) {
+    launch_spmv<T>(A, x, EpiCgResid<T, LK>{b, r, p, invL, c.sc}, c.ws, c.sc, st);
+    if constexpr (LK == PK_OTHER) {
+      precond_apply_dispatch(L, A->dtype, n, r, z, c.ws, c.sc, st);
+      launch_vec(n, OpCgReorthDot<T>{r, z, p, c.sc}, c.ws, c.sc, st);
+    }
+  }
+  const T* ph = p;
+  if (R) {
+    precond_apply_dispatch(R, A->dtype, n, p, hatp, c.ws, c.sc, st);
+    ph = hatp;
+  }
+  launch_spmv<T>(A, ph, EpiCgPq<T>{q, p, c.sc}, c.ws, c.sc, st);
+  launch_vec(n, OpCgUpdate<T, LK>{x, r, ph, q, invL, c.sc, c.hist, T(0)}, c.ws, c.sc, st);
+  if constexpr (LK == PK_OTHER) {
+    precond_apply_dispatch(L, A->dtype, n, r, z, c.ws, c.sc, st);
+    launch_vec(n, OpCgBeta<T>{r, z, c.sc}, c.ws, c.sc, st);
+  }
+  launch_vec(n, OpCgDirection<T, LK>{p, r, z, invL, T(0)}, c.ws, c.sc, st);
+}
+
+template <typename T>
+static sk_status cg_solve(sk_matrix A, sk_precond L, sk_precond R, const T* b, T* x,
+                          const sk_cg_config* cfg, sk_summary* out, double* history_host,
+                          cudaStream_t st) {
+  const i64 n = A->nrow;
+  const size_t vb = static_cast<size_t>(n + 8) * sizeof(T);
+  SolveCommon c;
+  std::vector<char*> v;
+  const i64 hist_cap = cfg->collect_residuals ? cfg->max_iterations : 0;
+  sk_status s = carve_common(A, st, 5, vb, 0, hist_cap, &c, &v, nullptr);
+  if (s != SK_OK) return s;
+  T *r = (T*)v[0], *z = (T*)v[1], *p = (T*)v[2], *hatp = (T*)v[3], *q = (T*)v[4];
+  *out = sk_summary{};
+  double bnorm = 0;
+  if ((s = norm_b<T>(b, n, c, st, &bnorm)) != SK_OK) return s;
+  if (bnorm == 0.0) {  // :195-199
+    SK_CUDA(cudaMemsetAsync(x, 0, n * sizeof(T), st));
+    SK_CUDA(cudaStreamSynchronize(st));
+    out->converged = 1;
+    return SK_OK;
+  }
+  Scalars h{};
+  h.bnorm = bnorm;
+  h.tol = cfg->tolerance;
+  h.max_iters = cfg->max_iterations;
+  h.hist_on = cfg->collect_residuals ? 1 : 0;
+  if ((s = put_scalars(c.sc, h, st)) != SK_OK) return s;
+  const int lk = prec_kind(L);
+  i64 k = 0, chunk = 8;
+  while (k < cfg->max_iterations) {
+    const i64 todo = std::min(chunk, cfg->max_iterations - k);
+    for (i64 j = 0; j < todo; ++j, ++k) {
+      const bool reorth = (k % cfg->restart_iterations) == 0;
+      if (lk == PK_IDENTITY)
+        cg_iteration<T, PK_IDENTITY>(A, L, R, reorth, b, x, r, z, p, hatp, q, c, st);
+      else if (lk == PK_JACOBI)
+        cg_iteration<T, PK_JACOBI>(A, L, R, reorth, b, x, r, z, p, hatp, q, c, st);
+      else
+        cg_iteration<T, PK_OTHER>(A, L, R, reorth, b, x, r, z, p, hatp, q, c, st);
+    }
+    SK_CUDA(cudaGetLastError());
+    if ((s = read_scalars(c.sc, &h, st)) != SK_OK) return s;
+    if (h.done) break;
+    chunk = std::min<i64>(chunk * 2, 64);
+  }
+  return finish_summary(c, st, out, history_host);
+}
+
+// ==================================================================
+// BiCGSTAB, bicgstab.hpp:93-361
+// ==================================================================
+
+// compute_initial_residual (:186-194), initialize_shadow_residual (:197),
+// and the first rho_new = <r_hat, r> (:203).
+template <typename T>
+struct EpiBiResid {
+  static constexpr int kNR = 1;
+  const T* b;
+  T* r;
+  T* r_hat;
+  Scalars* sc;
+  __device__ void operator()(int row, T ax, double* red) const {
+    const T ri = sub(b[row], ax);
+    r[row] = ri;
+    r_hat[row] = ri;
+    red[0] += static_cast<double>(mul(ri, ri));
+  }
+  __device__ void finalize(const double* t) const {
+    sc->rho_new = static_cast<double>(static_cast<T>(t[0]));
+    sc->rho = sc->alpha = sc->omega = 1.0;
+    if (sc->max_iters <= 0) {
+      sc->done = 1;
+    } else if (static_cast<T>(sc->rho_new) == T(0)) {  // :204 (the reference spins forever)
+      sc->status = SK_BREAKDOWN;
+      sc->done = 1;
+    }
+  }
+};
+
+// update_search_direction (:233-238) and, for identity / Jacobi
+// preconditioners, apply_preconditioner_to_p (:241-244) in registers.
+template <typename T, int LK, int RK>
+struct OpBiP {
+  static constexpr int kNR = 0;
+  T* p;
+  const T* r;
+  const T* v;
+  T* p_hat;
+  const T* invL;
+  const T* invR;
+  T beta, omega;
+  __device__ bool prepare(const Scalars* s) {
+    if (solve_done(s)) return false;
+    const T rho_new = static_cast<T>(s->rho_new);
+    omega = static_cast<T>(s->omega);
+    beta = (rho_new / static_cast<T>(s->rho)) * (static_cast<T>(s->alpha) / omega);
+    return true;
+  }
+  __device__ void operator()(i64 i, double*) const {
+    const T pi = add(r[i], mul(beta, sub(p[i], mul(omega, v[i]))));
+    p[i] = pi;
+    if constexpr (LK != PK_OTHER && RK != PK_OTHER) {
+      T t = pi;
+      if constexpr (LK == PK_JACOBI) t = mul(invL[i], t);
+      if constexpr (RK == PK_JACOBI) t = mul(invR[i], t);
+      p_hat[i] = t;
+    }
+  }
+  __device__ void finalize(const double*) const {}
+};
+
+// compute_v (:247-250) and alpha = rho_new / <r_hat, v> (:211).
+template <typename T>
+struct EpiBiV {
+  static constexpr int kNR = 1;
+  T* v;
+  const T* r_hat;
+  Scalars* sc;
+  __device__ void operator()(int row, T val, double* red) const {
+    v[row] = val;
+    red[0] += static_cast<double>(mul(r_hat[row], val));
+  }
+  __device__ void finalize(const double* t) const {
+    sc->iters += 1;
+    sc->alpha = static_cast<double>(static_cast<T>(sc->rho_new) / static_cast<T>(t[0]));
+  }
+};
+
+// compute_s (:253-258) and check_half_step_convergence (:261-268).
+template <typename T>
+struct OpBiS {
+  static constexpr int kNR = 1;
+  T* s;
+  const T* r;
+  const T* v;
+  Scalars* sc;
+  double* hist;
+  T alpha;
+  __device__ bool prepare(const Scalars* st) {
+    if (solve_done(st)) return false;
+    alpha = static_cast<T>(st->alpha);
+    return true;
+  }
+  __device__ void operator()(i64 i, double* red) const {
+    const T si = sub(r[i], mul(alpha, v[i]));
+    s[i] = si;
+    red[0] += static_cast<double>(mul(si, si));
+  }
+  __device__ void finalize(const double* t) const {
+    const T sn = sqrt(static_cast<T>(t[0]));
+    record(sc, hist, static_cast<double>(sn));
+    if (sn / static_cast<T>(sc->bnorm) < static_cast<T>(sc->tol)) {
+      sc->half = 1;
+      sc->converged = 1;
+      sc->done = 1;
+    }
+  }
+};
+
+// Either update_solution_half_step (:270-278) when the half step
+// converged, or apply_preconditioner_to_s (:281-284) for identity / Jacobi.
+template <typename T, int LK, int RK>
+struct OpBiHalfOrS {
+  static constexpr int kNR = 1;  // only to get a finalize that clears `half`
+  T* x;
+  const T* p_hat;
+  const T* s;
+  T* s_hat;
+  const T* invL;
+  const T* invR;
+  Scalars* sc;
+  T alpha;
+  int mode;  // 1 = half-step x update, 2 = s_hat
+  __device__ bool prepare(const Scalars* st) {
+    if (st->half) {
+      mode = 1;
+      alpha = static_cast<T>(st->alpha);
+      return true;
+    }
+    if (solve_done(st)) return false;
+    mode = 2;
+    return LK != PK_OTHER && RK != PK_OTHER;
+  }
+  __device__ void operator()(i64 i, double*) const {
+    if (mode == 1) {
+      x[i] = add(x[i], mul(alpha, p_hat[i]));
+    } else if constexpr (LK != PK_OTHER && RK != PK_OTHER) {
+      T t = s[i];
+      if constexpr (LK == PK_JACOBI) t = mul(invL[i], t);
+      if constexpr (RK == PK_JACOBI) t = mul(invR[i], t);
+      s_hat[i] = t;
+    }
+  }
+  __device__ void finalize(const double*) const {
+    if (mode == 1) sc->half = 0;
+  }
+};
+
+// compute_t (:287-290) and compute_omega (:293-297).
+template <typename T>
+struct EpiBiT {
+  static constexpr int kNR = 2;
+  T* t;
+  const T* s;
+  Scalars* sc;
+  __device__ void operator()(int row, T val, double* red) const {
+    t[row] = val;
+    red[0] += static_cast<double>(mul(val, val));
+    red[1] += static_cast<double>(mul(val, s[row]));
+  }
+  __device__ void finalize(const double* tot) const {
+    sc->iters += 1;
+    const T tt = static_cast<T>(tot[0]);
+    const T om = tt == T(0) ? T(0) : static_cast<T>(tot[1]) / tt;
+    sc->omega = static_cast<double>(om);
+    if (om == T(0)) {  // :223, step ends without the full update
+      sc->skip = 1;
+    }
+  }
+};
+
+// update_solution_full_step (:300-306), update_residual (:309-314),
+// rho = rho_new (:227), check_full_step_convergence (:317-324), and the
+// next step's rho_new = <r_hat, r> (:203) with its zero check (:204).
+template <typename T>
+struct OpBiUpdate {
+  static constexpr int kNR = 2;
+  T* x;
+  T* r;
+  const T* r_hat;
+  const T* p_hat;
+  const T* s_hat;
+  const T* s;
+  const T* t;
+  Scalars* sc;
+  double* hist;
+  T alpha, omega;
+  int skip;
+  __device__ bool prepare(const Scalars* st) {
+    if (solve_done(st)) return false;
+    alpha = static_cast<T>(st->alpha);
+    omega = static_cast<T>(st->omega);
+    skip = st->skip;
+    return true;
+  }
+  __device__ void operator()(i64 i, double* red) const {
+    if (skip) return;
+    x[i] = add(x[i], add(mul(alpha, p_hat[i]), mul(omega, s_hat[i])));
+    const T ri = sub(s[i], mul(omega, t[i]));
+    r[i] = ri;
+    red[0] += static_cast<double>(mul(ri, ri));
+    red[1] += static_cast<double>(mul(r_hat[i], ri));
+  }
+  __device__ void finalize(const double* tot) const {
+    if (skip) {
+      sc->skip = 0;
+    } else {
+      sc->rho = sc->rho_new;
+      const T rn = sqrt(static_cast<T>(tot[0]));
+      record(sc, hist, static_cast<double>(rn));
+      if (rn / static_cast<T>(sc->bnorm) < static_cast<T>(sc->tol)) {
+        sc->converged = 1;
+        sc->done = 1;
+        return;
+      }
+      sc->rho_new = static_cast<double>(static_cast<T>(tot[1]));
+    }
+    if (sc->iters >= sc->max_iters) {
+      sc->done = 1;
+    } else if (static_cast<T>(sc->rho_new) == T(0)) {
+      sc->status = SK_BREAKDOWN;
+      sc->done = 1;
+    }
+  }
+};
+
+template <typename T, int LK, int RK>
+static void bicgstab_step(sk_matrix A, const sk_precond_s* L, const sk_precond_s* R, T* x, T* r,
+                          T* r_hat, T* p, T* v, T* s, T* t, T* p_hat, T* s_hat, T* tmp,
+                          SolveCommon const& c, cudaStream_t st) {
+  const i64 n = A->nrow;
+  const T* invL = L && L->kind == 1 ? static_cast<const T*>(L->inv_diag) : nullptr;
+  const T* invR = R && R->kind == 1 ? static_cast<const T*>(R->inv_diag) : nullptr;
+  constexpr bool fused = LK != PK_OTHER && RK != PK_OTHER;
+  launch_vec(n, OpBiP<T, LK, RK>{p, r, v, p_hat, invL, invR, T(0), T(0)}, c.ws, c.sc, st);
+  if constexpr (!fused) {
+    precond_apply_dispatch(L, A->dtype, n, p, tmp, c.ws, c.sc, st);
+    precond_apply_dispatch(R, A->dtype, n, tmp, p_hat, c.ws, c.sc, st);
+  }
+  launch_spmv<T>(A, p_hat, EpiBiV<T>{v, r_hat, c.sc}, c.ws, c.sc, st);
+  launch_vec(n, OpBiS<T>{s, r, v, c.sc, c.hist, T(0)}, c.ws, c.sc, st);
+  launch_vec(n, OpBiHalfOrS<T, LK, RK>{x, p_hat, s, s_hat, invL, invR, c.sc, T(0), 0}, c.ws,
+             c.sc, st);
+  if constexpr (!fused) {
+    precond_apply_dispatch(L, A->dtype, n, s, tmp, c.ws, c.sc, st);
+    precond_apply_dispatch(R, A->dtype, n, tmp, s_hat, c.ws, c.sc, st);
+  }
+  launch_spmv<T>(A, s_hat, EpiBiT<T>{t, s, c.sc}, c.ws, c.sc, st);
+  launch_vec(n, OpBiUpdate<T>{x, r, r_hat, p_hat, s_hat, s, t, c.sc, c.hist, T(0), T(0), 0}, c.ws,
+             c.sc, st);
+}
+
+template <typename T>
+static sk_status bicgstab_solve(sk_matrix A, sk_precond L, sk_precond R, const T* b, T* x,
+                                const sk_bicgstab_config* cfg, sk_summary* out,
+                                double* history_host, cudaStream_t st) {
+  const i64 n = A->nrow;
+  const size_t vb = static_cast<size_t>(n + 8) * sizeof(T);
+  SolveCommon c;
+  std::vector<char*> vv;
+  const i64 hist_cap = cfg->collect_residuals ? cfg->max_iterations + 2 : 0;
+  sk_status s = carve_common(A, st, 9, vb, 0, hist_cap, &c, &vv, nullptr);
+  if (s != SK_OK) return s;
+  T *r = (T*)vv[0], *r_hat = (T*)vv[1], *p = (T*)vv[2], *v = (T*)vv[3], *sv = (T*)vv[4],
+    *t = (T*)vv[5], *p_hat = (T*)vv[6], *s_hat = (T*)vv[7], *tmp = (T*)vv[8];
+  *out = sk_summary{};
+  double bnorm = 0;
+  if ((s = norm_b<T>(b, n, c, st, &bnorm)) != SK_OK) return s;
+  if (bnorm == 0.0) {  // :161-165
+    SK_CUDA(cudaMemsetAsync(x, 0, n * sizeof(T), st));
+    SK_CUDA(cudaStreamSynchronize(st));
+    out->converged = 1;
+    return SK_OK;
+  }
+  Scalars h{};
+  h.bnorm = bnorm;
+  h.tol = cfg->tolerance;
+  h.max_iters = cfg->max_iterations;
+  h.hist_on = cfg->collect_residuals ? 1 : 0;
+  if ((s = put_scalars(c.sc, h, st)) != SK_OK) return s;
+  SK_CUDA(cudaMemsetAsync(p, 0, n * sizeof(T), st));  // :173-174
+  SK_CUDA(cudaMemsetAsync(v, 0, n * sizeof(T), st));
+  launch_spmv<T>(A, x, EpiBiResid<T>{b, r, r_hat, c.sc}, c.ws, nullptr, st);
+  const int lk = prec_kind(L), rk = prec_kind(R);
+  i64 steps = 0, chunk = 4;
+  while (steps < std::max<i64>(cfg->max_iterations, 1)) {
+    for (i64 j = 0; j < chunk; ++j, ++steps) {
+#define SK_BI_STEP(LKV, RKV)                                                                  \
+  bicgstab_step<T, LKV, RKV>(A, L, R, x, r, r_hat, p, v, sv, t, p_hat, s_hat, tmp, c, st)
+      if (lk == PK_IDENTITY && rk == PK_IDENTITY) SK_BI_STEP(PK_IDENTITY, PK_IDENTITY);
+      else if (lk == PK_JACOBI && rk == PK_IDENTITY) SK_BI_STEP(PK_JACOBI, PK_IDENTITY);
+      else if (lk == PK_IDENTITY && rk == PK_JACOBI) SK_BI_STEP(PK_IDENTITY, PK_JACOBI);
+      else if (lk == PK_JACOBI && rk == PK_JACOBI) SK_BI_STEP(PK_JACOBI, PK_JACOBI);
+      else SK_BI_STEP(PK_OTHER, PK_OTHER);
+#undef SK_BI_STEP
+    }
+    SK_CUDA(cudaGetLastError());
+    if ((s = read_scalars(c.sc, &h, st)) != SK_OK) return s;
+    if (h.done && !h.half) break;
+    chunk = std::min<i64>(chunk * 2, 32);
+  }
+  return finish_summary(c, st, out, history_host);
+}
+
+// ==================================================================
+// FGMRES(m), fgmres.hpp:96-428
+// ==================================================================
+
+struct FgSmall {  // device arrays of one restart cycle
+  double* H;   // (m+1) x m, column-major, leading dimension m+1
+  double* cs;
+  double* sn;
+  double* g;   // m+1
+  double* y;   // m
+};
+
+// compute_initial_residual (:207-224) and clear_hessenberg (:227-231).
+// A zero beta (the reference divides by it) ends the solve as converged.
+template <typename T>
+struct EpiFgInit {
+  static constexpr int kNR = 1;
+  const T* b;
+  T* v0;
+  Scalars* sc;
+  FgSmall sm;
+  int m;
+  __device__ void operator()(int row, T ax, double* red) const {
+    const T vi = sub(b[row], ax);
+    v0[row] = vi;
+    red[0] += static_cast<double>(mul(vi, vi));
+  }
+  __device__ void finalize(const double* t) const {
+    const T beta = sqrt(static_cast<T>(t[0]));
+    for (int i = 0; i < (m + 1) * m; ++i) sm.H[i] = 0.0;
+    for (int i = 0; i < m; ++i) sm.cs[i] = sm.sn[i] = 0.0;
+    for (int i = 0; i <= m; ++i) sm.g[i] = 0.0;
+    sm.g[0] = static_cast<double>(beta);
+    sc->jfinal = 0;
+    sc->done = 0;
+    sc->beta0 = 0;
+    if (beta == T(0)) {
+      sc->beta0 = 1;
+      sc->converged = 1;
+      sc->done = 1;
+      sc->rnorm = 0.0;
+    } else {
+      sc->aux = static_cast<double>(T(1) / beta);
+    }
+  }
+};
+
+// scale_vector (:403-408): v *= factor, factor = 1/beta or 1/h (from aux
+// or from H), skipped when the factor's norm is not positive.
+template <typename T>
+struct OpFgScale {
+  static constexpr int kNR = 0;
+  T* v;
+  const double* hsrc;  // null: factor = aux; else factor = 1 / *hsrc if > 0
+  T f;
+  __device__ bool prepare(const Scalars* s) {
+    if (solve_done(s)) return false;
+    if (!hsrc) {
+      f = static_cast<T>(s->aux);
+      return true;
+    }
+    const T h = static_cast<T>(*hsrc);
+    if (!(h > T(0))) return false;  // :283
+    f = T(1) / h;
+    return true;
+  }
+  __device__ void operator()(i64 i, double*) const { v[i] = mul(v[i], f); }
+  __device__ void finalize(const double*) const {}
+};
+
+// arnoldi_step (:247-256): w = A z_j into V_{j+1}; first MGS dot h_{0j}.
+template <typename T>
+struct EpiFgW {
+  static constexpr int kNR = 1;
+  T* w;
+  const T* v0;
+  double* h_out;
+  __device__ void operator()(int row, T val, double* red) const {
+    w[row] = val;
+    red[0] += static_cast<double>(mul(v0[row], val));
+  }
+  __device__ void finalize(const double* t) const { *h_out = static_cast<double>(static_cast<T>(t[0])); }
+};
+
+// orthogonalize (:259-273) step i: w -= h_ij v_i, then the next dot
+// h_{i+1,j} = <v_{i+1}, w>, or for i = j the norm h_{j+1,j} (:276-281).
+template <typename T>
+struct OpFgMgs {
+  static constexpr int kNR = 1;
+  T* w;
+  const T* vi;
+  const T* vnext;  // null at i = j
+  const double* h_in;
+  double* h_out;
+  T h;
+  __device__ bool prepare(const Scalars* s) {
+    if (solve_done(s)) return false;
+    h = static_cast<T>(*h_in);
+    return true;
+  }
+  __device__ void operator()(i64 k, double* red) const {
+    const T wk = sub(w[k], mul(h, vi[k]));
+    w[k] = wk;
+    red[0] += static_cast<double>(mul(vnext ? vnext[k] : wk, wk));
+  }
+  __device__ void finalize(const double* t) const {
+    const T d = static_cast<T>(t[0]);
+    *h_out = static_cast<double>(vnext ? d : sqrt(d));
+  }
+};
+
+// apply_givens_rotations (:287-337), record_residual (:340-346),
+// check_convergence (:349-356), in the value type T.
+template <typename T>
+struct FgGivens {
+  Scalars* sc;
+  double* hist;
+  FgSmall sm;
+  int j, m;
+  __device__ void operator()() const {
+    if (sc->done) return;
+    const int um1 = m + 1;
+    auto H = [&](int r, int c) -> double& { return sm.H[r + c * um1]; };
+    for (int i = 0; i < j; ++i) {
+      const T cs = static_cast<T>(sm.cs[i]), sn = static_cast<T>(sm.sn[i]);
+      const T hij = static_cast<T>(H(i, j)), hi1 = static_cast<T>(H(i + 1, j));
+      const T temp = add(mul(cs, hij), mul(sn, hi1));
+      H(i + 1, j) = static_cast<double>(add(mul(-sn, hij), mul(cs, hi1)));
+      H(i, j) = static_cast<double>(temp);
+    }
+    const T a = static_cast<T>(H(j, j)), bb = static_cast<T>(H(j + 1, j));
+    T cs, sn;
+    if (bb == T(0)) {
+      cs = T(1);
+      sn = T(0);
+    } else if (a == T(0)) {
+      cs = T(0);
+      sn = T(1);
+    } else {
+      const T rr = sqrt(add(mul(a, a), mul(bb, bb)));
+      cs = dvd(a, rr);
+      sn = dvd(bb, rr);
+    }
+    sm.cs[j] = static_cast<double>(cs);
+    sm.sn[j] = static_cast<double>(sn);
+    H(j, j) = static_cast<double>(add(mul(cs, a), mul(sn, bb)));
+    H(j + 1, j) = 0.0;
+    const T gj = static_cast<T>(sm.g[j]), gj1 = static_cast<T>(sm.g[j + 1]);
+    const T temp = add(mul(cs, gj), mul(sn, gj1));
+    sm.g[j + 1] = static_cast<double>(add(mul(-sn, gj), mul(cs, gj1)));
+    sm.g[j] = static_cast<double>(temp);
+    sc->iters += 1;
+    sc->jfinal = j;
+    const T absres = fabs(static_cast<T>(sm.g[j + 1]));
+    record(sc, hist, static_cast<double>(absres));
+    if (absres / static_cast<T>(sc->bnorm) < static_cast<T>(sc->tol)) {
+      sc->converged = 1;
+      sc->done = 1;
+    }
+  }
+};
+
+// back_substitute (:365-379).
+template <typename T>
+struct FgBackSub {
+  Scalars* sc;
+  FgSmall sm;
+  int m;
+  __device__ void operator()() const {
+    if (sc->beta0) return;
+    const int um1 = m + 1;
+    const int nj = static_cast<int>(sc->jfinal) + 1;
+    for (int ii = nj; ii > 0; --ii) {
+      const int i = ii - 1;
+      T yi = static_cast<T>(sm.g[i]);
+      for (int k = i + 1; k < nj; ++k)
+        yi = sub(yi, mul(static_cast<T>(sm.H[i + k * um1]), static_cast<T>(sm.y[k])));
+      yi = dvd(yi, static_cast<T>(sm.H[i + i * um1]));
+      sm.y[i] = static_cast<double>(yi);
+    }
+  }
+};
+
+// update_solution (:382-394): x_i += sum_k Z_k[i] y_k, summed in k order.
+template <typename T>
+struct OpFgUpdateX {
+  static constexpr int kNR = 0;
+  T* x;
+  const T* Z;
+  i64 ldz;
+  const double* y;
+  int nj;
+  __device__ bool prepare(const Scalars* s) {
+    if (s->beta0) return false;
+    nj = static_cast<int>(s->jfinal) + 1;
+    return true;
+  }
+  __device__ void operator()(i64 i, double*) const {
+    T sum = T(0);
+    for (int k = 0; k < nj; ++k) sum = add(sum, mul(Z[k * ldz + i], static_cast<T>(y[k])));
+    x[i] = add(x[i], sum);
+  }
+  __device__ void finalize(const double*) const {}
+};
+
+template <typename T>
+static sk_status fgmres_solve(sk_matrix A, sk_precond M, const T* b, T* x,
+                              const sk_fgmres_config* cfg, sk_summary* out, double* history_host,
+                              cudaStream_t st) {
+  const i64 n = A->nrow;
+  const int m = static_cast<int>(cfg->restart_dimension);
+  SK_CHECK(m >= 1 && m <= 4096, SK_INVALID_ARG, "restart_dimension must be in [1, 4096]");
+  const i64 ld = n + 8 + 32;  // leading dimension of V and Z, 256-byte rounded below
+  const i64 ldv = (ld * static_cast<i64>(sizeof(T)) + 255) / 256 * 256 / static_cast<i64>(sizeof(T));
+  const bool alias_z = (M == nullptr);  // identity: Z_j = V_j
+  const i64 nvecs = (m + 1) + (alias_z ? 0 : m);
+  const size_t small_bytes = static_cast<size_t>((m + 1) * m + 4 * (m + 2)) * 8;
+  SolveCommon c;
+  std::vector<char*> vv;
+  char* extra = nullptr;
+  const i64 hist_cap = cfg->collect_residuals ? cfg->max_iterations : 0;
+  sk_status s = carve_common(A, st, 0, 0, static_cast<size_t>(nvecs) * ldv * sizeof(T) + small_bytes + 512,
+                             hist_cap, &c, &vv, &extra);
+  if (s != SK_OK) return s;
+  T* V = reinterpret_cast<T*>(extra);
+  T* Z = alias_z ? V : V + (m + 1) * ldv;
+  FgSmall sm;
+  double* smallp = reinterpret_cast<double*>(
+      (reinterpret_cast<uintptr_t>(V + nvecs * ldv) + 255) & ~uintptr_t(255));
+  sm.H = smallp;
+  sm.cs = sm.H + (m + 1) * m;
+  sm.sn = sm.cs + (m + 2);
+  sm.g = sm.sn + (m + 2);
+  sm.y = sm.g + (m + 2);
+  *out = sk_summary{};
+  double bnorm = 0;
+  if ((s = norm_b<T>(b, n, c, st, &bnorm)) != SK_OK) return s;
+  if (bnorm == 0.0) {  // :169-173
+    SK_CUDA(cudaMemsetAsync(x, 0, n * sizeof(T), st));
+    SK_CUDA(cudaStreamSynchronize(st));
+    out->converged = 1;
+    return SK_OK;
+  }
+  Scalars h{};
+  h.bnorm = bnorm;
+  h.tol = cfg->tolerance;
+  h.max_iters = cfg->max_iterations;
+  h.hist_on = cfg->collect_residuals ? 1 : 0;
+  if ((s = put_scalars(c.sc, h, st)) != SK_OK) return s;
+  const int um1 = m + 1;
+  while (h.iters < cfg->max_iterations && !h.converged) {
+    launch_spmv<T>(A, x, EpiFgInit<T>{b, V, c.sc, sm, m}, c.ws, nullptr, st);
+    launch_vec(n, OpFgScale<T>{V, nullptr, T(0)}, c.ws, c.sc, st);
+    const i64 m_eff = std::min<i64>(m, cfg->max_iterations - h.iters);  // :241-244
+    for (int j = 0; j < m_eff; ++j) {
+      T* Vj = V + j * ldv;
+      T* Vj1 = V + (j + 1) * ldv;
+      T* Zj = Z + j * ldv;
+      if (!alias_z) precond_apply_dispatch(M, A->dtype, n, Vj, Zj, c.ws, c.sc, st);
+      launch_spmv<T>(A, Zj, EpiFgW<T>{Vj1, V, sm.H + j * um1}, c.ws, c.sc, st);
+      for (int i = 0; i <= j; ++i) {
+        const T* vnext = i < j ? V + (i + 1) * ldv : nullptr;
+        launch_vec(n, OpFgMgs<T>{Vj1, V + i * ldv, vnext, sm.H + i + j * um1, sm.H + (i + 1) + j * um1, T(0)},
+                   c.ws, c.sc, st);
+      }
+      launch_vec(n, OpFgScale<T>{Vj1, sm.H + (j + 1) + j * um1, T(0)}, c.ws, c.sc, st);
+      g_launches.fetch_add(1, std::memory_order_relaxed);
+      scalar_kernel<<<1, 1, 0, st>>>(FgGivens<T>{c.sc, c.hist, sm, j, m});
+    }
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+    scalar_kernel<<<1, 1, 0, st>>>(FgBackSub<T>{c.sc, sm, m});
+    launch_vec(n, OpFgUpdateX<T>{x, Z, ldv, sm.y, 0}, c.ws, nullptr, st);
+    SK_CUDA(cudaGetLastError());
+    if ((s = read_scalars(c.sc, &h, st)) != SK_OK) return s;
+  }
+  return finish_summary(c, st, out, history_host);
+}
+
+}  // namespace sk
+
+using namespace sk;
+
+namespace {
+
+sk_status check_solver_args(sk_matrix A, sk_precond L, sk_precond R, const void* b, void* x) {
+  SK_CHECK(A, SK_INVALID_ARG, "null matrix handle");
+  SK_CHECK(A->nrow == A->ncol, SK_INVALID_ARG, "solvers need a square matrix");
+  SK_CHECK(A->nrow == 0 || (b && x), SK_INVALID_ARG, "null b or x");
+  for (sk_precond M : {L, R})
+    if (M) {
+      SK_CHECK(M->dtype == A->dtype, SK_INVALID_ARG, "preconditioner dtype differs from the matrix");
+      SK_CHECK(M->n == A->nrow, SK_INVALID_ARG, "preconditioner size differs from the matrix");
+    }
+  return SK_OK;
+}
+
+template <typename Cfg, typename F>
+sk_status host_wrapper(sk_matrix A, const void* b_host, void* x_host, F&& solve_dev) {
+  SK_CHECK(A, SK_INVALID_ARG, "null matrix handle");
+  const size_t V = A->dtype == SK_F64 ? 8 : 4;
+  const size_t bytes = static_cast<size_t>(A->nrow) * V;
+  void* bx = nullptr;
+  SK_CUDA(cudaMalloc(&bx, 2 * bytes + 512));
+  char* bd = static_cast<char*>(bx);
+  char* xd = bd + ((bytes + 255) & ~size_t(255));
+  cudaError_t e = cudaMemcpyAsync(bd, b_host, bytes, cudaMemcpyHostToDevice, A->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(xd, x_host, bytes, cudaMemcpyHostToDevice, A->stream);
+  if (e != cudaSuccess) {
+    cudaFree(bx);
+    return cuda_fail(e, "copy in");
+  }
+  sk_status s = solve_dev(bd, xd);
+  if (s == SK_OK) {
+    e = cudaMemcpyAsync(x_host, xd, bytes, cudaMemcpyDeviceToHost, A->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(A->stream);
+    if (e != cudaSuccess) s = cuda_fail(e, "copy out");
+  }
+  cudaFree(bx);
+  return s;
+}
+
+}  // namespace
+
+extern "C" {
+
+sk_status sk_cg_solve(sk_matrix A, sk_precond left, sk_precond right, const void* b_dev, void* x_dev,
+                      const sk_cg_config* cfg, sk_summary* out, double* history_host, sk_stream s) {
+  sk_status st = check_solver_args(A, left, right, b_dev, x_dev);
+  if (st != SK_OK) return st;
+  SK_CHECK(cfg && out, SK_INVALID_ARG, "null config or summary");
+  SK_CHECK(cfg->restart_iterations > 0, SK_INVALID_ARG,
+           "restart_iterations must be positive (the reference takes k % restart_iterations)");
+  SK_CHECK(cfg->max_iterations >= 0, SK_INVALID_ARG, "negative max_iterations");
+  cudaStream_t cs = pick_stream(A, s);
+  if (A->dtype == SK_F64)
+    return cg_solve<double>(A, left, right, static_cast<const double*>(b_dev), static_cast<double*>(x_dev),
+                            cfg, out, history_host, cs);
+  return cg_solve<float>(A, left, right, static_cast<const float*>(b_dev), static_cast<float*>(x_dev), cfg,
+                         out, history_host, cs);
+}
+
+sk_status sk_bicgstab_solve(sk_matrix A, sk_precond left, sk_precond right, const void* b_dev,
+                            void* x_dev, const sk_bicgstab_config* cfg, sk_summary* out,
+                            double* history_host, sk_stream s) {
+  sk_status st = check_solver_args(A, left, right, b_dev, x_dev);
+  if (st != SK_OK) return st;
+  SK_CHECK(cfg && out, SK_INVALID_ARG, "null config or summary");
+  SK_CHECK(cfg->max_iterations >= 0, SK_INVALID_ARG, "negative max_iterations");
+  cudaStream_t cs = pick_stream(A, s);
+  if (A->dtype == SK_F64)
+    return bicgstab_solve<double>(A, left, right, static_cast<const double*>(b_dev),
+                                  static_cast<double*>(x_dev), cfg, out, history_host, cs);
+  return bicgstab_solve<float>(A, left, right, static_cast<const float*>(b_dev), static_cast<float*>(x_dev),
+                               cfg, out, history_host, cs);
+}
+
+sk_status sk_fgmres_solve(sk_matrix A, sk_precond M, const void* b_dev, void* x_dev,
+                          const sk_fgmres_config* cfg, sk_summary* out, double* history_host,
+                          sk_stream s) {
+  sk_status st = check_solver_args(A, M, nullptr, b_dev, x_dev);
+  if (st != SK_OK) return st;
+  SK_CHECK(cfg && out, SK_INVALID_ARG, "null config or summary");
+  SK_CHECK(cfg->max_iterations >= 0, SK_INVALID_ARG, "negative max_iterations");
+  cudaStream_t cs = pick_stream(A, s);
+  if (A->dtype == SK_F64)
+    return fgmres_solve<double>(A, M, static_cast<const double*>(b_dev), static_cast<double*>(x_dev), cfg,
+                                out, history_host, cs);
+  return fgmres_solve<float>(A, M, static_cast<const float*>(b_dev), static_cast<float*>(x_dev), cfg, out,
+                             history_host, cs);
+}
+
+sk_status sk_cg_solve_host(sk_matrix A, sk_precond left, sk_precond right, const void* b_host,
+                           void* x_host, const sk_cg_config* cfg, sk_summary* out, double* history_host) {
+  return host_wrapper<sk_cg_config>(A, b_host, x_host, [&](void* bd, void* xd) {
+    return sk_cg_solve(A, left, right, bd, xd, cfg, out, history_host, A->stream);
+  });
+}
+
+sk_status sk_bicgstab_solve_host(sk_matrix A, sk_precond left, sk_precond right, const void* b_host,
+                                 void* x_host, const sk_bicgstab_config* cfg, sk_summary* out,
+                                 double* history_host) {
+  return host_wrapper<sk_bicgstab_config>(A, b_host, x_host, [&](void* bd, void* xd) {
+    return sk_bicgstab_solve(A, left, right, bd, xd, cfg, out, history_host, A->stream);
+  });
+}
+
+sk_status sk_fgmres_solve_host(sk_matrix A, sk_precond M, const void* b_host, void* x_host,
+                               const sk_fgmres_config* cfg, sk_summary* out, double* history_host) {
+  return host_wrapper<sk_fgmres_config>(A, b_host, x_host, [&](void* bd, void* xd) {
+    return sk_fgmres_solve(A, M, bd, xd, cfg, out, history_host, A->stream);
+  });
+}
+
+}  // extern "C"

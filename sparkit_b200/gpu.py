@@ -1,0 +1,307 @@
+"""Python mirror of the drop-in GPU path (the C++ form is
+include/sparkit_b200/gpu.hpp); every call goes through the C ABI.
+
+Names and argument meaning follow the reference:
+
+* ``Device_matrix(A)`` uploads a Compressed_row_matrix / Ellpack_matrix /
+  Jagged_diagonal_matrix / Block_sparse_row_matrix once.
+* ``multiply(Ad, x)`` is multiply(A, span<T const>) -> vector<T>
+  (sparse_blas.hpp:19, spmv.hpp:119/148/182): host array in, host array out.
+* ``jacobi(Ad)``, ``chebyshev_preconditioner(Ad, lmin, lmax, degree)`` are
+  the set-up calls of jacobi.hpp:27 and chebyshev_preconditioner.hpp:46;
+  ``identity`` (None) is the copy callable of the reference tests.
+* ``conjugate_gradient(b, x, cfg, spmv(Ad), left, right)``,
+  ``bicgstab(b, x, cfg, spmv(Ad), left, right)`` and
+  ``fgmres(b, x, cfg, spmv(Ad), preconditioner)`` mirror
+  conjugate_gradient.hpp:347, bicgstab.hpp:391 and fgmres.hpp:459; b and x
+  are numpy arrays (x in/out, copied once each way) or CUDA torch tensors
+  (device resident, no copies).
+"""
+import ctypes
+from dataclasses import dataclass, field
+from typing import List
+
+import numpy as np
+
+from . import _lib
+from ._lib import check, lib
+from .formats import (Block_sparse_row_matrix, Compressed_row_matrix, Ellpack_matrix,
+                      Jagged_diagonal_matrix)
+
+identity = None
+
+
+def _dtype_code(dt):
+    dt = np.dtype(dt)
+    if dt == np.float64:
+        return _lib.SK_F64
+    if dt == np.float32:
+        return _lib.SK_F32
+    raise TypeError(f"unsupported value type {dt}")
+
+
+def _ptr(a):
+    if a is None:
+        return None
+    if isinstance(a, np.ndarray):
+        return a.ctypes.data_as(ctypes.c_void_p) if a.size else ctypes.c_void_p(a.ctypes.data)
+    return ctypes.c_void_p(int(a.data_ptr()))
+
+
+def _is_device(a):
+    return not isinstance(a, np.ndarray) and hasattr(a, "data_ptr")
+
+
+def _stream_of(a):
+    if _is_device(a):
+        import torch
+        return ctypes.c_void_p(torch.cuda.current_stream(a.device).cuda_stream)
+    return None
+
+
+class Device_matrix:
+    """A device-resident copy of one reference matrix object."""
+
+    def __init__(self, A, dtype=None):
+        values = A.values()
+        dt = np.dtype(dtype) if dtype is not None else values.dtype
+        values = np.ascontiguousarray(values, dtype=dt)
+        code = _dtype_code(dt)
+        h = ctypes.c_void_p()
+        n, m = A.shape()
+        if isinstance(A, Compressed_row_matrix):
+            check(lib().sk_csr_create(ctypes.byref(h), n, m, _ptr(A.row_ptr()), _ptr(A.col_ind()),
+                                      _ptr(values), code))
+        elif isinstance(A, Ellpack_matrix):
+            check(lib().sk_ell_create(ctypes.byref(h), n, m, A.max_nnz_per_row(), _ptr(A.col_ind()),
+                                      _ptr(values), code))
+        elif isinstance(A, Jagged_diagonal_matrix):
+            perm = A.perm() if A.perm().size else None
+            check(lib().sk_jad_create(ctypes.byref(h), n, m, A.num_jdiags(), _ptr(perm), _ptr(A.jdiag()),
+                                      _ptr(A.col_ind()), _ptr(values), code))
+        elif isinstance(A, Block_sparse_row_matrix):
+            check(lib().sk_bsr_create(ctypes.byref(h), n, m, A.block_rows(), A.block_cols(),
+                                      _ptr(A.row_ptr()), _ptr(A.col_ind()), _ptr(values), code))
+        else:
+            raise TypeError(f"no device form for {type(A).__name__}")
+        self.handle = h
+        self.dtype = dt
+        self._shape = (n, m)
+
+    def shape(self):
+        return self._shape
+
+    def info(self):
+        """dict of sk_matrix_info: format, dtype, nrow, ncol, nnz, width,
+        device_bytes, spmv_bytes (algorithmic bytes of one product)."""
+        arr = (ctypes.c_int64 * 8)()
+        check(lib().sk_matrix_info(self.handle, arr))
+        keys = ("format", "dtype", "nrow", "ncol", "nnz", "width", "device_bytes", "spmv_bytes")
+        return dict(zip(keys, list(arr)))
+
+    def add_f32_values(self):
+        check(lib().sk_matrix_add_f32_values(self.handle))
+
+    def spmv(self, x, y, stream=None):
+        """y = A x on device tensors (or raw device pointers)."""
+        xs = _ptr(x) if not isinstance(x, int) else ctypes.c_void_p(x)
+        ys = _ptr(y) if not isinstance(y, int) else ctypes.c_void_p(y)
+        st = stream if stream is not None else _stream_of(x)
+        check(lib().sk_spmv(self.handle, xs, ys, st))
+
+    def spmv_f32(self, x, y, stream=None):
+        st = stream if stream is not None else _stream_of(x)
+        check(lib().sk_spmv_f32(self.handle, _ptr(x), _ptr(y), st))
+
+    def close(self):
+        if getattr(self, "handle", None):
+            lib().sk_matrix_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def multiply(Ad, x):
+    """multiply(A, span<T const>) -> vector<T>, host in / host out."""
+    x = np.ascontiguousarray(x, dtype=Ad.dtype)
+    if x.shape[0] != Ad.shape()[1]:
+        raise ValueError("x length must equal the column count")
+    y = np.empty(Ad.shape()[0], dtype=Ad.dtype)
+    check(lib().sk_spmv_host(Ad.handle, _ptr(x), _ptr(y)))
+    return y
+
+
+class spmv:
+    """The linear-operator argument of the solvers: y = A x on the device."""
+
+    def __init__(self, Ad):
+        self.A = Ad
+
+
+class _Precond:
+    def __init__(self, handle, Ad, n):
+        self.handle = handle
+        self.A = Ad
+        self.n = n
+
+    def apply(self, r, z, stream=None):
+        """z = M^{-1} r on device tensors."""
+        st = stream if stream is not None else _stream_of(r)
+        check(lib().sk_precond_apply(self.handle, self.n, _ptr(r), _ptr(z), st))
+
+    def values(self):
+        cnt = ctypes.c_int64()
+        check(lib().sk_precond_values(self.handle, None, 0, ctypes.byref(cnt)))
+        out = np.empty(cnt.value, dtype=self.A.dtype)
+        check(lib().sk_precond_values(self.handle, _ptr(out), cnt.value, ctypes.byref(cnt)))
+        return out
+
+    def close(self):
+        if getattr(self, "handle", None):
+            lib().sk_precond_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class jacobi(_Precond):
+    """jacobi(A) (jacobi.hpp:27-35).  A zero diagonal raises ValueError,
+    the Python form of the reference's std::invalid_argument."""
+
+    def __init__(self, Ad):
+        h = ctypes.c_void_p()
+        st = lib().sk_jacobi_create(ctypes.byref(h), Ad.handle)
+        if st == 8:  # SK_ZERO_DIAGONAL
+            raise ValueError("jacobi: zero diagonal entry")
+        check(st)
+        super().__init__(h, Ad, min(Ad.shape()))
+
+
+class chebyshev_preconditioner(_Precond):
+    """chebyshev_preconditioner(A, lambda_min, lambda_max, degree)
+    (chebyshev_preconditioner.hpp:46-84)."""
+
+    def __init__(self, Ad, lambda_min, lambda_max, degree):
+        h = ctypes.c_void_p()
+        check(lib().sk_chebyshev_create(ctypes.byref(h), Ad.handle, float(lambda_min), float(lambda_max),
+                                        int(degree)))
+        super().__init__(h, Ad, Ad.shape()[0])
+        self.lambda_min, self.lambda_max, self.degree = lambda_min, lambda_max, degree
+
+
+@dataclass
+class CGConfig:
+    """CGConfig<T> (conjugate_gradient.hpp:48-74)."""
+    tolerance: float = 0.0
+    restart_iterations: int = 0
+    max_iterations: int = 0
+    collect_residuals: bool = False
+
+
+@dataclass
+class Bicgstab_config:
+    """Bicgstab_config<T> (bicgstab.hpp:25-42)."""
+    tolerance: float = 0.0
+    max_iterations: int = 0
+    collect_residuals: bool = False
+
+
+@dataclass
+class Fgmres_config:
+    """Fgmres_config<T> (fgmres.hpp:25-47)."""
+    tolerance: float = 0.0
+    restart_dimension: int = 0
+    max_iterations: int = 0
+    collect_residuals: bool = False
+
+
+@dataclass
+class Summary:
+    """CGSummary / Bicgstab_summary / Fgmres_summary, plus the device
+    status (0, or 4 = SK_BREAKDOWN)."""
+    residual_norm: float = 0.0
+    computed_iterations: int = 0
+    converged: bool = False
+    iteration_residuals: List[float] = field(default_factory=list)
+    status: int = 0
+
+
+CGSummary = Bicgstab_summary = Fgmres_summary = Summary
+
+
+def _handle(M):
+    return None if M is None else M.handle
+
+
+def _run(fn_dev, fn_host, b, x, Ad, cfg_struct, max_hist, collect):
+    s = _lib.Summary()
+    hist = np.zeros(max(int(max_hist), 1) + 4, dtype=np.float64) if collect else None
+    if _is_device(b):
+        st = _stream_of(b)
+        check(fn_dev(_ptr(b), _ptr(x), ctypes.byref(cfg_struct), ctypes.byref(s), _ptr(hist), st))
+    else:
+        if not (isinstance(x, np.ndarray) and x.flags.c_contiguous and x.dtype == Ad.dtype):
+            raise TypeError("x must be a contiguous numpy array of the matrix's value type")
+        bb = np.ascontiguousarray(b, dtype=Ad.dtype)
+        check(fn_host(_ptr(bb), _ptr(x), ctypes.byref(cfg_struct), ctypes.byref(s), _ptr(hist)))
+    out = Summary(s.residual_norm, s.computed_iterations, bool(s.converged), [], s.status)
+    if collect:
+        out.iteration_residuals = hist[: s.history_length].tolist()
+    return out
+
+
+def _op_matrix(op):
+    if not isinstance(op, spmv):
+        raise TypeError("the linear operator must be sparkit_b200.gpu.spmv(Device_matrix): "
+                        "arbitrary host callables are not accelerated")
+    return op.A
+
+
+def conjugate_gradient(b, x, cfg, op, left=identity, right=identity):
+    """conjugate_gradient(bfirst, blast, xfirst, xlast, cfg, op, left, right)."""
+    Ad = _op_matrix(op)
+    c = _lib.CgConfig(cfg.tolerance, cfg.restart_iterations, cfg.max_iterations, int(cfg.collect_residuals))
+    L = lib()
+    return _run(lambda bp, xp, cp, sp, hp, st: L.sk_cg_solve(Ad.handle, _handle(left), _handle(right), bp, xp,
+                                                             cp, sp, hp, st),
+                lambda bp, xp, cp, sp, hp: L.sk_cg_solve_host(Ad.handle, _handle(left), _handle(right), bp, xp,
+                                                              cp, sp, hp),
+                b, x, Ad, c, cfg.max_iterations, cfg.collect_residuals)
+
+
+def bicgstab(b, x, cfg, op, left=identity, right=identity):
+    """bicgstab(bfirst, blast, xfirst, xlast, cfg, op, left, right)."""
+    Ad = _op_matrix(op)
+    c = _lib.BicgstabConfig(cfg.tolerance, cfg.max_iterations, int(cfg.collect_residuals))
+    L = lib()
+    return _run(lambda bp, xp, cp, sp, hp, st: L.sk_bicgstab_solve(Ad.handle, _handle(left), _handle(right), bp,
+                                                                   xp, cp, sp, hp, st),
+                lambda bp, xp, cp, sp, hp: L.sk_bicgstab_solve_host(Ad.handle, _handle(left), _handle(right),
+                                                                    bp, xp, cp, sp, hp),
+                b, x, Ad, c, cfg.max_iterations + 2, cfg.collect_residuals)
+
+
+def fgmres(b, x, cfg, op, preconditioner=identity):
+    """fgmres(bfirst, blast, xfirst, xlast, cfg, op, preconditioner)."""
+    Ad = _op_matrix(op)
+    c = _lib.FgmresConfig(cfg.tolerance, cfg.restart_dimension, cfg.max_iterations, int(cfg.collect_residuals))
+    L = lib()
+    return _run(lambda bp, xp, cp, sp, hp, st: L.sk_fgmres_solve(Ad.handle, _handle(preconditioner), bp, xp, cp,
+                                                                 sp, hp, st),
+                lambda bp, xp, cp, sp, hp: L.sk_fgmres_solve_host(Ad.handle, _handle(preconditioner), bp, xp,
+                                                                  cp, sp, hp),
+                b, x, Ad, c, cfg.max_iterations, cfg.collect_residuals)
+
+
+def device_count():
+    n = ctypes.c_int()
+    check(lib().sk_device_count(ctypes.byref(n)))
+    return n.value

@@ -1,0 +1,177 @@
+"""Seeded matrix generators: the reference's own test matrices (restated
+from sparkit/data/matgen.hpp so that parity tests use the same inputs
+without the reference present) and the synthetic workloads of the
+benchmark (Dirichlet Laplacians, the 3x3-block vector Laplacian, the
+Zipf-row random matrix).
+
+All builders return a formats.Compressed_row_matrix with sorted, unique
+columns per row and int64 indices.
+"""
+import numpy as np
+
+from .formats import Compressed_row_matrix
+
+
+def _stencil_csr(n_rows, cand_cols, cand_vals, valid, dtype):
+    """CSR from per-row candidate columns (already in increasing order)."""
+    counts = valid.sum(axis=1).astype(np.int64)
+    rp = np.zeros(n_rows + 1, dtype=np.int64)
+    np.cumsum(counts, out=rp[1:])
+    cols = cand_cols[valid]
+    vals = cand_vals[valid].astype(dtype)
+    return Compressed_row_matrix((n_rows, n_rows), rp, cols, vals)
+
+
+# ------------------------------------------------------------------
+# Matrices of the reference's tests (matgen.hpp)
+# ------------------------------------------------------------------
+
+def tridiagonal_matrix(n, sub, diag, sup, dtype=np.float64):
+    """matgen.hpp:104-117."""
+    i = np.arange(n, dtype=np.int64)
+    cand = np.stack([i - 1, i, i + 1], axis=1)
+    vals = np.broadcast_to(np.array([sub, diag, sup], dtype=np.float64), cand.shape)
+    valid = (cand >= 0) & (cand < n)
+    return _stencil_csr(n, cand, vals, valid, dtype)
+
+
+def poisson_2d(nx, ny=None, shift=0.0, dtype=np.float64):
+    """Graph Laplacian of an nx x ny grid, diagonal = neighbour count + shift
+    (matgen.hpp:175-264).  poisson_2d(grid, shift) in the reference is
+    poisson_2d(grid, grid, shift)."""
+    if ny is None:
+        ny = nx
+    n = nx * ny
+    node = np.arange(n, dtype=np.int64)
+    r, c = node // nx, node % nx
+    # the reference pushes W, E, S, N then the diagonal; CSR sorts them to
+    # S, W, diag, E, N
+    cand = np.stack([node - nx, node - 1, node, node + 1, node + nx], axis=1)
+    valid = np.stack([r > 0, c > 0, np.ones(n, bool), c + 1 < nx, r + 1 < ny], axis=1)
+    degree = valid.sum(axis=1) - 1
+    vals = np.stack([-np.ones(n), -np.ones(n), degree.astype(np.float64) + shift,
+                     -np.ones(n), -np.ones(n)], axis=1)
+    return _stencil_csr(n, cand, vals, valid, dtype)
+
+
+def convdiff_centered_2d(nx, ny, diffusion, cx, cy, shift=0.0, dtype=np.float64):
+    """Centred convection-diffusion, matgen.hpp:341-391."""
+    n = nx * ny
+    node = np.arange(n, dtype=np.int64)
+    r, c = node // nx, node % nx
+    cand = np.stack([node - nx, node - 1, node, node + 1, node + nx], axis=1)
+    valid = np.stack([r > 0, c > 0, np.ones(n, bool), c + 1 < nx, r + 1 < ny], axis=1)
+    degree = (valid.sum(axis=1) - 1).astype(np.float64)
+    vals = np.stack([np.full(n, -(diffusion + cy)), np.full(n, -(diffusion + cx)),
+                     degree * diffusion + shift,
+                     np.full(n, -(diffusion - cx)), np.full(n, -(diffusion - cy))], axis=1)
+    return _stencil_csr(n, cand, vals, valid, dtype)
+
+
+def convection_diffusion_2d(nx, ny, diffusion, cx, cy, dtype=np.float64):
+    """First-order upwind convection-diffusion, matgen.hpp:276-330."""
+    n = nx * ny
+    node = np.arange(n, dtype=np.int64)
+    r, c = node // nx, node % nx
+    cand = np.stack([node - nx, node - 1, node, node + 1, node + nx], axis=1)
+    valid = np.stack([r > 0, c > 0, np.ones(n, bool), c + 1 < nx, r + 1 < ny], axis=1)
+    off = np.stack([np.full(n, -diffusion - cy), np.full(n, -diffusion - cx), np.zeros(n),
+                    np.full(n, -diffusion), np.full(n, -diffusion)], axis=1)
+    # the reference accumulates the diagonal as diag -= val in the order
+    # W, E, S, N
+    diag = np.zeros(n)
+    for col in (1, 3, 0, 4):
+        diag = np.where(valid[:, col], diag - off[:, col], diag)
+    vals = off.copy()
+    vals[:, 2] = diag
+    return _stencil_csr(n, cand, vals, valid, dtype)
+
+
+def nonsymmetric_sample(dtype=np.float64):
+    """The hard-coded 4x4 of matgen.hpp:147-166."""
+    rows = [0, 0, 0, 1, 1, 1, 2, 2, 2, 3, 3, 3]
+    cols = [0, 1, 2, 0, 1, 3, 0, 2, 3, 1, 2, 3]
+    vals = [4, -1, 0.5, -0.5, 4, -1, 0.3, 4, -0.8, -0.6, 0.2, 4]
+    return Compressed_row_matrix.from_entries((4, 4), rows, cols, vals, dtype=dtype)
+
+
+# ------------------------------------------------------------------
+# Benchmark workloads
+# ------------------------------------------------------------------
+
+def laplacian_2d_dirichlet(nx, ny=None, dtype=np.float64):
+    """5-point Dirichlet Laplacian: 4 on the diagonal everywhere, -1 to
+    in-grid neighbours (n = nx * ny)."""
+    if ny is None:
+        ny = nx
+    n = nx * ny
+    node = np.arange(n, dtype=np.int64)
+    r, c = node // nx, node % nx
+    cand = np.stack([node - nx, node - 1, node, node + 1, node + nx], axis=1)
+    valid = np.stack([r > 0, c > 0, np.ones(n, bool), c + 1 < nx, r + 1 < ny], axis=1)
+    vals = np.tile(np.array([-1.0, -1.0, 4.0, -1.0, -1.0]), (n, 1))
+    return _stencil_csr(n, cand, vals, valid, dtype)
+
+
+def laplacian_3d_dirichlet(nx, ny=None, nz=None, dtype=np.float64, diag=6.0):
+    """7-point Dirichlet Laplacian on nx x ny x nz (diagonal 6)."""
+    ny = nx if ny is None else ny
+    nz = nx if nz is None else nz
+    n = nx * ny * nz
+    node = np.arange(n, dtype=np.int64)
+    i = node % nx
+    j = (node // nx) % ny
+    k = node // (nx * ny)
+    pl = nx * ny
+    cand = np.stack([node - pl, node - nx, node - 1, node, node + 1, node + nx, node + pl], axis=1)
+    valid = np.stack([k > 0, j > 0, i > 0, np.ones(n, bool), i + 1 < nx, j + 1 < ny, k + 1 < nz], axis=1)
+    vals = np.tile(np.array([-1.0, -1.0, -1.0, diag, -1.0, -1.0, -1.0]), (n, 1))
+    return _stencil_csr(n, cand, vals, valid, dtype)
+
+
+def vector_laplacian_3d_bsr_csr(nx, seed=0, coupling=0.1, dtype=np.float64):
+    """Scalar CSR of the 3-component vector Laplacian: every block is
+    L_ij * I_3, and each diagonal block gets a dense 3x3 coupling with
+    off-diagonal entries U[-coupling, coupling] (seeded).  Converted with
+    to_block_sparse_row(., 3, 3) this is the BSR workload."""
+    L = laplacian_3d_dirichlet(nx, dtype=np.float64)
+    n = L.shape()[0]
+    rng = np.random.default_rng(seed)
+    coup = rng.uniform(-coupling, coupling, size=(n, 3, 3))
+    lens = L.row_lengths()
+    brow = np.repeat(np.arange(n, dtype=np.int64), lens)
+    bcol = L.col_ind()
+    bval = L.values()
+    is_diag = brow == bcol
+    # per block row: entries (3 scalar rows) x (blocks) x (3 columns)
+    nb = bcol.size
+    blk = np.zeros((nb, 3, 3))
+    blk[:, [0, 1, 2], [0, 1, 2]] = bval[:, None]
+    d_idx = np.nonzero(is_diag)[0]
+    cpl = coup[brow[d_idx]]
+    for a in range(3):
+        for b in range(3):
+            if a != b:
+                blk[d_idx, a, b] = cpl[:, a, b]
+    # scalar CSR: row 3I+a holds, block by block, columns 3J+b
+    rows = (3 * brow[:, None, None] + np.arange(3)[None, :, None]).repeat(3, axis=2)
+    cols = (3 * bcol[:, None, None] + np.arange(3)[None, None, :]).repeat(3, axis=1)
+    rows, cols, vals = rows.ravel(), cols.ravel(), blk.ravel()
+    keep = vals != 0.0
+    return Compressed_row_matrix.from_entries((3 * n, 3 * n), rows[keep], cols[keep], vals[keep], dtype=dtype)
+
+
+def zipf_random(n, s=1.5, cap=2048, seed=0, dtype=np.float64):
+    """n x n random matrix: row lengths min(Zipf(s), cap), columns uniform
+    in [0, n) (duplicates within a row dropped), values N(0, 1)."""
+    rng = np.random.default_rng(seed)
+    lens = np.minimum(rng.zipf(s, size=n), cap).astype(np.int64)
+    rows = np.repeat(np.arange(n, dtype=np.int64), lens)
+    cols = rng.integers(0, n, size=rows.size, dtype=np.int64)
+    vals = rng.standard_normal(rows.size)
+    return Compressed_row_matrix.from_entries((n, n), rows, cols, vals, dtype=dtype)
+
+
+def uniform_vector(n, seed=0, dtype=np.float64):
+    """x ~ U[-1, 1], seeded."""
+    return np.random.default_rng(seed).uniform(-1.0, 1.0, size=n).astype(dtype)
