@@ -28,6 +28,12 @@
 #include <stddef.h>
 #include <stdint.h>
 
+#if defined(__GNUC__)
+#define SK_API __attribute__((visibility("default")))
+#else
+#define SK_API
+#endif
+
 #ifdef __cplusplus
 extern "C" {
 #endif
@@ -58,20 +64,20 @@ typedef void* sk_stream;
 /* ---------------------------------------------------------------- */
 
 /* Version string of this library. */
-const char* sk_version(void);
+SK_API const char* sk_version(void);
 /* Message of the calling thread's most recent failed call. */
-const char* sk_last_error(void);
+SK_API const char* sk_last_error(void);
 /* Number of CUDA devices visible (0 on a machine without a GPU). */
-sk_status sk_device_count(int* count);
+SK_API sk_status sk_device_count(int* count);
 /* Count of this library's kernel launches since load (for accounting). */
-sk_status sk_launch_count(int64_t* count);
+SK_API sk_status sk_launch_count(int64_t* count);
 
 /* Device memory helpers, so that a C/C++ caller needs no CUDA headers. */
-sk_status sk_device_alloc(void** dev, size_t bytes);
-sk_status sk_device_free(void* dev);
-sk_status sk_memcpy_h2d(void* dev, const void* host, size_t bytes, sk_stream s);
-sk_status sk_memcpy_d2h(void* host, const void* dev, size_t bytes, sk_stream s);
-sk_status sk_stream_synchronize(sk_stream s);
+SK_API sk_status sk_device_alloc(void** dev, size_t bytes);
+SK_API sk_status sk_device_free(void* dev);
+SK_API sk_status sk_memcpy_h2d(void* dev, const void* host, size_t bytes, sk_stream s);
+SK_API sk_status sk_memcpy_d2h(void* host, const void* dev, size_t bytes, sk_stream s);
+SK_API sk_status sk_stream_synchronize(sk_stream s);
 
 /* ---------------------------------------------------------------- */
 /* Matrix handles (upload once, device resident)                     */
@@ -79,14 +85,14 @@ sk_status sk_stream_synchronize(sk_stream s);
 
 /* Compressed_row_matrix<T> (sparkit/data/Compressed_row_matrix.hpp:20-132):
  * row_ptr[nrow+1], col_ind[nnz] sorted within each row, values[nnz]. */
-sk_status sk_csr_create(sk_matrix* out, int64_t nrow, int64_t ncol,
+SK_API sk_status sk_csr_create(sk_matrix* out, int64_t nrow, int64_t ncol,
                         const int64_t* row_ptr, const int64_t* col_ind,
                         const void* values, sk_dtype dtype);
 
 /* Ellpack_matrix<T> (sparkit/data/Ellpack_matrix.hpp:20-122): row-major
  * nrow x width col_ind padded with -1 (Ellpack_sparsity_Impl.cpp:33-36),
  * values with the same layout.  width = max_nnz_per_row(). */
-sk_status sk_ell_create(sk_matrix* out, int64_t nrow, int64_t ncol,
+SK_API sk_status sk_ell_create(sk_matrix* out, int64_t nrow, int64_t ncol,
                         int64_t width, const int64_t* col_ind,
                         const void* values, sk_dtype dtype);
 
@@ -94,7 +100,7 @@ sk_status sk_ell_create(sk_matrix* out, int64_t nrow, int64_t ncol,
  * perm[nrow], jdiag[njd+1], col_ind[nnz] and values[nnz] in
  * jagged-diagonal order (Jagged_diagonal_sparsity_Impl.cpp:11-93).  perm
  * may be NULL when njd == 0 (the reference's empty JAD holds no perm). */
-sk_status sk_jad_create(sk_matrix* out, int64_t nrow, int64_t ncol,
+SK_API sk_status sk_jad_create(sk_matrix* out, int64_t nrow, int64_t ncol,
                         int64_t njd, const int64_t* perm, const int64_t* jdiag,
                         const int64_t* col_ind, const void* values,
                         sk_dtype dtype);
@@ -102,21 +108,21 @@ sk_status sk_jad_create(sk_matrix* out, int64_t nrow, int64_t ncol,
 /* Block_sparse_row_matrix<T> (sparkit/data/Block_sparse_row_matrix.hpp:21-150):
  * row_ptr over ceil(nrow/block_rows) block rows, col_ind[nblocks] block
  * columns, values = nblocks dense row-major block_rows x block_cols blocks. */
-sk_status sk_bsr_create(sk_matrix* out, int64_t nrow, int64_t ncol,
+SK_API sk_status sk_bsr_create(sk_matrix* out, int64_t nrow, int64_t ncol,
                         int64_t block_rows, int64_t block_cols,
                         const int64_t* row_ptr, const int64_t* col_ind,
                         const void* values, sk_dtype dtype);
 
-sk_status sk_matrix_destroy(sk_matrix A);
+SK_API sk_status sk_matrix_destroy(sk_matrix A);
 
 /* info[0..7] = format, dtype, nrow, ncol, nnz (stored entries), width
  * (ELL width / JAD diagonal count / BSR block count), device bytes held,
  * algorithmic bytes of one FP SpMV (the roofline byte model). */
-sk_status sk_matrix_info(sk_matrix A, int64_t info[8]);
+SK_API sk_status sk_matrix_info(sk_matrix A, int64_t info[8]);
 
 /* Adds an FP32 copy of the values of an FP64 CSR handle (indices shared),
  * used by the mixed-precision solver and the FP32 SpMV. */
-sk_status sk_matrix_add_f32_values(sk_matrix A);
+SK_API sk_status sk_matrix_add_f32_values(sk_matrix A);
 
 /* ---------------------------------------------------------------- */
 /* SpMV: y = A x                                                     */
@@ -127,17 +133,17 @@ sk_status sk_matrix_add_f32_values(sk_matrix A);
  * multiply(Ellpack_matrix const&, span)         spmv.hpp:119-140,
  * multiply(Block_sparse_row_matrix const&, span) spmv.hpp:148-174,
  * multiply(Jagged_diagonal_matrix const&, span) spmv.hpp:182-200. */
-sk_status sk_spmv(sk_matrix A, const void* x_dev, void* y_dev, sk_stream s);
+SK_API sk_status sk_spmv(sk_matrix A, const void* x_dev, void* y_dev, sk_stream s);
 
 /* Same product with the FP32 value copy (sk_matrix_add_f32_values) on
  * float vectors. */
-sk_status sk_spmv_f32(sk_matrix A, const float* x_dev, float* y_dev,
+SK_API sk_status sk_spmv_f32(sk_matrix A, const float* x_dev, float* y_dev,
                       sk_stream s);
 
 /* The drop-in form of multiply(A, span<T const>) -> std::vector<T>: x is
  * a host array of ncol values, y a host array of nrow values.  Copies x in,
  * runs the product and copies y out (synchronous). */
-sk_status sk_spmv_host(sk_matrix A, const void* x_host, void* y_host);
+SK_API sk_status sk_spmv_host(sk_matrix A, const void* x_host, void* y_host);
 
 /* ---------------------------------------------------------------- */
 /* BLAS-1 on device vectors (deterministic reductions)                */
@@ -146,16 +152,16 @@ sk_status sk_spmv_host(sk_matrix A, const void* x_host, void* y_host);
 /* std::inner_product(a, a+n, b, 0) as used by every solver
  * (e.g. conjugate_gradient.hpp:227, bicgstab.hpp:327-329). result is a host
  * double; the call synchronizes on s. */
-sk_status sk_dot(sk_dtype dtype, int64_t n, const void* a_dev,
+SK_API sk_status sk_dot(sk_dtype dtype, int64_t n, const void* a_dev,
                  const void* b_dev, double* result, sk_stream s);
 /* sqrt(<a, a>), e.g. bicgstab.hpp:333-336, fgmres.hpp:398-401. */
-sk_status sk_nrm2(sk_dtype dtype, int64_t n, const void* a_dev,
+SK_API sk_status sk_nrm2(sk_dtype dtype, int64_t n, const void* a_dev,
                   double* result, sk_stream s);
 /* y = alpha * x + y (conjugate_gradient.hpp:243-248 order). */
-sk_status sk_axpy(sk_dtype dtype, int64_t n, double alpha, const void* x_dev,
+SK_API sk_status sk_axpy(sk_dtype dtype, int64_t n, double alpha, const void* x_dev,
                   void* y_dev, sk_stream s);
 /* y = x + beta * y (conjugate_gradient.hpp:285-290 order). */
-sk_status sk_xpay(sk_dtype dtype, int64_t n, const void* x_dev, double beta,
+SK_API sk_status sk_xpay(sk_dtype dtype, int64_t n, const void* x_dev, double beta,
                   void* y_dev, sk_stream s);
 
 /* ---------------------------------------------------------------- */
@@ -165,26 +171,26 @@ sk_status sk_xpay(sk_dtype dtype, int64_t n, const void* x_dev, double beta,
 /* jacobi(A) (sparkit/data/jacobi.hpp:27-35) on a CSR handle: inverse
  * diagonal kept on the device.  An exact zero diagonal entry fails with
  * SK_ZERO_DIAGONAL (the reference throws std::invalid_argument). */
-sk_status sk_jacobi_create(sk_precond* out, sk_matrix A);
+SK_API sk_status sk_jacobi_create(sk_precond* out, sk_matrix A);
 
 /* chebyshev_preconditioner(A, lmin, lmax, degree)
  * (sparkit/data/chebyshev_preconditioner.hpp:46-84) on a CSR handle.
  * The coefficients are computed on the host as the reference does. */
-sk_status sk_chebyshev_create(sk_precond* out, sk_matrix A, double lambda_min,
+SK_API sk_status sk_chebyshev_create(sk_precond* out, sk_matrix A, double lambda_min,
                               double lambda_max, int64_t degree);
 
 /* z = M^{-1} r on device vectors: jacobi_apply (jacobi.hpp:44-51) or
  * chebyshev_preconditioner_apply (chebyshev_preconditioner.hpp:98-169).
  * A NULL precond is the identity (a copy). */
-sk_status sk_precond_apply(sk_precond M, int64_t n, const void* r_dev,
+SK_API sk_status sk_precond_apply(sk_precond M, int64_t n, const void* r_dev,
                            void* z_dev, sk_stream s);
 
 /* Copies the preconditioner's parameters to the host: the inverse
  * diagonal (Jacobi, n values) or the degree+1 coefficients (Chebyshev). */
-sk_status sk_precond_values(sk_precond M, void* host_out, int64_t capacity,
+SK_API sk_status sk_precond_values(sk_precond M, void* host_out, int64_t capacity,
                             int64_t* count);
 
-sk_status sk_precond_destroy(sk_precond M);
+SK_API sk_status sk_precond_destroy(sk_precond M);
 
 /* ---------------------------------------------------------------- */
 /* Solvers                                                           */
@@ -232,32 +238,32 @@ typedef struct {
  * and left / right = a preconditioner handle or NULL (identity).  b and x
  * are device vectors in the handle's dtype; x holds the initial guess and
  * receives the solution.  history_host may be NULL. */
-sk_status sk_cg_solve(sk_matrix A, sk_precond left, sk_precond right,
+SK_API sk_status sk_cg_solve(sk_matrix A, sk_precond left, sk_precond right,
                       const void* b_dev, void* x_dev, const sk_cg_config* cfg,
                       sk_summary* out, double* history_host, sk_stream s);
 
 /* bicgstab(b, x, cfg, op, left, right) (sparkit/data/bicgstab.hpp:383-410). */
-sk_status sk_bicgstab_solve(sk_matrix A, sk_precond left, sk_precond right,
+SK_API sk_status sk_bicgstab_solve(sk_matrix A, sk_precond left, sk_precond right,
                             const void* b_dev, void* x_dev,
                             const sk_bicgstab_config* cfg, sk_summary* out,
                             double* history_host, sk_stream s);
 
 /* fgmres(b, x, cfg, op, preconditioner) (sparkit/data/fgmres.hpp:452-470). */
-sk_status sk_fgmres_solve(sk_matrix A, sk_precond M, const void* b_dev,
+SK_API sk_status sk_fgmres_solve(sk_matrix A, sk_precond M, const void* b_dev,
                           void* x_dev, const sk_fgmres_config* cfg,
                           sk_summary* out, double* history_host, sk_stream s);
 
 /* Host-buffer forms of the three solvers (b and x in host memory, copied
  * in and out inside the call): the drop-in boundary of the C++ overloads. */
-sk_status sk_cg_solve_host(sk_matrix A, sk_precond left, sk_precond right,
+SK_API sk_status sk_cg_solve_host(sk_matrix A, sk_precond left, sk_precond right,
                            const void* b_host, void* x_host,
                            const sk_cg_config* cfg, sk_summary* out,
                            double* history_host);
-sk_status sk_bicgstab_solve_host(sk_matrix A, sk_precond left,
+SK_API sk_status sk_bicgstab_solve_host(sk_matrix A, sk_precond left,
                                  sk_precond right, const void* b_host,
                                  void* x_host, const sk_bicgstab_config* cfg,
                                  sk_summary* out, double* history_host);
-sk_status sk_fgmres_solve_host(sk_matrix A, sk_precond M, const void* b_host,
+SK_API sk_status sk_fgmres_solve_host(sk_matrix A, sk_precond M, const void* b_host,
                                void* x_host, const sk_fgmres_config* cfg,
                                sk_summary* out, double* history_host);
 

@@ -941,7 +941,7 @@ static sk_status fgmres_solve(sk_matrix A, sk_precond M, const T* b, T* x,
     }
     g_launches.fetch_add(1, std::memory_order_relaxed);
     scalar_kernel<<<1, 1, 0, st>>>(FgBackSub<T>{c.sc, sm, m});
-    launch_vec(n, OpFgUpdateX<T>{x, Z, ldv, sm.y, 0}, c.ws, nullptr, st);
+    launch_vec(n, OpFgUpdateX<T>{x, Z, ldv, sm.y, 0}, c.ws, c.sc, st);
     SK_CUDA(cudaGetLastError());
     if ((s = read_scalars(c.sc, &h, st)) != SK_OK) return s;
   }

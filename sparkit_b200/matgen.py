@@ -175,3 +175,24 @@ def zipf_random(n, s=1.5, cap=2048, seed=0, dtype=np.float64):
 def uniform_vector(n, seed=0, dtype=np.float64):
     """x ~ U[-1, 1], seeded."""
     return np.random.default_rng(seed).uniform(-1.0, 1.0, size=n).astype(dtype)
+
+
+def vector_laplacian_3d_bsr(nx, seed=0, coupling=0.1, dtype=np.float64):
+    """The same 3-component vector Laplacian as vector_laplacian_3d_bsr_csr,
+    built directly as a 3x3 Block_sparse_row_matrix (no scalar CSR pass):
+    block (I, J) = L_IJ * I_3, plus a dense U[-coupling, coupling] coupling
+    (seeded, per block row) off the diagonal of every diagonal block."""
+    from .formats import Block_sparse_row_matrix
+    L = laplacian_3d_dirichlet(nx, dtype=np.float64)
+    n = L.shape()[0]
+    rng = np.random.default_rng(seed)
+    coup = rng.uniform(-coupling, coupling, size=(n, 3, 3))
+    lens = L.row_lengths()
+    brow = np.repeat(np.arange(n, dtype=np.int64), lens)
+    bcol = L.col_ind()
+    blk = np.zeros((bcol.size, 3, 3), dtype=np.float64)
+    blk[:, [0, 1, 2], [0, 1, 2]] = L.values()[:, None]
+    d_idx = np.nonzero(brow == bcol)[0]
+    off = ~np.eye(3, dtype=bool)
+    blk[d_idx] = np.where(off[None], coup[brow[d_idx]], blk[d_idx])
+    return Block_sparse_row_matrix((3 * n, 3 * n), 3, 3, L.row_ptr(), bcol, blk.reshape(-1).astype(dtype))

@@ -1,0 +1,126 @@
+"""Generates the golden fixtures in tests/golden/ by running the sparkit
+reference itself (compiled from its sources into oracle/_ref by
+oracle/build_ref.sh).  Run from the repository root:
+
+    python -m tests.golden.make_golden
+
+Outputs
+  reference_outputs.npz  -- inputs and reference outputs, keyed by case:
+      SpMV of every format (reference conversions + multiply) on seeded
+      matrices, Jacobi inverse diagonals, Chebyshev coefficients and applies,
+      and CG / BiCGSTAB / FGMRES solutions, summaries and residual histories
+      on the matrices of the reference's solver tests.
+known_answers.json (hand-written, not generated) holds the known-answer
+vectors of the reference's Catch2 tests.
+"""
+import os
+import sys
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+sys.path.insert(0, ROOT)
+
+from oracle.binding import Reference  # noqa: E402
+from sparkit_b200 import matgen  # noqa: E402
+from sparkit_b200.formats import Compressed_row_matrix  # noqa: E402
+
+OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "reference_outputs.npz")
+
+
+def spmv_matrices():
+    """Seeded small matrices covering the layouts' edge cases."""
+    rng = np.random.default_rng(7)
+    mats = {
+        "lap2d_16": matgen.laplacian_2d_dirichlet(16),
+        "lap3d_6": matgen.laplacian_3d_dirichlet(6),
+        "zipf_400": matgen.zipf_random(400, s=1.5, cap=96, seed=3),
+        "vec3_4": matgen.vector_laplacian_3d_bsr_csr(4, seed=1),
+    }
+    # rectangular with empty rows
+    n, m = 37, 53
+    rows = rng.integers(0, n, 160)
+    cols = rng.integers(0, m, 160)
+    keep = rows % 5 != 2  # rows 2, 7, 12, ... stay empty
+    mats["rect_37x53"] = Compressed_row_matrix.from_entries((n, m), rows[keep], cols[keep],
+                                                            rng.standard_normal(keep.sum()))
+    # one long row among short ones (exercises the long-row CSR path)
+    n = 3000
+    rows = np.concatenate([np.full(2600, 5), rng.integers(0, n, 4000)])
+    cols = np.concatenate([rng.permutation(n)[:2600], rng.integers(0, n, 4000)])
+    mats["longrow_3000"] = Compressed_row_matrix.from_entries((n, n), rows, cols,
+                                                              rng.standard_normal(rows.size))
+    # nrow not a multiple of the BSR block size (the reference truncates)
+    mats["odd_7"] = matgen.tridiagonal_matrix(7, -1.0, 4.0, -2.0)
+    return mats
+
+
+def main():
+    R = Reference()
+    out = {}
+    for name, A in spmv_matrices().items():
+        for dt in (np.float64, np.float32):
+            Ad = A.astype(dt)
+            tag = f"spmv/{name}/{np.dtype(dt).name}"
+            x = matgen.uniform_vector(Ad.shape()[1], seed=11, dtype=dt)
+            out[f"{tag}/row_ptr"] = Ad.row_ptr()
+            out[f"{tag}/col_ind"] = Ad.col_ind()
+            out[f"{tag}/values"] = Ad.values()
+            out[f"{tag}/shape"] = np.array(Ad.shape())
+            out[f"{tag}/x"] = x
+            out[f"{tag}/y_csr"] = R.spmv(Ad, x, "csr")
+            out[f"{tag}/y_ell"] = R.spmv(Ad, x, "ell")
+            out[f"{tag}/y_jad"] = R.spmv(Ad, x, "jad")
+            for br, bc in ((2, 2), (3, 3), (2, 3)):
+                out[f"{tag}/y_bsr{br}{bc}"] = R.spmv(Ad, x, "bsr", (br, bc))
+    # preconditioners
+    P = matgen.poisson_2d(8, 8, 0.5)
+    out["jacobi/poisson8/inv_d"] = R.jacobi(P)
+    for lmin, lmax, deg in ((0.5, 8.5, 8), (3.0, 13.0, 4), (1.0, 1.0, 5), (2.0, 6.0, 0)):
+        key = f"cheb/{lmin}_{lmax}_{deg}"
+        out[f"{key}/coeffs_f64"] = R.chebyshev_coeffs(P, lmin, lmax, deg)
+        out[f"{key}/coeffs_f32"] = R.chebyshev_coeffs(P.astype(np.float32), lmin, lmax, deg)
+        r = matgen.uniform_vector(P.shape()[0], seed=5)
+        out[f"{key}/r"] = r
+        out[f"{key}/z"] = R.chebyshev_apply(P, lmin, lmax, deg, r)
+    # solvers on the reference tests' matrices (and a Dirichlet grid)
+    problems = {
+        "grid16": matgen.poisson_2d(4, 4, 5.0),
+        "tridiag4": matgen.tridiagonal_matrix(4, -1.0, 4.0, -1.0),
+        "convdiff": matgen.convdiff_centered_2d(4, 4, 1.0, 0.3, 0.3, 5.0),
+        "nonsym": matgen.nonsymmetric_sample(),
+        "lap2d_24": matgen.laplacian_2d_dirichlet(24),
+        "upwind_20": matgen.convection_diffusion_2d(20, 20, 1.0, 0.8, 0.4),
+    }
+    spd = {"grid16", "tridiag4", "lap2d_24"}
+    for name, A in problems.items():
+        n = A.shape()[0]
+        xt = np.arange(1, n + 1, dtype=np.float64) if n <= 16 else matgen.uniform_vector(n, seed=0)
+        b = R.spmv(A, xt, "csr")
+        base = f"solve/{name}"
+        out[f"{base}/row_ptr"] = A.row_ptr()
+        out[f"{base}/col_ind"] = A.col_ind()
+        out[f"{base}/values"] = A.values()
+        out[f"{base}/b"] = b
+        precs = {"none": None, "jacobi": "jacobi", "cheb": ("chebyshev", 0.5, 9.0, 6)}
+        for pname, spec in precs.items():
+            runs = []
+            if name in spd:
+                runs.append(("cg_left", lambda: R.cg(A, b, np.zeros(n), 1e-12, 50, 500, left=spec, collect=True)))
+                runs.append(("cg_right", lambda: R.cg(A, b, np.zeros(n), 1e-12, 7, 500, right=spec, collect=True)))
+            runs.append(("bicgstab", lambda: R.bicgstab(A, b, np.zeros(n), 1e-12, 500, left=spec, collect=True)))
+            runs.append(("fgmres", lambda: R.fgmres(A, b, np.zeros(n), 1e-12, 5, 500, prec=spec, collect=True)))
+            for rname, fn in runs:
+                x, s = fn()
+                key = f"{base}/{pname}/{rname}"
+                out[f"{key}/x"] = x
+                out[f"{key}/iters"] = np.array(s["computed_iterations"])
+                out[f"{key}/converged"] = np.array(int(s["converged"]))
+                out[f"{key}/residual_norm"] = np.array(s["residual_norm"])
+                out[f"{key}/history"] = np.array(s["iteration_residuals"])
+    np.savez_compressed(OUT, **out)
+    print(f"wrote {OUT}: {len(out)} arrays, {os.path.getsize(OUT)} bytes")
+
+
+if __name__ == "__main__":
+    main()

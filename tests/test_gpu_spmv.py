@@ -1,0 +1,143 @@
+"""SpMV parity on the GPU, through the C ABI.
+
+Bar: bit-exact against the reference wherever each row is summed by one
+thread in storage order (every ELL, JAD and BSR row; CSR row blocks whose
+rows hold at most 32 entries).  CSR blocks with longer rows are summed by
+several lanes; there the normwise error
+||y - y_ref||_inf / || |A| |x| ||_inf must stay below 1e-14 (FP64) or
+1e-6 (FP32)."""
+import numpy as np
+import pytest
+
+from sparkit_b200 import _lib, formats, gpu, matgen
+from tests.helpers import BSR_BLOCKS, SPMV_CASES, convert, csr_from_entries, golden_csr
+
+pytestmark = pytest.mark.gpu
+
+TOL = {np.dtype(np.float64): 1e-14, np.dtype(np.float32): 1e-6}
+
+
+def normwise_err(A, x, y, y_ref):
+    absA = formats.Compressed_row_matrix(A.shape(), A.row_ptr(), A.col_ind(), np.abs(A.values()).astype(np.float64))
+    rows = np.repeat(np.arange(A.shape()[0]), A.row_lengths())
+    scale = np.zeros(A.shape()[0])
+    np.add.at(scale, rows, np.abs(A.values()).astype(np.float64) * np.abs(x.astype(np.float64))[A.col_ind()])
+    denom = max(scale.max() if scale.size else 0.0, np.finfo(np.float64).tiny)
+    del absA
+    return np.max(np.abs(y.astype(np.float64) - y_ref.astype(np.float64))) / denom if y.size else 0.0
+
+
+def test_known_answers(gpu_lib, known):
+    for case in known["spmv"]:
+        A = csr_from_entries(tuple(case["shape"]), case["entries"])
+        M = convert(A, case["format"], tuple(case.get("block", (3, 3))))
+        Ad = gpu.Device_matrix(M)
+        y = gpu.multiply(Ad, np.array(case["x"]))
+        assert y.tolist() == case["y"], case["name"]
+
+
+@pytest.mark.parametrize("name", SPMV_CASES)
+@pytest.mark.parametrize("dtype", ["float64", "float32"])
+def test_golden_all_formats(gpu_lib, golden, name, dtype):
+    tag = f"spmv/{name}/{dtype}"
+    A = golden_csr(golden, tag)
+    x = golden[f"{tag}/x"]
+    for fmt in ("csr", "ell", "jad"):
+        y = gpu.multiply(gpu.Device_matrix(convert(A, fmt)), x)
+        y_ref = golden[f"{tag}/y_{fmt}"]
+        if fmt == "csr" and A.row_lengths().max(initial=0) > 32:
+            assert normwise_err(A, x, y, y_ref) <= TOL[A.dtype], fmt
+        else:
+            assert np.array_equal(y, y_ref), fmt
+    for key, blk in BSR_BLOCKS.items():
+        y = gpu.multiply(gpu.Device_matrix(formats.to_block_sparse_row(A, *blk)), x)
+        assert np.array_equal(y, golden[f"{tag}/y_bsr{blk[0]}{blk[1]}"]), key
+
+
+def test_lap3d_128_full_size_bitwise(gpu_lib, oracle):
+    """The benchmark matrix (n = 2,097,152, nnz = 14,581,760) in every
+    scalar format, bit for bit against the oracle."""
+    A = matgen.laplacian_3d_dirichlet(128)
+    assert A.size() == 14581760
+    x = matgen.uniform_vector(A.shape()[0], seed=1)
+    y_ref = oracle.spmv(A, x)
+    for fmt in ("csr", "ell", "jad"):
+        M = convert(A, fmt)
+        Ad = gpu.Device_matrix(M)
+        assert np.array_equal(gpu.multiply(Ad, x), y_ref), fmt
+        Ad.close()
+    A32 = A.astype(np.float32)
+    x32 = x.astype(np.float32)
+    assert np.array_equal(gpu.multiply(gpu.Device_matrix(A32), x32), oracle.spmv(A32, x32))
+
+
+def test_vector_laplacian_bsr33_bitwise(gpu_lib, oracle):
+    V = matgen.vector_laplacian_3d_bsr_csr(24, seed=3)
+    B = formats.to_block_sparse_row(V, 3, 3)
+    x = matgen.uniform_vector(V.shape()[0], seed=2)
+    assert np.array_equal(gpu.multiply(gpu.Device_matrix(B), x), oracle.spmv(B, x))
+
+
+def test_zipf_skewed_rows(gpu_lib, oracle):
+    """Skewed rows (Zipf(1.5) lengths capped at 2048) exercise the lane and
+    long-row paths; checked normwise, and bit-exact for ELL / JAD."""
+    A = matgen.zipf_random(60000, s=1.5, cap=2048, seed=5)
+    x = matgen.uniform_vector(A.shape()[0], seed=6)
+    y_ref = oracle.spmv(A, x)
+    y = gpu.multiply(gpu.Device_matrix(A), x)
+    assert normwise_err(A, x, y, y_ref) <= 1e-14
+    J = formats.to_jagged_diagonal(A)
+    assert np.array_equal(gpu.multiply(gpu.Device_matrix(J), x), oracle.spmv(J, x))
+    # a row longer than one CTA tile (2048 entries) takes the long-row path
+    n = 5000
+    rng = np.random.default_rng(9)
+    rows = np.concatenate([np.full(4500, 17), rng.integers(0, n, 3000)])
+    cols = np.concatenate([rng.permutation(n)[:4500], rng.integers(0, n, 3000)])
+    L = formats.Compressed_row_matrix.from_entries((n, n), rows, cols, rng.standard_normal(rows.size))
+    xl = matgen.uniform_vector(n, seed=8)
+    yl = gpu.multiply(gpu.Device_matrix(L), xl)
+    assert normwise_err(L, xl, yl, oracle.spmv(L, xl)) <= 1e-14
+
+
+def test_device_pointer_path_and_fp32_copy(gpu_lib, oracle):
+    import torch
+    A = matgen.laplacian_3d_dirichlet(32)
+    n = A.shape()[0]
+    x = matgen.uniform_vector(n, seed=3)
+    Ad = gpu.Device_matrix(A)
+    xd = torch.from_numpy(x).cuda()
+    yd = torch.empty_like(xd)
+    Ad.spmv(xd, yd)
+    torch.cuda.synchronize()
+    assert np.array_equal(yd.cpu().numpy(), oracle.spmv(A, x))
+    Ad.add_f32_values()
+    x32 = xd.float()
+    y32 = torch.empty_like(x32)
+    Ad.spmv_f32(x32, y32)
+    torch.cuda.synchronize()
+    assert np.array_equal(y32.cpu().numpy(), oracle.spmv(A.astype(np.float32), x.astype(np.float32)))
+
+
+def test_edge_shapes(gpu_lib):
+    # zero rows, zero columns, all-empty rows
+    for shape in ((0, 0), (0, 5), (4, 0), (6, 6)):
+        A = formats.Compressed_row_matrix(shape, np.zeros(shape[0] + 1, np.int64), np.zeros(0, np.int64),
+                                          np.zeros(0))
+        for fmt in ("csr", "ell", "jad", "bsr22"):
+            M = convert(A, fmt, (2, 2))
+            y = gpu.multiply(gpu.Device_matrix(M), np.ones(shape[1]))
+            assert y.shape == (shape[0],) and not y.any()
+
+
+def test_index_validation(gpu_lib):
+    A = formats.Compressed_row_matrix((2, 2), [0, 1, 2], [0, 5], [1.0, 2.0])  # column 5 >= ncol
+    with pytest.raises(_lib.SkError) as e:
+        gpu.Device_matrix(A)
+    assert e.value.status == 2  # SK_INDEX_OVERFLOW
+    E = formats.Ellpack_matrix((2, 2), 1, [0, 1 << 33], [1.0, 1.0])  # beyond int32
+    with pytest.raises(_lib.SkError):
+        gpu.Device_matrix(E)
+    big = formats.Compressed_row_matrix((1, 1 << 31), [0, 0], np.zeros(0, np.int64), np.zeros(0))
+    with pytest.raises(_lib.SkError) as e:
+        gpu.Device_matrix(big)
+    assert e.value.status == 2

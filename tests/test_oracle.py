@@ -1,0 +1,142 @@
+"""Pins the CPU oracle (oracle/sk_oracle.c) before it is trusted:
+against the known-answer vectors of the reference's Catch2 tests and, bit
+for bit, against outputs of the reference itself (tests/golden/, made by
+tests/golden/make_golden.py; plus live runs when the compiled reference is
+present)."""
+import numpy as np
+import pytest
+
+from sparkit_b200 import formats, matgen
+from tests.helpers import BSR_BLOCKS, SPMV_CASES, convert, csr_from_entries, golden_csr, golden_problem
+
+
+def test_spmv_known_answers(oracle, known):
+    for case in known["spmv"]:
+        A = csr_from_entries(tuple(case["shape"]), case["entries"])
+        M = convert(A, case["format"], tuple(case.get("block", (3, 3))))
+        y = oracle.spmv(M, np.array(case["x"]))
+        assert y.tolist() == case["y"], case["name"]
+
+
+def test_jacobi_known_answers(oracle, known):
+    for case in known["jacobi"]:
+        A = csr_from_entries(tuple(case["shape"]), case["entries"])
+        if case.get("throws"):
+            with pytest.raises(ValueError):
+                oracle.jacobi(A)
+            continue
+        inv = oracle.jacobi(A)
+        if "inv_d" in case:
+            np.testing.assert_allclose(inv, case["inv_d"], rtol=1e-15)
+        if "z" in case:
+            assert (inv * np.array(case["r"])).tolist() == case["z"]
+
+
+def test_layout_known_answers(known):
+    for case in known["layouts"]:
+        A = csr_from_entries(tuple(case["shape"]), case["entries"])
+        if "perm" in case:
+            J = formats.to_jagged_diagonal(A)
+            assert J.perm().tolist() == case["perm"]
+            assert J.jdiag().tolist() == case["jdiag"]
+        if "width" in case:
+            E = formats.to_ellpack(A)
+            assert E.max_nnz_per_row() == case["width"]
+            assert E.col_ind().tolist() == case["col_ind"]
+
+
+@pytest.mark.parametrize("name", SPMV_CASES)
+@pytest.mark.parametrize("dtype", ["float64", "float32"])
+def test_spmv_matches_reference_bitwise(oracle, golden, name, dtype):
+    tag = f"spmv/{name}/{dtype}"
+    A = golden_csr(golden, tag)
+    x = golden[f"{tag}/x"]
+    for fmt in ("csr", "ell", "jad"):
+        y = oracle.spmv(convert(A, fmt), x)
+        assert np.array_equal(y, golden[f"{tag}/y_{fmt}"]), fmt
+    for key, blk in BSR_BLOCKS.items():
+        y = oracle.spmv(formats.to_block_sparse_row(A, *blk), x)
+        assert np.array_equal(y, golden[f"{tag}/y_bsr{blk[0]}{blk[1]}"]), key
+
+
+def test_preconditioners_match_reference_bitwise(oracle, golden):
+    P = matgen.poisson_2d(8, 8, 0.5)
+    assert np.array_equal(oracle.jacobi(P), golden["jacobi/poisson8/inv_d"])
+    for lmin, lmax, deg in ((0.5, 8.5, 8), (3.0, 13.0, 4), (1.0, 1.0, 5), (2.0, 6.0, 0)):
+        key = f"cheb/{lmin}_{lmax}_{deg}"
+        assert np.array_equal(oracle.chebyshev_coeffs(lmin, lmax, deg), golden[f"{key}/coeffs_f64"])
+        assert np.array_equal(oracle.chebyshev_coeffs(lmin, lmax, deg, np.float32), golden[f"{key}/coeffs_f32"])
+        z = oracle.chebyshev_apply(P, lmin, lmax, deg, golden[f"{key}/r"])
+        assert np.array_equal(z, golden[f"{key}/z"]), key
+
+
+PROBLEMS = ["grid16", "tridiag4", "convdiff", "nonsym", "lap2d_24", "upwind_20"]
+SPD = {"grid16", "tridiag4", "lap2d_24"}
+PRECS = {"none": None, "jacobi": "jacobi", "cheb": ("chebyshev", 0.5, 9.0, 6)}
+
+
+@pytest.mark.parametrize("name", PROBLEMS)
+@pytest.mark.parametrize("pname", list(PRECS))
+def test_solvers_match_reference_bitwise(oracle, golden, name, pname):
+    A = golden_problem(golden, name)
+    n = A.shape()[0]
+    b = golden[f"solve/{name}/b"]
+    spec = PRECS[pname]
+    runs = {"bicgstab": lambda: oracle.bicgstab(A, b, np.zeros(n), 1e-12, 500, left=spec, collect=True),
+            "fgmres": lambda: oracle.fgmres(A, b, np.zeros(n), 1e-12, 5, 500, prec=spec, collect=True)}
+    if name in SPD:
+        runs["cg_left"] = lambda: oracle.cg(A, b, np.zeros(n), 1e-12, 50, 500, left=spec, collect=True)
+        runs["cg_right"] = lambda: oracle.cg(A, b, np.zeros(n), 1e-12, 7, 500, right=spec, collect=True)
+    for rname, fn in runs.items():
+        key = f"solve/{name}/{pname}/{rname}"
+        x, s = fn()
+        assert np.array_equal(x, golden[f"{key}/x"]), key
+        assert s["computed_iterations"] == int(golden[f"{key}/iters"]), key
+        assert int(s["converged"]) == int(golden[f"{key}/converged"]), key
+        assert s["residual_norm"] == float(golden[f"{key}/residual_norm"]), key
+        assert np.array_equal(np.array(s["iteration_residuals"]), golden[f"{key}/history"]), key
+
+
+def test_cg_edge_cases_match_reference(oracle, reference):
+    A = matgen.poisson_2d(4, 4, 5.0)
+    n = 16
+    b = oracle.spmv(A, np.arange(1, n + 1, dtype=np.float64))
+    # zero right-hand side: x = 0, converged, no iterations
+    x, s = oracle.cg(A, np.zeros(n), np.ones(n), 1e-12, 50, 100)
+    xr, sr = reference.cg(A, np.zeros(n), np.ones(n), 1e-12, 50, 100)
+    assert np.array_equal(x, xr) and not x.any() and s["converged"] and s["computed_iterations"] == 0
+    assert s == sr
+    # max_iterations = 1: not converged after exactly one iteration
+    x, s = oracle.cg(A, b, np.zeros(n), 1e-14, 50, 1)
+    xr, sr = reference.cg(A, b, np.zeros(n), 1e-14, 50, 1)
+    assert s["computed_iterations"] == 1 and not s["converged"] and s == sr and np.array_equal(x, xr)
+
+
+def test_float_solvers_match_reference(oracle, reference):
+    A = matgen.laplacian_2d_dirichlet(20, dtype=np.float32)
+    n = A.shape()[0]
+    b = matgen.uniform_vector(n, seed=4, dtype=np.float32)
+    for spec in (None, "jacobi"):
+        x, s = oracle.cg(A, b, np.zeros(n, np.float32), 1e-5, 1000, 1000, left=spec, collect=True)
+        xr, sr = reference.cg(A, b, np.zeros(n, np.float32), 1e-5, 1000, 1000, left=spec, collect=True)
+        assert np.array_equal(x, xr) and s == sr
+        x, s = oracle.bicgstab(A, b, np.zeros(n, np.float32), 1e-5, 1000, left=spec, collect=True)
+        xr, sr = reference.bicgstab(A, b, np.zeros(n, np.float32), 1e-5, 1000, left=spec, collect=True)
+        assert np.array_equal(x, xr) and s == sr
+        x, s = oracle.fgmres(A, b, np.zeros(n, np.float32), 1e-5, 10, 1000, prec=spec, collect=True)
+        xr, sr = reference.fgmres(A, b, np.zeros(n, np.float32), 1e-5, 10, 1000, prec=spec, collect=True)
+        assert np.array_equal(x, xr) and s == sr
+
+
+def test_generators_match_reference(reference):
+    pairs = [(matgen.poisson_2d(4, 4, 5.0), reference.poisson_2d(4, 4, 5.0)),
+             (matgen.poisson_2d(5, 3), reference.poisson_2d(5, 3)),
+             (matgen.convdiff_centered_2d(4, 4, 1.0, 0.3, 0.3, 5.0),
+              reference.convdiff_centered_2d(4, 4, 1.0, 0.3, 0.3, 5.0)),
+             (matgen.convection_diffusion_2d(6, 5, 1.0, 0.7, 0.2),
+              reference.convection_diffusion_2d(6, 5, 1.0, 0.7, 0.2)),
+             (matgen.tridiagonal_matrix(6, -1.0, 4.0, -1.0), reference.tridiagonal(6, -1.0, 4.0, -1.0)),
+             (matgen.nonsymmetric_sample(), reference.nonsymmetric_sample())]
+    for a, b in pairs:
+        for f in ("row_ptr", "col_ind", "values"):
+            assert np.array_equal(getattr(a, f)(), getattr(b, f)())
