@@ -199,6 +199,7 @@ def run_reference(args):
 # ---------------------------------------------------------------------
 def time_device(fn, steps, warmup, stream):
     import torch
+    torch.cuda.synchronize()
     for _ in range(warmup):
         fn()
     torch.cuda.synchronize()
@@ -218,6 +219,7 @@ def sweep(stream, grid):
 
     from sparkit_b200 import formats, gpu, matgen
     out = {}
+    sptr = gpu.torch_stream(stream)
     A, x = build_workload(grid)
     for dt, tag in ((np.float64, "f64"), (np.float32, "f32")):
         Adt = A.astype(dt)
@@ -225,7 +227,7 @@ def sweep(stream, grid):
         yd = torch.empty_like(xd)
         for fmt, M in (("csr", Adt), ("ell", formats.to_ellpack(Adt)), ("jad", formats.to_jagged_diagonal(Adt))):
             Ad = gpu.Device_matrix(M)
-            ms = time_device(lambda: Ad.spmv(xd, yd, stream=ctypes.c_void_p(stream.cuda_stream)), 300, 20, stream)
+            ms = time_device(lambda: Ad.spmv(xd, yd, stream=sptr), 300, 20, stream)
             out[f"lap3d_{fmt}_{tag}"] = {"gbs": Ad.info()["spmv_bytes"] / ms / 1e6, "us": ms * 1e3}
             Ad.close()
     del A
@@ -233,7 +235,7 @@ def sweep(stream, grid):
     Bd = gpu.Device_matrix(B)
     xb = torch.from_numpy(matgen.uniform_vector(B.shape()[0], seed=2)).cuda()
     yb = torch.empty_like(xb)
-    ms = time_device(lambda: Bd.spmv(xb, yb, stream=ctypes.c_void_p(stream.cuda_stream)), 200, 20, stream)
+    ms = time_device(lambda: Bd.spmv(xb, yb, stream=sptr), 200, 20, stream)
     out["vec3_bsr33_f64"] = {"gbs": Bd.info()["spmv_bytes"] / ms / 1e6, "us": ms * 1e3}
     Bd.close()
     del B
@@ -241,7 +243,7 @@ def sweep(stream, grid):
     Zd = gpu.Device_matrix(Z)
     xz = torch.from_numpy(matgen.uniform_vector(Z.shape()[0], seed=3)).cuda()
     yz = torch.empty_like(xz)
-    ms = time_device(lambda: Zd.spmv(xz, yz, stream=ctypes.c_void_p(stream.cuda_stream)), 200, 20, stream)
+    ms = time_device(lambda: Zd.spmv(xz, yz, stream=sptr), 200, 20, stream)
     out["zipf_csr_f64"] = {"gbs": Zd.info()["spmv_bytes"] / ms / 1e6, "us": ms * 1e3, "nnz": Z.size(),
                            "mean_row": Z.size() / Z.shape()[0]}
     return out
@@ -289,8 +291,10 @@ def main():
         torch.cuda.set_device(0)
     from sparkit_b200 import _lib, gpu
     dev = torch.cuda.current_device()
-    stream = torch.cuda.current_stream()
-    sptr = ctypes.c_void_p(stream.cuda_stream)
+    # a dedicated stream: the kernels and the CUDA events share it
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    sptr = gpu.torch_stream(stream)
 
     A, x = build_workload(args.grid)
     n = A.shape()[0]

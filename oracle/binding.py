@@ -97,6 +97,10 @@ class Oracle:
             raise TypeError(type(A))
         return op, keep
 
+    def set_dot_order(self, mode):
+        """0: the reference's sequential dot products; 1: chunked order."""
+        self.L.sko_set_dot_order(int(mode))
+
     def spmv(self, A, x):
         x = np.ascontiguousarray(x, dtype=A.dtype)
         y = np.zeros(A.shape()[0], dtype=A.dtype)

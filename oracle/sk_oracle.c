@@ -12,6 +12,10 @@
 
 #define SKO_PI 3.141592653589793238462643383279502884
 
+/* 0: reference order (sequential); 1: chunked order (sensitivity studies). */
+static int sko_dot_order = 0;
+void sko_set_dot_order(int mode) { sko_dot_order = mode; }
+
 #define SKO_T double
 #define SKO_SFX f64
 #define SKO_SQRT sqrt

@@ -111,6 +111,10 @@ typedef struct {
   void sko_fgmres_##S(const sko_operator*, const sko_precond*, const T*, T*,  \
                       const sko_fgmres_config*, sko_summary*, double*);
 
+/* Summation order of the solvers' dot products: 0 = the reference's
+ * sequential order (default), 1 = 256-element chunks added in order. */
+void sko_set_dot_order(int mode);
+
 SKO_DECLARE(double, f64)
 SKO_DECLARE(float, f32)
 

@@ -230,7 +230,23 @@ static void SKO_FN(sko_apply_prec_)(const sko_precond* M, const sko_operator* A,
   }
 }
 
+/* std::inner_product(a, a+n, b, T{0}): sequential, as every solver of the
+ * reference sums its dot products.  With sko_set_dot_order(1) the sum is
+ * instead taken in 256-element sequential chunks whose partial sums are then
+ * added in order -- a different association of the same products, used only
+ * to measure how sensitive a solver's iteration count is to the summation
+ * order (the GPU sums in a fixed tree). */
 static SKO_T SKO_FN(sko_dot_)(const SKO_T* a, const SKO_T* b, int64_t n) {
+  if (sko_dot_order == 1) {
+    SKO_T total = 0;
+    for (int64_t c = 0; c < n; c += 256) {
+      SKO_T part = 0;
+      int64_t e = c + 256 < n ? c + 256 : n;
+      for (int64_t i = c; i < e; ++i) part += a[i] * b[i];
+      total += part;
+    }
+    return total;
+  }
   SKO_T s = 0;
   for (int64_t i = 0; i < n; ++i) s += a[i] * b[i];
   return s;

@@ -3,6 +3,7 @@
 Loads the in-tree ``libsparkit_b200.so``.  There is no fallback: if the
 library is missing or cannot load, every entry point raises.
 """
+import atexit
 import ctypes
 import os
 import threading
@@ -99,6 +100,21 @@ SIGNATURES = [
 
 _lock = threading.Lock()
 _lib = None
+_shutting_down = False
+
+
+def _mark_shutdown():
+    global _shutting_down
+    _shutting_down = True
+
+
+atexit.register(_mark_shutdown)
+
+
+def shutting_down():
+    """True once the interpreter exits: handles are then left to the
+    process teardown instead of being destroyed in arbitrary GC order."""
+    return _shutting_down
 
 
 def lib():

@@ -318,7 +318,7 @@ sk_status sk_precond_values(sk_precond M, void* host_out, int64_t capacity, int6
 
 sk_status sk_precond_destroy(sk_precond M) {
   if (!M) return SK_OK;
-  if (M->A && M->A->stream) cudaStreamSynchronize(M->A->stream);
+  // cudaFree waits for the device; the matrix M->A may already be gone.
   if (M->inv_diag) cudaFree(M->inv_diag);
   if (M->inv_diag32) cudaFree(M->inv_diag32);
   if (M->work) cudaFree(M->work);

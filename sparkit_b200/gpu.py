@@ -52,10 +52,22 @@ def _is_device(a):
     return not isinstance(a, np.ndarray) and hasattr(a, "data_ptr")
 
 
+CUDA_STREAM_LEGACY = 1  # cudaStreamLegacy
+
+
+def torch_stream(s=None):
+    """The sk_stream of a torch stream (default: the current one).  torch's
+    default stream has handle 0, which the C ABI would read as "the
+    handle's own stream", so it is passed as cudaStreamLegacy instead."""
+    import torch
+    s = torch.cuda.current_stream() if s is None else s
+    return ctypes.c_void_p(s.cuda_stream if s.cuda_stream else CUDA_STREAM_LEGACY)
+
+
 def _stream_of(a):
     if _is_device(a):
         import torch
-        return ctypes.c_void_p(torch.cuda.current_stream(a.device).cuda_stream)
+        return torch_stream(torch.cuda.current_stream(a.device))
     return None
 
 
@@ -114,9 +126,9 @@ class Device_matrix:
         check(lib().sk_spmv_f32(self.handle, _ptr(x), _ptr(y), st))
 
     def close(self):
-        if getattr(self, "handle", None):
+        if getattr(self, "handle", None) and not _lib.shutting_down():
             lib().sk_matrix_destroy(self.handle)
-            self.handle = None
+        self.handle = None
 
     def __del__(self):
         try:
@@ -161,9 +173,9 @@ class _Precond:
         return out
 
     def close(self):
-        if getattr(self, "handle", None):
+        if getattr(self, "handle", None) and not _lib.shutting_down():
             lib().sk_precond_destroy(self.handle)
-            self.handle = None
+        self.handle = None
 
     def __del__(self):
         try:

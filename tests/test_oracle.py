@@ -140,3 +140,26 @@ def test_generators_match_reference(reference):
     for a, b in pairs:
         for f in ("row_ptr", "col_ind", "values"):
             assert np.array_equal(getattr(a, f)(), getattr(b, f)())
+
+
+def test_bicgstab_iteration_count_depends_on_summation_order(oracle):
+    """Evidence for the BiCGSTAB parity band of the GPU tests: the
+    reference algorithm itself, with its dot products summed in 256-entry
+    chunks instead of sequentially, needs a different number of matrix-
+    vector products on a nonsymmetric problem, while FGMRES and CG need
+    exactly the same."""
+    A = matgen.convection_diffusion_2d(48, 48, 1.0, 0.9, 0.5)
+    n = A.shape()[0]
+    b = oracle.spmv(A, matgen.uniform_vector(n, seed=2))
+    counts = {}
+    try:
+        for mode in (0, 1):
+            oracle.set_dot_order(mode)
+            _, s = oracle.bicgstab(A, b, np.zeros(n), 1e-10, 3000, left="jacobi")
+            _, f = oracle.fgmres(A, b, np.zeros(n), 1e-10, 30, 3000, prec="jacobi")
+            counts[mode] = (s["computed_iterations"], f["computed_iterations"])
+    finally:
+        oracle.set_dot_order(0)
+    assert counts[0][0] != counts[1][0]          # BiCGSTAB moves
+    assert counts[0][1] == counts[1][1]          # FGMRES does not
+    assert abs(counts[0][0] - counts[1][0]) <= 0.05 * counts[0][0]
