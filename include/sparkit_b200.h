@@ -5,8 +5,6 @@
  * own: its hot path is reached through C++ overloads and templates
  * (namespace sparkit::data::detail).  Each entry point below states which
  * reference interface it replaces (file:line within the sparkit project).
- * include/sparkit_b200/gpu.hpp wraps these calls in C++ overloads with the
- * reference's own names and signatures.
  *
  * Conventions
  *  - Every call returns sk_status; SK_OK is 0.  sk_last_error() gives a

@@ -1,5 +1,5 @@
-"""Python mirror of the drop-in GPU path (the C++ form is
-include/sparkit_b200/gpu.hpp); every call goes through the C ABI.
+"""Python mirror of the drop-in GPU path; every call goes through the C ABI
+of include/sparkit_b200.h.
 
 Names and argument meaning follow the reference:
 
