@@ -190,6 +190,24 @@ SK_API sk_status sk_precond_values(sk_precond M, void* host_out, int64_t capacit
 
 SK_API sk_status sk_precond_destroy(sk_precond M);
 
+/* No reference counterpart: an addition of this library.  The Chebyshev
+ * apply z = p(A) r of sk_precond_apply, for callers that cannot allocate
+ * device memory when they apply the preconditioner (a callback inside
+ * another solver's loop with its memory reserved up front, or a stream being
+ * captured into a CUDA graph).  It takes the parameters of
+ * sk_chebyshev_create directly and keeps its two work vectors in a static
+ * device array instead of allocating them: A is a square CSR handle of at
+ * most 1,048,576 rows (larger ones fail with SK_INVALID_ARG), degree is at
+ * most 64, and every GPU that runs it holds that 16 MiB array until the
+ * process exits.  Calls share the array, so calls that overlap on the GPU
+ * race; serialize them.  The first call on a device looks the array up and
+ * should come before any stream capture.  Results are identical to
+ * sk_precond_apply with a preconditioner from sk_chebyshev_create. */
+SK_API sk_status sk_chebyshev_apply_noalloc(sk_matrix A, double lambda_min,
+                                            double lambda_max, int64_t degree,
+                                            const void* r_dev, void* z_dev,
+                                            sk_stream s);
+
 /* ---------------------------------------------------------------- */
 /* Solvers                                                           */
 /* ---------------------------------------------------------------- */

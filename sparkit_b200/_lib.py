@@ -84,6 +84,7 @@ SIGNATURES = [
     ("sk_precond_apply", [c_vp, c_i64, c_vp, c_vp, c_vp]),
     ("sk_precond_values", [c_vp, c_vp, c_i64, P_i64]),
     ("sk_precond_destroy", [c_vp]),
+    ("sk_chebyshev_apply_noalloc", [c_vp, c_dbl, c_dbl, c_i64, c_vp, c_vp, c_vp]),
     ("sk_cg_solve", [c_vp, c_vp, c_vp, c_vp, c_vp, ctypes.POINTER(CgConfig), ctypes.POINTER(Summary),
                      c_vp, c_vp]),
     ("sk_bicgstab_solve", [c_vp, c_vp, c_vp, c_vp, c_vp, ctypes.POINTER(BicgstabConfig),

@@ -209,6 +209,18 @@ class chebyshev_preconditioner(_Precond):
         self.lambda_min, self.lambda_max, self.degree = lambda_min, lambda_max, degree
 
 
+def chebyshev_apply_noalloc(Ad, lambda_min, lambda_max, degree, r, z, stream=None):
+    """z = p(A) r like chebyshev_preconditioner(Ad, ...).apply(r, z), for
+    callers that cannot allocate device memory at apply time: no handle is
+    created and the work vectors live in the library's static device array
+    (square CSR, at most 1,048,576 rows, degree <= 64; overlapping calls on
+    the GPU race; the first call on a device should precede any stream
+    capture)."""
+    st = stream if stream is not None else _stream_of(r)
+    check(lib().sk_chebyshev_apply_noalloc(Ad.handle, float(lambda_min), float(lambda_max), int(degree),
+                                           _ptr(r), _ptr(z), st))
+
+
 @dataclass
 class CGConfig:
     """CGConfig<T> (conjugate_gradient.hpp:48-74)."""
