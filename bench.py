@@ -49,6 +49,8 @@ def parse():
     p.add_argument("--grid", type=int, default=128)
     p.add_argument("--no-sweep", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
+    p.add_argument("--profile-formats", action="store_true",
+                   help="run one product of every sweep format and precision (for ncu captures), no timing")
     return p.parse_args()
 
 
@@ -275,10 +277,41 @@ def cpu_baseline(A, x, bytes_one):
                       f"same int32-index byte model as the GPU figure", "ms_per_product": secs / reps * 1e3}
 
 
+def profile_formats(grid):
+    """One product per sweep format / precision, for an ncu capture that
+    selects the kernels by name (-k regex:spmv)."""
+    import torch
+
+    from sparkit_b200 import formats, gpu, matgen
+    torch.cuda.set_device(0)
+    A, x = build_workload(grid)
+    for dt in (np.float64, np.float32):
+        Adt = A.astype(dt)
+        xd = torch.from_numpy(x.astype(dt)).cuda()
+        yd = torch.empty_like(xd)
+        for M in (Adt, formats.to_ellpack(Adt), formats.to_jagged_diagonal(Adt)):
+            Ad = gpu.Device_matrix(M)
+            Ad.spmv(xd, yd)
+            torch.cuda.synchronize()
+            Ad.close()
+    B = matgen.vector_laplacian_3d_bsr(grid // 2, seed=1)
+    Bd = gpu.Device_matrix(B)
+    xb = torch.from_numpy(matgen.uniform_vector(B.shape()[0], seed=2)).cuda()
+    Bd.spmv(xb, torch.empty_like(xb))
+    Z = matgen.zipf_random(250_000, s=1.5, cap=2048, seed=0)
+    Zd = gpu.Device_matrix(Z)
+    xz = torch.from_numpy(matgen.uniform_vector(Z.shape()[0], seed=3)).cuda()
+    Zd.spmv(xz, torch.empty_like(xz))
+    torch.cuda.synchronize()
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
+    if args.profile_formats:
+        return profile_formats(args.grid)
     import torch
     world, rank, local = dist_setup()
     if world > 1:

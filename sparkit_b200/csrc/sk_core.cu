@@ -62,7 +62,7 @@ __global__ void narrow_kernel(const long long* __restrict__ in, int* __restrict_
 template <typename T>
 __global__ void ell_transpose_kernel(const long long* __restrict__ col_rm,
                                      const T* __restrict__ val_rm, i64 g0, i64 count,
-                                     i64 nrow, i64 width, long long ncol,
+                                     i64 ld, i64 width, long long ncol,
                                      int* __restrict__ col_sm, T* __restrict__ val_sm,
                                      int* __restrict__ rowlen, unsigned long long* bad) {
   i64 t = blockIdx.x * static_cast<i64>(blockDim.x) + threadIdx.x;
@@ -71,7 +71,7 @@ __global__ void ell_transpose_kernel(const long long* __restrict__ col_rm,
     i64 g = g0 + t;
     i64 i = g / width, k = g - i * width;
     long long c = col_rm[t];
-    size_t dst = static_cast<size_t>(k) * static_cast<size_t>(nrow) + static_cast<size_t>(i);
+    size_t dst = static_cast<size_t>(k) * static_cast<size_t>(ld) + static_cast<size_t>(i);
     if (c == -1) {
       atomicMin(rowlen + i, static_cast<int>(k));
       col_sm[dst] = 0;
@@ -81,6 +81,25 @@ __global__ void ell_transpose_kernel(const long long* __restrict__ col_rm,
       col_sm[dst] = (c >= 0 && c < ncol) ? static_cast<int>(c) : 0;
       val_sm[dst] = val_rm[t];
     }
+  }
+}
+
+// Scatters CSR rows into the SELL-32 copy: entry k of row i goes to
+// off[i / 32] + 32 k + i % 32; padding stays zero (column 0, value 0, never
+// read because len[i] bounds every row).
+template <typename T>
+__global__ void csr_to_sell_kernel(i64 nrow, const int* __restrict__ rp, const int* __restrict__ ci,
+                                   const T* __restrict__ va, const int* __restrict__ off,
+                                   int* __restrict__ scol, T* __restrict__ sval,
+                                   unsigned char* __restrict__ len) {
+  i64 i = blockIdx.x * static_cast<i64>(blockDim.x) + threadIdx.x;
+  if (i >= nrow) return;
+  const int a = rp[i], b = rp[i + 1];
+  len[i] = static_cast<unsigned char>(b - a);
+  const i64 base = off[i >> 5] + (i & 31);
+  for (int k = 0; k < b - a; ++k) {
+    scol[base + 32 * k] = ci[a + k];
+    sval[base + 32 * k] = va[a + k];
   }
 }
 
@@ -249,6 +268,50 @@ struct HandleGuard {
   }
 };
 
+// Adds the SELL-32 copy of a CSR handle when every row has at most
+// kSellMaxRow entries and the padding stays within a quarter of nnz.
+static sk_status build_sell(sk_matrix A, const int64_t* rp, cudaStream_t st_) {
+  const i64 n = A->nrow;
+  if (n == 0 || A->nnz == 0) return SK_OK;
+  const i64 nslices = (n + 31) / 32;
+  std::vector<int> off(static_cast<size_t>(nslices) + 1, 0);
+  i64 total = 0;
+  for (i64 s = 0; s < nslices; ++s) {
+    i64 w = 0;
+    for (i64 i = 32 * s; i < std::min(n, 32 * s + 32); ++i) w = std::max<i64>(w, rp[i + 1] - rp[i]);
+    if (w > kSellMaxRow) return SK_OK;
+    off[static_cast<size_t>(s)] = static_cast<int>(total);
+    total += 32 * w;
+    if (total > (i64(1) << 31) - 64) return SK_OK;
+  }
+  off[static_cast<size_t>(nslices)] = static_cast<int>(total);
+  if (total > A->nnz + A->nnz / 4 + 64) return SK_OK;
+  const size_t V = vbytes(A->dtype);
+  void *col = nullptr, *val = nullptr, *len = nullptr;
+  sk_status st;
+  if ((st = dev_alloc(A, &col, (total + 64) * 4)) != SK_OK) return st;
+  if ((st = dev_alloc(A, &val, (total + 64) * V)) != SK_OK) return st;
+  if ((st = dev_alloc(A, &len, n + 64)) != SK_OK) return st;
+  SK_CUDA(cudaMemsetAsync(col, 0, (total + 64) * 4, st_));
+  SK_CUDA(cudaMemsetAsync(val, 0, (total + 64) * V, st_));
+  if ((st = upload_vector(A, off, &A->csr.sell_off, st_)) != SK_OK) return st;
+  A->csr.sell_col = static_cast<int*>(col);
+  A->csr.sell_vals = val;
+  A->csr.sell_len = static_cast<unsigned char*>(len);
+  A->csr.sell_entries = total;
+  if (A->dtype == SK_F64)
+    SK_LAUNCH(csr_to_sell_kernel<double>, ceil_div(n, kThreads), kThreads, 0, st_, n, A->csr.row_ptr,
+              A->csr.col_ind, static_cast<const double*>(A->csr.vals), A->csr.sell_off, A->csr.sell_col,
+              static_cast<double*>(val), A->csr.sell_len);
+  else
+    SK_LAUNCH(csr_to_sell_kernel<float>, ceil_div(n, kThreads), kThreads, 0, st_, n, A->csr.row_ptr,
+              A->csr.col_ind, static_cast<const float*>(A->csr.vals), A->csr.sell_off, A->csr.sell_col,
+              static_cast<float*>(val), A->csr.sell_len);
+  SK_CUDA(cudaGetLastError());
+  A->csr.sell = true;
+  return SK_OK;
+}
+
 }  // namespace sk
 
 using namespace sk;
@@ -345,8 +408,12 @@ sk_status sk_csr_create(sk_matrix* out, int64_t nrow, int64_t ncol, const int64_
   std::vector<unsigned char> lanes;
   csr_partition(row_ptr, nrow, part, lanes);
   A->csr.nparts = static_cast<int>(part.size()) - 1;
-  if ((st = upload_vector(A, part, &A->csr.part, st_)) != SK_OK) return st;
+  std::vector<int2> tiles(part.size());
+  for (size_t b = 0; b < part.size(); ++b)
+    tiles[b] = make_int2(part[b], static_cast<int>(row_ptr[part[b]]));
+  if ((st = upload_vector(A, tiles, &A->csr.tiles, st_)) != SK_OK) return st;
   if ((st = upload_vector(A, lanes, &A->csr.lanes, st_)) != SK_OK) return st;
+  if ((st = build_sell(A, row_ptr, st_)) != SK_OK) return st;
   SK_CUDA(cudaStreamSynchronize(st_));
   guard.ok = true;
   return SK_OK;
@@ -364,9 +431,14 @@ sk_status sk_ell_create(sk_matrix* out, int64_t nrow, int64_t ncol, int64_t widt
   cudaStream_t st_ = A->stream;
   const size_t V = vbytes(dtype);
   A->ell.width = width;
+  // slot stride: nrow rounded up to 32 plus 96, so that the slot streams a
+  // warp reads together never sit a large power of two apart
+  const i64 ld = (nrow + 31) / 32 * 32 + 96;
+  A->ell.ld = ld;
+  const i64 stored = ld * width;
   void *col = nullptr, *va = nullptr, *rl = nullptr;
-  if ((st = dev_alloc(A, &col, (slots + 8) * 4)) != SK_OK) return st;
-  if ((st = dev_alloc(A, &va, (slots + 8) * V)) != SK_OK) return st;
+  if ((st = dev_alloc(A, &col, (stored + 8) * 4)) != SK_OK) return st;
+  if ((st = dev_alloc(A, &va, (stored + 8) * V)) != SK_OK) return st;
   if ((st = dev_alloc(A, &rl, (nrow + 8) * 4)) != SK_OK) return st;
   A->ell.col = static_cast<int*>(col);
   A->ell.vals = va;
@@ -387,13 +459,13 @@ sk_status sk_ell_create(sk_matrix* out, int64_t nrow, int64_t ncol, int64_t widt
       SK_CUDA(cudaMemcpyAsync(stage, col_ind + off, c * 8, cudaMemcpyHostToDevice, st_));
       SK_CUDA(cudaMemcpyAsync(vstage, static_cast<const char*>(values) + off * V, c * V,
                               cudaMemcpyHostToDevice, st_));
-      if (dtype == SK_F64)
+        if (dtype == SK_F64)
         SK_LAUNCH(ell_transpose_kernel<double>, grid_for(c), kThreads, 0, st_, stage,
-                  static_cast<const double*>(vstage), off, c, nrow, width, ncol, A->ell.col,
+                  static_cast<const double*>(vstage), off, c, ld, width, ncol, A->ell.col,
                   static_cast<double*>(va), A->ell.rowlen, bad);
       else
         SK_LAUNCH(ell_transpose_kernel<float>, grid_for(c), kThreads, 0, st_, stage,
-                  static_cast<const float*>(vstage), off, c, nrow, width, ncol, A->ell.col,
+                  static_cast<const float*>(vstage), off, c, ld, width, ncol, A->ell.col,
                   static_cast<float*>(va), A->ell.rowlen, bad);
     }
     unsigned long long nbad = 0;
@@ -555,6 +627,15 @@ sk_status sk_matrix_add_f32_values(sk_matrix A) {
     SK_LAUNCH(to_float_kernel<double>, grid_for(A->nnz), kThreads, 0, A->stream,
               static_cast<const double*>(A->csr.vals), static_cast<float*>(p), A->nnz);
   A->csr.vals32 = static_cast<float*>(p);
+  if (A->csr.sell) {
+    void* q = nullptr;
+    st = dev_alloc(A, &q, (A->csr.sell_entries + 64) * 4);
+    if (st != SK_OK) return st;
+    SK_CUDA(cudaMemsetAsync(q, 0, (A->csr.sell_entries + 64) * 4, A->stream));
+    SK_LAUNCH(to_float_kernel<double>, grid_for(A->csr.sell_entries), kThreads, 0, A->stream,
+              static_cast<const double*>(A->csr.sell_vals), static_cast<float*>(q), A->csr.sell_entries);
+    A->csr.sell_vals32 = static_cast<float*>(q);
+  }
   SK_CUDA(cudaStreamSynchronize(A->stream));
   return SK_OK;
 }

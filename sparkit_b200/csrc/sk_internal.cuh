@@ -22,6 +22,7 @@ constexpr int kTileNnz = 2048;   // CSR: stored entries staged per CTA
 constexpr int kRowsMax = 256;    // CSR: rows per CTA (one per thread)
 constexpr int kBsrTileVals = 4096;  // BSR: block values staged per CTA
 constexpr int kMaxRed = 4;       // fused reductions carried per kernel
+constexpr int kSellMaxRow = 64;  // CSR rows up to this length use SELL-32
 
 // ------------------------------------------------------------------
 // Status plumbing
@@ -62,19 +63,31 @@ struct Csr {
   int* col_ind = nullptr;
   void* vals = nullptr;
   float* vals32 = nullptr;  // optional FP32 copy of FP64 values
-  int* part = nullptr;
-  unsigned char* lanes = nullptr;  // per row block: 1 = one thread per row
+  int2* tiles = nullptr;  // nparts + 1 of {first row, first entry}
+  unsigned char* lanes = nullptr;  // per tile: 1 = one thread per row
   int nparts = 0;
+  // SELL-32 copy used by the product when every row is short: slice s holds
+  // rows 32s..32s+31, padded to the slice's longest row and stored slot by
+  // slot (entry k of row 32s+l at sell_off[s] + 32k + l), so that a warp
+  // reads each slot of its 32 rows as one contiguous segment.
+  bool sell = false;
+  int* sell_col = nullptr;
+  void* sell_vals = nullptr;
+  float* sell_vals32 = nullptr;
+  int* sell_off = nullptr;             // nslices + 1 entry offsets
+  unsigned char* sell_len = nullptr;   // entries per row
+  i64 sell_entries = 0;                // padded size
 };
 
 // ELLPACK: slot-major (column-major) copy of the reference's row-major
-// layout: entry k of row i at k * nrow + i; rowlen[i] = entries before the
+// layout: entry k of row i at k * ld + i; rowlen[i] = entries before the
 // first -1 sentinel.
 struct Ell {
   int* col = nullptr;
   void* vals = nullptr;
   int* rowlen = nullptr;
   i64 width = 0;
+  i64 ld = 0;  // slot stride (nrow rounded up, kept off powers of two)
 };
 
 // Jagged diagonal: the reference layout with int32 indices; plen[i] is the
@@ -133,6 +146,11 @@ struct sk_precond_s {
 };
 
 namespace sk {
+
+// The FP32 value copy in the layout the product kernel reads.
+inline const float* f32_values(const sk_matrix_s* A) {
+  return A->csr.sell ? A->csr.sell_vals32 : A->csr.vals32;
+}
 
 cudaStream_t pick_stream(sk_matrix A, sk_stream s);
 sk_status dev_alloc(sk_matrix A, void** p, size_t bytes);

@@ -121,27 +121,44 @@ struct EpiStore {
 };
 
 // ------------------------------------------------------------------
-// CSR: one CTA per row block (part[]), entries staged through shared
-// memory with 16-byte streaming loads; rows of a short-row block summed
-// sequentially by one thread each (bit-exact), longer rows by L lanes.
+// Asynchronous 16-byte global -> shared copies (cp.async, L2 only).
+// ------------------------------------------------------------------
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit_wait_all() {
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
+  asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+}
+
+// ------------------------------------------------------------------
+// CSR: one CTA per tile of rows (tiles[b] = {first row, first entry};
+// at most 256 rows and 2048 entries, or one longer row).  The tile's column
+// indices and values are copied into shared memory with cp.async as soon as
+// the CTA starts; then each row is summed by one thread in storage order
+// (bit-exact with the reference) -- the thread gathers x for its own row,
+// so for banded matrices a warp's gathers of the j-th neighbour are
+// coalesced -- or, in tiles holding a row longer than 32 entries, by L
+// lanes with strided partial sums and a shuffle tree.
 // ------------------------------------------------------------------
 template <typename T, class Epi>
 __global__ void __launch_bounds__(kThreads)
 csr_spmv_kernel(const int* __restrict__ rp, const int* __restrict__ ci,
                 const T* __restrict__ va, const T* __restrict__ x,
-                const int* __restrict__ part,
+                const int2* __restrict__ tiles,
                 const unsigned char* __restrict__ lanes, Epi epi, RedWs ws,
                 const Scalars* sc) {
   constexpr int NR = Epi::kNR;
-  __shared__ T prod[kTileNnz];
+  __shared__ __align__(16) int scol[kTileNnz + 8];
+  __shared__ __align__(16) T sval[kTileNnz + 8];
   __shared__ int srp[kRowsMax + 1];
   if (solve_done(sc)) return;
   const int tid = threadIdx.x;
-  const int r0 = part[blockIdx.x];
-  const int nr = part[blockIdx.x + 1] - r0;
-  for (int t = tid; t <= nr; t += kThreads) srp[t] = rp[r0 + t];
-  __syncthreads();
-  const int s = srp[0], e = srp[nr];
+  const int2 t0 = tiles[blockIdx.x];
+  const int2 t1 = tiles[blockIdx.x + 1];
+  const int r0 = t0.x, nr = t1.x - t0.x;
+  const int s = t0.y, e = t1.y;
   double red[NR > 0 ? NR : 1];
 #pragma unroll
   for (int j = 0; j < (NR > 0 ? NR : 1); ++j) red[j] = 0.0;
@@ -159,28 +176,39 @@ csr_spmv_kernel(const int* __restrict__ rp, const int* __restrict__ ci,
     const int as = s & ~3;
     const int ngroups = (((e + 3) & ~3) - as) >> 2;
     for (int g = tid; g < ngroups; g += kThreads) {
-      const int k0 = as + 4 * g;
-      int c[4];
-      T v[4];
-      load4_stream(ci + k0, c);
-      load4_stream(va + k0, v);
-#pragma unroll
-      for (int j = 0; j < 4; ++j) {
-        const int k = k0 + j;
-        if (k >= s && k < e) prod[k - s] = mul(v[j], __ldg(x + c[j]));
+      cp_async16(scol + 4 * g, ci + as + 4 * g);
+      if constexpr (sizeof(T) == 8) {
+        cp_async16(sval + 4 * g, va + as + 4 * g);
+        cp_async16(sval + 4 * g + 2, va + as + 4 * g + 2);
+      } else {
+        cp_async16(sval + 4 * g, va + as + 4 * g);
       }
     }
+    for (int t = tid; t <= nr; t += kThreads) srp[t] = __ldg(rp + r0 + t) - as;
+    cp_async_commit_wait_all();
     __syncthreads();
     const int L = lanes[blockIdx.x];
     if (L == 1) {
       if (tid < nr) {
+        const int a = srp[tid], b = srp[tid + 1];
         T sum = T(0);
-        const int a = srp[tid] - s, b = srp[tid + 1] - s;
-        for (int k = a; k < b; ++k) sum = add(sum, prod[k]);
+        for (int k = a; k < b; k += 8) {
+          T xv[8], vv[8];
+#pragma unroll
+          for (int j = 0; j < 8; ++j) {
+            if (k + j < b) {
+              xv[j] = __ldg(x + scol[k + j]);
+              vv[j] = sval[k + j];
+            }
+          }
+#pragma unroll
+          for (int j = 0; j < 8; ++j)
+            if (k + j < b) sum = add(sum, mul(vv[j], xv[j]));
+        }
         epi(r0 + tid, sum, red);
       }
     } else {
-      // L lanes per row (a power of two chosen at upload from the block's
+      // L lanes per row (a power of two chosen at upload from the tile's
       // longest row), strided partial sums then a shuffle tree.
       const int rows_per_pass = kThreads / L;
       const int npass = (nr + rows_per_pass - 1) / rows_per_pass;
@@ -189,8 +217,20 @@ csr_spmv_kernel(const int* __restrict__ rp, const int* __restrict__ ci,
         const int row = pass * rows_per_pass + tid / L;
         T sum = T(0);
         if (row < nr) {
-          const int a = srp[row] - s, b = srp[row + 1] - s;
-          for (int k = a + lane; k < b; k += L) sum = add(sum, prod[k]);
+          const int a = srp[row], b = srp[row + 1];
+          for (int k = a + lane; k < b; k += 4 * L) {
+            T xv[4], vv[4];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+              if (k + j * L < b) {
+                xv[j] = __ldg(x + scol[k + j * L]);
+                vv[j] = sval[k + j * L];
+              }
+            }
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+              if (k + j * L < b) sum = add(sum, mul(vv[j], xv[j]));
+          }
         }
         for (int off = L >> 1; off > 0; off >>= 1)
           sum = add(sum, __shfl_xor_sync(0xffffffffu, sum, off));
@@ -204,12 +244,58 @@ csr_spmv_kernel(const int* __restrict__ rp, const int* __restrict__ ci,
 }
 
 // ------------------------------------------------------------------
+// CSR through its SELL-32 copy: one warp per slice of 32 rows, one thread
+// per row.  Slot k of the 32 rows is one contiguous segment, so every load
+// of column indices and values is a full coalesced line, and a thread's
+// slots are independent loads issued together (8 at a time).  Each row is
+// summed in storage order from 0, exactly as sparse_blas.hpp:25-28.
+// ------------------------------------------------------------------
+template <typename T, class Epi>
+__global__ void __launch_bounds__(kThreads, 8)
+sell_spmv_kernel(int nrow, const int* __restrict__ off, const unsigned char* __restrict__ len,
+                 const int* __restrict__ col, const T* __restrict__ va, const T* __restrict__ x,
+                 Epi epi, RedWs ws, const Scalars* sc) {
+  constexpr int NR = Epi::kNR;
+  if (solve_done(sc)) return;
+  double red[NR > 0 ? NR : 1];
+#pragma unroll
+  for (int j = 0; j < (NR > 0 ? NR : 1); ++j) red[j] = 0.0;
+  const int i = blockIdx.x * kThreads + threadIdx.x;
+  if (i < nrow) {
+    const int n = len[i];
+    const int* cp = col + __ldg(off + (i >> 5)) + (i & 31);
+    const T* vp = va + (cp - col);
+    T sum = T(0);
+    int k = 0;
+    for (; k + 4 <= n; k += 4) {
+      int c[4];
+      T v[4];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        c[j] = __ldcs(cp + 32 * (k + j));
+        v[j] = __ldcs(vp + 32 * (k + j));
+      }
+      T p[4];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) p[j] = mul(v[j], __ldg(x + c[j]));
+#pragma unroll
+      for (int j = 0; j < 4; ++j) sum = add(sum, p[j]);
+    }
+    for (; k < n; ++k) sum = add(sum, mul(__ldcs(vp + 32 * k), __ldg(x + __ldcs(cp + 32 * k))));
+    epi(i, sum, red);
+  }
+  if constexpr (NR > 0) {
+    grid_reduce<NR>(red, ws, [&](const double* t) { epi.finalize(t); });
+  }
+}
+
+// ------------------------------------------------------------------
 // ELLPACK (slot-major): one thread per row, sequential over its slots,
 // stopping at the row's length (the reference stops at the first -1).
 // ------------------------------------------------------------------
 template <typename T, class Epi>
-__global__ void __launch_bounds__(kThreads)
-ell_spmv_kernel(int nrow, const int* __restrict__ col, const T* __restrict__ va,
+__global__ void __launch_bounds__(kThreads, 8)
+ell_spmv_kernel(int nrow, long long ld, const int* __restrict__ col, const T* __restrict__ va,
                 const int* __restrict__ rowlen, const T* __restrict__ x,
                 Epi epi, RedWs ws, const Scalars* sc) {
   constexpr int NR = Epi::kNR;
@@ -220,8 +306,8 @@ ell_spmv_kernel(int nrow, const int* __restrict__ col, const T* __restrict__ va,
   const int i = blockIdx.x * kThreads + threadIdx.x;
   if (i < nrow) {
     const int len = rowlen[i];
-    const size_t stride = static_cast<size_t>(nrow);
-    size_t idx = static_cast<size_t>(i);
+    const int* cp = col + i;
+    const T* vp = va + i;
     T sum = T(0);
     int k = 0;
     for (; k + 4 <= len; k += 4) {
@@ -229,19 +315,21 @@ ell_spmv_kernel(int nrow, const int* __restrict__ col, const T* __restrict__ va,
       T v[4];
 #pragma unroll
       for (int j = 0; j < 4; ++j) {
-        c[j] = __ldcs(col + idx + j * stride);
-        v[j] = __ldcs(va + idx + j * stride);
+        c[j] = __ldcs(cp + j * ld);
+        v[j] = __ldcs(vp + j * ld);
       }
       T p[4];
 #pragma unroll
       for (int j = 0; j < 4; ++j) p[j] = mul(v[j], __ldg(x + c[j]));
 #pragma unroll
       for (int j = 0; j < 4; ++j) sum = add(sum, p[j]);
-      idx += 4 * stride;
+      cp += 4 * ld;
+      vp += 4 * ld;
     }
     for (; k < len; ++k) {
-      sum = add(sum, mul(__ldcs(va + idx), __ldg(x + __ldcs(col + idx))));
-      idx += stride;
+      sum = add(sum, mul(__ldcs(vp), __ldg(x + __ldcs(cp))));
+      cp += ld;
+      vp += ld;
     }
     epi(i, sum, red);
   }
@@ -389,7 +477,7 @@ bsr_spmv_kernel(int nrow, int ncol, int br_rt, int bc_rt, int nbr_trunc,
 // Grid size of the SpMV launch for a handle (for sizing RedWs).
 inline int spmv_grid(const sk_matrix_s* A) {
   switch (A->format) {
-    case SK_CSR: return A->csr.nparts;
+    case SK_CSR: return A->csr.sell ? ceil_div(A->nrow, kThreads) : A->csr.nparts;
     case SK_BSR: return A->bsr.nparts;
     default: return ceil_div(A->nrow, kThreads);
   }
@@ -404,15 +492,23 @@ void launch_spmv(const sk_matrix_s* A, const T* x, Epi const& epi, RedWs ws,
   if (A->nrow == 0) return;
   switch (A->format) {
     case SK_CSR: {
+      if (A->csr.sell) {
+        const T* v = vals_override ? vals_override : static_cast<const T*>(A->csr.sell_vals);
+        SK_LAUNCH((sell_spmv_kernel<T, Epi>), ceil_div(A->nrow, kThreads), kThreads, 0, st,
+                  static_cast<int>(A->nrow), A->csr.sell_off, A->csr.sell_len, A->csr.sell_col, v, x,
+                  epi, ws, sc);
+        break;
+      }
       const T* v = vals_override ? vals_override : static_cast<const T*>(A->csr.vals);
       SK_LAUNCH((csr_spmv_kernel<T, Epi>), A->csr.nparts, kThreads, 0, st,
-                A->csr.row_ptr, A->csr.col_ind, v, x, A->csr.part, A->csr.lanes, epi,
+                A->csr.row_ptr, A->csr.col_ind, v, x, A->csr.tiles, A->csr.lanes, epi,
                 ws, sc);
       break;
     }
     case SK_ELL:
       SK_LAUNCH((ell_spmv_kernel<T, Epi>), ceil_div(A->nrow, kThreads), kThreads, 0, st,
-                static_cast<int>(A->nrow), A->ell.col, static_cast<const T*>(A->ell.vals),
+                static_cast<int>(A->nrow), static_cast<long long>(A->ell.ld), A->ell.col,
+                static_cast<const T*>(A->ell.vals),
                 A->ell.rowlen, x, epi, ws, sc);
       break;
     case SK_JAD:

@@ -123,9 +123,9 @@ sk_status sk_spmv_f32(sk_matrix A, const float* x_dev, float* y_dev, sk_stream s
   SK_CHECK(A, SK_INVALID_ARG, "null handle");
   cudaStream_t st = pick_stream(A, s);
   if (A->dtype == SK_F32) return sk_spmv(A, x_dev, y_dev, s);
-  SK_CHECK(A->format == SK_CSR && A->csr.vals32, SK_INVALID_ARG,
+  SK_CHECK(A->format == SK_CSR && f32_values(A), SK_INVALID_ARG,
            "no FP32 value copy: call sk_matrix_add_f32_values first");
-  launch_spmv<float>(A, x_dev, EpiStore<float>{y_dev}, RedWs{}, nullptr, st, A->csr.vals32);
+  launch_spmv<float>(A, x_dev, EpiStore<float>{y_dev}, RedWs{}, nullptr, st, f32_values(A));
   SK_CUDA(cudaGetLastError());
   return SK_OK;
 }
