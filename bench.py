@@ -49,6 +49,9 @@ def parse():
     p.add_argument("--grid", type=int, default=128)
     p.add_argument("--no-sweep", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
+    p.add_argument("--no-solvers", action="store_true")
+    p.add_argument("--profile-solvers", action="store_true",
+                   help="run 20 FP64 and 20 FP32 CG iterations on the GRF diffusion matrix (for ncu launch lists)")
     p.add_argument("--profile-formats", action="store_true",
                    help="run one product of every sweep format and precision (for ncu captures), no timing")
     return p.parse_args()
@@ -251,6 +254,93 @@ def sweep(stream, grid):
     return out
 
 
+def solver_runs(grid3):
+    """Time-to-solution of the solver configurations (wall time of the
+    solve call, inputs resident on the device, one warm-up solve first).
+
+    c1: Jacobi-CG, 256^2 Dirichlet 5-point Laplacian, b = A x*, x* ~ U[-1,1]
+        seed 0, to 1e-10 -- GPU FP64 vs the reference on one host core.
+    c3: 3-D 7-point diffusion, GRF coefficients exp(g) (sigma 2, correlation
+        8 cells) on grid3^3, b ~ U[-1,1] seed 0, to a 1e-10 relative residual
+        -- plain FP64 Jacobi-CG vs FP32-inner (1e-5) / FP64-refinement."""
+    import torch
+
+    from sparkit_b200 import gpu, matgen
+    out = {}
+    # ---- c1
+    A = matgen.laplacian_2d_dirichlet(256)
+    n = A.shape()[0]
+    Ad = gpu.Device_matrix(A)
+    xs = matgen.uniform_vector(n, seed=0)
+    b = gpu.multiply(Ad, xs)
+    bd = torch.from_numpy(b).cuda()
+    J = gpu.jacobi(Ad)
+    cfg = gpu.CGConfig(1e-10, 100000, 100000)
+    for rep in range(2):
+        xd = torch.zeros_like(bd)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        s1 = gpu.conjugate_gradient(bd, xd, cfg, gpu.spmv(Ad), J)
+        torch.cuda.synchronize()
+        t_gpu = time.perf_counter() - t0
+    r = b - gpu.multiply(Ad, xd.cpu().numpy())
+    c1 = {"gpu_ms": t_gpu * 1e3, "iterations": s1.computed_iterations, "converged": s1.converged,
+          "true_rel_residual": float(np.linalg.norm(r) / np.linalg.norm(b))}
+    try:
+        from oracle.binding import Reference, reference_available
+        if reference_available():
+            R = Reference()
+            t0 = time.perf_counter()
+            _, sr = R.cg(A, b, np.zeros(n), 1e-10, 100000, 100000, left="jacobi")
+            c1["cpu_reference_ms"] = (time.perf_counter() - t0) * 1e3
+            c1["cpu_reference_iterations"] = sr["computed_iterations"]
+            c1["cpu_cores"] = 1
+    except Exception as e:  # the CPU leg is informational
+        c1["cpu_reference_error"] = str(e)[:200]
+    out["c1_jacobi_cg_256sq"] = c1
+    Ad.close()
+    # ---- c3
+    G = matgen.diffusion_3d_grf(grid3, sigma=2.0, corr_len=8.0, seed=0)
+    n = G.shape()[0]
+    Gd = gpu.Device_matrix(G)
+    Gd.add_f32_values()
+    b = matgen.uniform_vector(n, seed=0)
+    bd = torch.from_numpy(b).cuda()
+    JG = gpu.jacobi(Gd)
+    res = {}
+    reps_p, reps_m = [], []
+    for rep in range(3):
+        xd = torch.zeros_like(bd)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        sp = gpu.conjugate_gradient(bd, xd, gpu.CGConfig(1e-10, 10 ** 6, 200000), gpu.spmv(Gd), JG)
+        torch.cuda.synchronize()
+        tp = time.perf_counter() - t0
+        reps_p.append(tp * 1e3)
+    tp = min(reps_p[1:]) / 1e3
+    rp = float(np.linalg.norm(b - gpu.multiply(Gd, xd.cpu().numpy())) / np.linalg.norm(b))
+    res["plain_fp64"] = {"ms": tp * 1e3, "iterations": sp.computed_iterations, "converged": sp.converged,
+                         "true_rel_residual": rp}
+    for rep in range(3):
+        xd = torch.zeros_like(bd)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        sm = gpu.mixed_cg(bd, xd, gpu.Mixed_config(1e-10, 1e-5, 100, 200000), gpu.spmv(Gd))
+        torch.cuda.synchronize()
+        tm = time.perf_counter() - t0
+        reps_m.append(tm * 1e3)
+    tm = min(reps_m[1:]) / 1e3
+    rm = float(np.linalg.norm(b - gpu.multiply(Gd, xd.cpu().numpy())) / np.linalg.norm(b))
+    res["mixed_fp32_fp64"] = {"ms": tm * 1e3, "outer": sm.outer_iterations, "inner_iterations": sm.inner_iterations,
+                              "converged": sm.converged, "true_rel_residual": rm}
+    res["speedup_mixed_vs_plain"] = tp / tm
+    res["reps_ms"] = {"plain_fp64": reps_p, "mixed": reps_m, "reported": "best of the repetitions after the first"}
+    res["n"] = n
+    res["nnz"] = G.size()
+    out[f"c3_grf_diffusion_{grid3}cubed"] = res
+    return out
+
+
 def cpu_baseline(A, x, bytes_one):
     """The reference's own multiply (oracle/_ref) on one host core, over a
     bounded number of full products; falls back to the C oracle port."""
@@ -306,12 +396,33 @@ def profile_formats(grid):
     return 0
 
 
+def profile_solvers(grid):
+    """A short plain FP64 Jacobi-CG (20 iterations) and a short mixed solve
+    (one outer step of 20 FP32 iterations) for per-kernel launch lists."""
+    import torch
+
+    from sparkit_b200 import gpu, matgen
+    torch.cuda.set_device(0)
+    G = matgen.diffusion_3d_grf(grid, sigma=2.0, corr_len=8.0, seed=0)
+    Gd = gpu.Device_matrix(G)
+    Gd.add_f32_values()
+    bd = torch.from_numpy(matgen.uniform_vector(G.shape()[0], seed=0)).cuda()
+    xd = torch.zeros_like(bd)
+    gpu.conjugate_gradient(bd, xd, gpu.CGConfig(1e-10, 10 ** 6, 20), gpu.spmv(Gd), gpu.jacobi(Gd))
+    xd.zero_()
+    gpu.mixed_cg(bd, xd, gpu.Mixed_config(1e-10, 1e-5, 1, 20), gpu.spmv(Gd))
+    torch.cuda.synchronize()
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
     if args.profile_formats:
         return profile_formats(args.grid)
+    if args.profile_solvers:
+        return profile_solvers(args.grid)
     import torch
     world, rank, local = dist_setup()
     if world > 1:
@@ -406,6 +517,8 @@ def main():
     if rank == 0 and world == 1 and not args.no_sweep:
         Ad.close()
         extra["sweep"] = sweep(stream, args.grid)
+    if rank == 0 and world == 1 and not args.no_solvers:
+        extra["solvers"] = solver_runs(args.grid)
 
     if rank == 0:
         line = {

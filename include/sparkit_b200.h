@@ -269,6 +269,44 @@ SK_API sk_status sk_fgmres_solve(sk_matrix A, sk_precond M, const void* b_dev,
                           void* x_dev, const sk_fgmres_config* cfg,
                           sk_summary* out, double* history_host, sk_stream s);
 
+/* Mixed precision (no reference counterpart; the reference solves in one
+ * value type): FP64 iterative refinement around conjugate_gradient
+ * (conjugate_gradient.hpp:347) instantiated for float.  Each outer step
+ * forms r = b - A x in FP64, stops when ||r|| / ||b|| < tolerance, solves
+ * A d = r / ||r|| in FP32 with (Jacobi-preconditioned when jacobi != 0) CG
+ * to inner_tolerance on the FP32 copy of the values, and adds ||r|| d to x
+ * in FP64.  A is an FP64 CSR handle; b and x are FP64 device vectors. */
+typedef struct {
+  double tolerance;        /* outer, on the true FP64 residual */
+  double inner_tolerance;  /* FP32 CG relative tolerance */
+  int64_t max_outer;
+  int64_t max_inner;
+  int32_t collect_residuals;  /* true residual norm per outer step */
+  int32_t adaptive_last_step; /* tighten the inner tolerance of a step to
+                                 half the remaining factor tol ||b|| / ||r||
+                                 when that is below inner_tolerance */
+  int32_t l2_window;          /* keep the FP32 inner vectors resident in L2
+                                 (a persisting access-policy window on the
+                                 handle's stream, this process only) */
+} sk_mixed_config;
+
+typedef struct {
+  double residual_norm;      /* true FP64 ||b - A x|| at exit */
+  int64_t outer_iterations;
+  int64_t inner_iterations;  /* FP32 CG iterations summed */
+  int32_t converged;
+  int32_t status;
+  double setup_ms;           /* host wall time: FP32 copies, Jacobi, ||b|| */
+  double inner_ms;           /* host wall time in the FP32 inner solves */
+  double outer_ms;           /* host wall time in the FP64 residual / update */
+} sk_mixed_summary;
+
+SK_API sk_status sk_mixed_cg_solve(sk_matrix A, int32_t jacobi,
+                                   const double* b_dev, double* x_dev,
+                                   const sk_mixed_config* cfg,
+                                   sk_mixed_summary* out, double* history_host,
+                                   sk_stream s);
+
 /* Host-buffer forms of the three solvers (b and x in host memory, copied
  * in and out inside the call): the drop-in boundary of the C++ overloads. */
 SK_API sk_status sk_cg_solve_host(sk_matrix A, sk_precond left, sk_precond right,

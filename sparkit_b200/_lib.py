@@ -49,6 +49,18 @@ class FgmresConfig(ctypes.Structure):
                 ("max_iterations", c_i64), ("collect_residuals", c_i32)]
 
 
+class MixedConfig(ctypes.Structure):
+    _fields_ = [("tolerance", c_dbl), ("inner_tolerance", c_dbl), ("max_outer", c_i64),
+                ("max_inner", c_i64), ("collect_residuals", c_i32), ("adaptive_last_step", c_i32),
+                ("l2_window", c_i32)]
+
+
+class MixedSummary(ctypes.Structure):
+    _fields_ = [("residual_norm", c_dbl), ("outer_iterations", c_i64), ("inner_iterations", c_i64),
+                ("converged", c_i32), ("status", c_i32), ("setup_ms", c_dbl), ("inner_ms", c_dbl),
+                ("outer_ms", c_dbl)]
+
+
 class Summary(ctypes.Structure):
     _fields_ = [("residual_norm", c_dbl), ("computed_iterations", c_i64),
                 ("converged", c_i32), ("status", c_i32), ("history_length", c_i64)]
@@ -91,6 +103,8 @@ SIGNATURES = [
                            ctypes.POINTER(Summary), c_vp, c_vp]),
     ("sk_fgmres_solve", [c_vp, c_vp, c_vp, c_vp, ctypes.POINTER(FgmresConfig), ctypes.POINTER(Summary),
                          c_vp, c_vp]),
+    ("sk_mixed_cg_solve", [c_vp, c_i32, c_vp, c_vp, ctypes.POINTER(MixedConfig), ctypes.POINTER(MixedSummary),
+                           c_vp, c_vp]),
     ("sk_cg_solve_host", [c_vp, c_vp, c_vp, c_vp, c_vp, ctypes.POINTER(CgConfig), ctypes.POINTER(Summary),
                           c_vp]),
     ("sk_bicgstab_solve_host", [c_vp, c_vp, c_vp, c_vp, c_vp, ctypes.POINTER(BicgstabConfig),

@@ -103,6 +103,25 @@ __global__ void csr_to_sell_kernel(i64 nrow, const int* __restrict__ rp, const i
   }
 }
 
+// Scatters BSR block rows into the sliced copy (layout in sk_internal.cuh).
+template <typename T>
+__global__ void bsr_to_sell_kernel(i64 nbr, int bsz, const int* __restrict__ rp, const int* __restrict__ bc,
+                                   const T* __restrict__ va, const int* __restrict__ off,
+                                   int* __restrict__ scol, T* __restrict__ sval,
+                                   unsigned char* __restrict__ len) {
+  i64 I = blockIdx.x * static_cast<i64>(blockDim.x) + threadIdx.x;
+  if (I >= nbr) return;
+  const int a = rp[I], b = rp[I + 1];
+  len[I] = static_cast<unsigned char>(b - a);
+  const i64 o = off[I >> 5];
+  const i64 l = I & 31;
+  for (int k = 0; k < b - a; ++k) {
+    scol[o + 32 * k + l] = bc[a + k];
+    for (int e = 0; e < bsz; ++e)
+      sval[(o + 32 * k) * bsz + 32 * e + l] = va[static_cast<i64>(a + k) * bsz + e];
+  }
+}
+
 __global__ void fill_int_kernel(int* p, i64 n, int v) {
   i64 i = blockIdx.x * static_cast<i64>(blockDim.x) + threadIdx.x;
   i64 stride = static_cast<i64>(gridDim.x) * blockDim.x;
@@ -238,6 +257,8 @@ static sk_status new_handle(sk_matrix* out, sk_format f, sk_dtype dt, i64 nrow, 
   A->nrow = nrow;
   A->ncol = ncol;
   cudaGetDevice(&A->device);
+  cudaDeviceGetAttribute(&A->sm_count, cudaDevAttrMultiProcessorCount, A->device);
+  if (A->sm_count <= 0) A->sm_count = 148;
   e = cudaStreamCreateWithFlags(&A->stream, cudaStreamNonBlocking);
   if (e != cudaSuccess) {
     delete A;
@@ -253,6 +274,7 @@ static void destroy_handle(sk_matrix A) {
   for (void* p : A->allocations) cudaFree(p);
   if (A->io) cudaFree(A->io);
   if (A->ws) cudaFree(A->ws);
+  if (A->ws2) cudaFree(A->ws2);
   if (A->stream) cudaStreamDestroy(A->stream);
   delete A;
 }
@@ -309,6 +331,53 @@ static sk_status build_sell(sk_matrix A, const int64_t* rp, cudaStream_t st_) {
               static_cast<float*>(val), A->csr.sell_len);
   SK_CUDA(cudaGetLastError());
   A->csr.sell = true;
+  return SK_OK;
+}
+
+// Adds the sliced copy of a 2x2 or 3x3 BSR handle when every block row has
+// at most kSellMaxRow blocks and the padding stays within a quarter.
+static sk_status build_bsr_sell(sk_matrix A, const int64_t* rp, cudaStream_t st_) {
+  auto& B = A->bsr;
+  if (!((B.br == 3 && B.bc == 3) || (B.br == 2 && B.bc == 2))) return SK_OK;
+  const i64 nbr = B.nbr;
+  if (nbr == 0 || B.nblocks == 0) return SK_OK;
+  const i64 nslices = (nbr + 31) / 32;
+  std::vector<int> off(static_cast<size_t>(nslices) + 1, 0);
+  i64 total = 0;
+  const i64 bsz = B.br * B.bc;
+  for (i64 s = 0; s < nslices; ++s) {
+    i64 w = 0;
+    for (i64 I = 32 * s; I < std::min(nbr, 32 * s + 32); ++I) w = std::max<i64>(w, rp[I + 1] - rp[I]);
+    if (w > kSellMaxRow) return SK_OK;
+    off[static_cast<size_t>(s)] = static_cast<int>(total);
+    total += 32 * w;
+    if (total * bsz > (i64(1) << 31) - 64) return SK_OK;
+  }
+  off[static_cast<size_t>(nslices)] = static_cast<int>(total);
+  if (total > B.nblocks + B.nblocks / 4 + 64) return SK_OK;
+  const size_t V = vbytes(A->dtype);
+  void *col = nullptr, *val = nullptr, *len = nullptr;
+  sk_status st;
+  if ((st = dev_alloc(A, &col, (total + 64) * 4)) != SK_OK) return st;
+  if ((st = dev_alloc(A, &val, (total * bsz + 64) * V)) != SK_OK) return st;
+  if ((st = dev_alloc(A, &len, nbr + 64)) != SK_OK) return st;
+  SK_CUDA(cudaMemsetAsync(col, 0, (total + 64) * 4, st_));
+  SK_CUDA(cudaMemsetAsync(val, 0, (total * bsz + 64) * V, st_));
+  if ((st = upload_vector(A, off, &B.sell_off, st_)) != SK_OK) return st;
+  B.sell_col = static_cast<int*>(col);
+  B.sell_vals = val;
+  B.sell_len = static_cast<unsigned char*>(len);
+  B.sell_blocks = total;
+  if (A->dtype == SK_F64)
+    SK_LAUNCH(bsr_to_sell_kernel<double>, ceil_div(nbr, kThreads), kThreads, 0, st_, nbr, static_cast<int>(bsz),
+              B.row_ptr, B.col, static_cast<const double*>(B.vals), B.sell_off, B.sell_col,
+              static_cast<double*>(val), B.sell_len);
+  else
+    SK_LAUNCH(bsr_to_sell_kernel<float>, ceil_div(nbr, kThreads), kThreads, 0, st_, nbr, static_cast<int>(bsz),
+              B.row_ptr, B.col, static_cast<const float*>(B.vals), B.sell_off, B.sell_col,
+              static_cast<float*>(val), B.sell_len);
+  SK_CUDA(cudaGetLastError());
+  B.sell = true;
   return SK_OK;
 }
 
@@ -589,6 +658,7 @@ sk_status sk_bsr_create(sk_matrix* out, int64_t nrow, int64_t ncol, int64_t bloc
   bsr_partition(row_ptr, nbr, block_rows, bsz, part);
   b.nparts = static_cast<int>(part.size()) - 1;
   if ((st = upload_vector(A, part, &b.part, st_)) != SK_OK) return st;
+  if ((st = build_bsr_sell(A, row_ptr, st_)) != SK_OK) return st;
   SK_CUDA(cudaStreamSynchronize(st_));
   guard.ok = true;
   return SK_OK;

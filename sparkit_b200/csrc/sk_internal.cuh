@@ -109,6 +109,16 @@ struct Bsr {
   int* part = nullptr;
   int nparts = 0;
   i64 br = 0, bc = 0, nbr = 0, nbr_mult = 0, nblocks = 0;
+  // Sliced copy for 2x2 and 3x3 blocks with at most kSellMaxRow blocks per
+  // block row: slice s holds block rows 32s..32s+31 padded to the slice's
+  // longest; block k of block row 32s+l has its column at sell_off[s] +
+  // 32k + l and its element e at (sell_off[s] + 32k) * br * bc + 32e + l.
+  bool sell = false;
+  int* sell_col = nullptr;
+  void* sell_vals = nullptr;
+  int* sell_off = nullptr;
+  unsigned char* sell_len = nullptr;
+  i64 sell_blocks = 0;
 };
 
 }  // namespace sk
@@ -117,6 +127,7 @@ struct sk_matrix_s {
   sk_format format;
   sk_dtype dtype;
   int device = 0;
+  int sm_count = 148;
   sk::i64 nrow = 0, ncol = 0, nnz = 0;
   sk::Csr csr;
   sk::Ell ell;
@@ -129,6 +140,9 @@ struct sk_matrix_s {
   // Grow-only workspace of the solver calls on this handle.
   void* ws = nullptr;
   size_t ws_bytes = 0;
+  void* ws2 = nullptr;  // second workspace (outer loop of the mixed solver)
+  size_t ws2_bytes = 0;
+  bool mixed_jacobi_ready = false;  // FP32 inverse diagonal held in ws2
   sk::i64 spmv_bytes() const;
 };
 

@@ -93,7 +93,22 @@ __device__ __forceinline__ void grid_reduce(double (&v)[NR], RedWs ws, Fin const
   double t[NR];
 #pragma unroll
   for (int j = 0; j < NR; ++j) t[j] = 0.0;
-  for (unsigned b = threadIdx.x; b < gridDim.x; b += blockDim.x)
+  // 4 partials per thread in flight at a time: the loads are independent,
+  // only their (fixed-order) sum is sequential
+  unsigned b = threadIdx.x;
+  for (; b + 3 * blockDim.x < gridDim.x; b += 4 * blockDim.x) {
+    double q[4][NR];
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+#pragma unroll
+      for (int j = 0; j < NR; ++j)
+        q[u][j] = __ldcg(ws.partials + static_cast<size_t>(b + u * blockDim.x) * kMaxRed + j);
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+#pragma unroll
+      for (int j = 0; j < NR; ++j) t[j] += q[u][j];
+  }
+  for (; b < gridDim.x; b += blockDim.x)
 #pragma unroll
     for (int j = 0; j < NR; ++j) t[j] += __ldcg(ws.partials + static_cast<size_t>(b) * kMaxRed + j);
   block_reduce<NR>(t);
@@ -244,14 +259,63 @@ csr_spmv_kernel(const int* __restrict__ rp, const int* __restrict__ ci,
 }
 
 // ------------------------------------------------------------------
+// Sum over one row of v_k * x[c_k], k = 0..n-1, accumulated from 0 in
+// storage order (the reference's order, so the result is bit-exact);
+// fetch(k, c, v) loads entry k.  PRED: rounds of U entries whose loads are
+// all issued together (predicated); otherwise rounds of U plus a serial
+// tail, which needs fewer registers.  The measured best per value type is
+// chosen in launch_spmv.
+// ------------------------------------------------------------------
+template <typename T, int U, bool PRED, class Fetch>
+__device__ __forceinline__ T row_dot(int n, const T* __restrict__ x, Fetch const& fetch) {
+  T sum = T(0);
+  if constexpr (PRED) {
+    for (int k = 0; k < n; k += U) {
+      int c[U];
+      T v[U];
+#pragma unroll
+      for (int j = 0; j < U; ++j)
+        if (k + j < n) fetch(k + j, c[j], v[j]);
+      T xv[U];
+#pragma unroll
+      for (int j = 0; j < U; ++j)
+        if (k + j < n) xv[j] = __ldg(x + c[j]);
+#pragma unroll
+      for (int j = 0; j < U; ++j)
+        if (k + j < n) sum = add(sum, mul(v[j], xv[j]));
+    }
+  } else {
+    int k = 0;
+    for (; k + U <= n; k += U) {
+      int c[U];
+      T v[U];
+#pragma unroll
+      for (int j = 0; j < U; ++j) fetch(k + j, c[j], v[j]);
+      T p[U];
+#pragma unroll
+      for (int j = 0; j < U; ++j) p[j] = mul(v[j], __ldg(x + c[j]));
+#pragma unroll
+      for (int j = 0; j < U; ++j) sum = add(sum, p[j]);
+    }
+    for (; k < n; ++k) {
+      int c;
+      T v;
+      fetch(k, c, v);
+      sum = add(sum, mul(v, __ldg(x + c)));
+    }
+  }
+  return sum;
+}
+
+// ------------------------------------------------------------------
 // CSR through its SELL-32 copy: one warp per slice of 32 rows, one thread
 // per row.  Slot k of the 32 rows is one contiguous segment, so every load
 // of column indices and values is a full coalesced line, and a thread's
 // slots are independent loads issued together (8 at a time).  Each row is
 // summed in storage order from 0, exactly as sparse_blas.hpp:25-28.
 // ------------------------------------------------------------------
-template <typename T, class Epi>
-__global__ void __launch_bounds__(kThreads, 8)
+template <typename T, class Epi, int U, bool PRED, int MINB>
+__global__ void __launch_bounds__(kThreads, MINB)
 sell_spmv_kernel(int nrow, const int* __restrict__ off, const unsigned char* __restrict__ len,
                  const int* __restrict__ col, const T* __restrict__ va, const T* __restrict__ x,
                  Epi epi, RedWs ws, const Scalars* sc) {
@@ -260,28 +324,16 @@ sell_spmv_kernel(int nrow, const int* __restrict__ off, const unsigned char* __r
   double red[NR > 0 ? NR : 1];
 #pragma unroll
   for (int j = 0; j < (NR > 0 ? NR : 1); ++j) red[j] = 0.0;
-  const int i = blockIdx.x * kThreads + threadIdx.x;
-  if (i < nrow) {
+  // grid-stride over rows: a kernel that carries a reduction runs at most
+  // one wave of CTAs, so that few CTAs take part in the grid reduction
+  for (int i = blockIdx.x * kThreads + threadIdx.x; i < nrow; i += gridDim.x * kThreads) {
     const int n = len[i];
     const int* cp = col + __ldg(off + (i >> 5)) + (i & 31);
     const T* vp = va + (cp - col);
-    T sum = T(0);
-    int k = 0;
-    for (; k + 4 <= n; k += 4) {
-      int c[4];
-      T v[4];
-#pragma unroll
-      for (int j = 0; j < 4; ++j) {
-        c[j] = __ldcs(cp + 32 * (k + j));
-        v[j] = __ldcs(vp + 32 * (k + j));
-      }
-      T p[4];
-#pragma unroll
-      for (int j = 0; j < 4; ++j) p[j] = mul(v[j], __ldg(x + c[j]));
-#pragma unroll
-      for (int j = 0; j < 4; ++j) sum = add(sum, p[j]);
-    }
-    for (; k < n; ++k) sum = add(sum, mul(__ldcs(vp + 32 * k), __ldg(x + __ldcs(cp + 32 * k))));
+    const T sum = row_dot<T, U, PRED>(n, x, [&](int k, int& c, T& v) {
+      c = __ldcs(cp + 32 * k);
+      v = __ldcs(vp + 32 * k);
+    });
     epi(i, sum, red);
   }
   if constexpr (NR > 0) {
@@ -293,8 +345,8 @@ sell_spmv_kernel(int nrow, const int* __restrict__ off, const unsigned char* __r
 // ELLPACK (slot-major): one thread per row, sequential over its slots,
 // stopping at the row's length (the reference stops at the first -1).
 // ------------------------------------------------------------------
-template <typename T, class Epi>
-__global__ void __launch_bounds__(kThreads, 8)
+template <typename T, class Epi, int U, bool PRED, int MINB>
+__global__ void __launch_bounds__(kThreads, MINB)
 ell_spmv_kernel(int nrow, long long ld, const int* __restrict__ col, const T* __restrict__ va,
                 const int* __restrict__ rowlen, const T* __restrict__ x,
                 Epi epi, RedWs ws, const Scalars* sc) {
@@ -303,34 +355,13 @@ ell_spmv_kernel(int nrow, long long ld, const int* __restrict__ col, const T* __
   double red[NR > 0 ? NR : 1];
 #pragma unroll
   for (int j = 0; j < (NR > 0 ? NR : 1); ++j) red[j] = 0.0;
-  const int i = blockIdx.x * kThreads + threadIdx.x;
-  if (i < nrow) {
-    const int len = rowlen[i];
+  for (int i = blockIdx.x * kThreads + threadIdx.x; i < nrow; i += gridDim.x * kThreads) {
     const int* cp = col + i;
     const T* vp = va + i;
-    T sum = T(0);
-    int k = 0;
-    for (; k + 4 <= len; k += 4) {
-      int c[4];
-      T v[4];
-#pragma unroll
-      for (int j = 0; j < 4; ++j) {
-        c[j] = __ldcs(cp + j * ld);
-        v[j] = __ldcs(vp + j * ld);
-      }
-      T p[4];
-#pragma unroll
-      for (int j = 0; j < 4; ++j) p[j] = mul(v[j], __ldg(x + c[j]));
-#pragma unroll
-      for (int j = 0; j < 4; ++j) sum = add(sum, p[j]);
-      cp += 4 * ld;
-      vp += 4 * ld;
-    }
-    for (; k < len; ++k) {
-      sum = add(sum, mul(__ldcs(vp), __ldg(x + __ldcs(cp))));
-      cp += ld;
-      vp += ld;
-    }
+    const T sum = row_dot<T, U, PRED>(rowlen[i], x, [&](int k, int& c, T& v) {
+      c = __ldcs(cp + k * ld);
+      v = __ldcs(vp + k * ld);
+    });
     epi(i, sum, red);
   }
   if constexpr (NR > 0) {
@@ -342,8 +373,8 @@ ell_spmv_kernel(int nrow, long long ld, const int* __restrict__ col, const T* __
 // Jagged diagonal: one thread per permuted position i, sweeping the
 // diagonals that reach it (coalesced across i), then y[perm[i]] = sum.
 // ------------------------------------------------------------------
-template <typename T, class Epi>
-__global__ void __launch_bounds__(kThreads)
+template <typename T, class Epi, int U, bool PRED, int MINB>
+__global__ void __launch_bounds__(kThreads, MINB)
 jad_spmv_kernel(int nrow, const int* __restrict__ perm, const int* __restrict__ jd,
                 const int* __restrict__ col, const T* __restrict__ va,
                 const int* __restrict__ plen, const T* __restrict__ x,
@@ -353,30 +384,12 @@ jad_spmv_kernel(int nrow, const int* __restrict__ perm, const int* __restrict__ 
   double red[NR > 0 ? NR : 1];
 #pragma unroll
   for (int j = 0; j < (NR > 0 ? NR : 1); ++j) red[j] = 0.0;
-  const int i = blockIdx.x * kThreads + threadIdx.x;
-  if (i < nrow) {
-    const int len = plen[i];
-    T sum = T(0);
-    int k = 0;
-    for (; k + 4 <= len; k += 4) {
-      int c[4];
-      T v[4];
-#pragma unroll
-      for (int j = 0; j < 4; ++j) {
-        const int idx = __ldg(jd + k + j) + i;
-        c[j] = __ldcs(col + idx);
-        v[j] = __ldcs(va + idx);
-      }
-      T p[4];
-#pragma unroll
-      for (int j = 0; j < 4; ++j) p[j] = mul(v[j], __ldg(x + c[j]));
-#pragma unroll
-      for (int j = 0; j < 4; ++j) sum = add(sum, p[j]);
-    }
-    for (; k < len; ++k) {
+  for (int i = blockIdx.x * kThreads + threadIdx.x; i < nrow; i += gridDim.x * kThreads) {
+    const T sum = row_dot<T, U, PRED>(plen[i], x, [&](int k, int& c, T& v) {
       const int idx = __ldg(jd + k) + i;
-      sum = add(sum, mul(__ldcs(va + idx), __ldg(x + __ldcs(col + idx))));
-    }
+      c = __ldcs(col + idx);
+      v = __ldcs(va + idx);
+    });
     epi(perm[i], sum, red);
   }
   if constexpr (NR > 0) {
@@ -474,13 +487,95 @@ bsr_spmv_kernel(int nrow, int ncol, int br_rt, int bc_rt, int nbr_trunc,
   }
 }
 
+// ------------------------------------------------------------------
+// BSR through its sliced copy (2x2 / 3x3 blocks): one thread per block
+// row, reading each block's column and its BR*BC elements as coalesced
+// 32-lane segments; row r of the block row accumulates
+// y = ((0 + s_0) + s_1) + ..., s_b the sequential sum over the block's row r
+// (spmv.hpp:158-170).  Block rows at or past nrow / br give 0.
+// ------------------------------------------------------------------
+template <typename T, int BR, int BC, class Epi>
+__global__ void __launch_bounds__(kThreads, 4)
+bsr_sell_kernel(int nrow, int ncol, int nbr, int nbr_trunc, const int* __restrict__ off,
+                const unsigned char* __restrict__ len, const int* __restrict__ col,
+                const T* __restrict__ va, const T* __restrict__ x, Epi epi, RedWs ws,
+                const Scalars* sc) {
+  constexpr int NR = Epi::kNR;
+  constexpr int BSZ = BR * BC;
+  if (solve_done(sc)) return;
+  double red[NR > 0 ? NR : 1];
+#pragma unroll
+  for (int j = 0; j < (NR > 0 ? NR : 1); ++j) red[j] = 0.0;
+  for (int I = blockIdx.x * kThreads + threadIdx.x; I < nbr; I += gridDim.x * kThreads) {
+    const int n = I < nbr_trunc ? len[I] : 0;
+    const int o = __ldg(off + (I >> 5));
+    const int l = I & 31;
+    T acc[BR];
+#pragma unroll
+    for (int r = 0; r < BR; ++r) acc[r] = T(0);
+    for (int k = 0; k < n; ++k) {
+      const int J = __ldcs(col + o + 32 * k + l);
+      const T* vp = va + static_cast<size_t>(o + 32 * k) * BSZ + l;
+      T v[BSZ];
+#pragma unroll
+      for (int e = 0; e < BSZ; ++e) v[e] = __ldcs(vp + 32 * e);
+      T xv[BC];
+#pragma unroll
+      for (int c = 0; c < BC; ++c) {
+        const int xc = J * BC + c;
+        xv[c] = xc < ncol ? __ldg(x + xc) : T(0);
+      }
+#pragma unroll
+      for (int r = 0; r < BR; ++r) {
+        T sum = T(0);
+#pragma unroll
+        for (int c = 0; c < BC; ++c) sum = add(sum, mul(v[r * BC + c], xv[c]));
+        acc[r] = add(acc[r], sum);
+      }
+    }
+#pragma unroll
+    for (int r = 0; r < BR; ++r) {
+      const int row = I * BR + r;
+      if (row < nrow) epi(row, acc[r], red);
+    }
+  }
+  if constexpr (NR > 0) {
+    grid_reduce<NR>(red, ws, [&](const double* t) { epi.finalize(t); });
+  }
+}
+
 // Grid size of the SpMV launch for a handle (for sizing RedWs).
 inline int spmv_grid(const sk_matrix_s* A) {
   switch (A->format) {
     case SK_CSR: return A->csr.sell ? ceil_div(A->nrow, kThreads) : A->csr.nparts;
-    case SK_BSR: return A->bsr.nparts;
+    case SK_BSR: return A->bsr.sell ? ceil_div(A->bsr.nbr, kThreads) : A->bsr.nparts;
     default: return ceil_div(A->nrow, kThreads);
   }
+}
+
+// Row-loop variants per value type, as measured on B200 (3-D 7-point
+// Laplacian, 128^3): FP64 rows run fastest as rounds of 4 plus a serial tail
+// at 8 CTAs per SM (32 registers); FP32 SELL rows as predicated rounds of 8
+// at 6 CTAs per SM.  A fused reduction needs more registers, so those
+// kernels are bounded at 6 CTAs per SM.  Every variant sums each row in the
+// same order, so the choice never changes a result.
+template <typename T, class Epi>
+struct SpmvTune {
+  static constexpr int kMinB = Epi::kNR > 0 ? 6 : 8;
+  static constexpr int kSellU = sizeof(T) == 8 ? 4 : 8;
+  static constexpr bool kSellPred = sizeof(T) != 8;
+  static constexpr int kSellMinB = sizeof(T) == 8 ? kMinB : 5;
+};
+
+// Grid of a thread-per-row product over `rows` rows: one CTA per 256
+// rows, or, when the epilogue carries a reduction, at most one wave
+// (SMs x resident CTAs per SM) looping over the rows.
+template <class Epi>
+inline int row_grid(const sk_matrix_s* A, i64 rows, int minb) {
+  const int full = ceil_div(rows, kThreads);
+  if (Epi::kNR == 0) return full > 0 ? full : 1;
+  const int wave = A->sm_count * minb;
+  return full < wave ? (full > 0 ? full : 1) : wave;
 }
 
 // Launches y-epilogue SpMV on any format.  vals_override lets the
@@ -494,7 +589,9 @@ void launch_spmv(const sk_matrix_s* A, const T* x, Epi const& epi, RedWs ws,
     case SK_CSR: {
       if (A->csr.sell) {
         const T* v = vals_override ? vals_override : static_cast<const T*>(A->csr.sell_vals);
-        SK_LAUNCH((sell_spmv_kernel<T, Epi>), ceil_div(A->nrow, kThreads), kThreads, 0, st,
+        SK_LAUNCH((sell_spmv_kernel<T, Epi, SpmvTune<T, Epi>::kSellU, SpmvTune<T, Epi>::kSellPred,
+                                    SpmvTune<T, Epi>::kSellMinB>),
+                  row_grid<Epi>(A, A->nrow, SpmvTune<T, Epi>::kSellMinB), kThreads, 0, st,
                   static_cast<int>(A->nrow), A->csr.sell_off, A->csr.sell_len, A->csr.sell_col, v, x,
                   epi, ws, sc);
         break;
@@ -506,18 +603,32 @@ void launch_spmv(const sk_matrix_s* A, const T* x, Epi const& epi, RedWs ws,
       break;
     }
     case SK_ELL:
-      SK_LAUNCH((ell_spmv_kernel<T, Epi>), ceil_div(A->nrow, kThreads), kThreads, 0, st,
+      SK_LAUNCH((ell_spmv_kernel<T, Epi, 4, false, SpmvTune<T, Epi>::kMinB>),
+                row_grid<Epi>(A, A->nrow, SpmvTune<T, Epi>::kMinB), kThreads, 0, st,
                 static_cast<int>(A->nrow), static_cast<long long>(A->ell.ld), A->ell.col,
                 static_cast<const T*>(A->ell.vals),
                 A->ell.rowlen, x, epi, ws, sc);
       break;
     case SK_JAD:
-      SK_LAUNCH((jad_spmv_kernel<T, Epi>), ceil_div(A->nrow, kThreads), kThreads, 0, st,
+      SK_LAUNCH((jad_spmv_kernel<T, Epi, 4, false, SpmvTune<T, Epi>::kMinB>),
+                row_grid<Epi>(A, A->nrow, SpmvTune<T, Epi>::kMinB), kThreads, 0, st,
                 static_cast<int>(A->nrow), A->jad.perm, A->jad.jdiag, A->jad.col,
                 static_cast<const T*>(A->jad.vals), A->jad.plen, x, epi, ws, sc);
       break;
     case SK_BSR: {
       const auto& b = A->bsr;
+      if (b.sell) {
+        const T* sv = static_cast<const T*>(b.sell_vals);
+        if (b.br == 3)
+          SK_LAUNCH((bsr_sell_kernel<T, 3, 3, Epi>), row_grid<Epi>(A, b.nbr, 4), kThreads, 0, st,
+                    static_cast<int>(A->nrow), static_cast<int>(A->ncol), static_cast<int>(b.nbr),
+                    static_cast<int>(b.nbr_mult), b.sell_off, b.sell_len, b.sell_col, sv, x, epi, ws, sc);
+        else
+          SK_LAUNCH((bsr_sell_kernel<T, 2, 2, Epi>), row_grid<Epi>(A, b.nbr, 4), kThreads, 0, st,
+                    static_cast<int>(A->nrow), static_cast<int>(A->ncol), static_cast<int>(b.nbr),
+                    static_cast<int>(b.nbr_mult), b.sell_off, b.sell_len, b.sell_col, sv, x, epi, ws, sc);
+        break;
+      }
       const T* v = static_cast<const T*>(b.vals);
       if (b.br == 3 && b.bc == 3)
         SK_LAUNCH((bsr_spmv_kernel<T, 3, 3, Epi>), b.nparts, kThreads, 0, st,

@@ -10,6 +10,7 @@
 // kernel), with the reference's element-wise arithmetic order; only the
 // dot products are summed in a different (fixed, deterministic) order.
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <vector>
 
@@ -64,16 +65,24 @@ struct SolveCommon {
 
 // Reserves scalars, the reduction slots and the history buffer, then
 // `nvec` n-vectors of `vb` bytes each plus `extra` bytes.
+static size_t common_bytes(sk_matrix A, i64 nvec, size_t vb, size_t extra, i64 hist_cap) {
+  const int cap = std::max(spmv_grid(A), vec_grid(A->nrow));
+  return 4096 + sizeof(Scalars) + 256 + static_cast<size_t>(cap) * kMaxRed * 8 +
+         static_cast<size_t>(hist_cap + 8) * 8 + static_cast<size_t>(nvec) * (vb + 256) + extra + 1024;
+}
+
+// Carves from `base` when given (the caller sized it with common_bytes),
+// else from the handle's grow-only workspace.
 static sk_status carve_common(sk_matrix A, cudaStream_t st, i64 nvec, size_t vb, size_t extra,
                               i64 hist_cap, SolveCommon* c, std::vector<char*>* vecs,
-                              char** extra_ptr) {
-  int cap = std::max(spmv_grid(A), vec_grid(A->nrow));
-  size_t need = 4096 + sizeof(Scalars) + 256 + static_cast<size_t>(cap) * kMaxRed * 8 +
-                static_cast<size_t>(hist_cap + 8) * 8 + static_cast<size_t>(nvec) * (vb + 256) +
-                extra + 1024;
-  sk_status s = ensure_ws(A, need);
-  if (s != SK_OK) return s;
-  Carver cv{static_cast<char*>(A->ws)};
+                              char** extra_ptr, char* base = nullptr) {
+  const int cap = std::max(spmv_grid(A), vec_grid(A->nrow));
+  if (!base) {
+    sk_status s = ensure_ws(A, common_bytes(A, nvec, vb, extra, hist_cap));
+    if (s != SK_OK) return s;
+    base = static_cast<char*>(A->ws);
+  }
+  Carver cv{base};
   c->sc = cv.take<Scalars>(sizeof(Scalars));
   c->ws.counter = cv.take<unsigned>(sizeof(unsigned) * 4);
   c->ws.partials = cv.take<double>(static_cast<size_t>(cap) * kMaxRed * 8);
@@ -125,8 +134,10 @@ struct OpNormB {
   static constexpr int kNR = 1;
   const T* b;
   Scalars* sc;
+  struct In { T b; };
   __device__ bool prepare(const Scalars*) { return true; }
-  __device__ void operator()(i64 i, double* red) const { red[0] += static_cast<double>(mul(b[i], b[i])); }
+  __device__ In load(i64 i) const { return {b[i]}; }
+  __device__ void apply(i64, In const& v, double* red) const { red[0] += static_cast<double>(mul(v.b, v.b)); }
   __device__ void finalize(const double* t) const {
     sc->bnorm = static_cast<double>(sqrt(static_cast<T>(t[0])));
   }
@@ -182,11 +193,12 @@ struct OpCgReorthDot {
   const T* z;
   T* p;
   Scalars* sc;
+  struct In { T r, z; };
   __device__ bool prepare(const Scalars* s) { return !solve_done(s); }
-  __device__ void operator()(i64 i, double* red) const {
-    const T zi = z[i];
-    p[i] = zi;
-    red[0] += static_cast<double>(mul(r[i], zi));
+  __device__ In load(i64 i) const { return {r[i], z[i]}; }
+  __device__ void apply(i64 i, In const& v, double* red) const {
+    p[i] = v.z;
+    red[0] += static_cast<double>(mul(v.r, v.z));
   }
   __device__ void finalize(const double* t) const { sc->rz = static_cast<double>(static_cast<T>(t[0])); }
 };
@@ -226,12 +238,16 @@ struct OpCgUpdate {
     alpha = static_cast<T>(s->alpha);
     return true;
   }
-  __device__ void operator()(i64 i, double* red) const {
-    x[i] = add(mul(alpha, hatp[i]), x[i]);
-    const T ri = sub(r[i], mul(alpha, q[i]));
+  struct In { T x, h, r, q, d; };
+  __device__ In load(i64 i) const {
+    return {x[i], hatp[i], r[i], q[i], LK == PK_JACOBI ? inv_d[i] : T(0)};
+  }
+  __device__ void apply(i64 i, In const& v, double* red) const {
+    x[i] = add(mul(alpha, v.h), v.x);
+    const T ri = sub(v.r, mul(alpha, v.q));
     r[i] = ri;
     red[0] += static_cast<double>(mul(ri, ri));
-    if constexpr (LK == PK_JACOBI) red[1] += static_cast<double>(mul(ri, mul(inv_d[i], ri)));
+    if constexpr (LK == PK_JACOBI) red[1] += static_cast<double>(mul(ri, mul(v.d, ri)));
   }
   __device__ void finalize(const double* t) const {
     sc->iters += 1;
@@ -256,8 +272,10 @@ struct OpCgBeta {
   const T* r;
   const T* z;
   Scalars* sc;
+  struct In { T r, z; };
   __device__ bool prepare(const Scalars* s) { return !solve_done(s); }
-  __device__ void operator()(i64 i, double* red) const { red[0] += static_cast<double>(mul(r[i], z[i])); }
+  __device__ In load(i64 i) const { return {r[i], z[i]}; }
+  __device__ void apply(i64, In const& v, double* red) const { red[0] += static_cast<double>(mul(v.r, v.z)); }
   __device__ void finalize(const double* t) const {
     const T rz_new = static_cast<T>(t[0]);
     sc->beta = static_cast<double>(rz_new / static_cast<T>(sc->rz));
@@ -279,38 +297,44 @@ struct OpCgDirection {
     beta = static_cast<T>(s->beta);
     return true;
   }
-  __device__ void operator()(i64 i, double*) const {
+  struct In { T z, p; };
+  __device__ In load(i64 i) const {
     T zi;
     if constexpr (LK == PK_IDENTITY) zi = r[i];
     else if constexpr (LK == PK_JACOBI) zi = mul(inv_d[i], r[i]);
     else zi = z[i];
-    p[i] = add(zi, mul(beta, p[i]));
+    return {zi, p[i]};
   }
+  __device__ void apply(i64 i, In const& v, double*) const { p[i] = add(v.z, mul(beta, v.p)); }
   __device__ void finalize(const double*) const {}
 };
 
+// One CG iteration.  `vals` (may be null) replaces the handle's values:
+// the mixed-precision solver runs T = float over the FP32 value copy of an
+// FP64 handle; its preconditioner is then identity or an FP32 Jacobi.
 template <typename T, int LK>
 static void cg_iteration(sk_matrix A, const sk_precond_s* L, const sk_precond_s* R, bool reorth,
                          const T* b, T* x, T* r, T* z, T* p, T* hatp, T* q, SolveCommon const& c,
-                         cudaStream_t st) {
+                         cudaStream_t st, const T* vals) {
   const i64 n = A->nrow;
+  const sk_dtype dt = sizeof(T) == 8 ? SK_F64 : SK_F32;
   const T* invL = L && L->kind == 1 ? static_cast<const T*>(L->inv_diag) : nullptr;
   if (reorth) {
-    launch_spmv<T>(A, x, EpiCgResid<T, LK>{b, r, p, invL, c.sc}, c.ws, c.sc, st);
+    launch_spmv<T>(A, x, EpiCgResid<T, LK>{b, r, p, invL, c.sc}, c.ws, c.sc, st, vals);
     if constexpr (LK == PK_OTHER) {
-      precond_apply_dispatch(L, A->dtype, n, r, z, c.ws, c.sc, st);
+      precond_apply_dispatch(L, dt, n, r, z, c.ws, c.sc, st);
       launch_vec(n, OpCgReorthDot<T>{r, z, p, c.sc}, c.ws, c.sc, st);
     }
   }
   const T* ph = p;
   if (R) {
-    precond_apply_dispatch(R, A->dtype, n, p, hatp, c.ws, c.sc, st);
+    precond_apply_dispatch(R, dt, n, p, hatp, c.ws, c.sc, st);
     ph = hatp;
   }
-  launch_spmv<T>(A, ph, EpiCgPq<T>{q, p, c.sc}, c.ws, c.sc, st);
+  launch_spmv<T>(A, ph, EpiCgPq<T>{q, p, c.sc}, c.ws, c.sc, st, vals);
   launch_vec(n, OpCgUpdate<T, LK>{x, r, ph, q, invL, c.sc, c.hist, T(0)}, c.ws, c.sc, st);
   if constexpr (LK == PK_OTHER) {
-    precond_apply_dispatch(L, A->dtype, n, r, z, c.ws, c.sc, st);
+    precond_apply_dispatch(L, dt, n, r, z, c.ws, c.sc, st);
     launch_vec(n, OpCgBeta<T>{r, z, c.sc}, c.ws, c.sc, st);
   }
   launch_vec(n, OpCgDirection<T, LK>{p, r, z, invL, T(0)}, c.ws, c.sc, st);
@@ -319,13 +343,13 @@ static void cg_iteration(sk_matrix A, const sk_precond_s* L, const sk_precond_s*
 template <typename T>
 static sk_status cg_solve(sk_matrix A, sk_precond L, sk_precond R, const T* b, T* x,
                           const sk_cg_config* cfg, sk_summary* out, double* history_host,
-                          cudaStream_t st) {
+                          cudaStream_t st, const T* vals = nullptr, char* ws_base = nullptr) {
   const i64 n = A->nrow;
   const size_t vb = static_cast<size_t>(n + 8) * sizeof(T);
   SolveCommon c;
   std::vector<char*> v;
   const i64 hist_cap = cfg->collect_residuals ? cfg->max_iterations : 0;
-  sk_status s = carve_common(A, st, 5, vb, 0, hist_cap, &c, &v, nullptr);
+  sk_status s = carve_common(A, st, 5, vb, 0, hist_cap, &c, &v, nullptr, ws_base);
   if (s != SK_OK) return s;
   T *r = (T*)v[0], *z = (T*)v[1], *p = (T*)v[2], *hatp = (T*)v[3], *q = (T*)v[4];
   *out = sk_summary{};
@@ -350,11 +374,11 @@ static sk_status cg_solve(sk_matrix A, sk_precond L, sk_precond R, const T* b, T
     for (i64 j = 0; j < todo; ++j, ++k) {
       const bool reorth = (k % cfg->restart_iterations) == 0;
       if (lk == PK_IDENTITY)
-        cg_iteration<T, PK_IDENTITY>(A, L, R, reorth, b, x, r, z, p, hatp, q, c, st);
+        cg_iteration<T, PK_IDENTITY>(A, L, R, reorth, b, x, r, z, p, hatp, q, c, st, vals);
       else if (lk == PK_JACOBI)
-        cg_iteration<T, PK_JACOBI>(A, L, R, reorth, b, x, r, z, p, hatp, q, c, st);
+        cg_iteration<T, PK_JACOBI>(A, L, R, reorth, b, x, r, z, p, hatp, q, c, st, vals);
       else
-        cg_iteration<T, PK_OTHER>(A, L, R, reorth, b, x, r, z, p, hatp, q, c, st);
+        cg_iteration<T, PK_OTHER>(A, L, R, reorth, b, x, r, z, p, hatp, q, c, st, vals);
     }
     SK_CUDA(cudaGetLastError());
     if ((s = read_scalars(c.sc, &h, st)) != SK_OK) return s;
@@ -414,13 +438,17 @@ struct OpBiP {
     beta = (rho_new / static_cast<T>(s->rho)) * (static_cast<T>(s->alpha) / omega);
     return true;
   }
-  __device__ void operator()(i64 i, double*) const {
-    const T pi = add(r[i], mul(beta, sub(p[i], mul(omega, v[i]))));
+  struct In { T r, p, v, dl, dr; };
+  __device__ In load(i64 i) const {
+    return {r[i], p[i], v[i], LK == PK_JACOBI ? invL[i] : T(0), RK == PK_JACOBI ? invR[i] : T(0)};
+  }
+  __device__ void apply(i64 i, In const& q, double*) const {
+    const T pi = add(q.r, mul(beta, sub(q.p, mul(omega, q.v))));
     p[i] = pi;
     if constexpr (LK != PK_OTHER && RK != PK_OTHER) {
       T t = pi;
-      if constexpr (LK == PK_JACOBI) t = mul(invL[i], t);
-      if constexpr (RK == PK_JACOBI) t = mul(invR[i], t);
+      if constexpr (LK == PK_JACOBI) t = mul(q.dl, t);
+      if constexpr (RK == PK_JACOBI) t = mul(q.dr, t);
       p_hat[i] = t;
     }
   }
@@ -459,8 +487,10 @@ struct OpBiS {
     alpha = static_cast<T>(st->alpha);
     return true;
   }
-  __device__ void operator()(i64 i, double* red) const {
-    const T si = sub(r[i], mul(alpha, v[i]));
+  struct In { T r, v; };
+  __device__ In load(i64 i) const { return {r[i], v[i]}; }
+  __device__ void apply(i64 i, In const& q, double* red) const {
+    const T si = sub(q.r, mul(alpha, q.v));
     s[i] = si;
     red[0] += static_cast<double>(mul(si, si));
   }
@@ -499,13 +529,18 @@ struct OpBiHalfOrS {
     mode = 2;
     return LK != PK_OTHER && RK != PK_OTHER;
   }
-  __device__ void operator()(i64 i, double*) const {
+  struct In { T a, b, dl, dr; };
+  __device__ In load(i64 i) const {
+    if (mode == 1) return {x[i], p_hat[i], T(0), T(0)};
+    return {s[i], T(0), LK == PK_JACOBI ? invL[i] : T(0), RK == PK_JACOBI ? invR[i] : T(0)};
+  }
+  __device__ void apply(i64 i, In const& q, double*) const {
     if (mode == 1) {
-      x[i] = add(x[i], mul(alpha, p_hat[i]));
+      x[i] = add(q.a, mul(alpha, q.b));
     } else if constexpr (LK != PK_OTHER && RK != PK_OTHER) {
-      T t = s[i];
-      if constexpr (LK == PK_JACOBI) t = mul(invL[i], t);
-      if constexpr (RK == PK_JACOBI) t = mul(invR[i], t);
+      T t = q.a;
+      if constexpr (LK == PK_JACOBI) t = mul(q.dl, t);
+      if constexpr (RK == PK_JACOBI) t = mul(q.dr, t);
       s_hat[i] = t;
     }
   }
@@ -561,13 +596,18 @@ struct OpBiUpdate {
     skip = st->skip;
     return true;
   }
-  __device__ void operator()(i64 i, double* red) const {
+  struct In { T x, ph, sh, s, t, rh; };
+  __device__ In load(i64 i) const {
+    if (skip) return {};
+    return {x[i], p_hat[i], s_hat[i], s[i], t[i], r_hat[i]};
+  }
+  __device__ void apply(i64 i, In const& q, double* red) const {
     if (skip) return;
-    x[i] = add(x[i], add(mul(alpha, p_hat[i]), mul(omega, s_hat[i])));
-    const T ri = sub(s[i], mul(omega, t[i]));
+    x[i] = add(q.x, add(mul(alpha, q.ph), mul(omega, q.sh)));
+    const T ri = sub(q.s, mul(omega, q.t));
     r[i] = ri;
     red[0] += static_cast<double>(mul(ri, ri));
-    red[1] += static_cast<double>(mul(r_hat[i], ri));
+    red[1] += static_cast<double>(mul(q.rh, ri));
   }
   __device__ void finalize(const double* tot) const {
     if (skip) {
@@ -736,7 +776,9 @@ struct OpFgScale {
     f = T(1) / h;
     return true;
   }
-  __device__ void operator()(i64 i, double*) const { v[i] = mul(v[i], f); }
+  struct In { T v; };
+  __device__ In load(i64 i) const { return {v[i]}; }
+  __device__ void apply(i64 i, In const& q, double*) const { v[i] = mul(q.v, f); }
   __device__ void finalize(const double*) const {}
 };
 
@@ -770,10 +812,12 @@ struct OpFgMgs {
     h = static_cast<T>(*h_in);
     return true;
   }
-  __device__ void operator()(i64 k, double* red) const {
-    const T wk = sub(w[k], mul(h, vi[k]));
+  struct In { T w, vi, vn; };
+  __device__ In load(i64 k) const { return {w[k], vi[k], vnext ? vnext[k] : T(0)}; }
+  __device__ void apply(i64 k, In const& q, double* red) const {
+    const T wk = sub(q.w, mul(h, q.vi));
     w[k] = wk;
-    red[0] += static_cast<double>(mul(vnext ? vnext[k] : wk, wk));
+    red[0] += static_cast<double>(mul(vnext ? q.vn : wk, wk));
   }
   __device__ void finalize(const double* t) const {
     const T d = static_cast<T>(t[0]);
@@ -867,10 +911,12 @@ struct OpFgUpdateX {
     nj = static_cast<int>(s->jfinal) + 1;
     return true;
   }
-  __device__ void operator()(i64 i, double*) const {
+  struct In { T x; };
+  __device__ In load(i64 i) const { return {x[i]}; }
+  __device__ void apply(i64 i, In const& q, double*) const {
     T sum = T(0);
     for (int k = 0; k < nj; ++k) sum = add(sum, mul(Z[k * ldz + i], static_cast<T>(y[k])));
-    x[i] = add(x[i], sum);
+    x[i] = add(q.x, sum);
   }
   __device__ void finalize(const double*) const {}
 };
@@ -946,6 +992,257 @@ static sk_status fgmres_solve(sk_matrix A, sk_precond M, const T* b, T* x,
     if ((s = read_scalars(c.sc, &h, st)) != SK_OK) return s;
   }
   return finish_summary(c, st, out, history_host);
+}
+
+// Keeps [base, base + bytes) resident in L2 for the kernels of stream `st`
+// while it lives: a persisting access-policy window on the stream and a
+// persisting set-aside of the same size (both settings of this process's
+// context only; the previous limit is restored and the persisting lines are
+// released on release()).  Sizes above the device's maximum shrink the hit
+// ratio accordingly.  A null stream disables it.
+struct L2Window {
+  cudaStream_t st = nullptr;
+  size_t prev_limit = 0;
+  bool on = false;
+  L2Window(cudaStream_t s, void* base, size_t bytes) {
+    if (!s || bytes == 0) return;
+    int dev = 0, maxp = 0, maxw = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return;
+    cudaDeviceGetAttribute(&maxp, cudaDevAttrMaxPersistingL2CacheSize, dev);
+    cudaDeviceGetAttribute(&maxw, cudaDevAttrMaxAccessPolicyWindowSize, dev);
+    if (maxp <= 0 || maxw <= 0) return;
+    if (cudaDeviceGetLimit(&prev_limit, cudaLimitPersistingL2CacheSize) != cudaSuccess) return;
+    const size_t want = std::min<size_t>(bytes, static_cast<size_t>(maxw));
+    const size_t setaside = std::min<size_t>(want, static_cast<size_t>(maxp));
+    if (cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, setaside) != cudaSuccess) {
+      cudaGetLastError();
+      return;
+    }
+    cudaStreamAttrValue attr{};
+    attr.accessPolicyWindow.base_ptr = base;
+    attr.accessPolicyWindow.num_bytes = want;
+    attr.accessPolicyWindow.hitRatio = static_cast<float>(std::min(1.0, double(setaside) / double(want)));
+    attr.accessPolicyWindow.hitProp = cudaAccessPropertyPersisting;
+    attr.accessPolicyWindow.missProp = cudaAccessPropertyStreaming;
+    if (cudaStreamSetAttribute(s, cudaStreamAttributeAccessPolicyWindow, &attr) != cudaSuccess) {
+      cudaGetLastError();
+      cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, prev_limit);
+      return;
+    }
+    st = s;
+    on = true;
+  }
+  void release() {
+    if (!on) return;
+    cudaStreamAttrValue attr{};
+    attr.accessPolicyWindow.num_bytes = 0;
+    cudaStreamSetAttribute(st, cudaStreamAttributeAccessPolicyWindow, &attr);
+    cudaStreamSynchronize(st);
+    cudaCtxResetPersistingL2Cache();
+    cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, prev_limit);
+    on = false;
+  }
+  ~L2Window() { release(); }
+};
+
+// ==================================================================
+// Mixed precision: FP32 Jacobi-CG inside FP64 iterative refinement.
+// No reference counterpart (the reference runs one precision per solve);
+// its inner solver is conjugate_gradient.hpp:122-312 instantiated for float
+// on the FP32 copy of the matrix values, and the outer loop keeps the
+// residual r = b - A x, the solution update and the stopping test in FP64.
+// ==================================================================
+
+// r = b - A x in FP64 with ||r||^2.
+struct EpiResid64 {
+  static constexpr int kNR = 1;
+  const double* b;
+  double* r;
+  Scalars* sc;
+  __device__ void operator()(int row, double ax, double* red) const {
+    const double ri = __dsub_rn(b[row], ax);
+    r[row] = ri;
+    red[0] += ri * ri;
+  }
+  __device__ void finalize(const double* t) const { sc->rnorm = sqrt(t[0]); }
+};
+
+// inner right-hand side: r32 = r / ||r||, and the inner guess d = 0
+struct OpScaleDown {
+  static constexpr int kNR = 0;
+  const double* r;
+  float* r32;
+  float* d32;
+  double inv;
+  __device__ bool prepare(const Scalars* s) {
+    inv = 1.0 / s->rnorm;
+    return true;
+  }
+  struct In { double r; };
+  __device__ In load(i64 i) const { return {r[i]}; }
+  __device__ void apply(i64 i, In const& q, double*) const {
+    r32[i] = static_cast<float>(q.r * inv);
+    d32[i] = 0.0f;
+  }
+  __device__ void finalize(const double*) const {}
+};
+
+// x += ||r|| d
+struct OpRefine {
+  static constexpr int kNR = 0;
+  double* x;
+  const float* d32;
+  double scale;
+  __device__ bool prepare(const Scalars* s) {
+    scale = s->rnorm;
+    return true;
+  }
+  struct In { double x; float d; };
+  __device__ In load(i64 i) const { return {x[i], d32[i]}; }
+  __device__ void apply(i64 i, In const& q, double*) const { x[i] = q.x + scale * static_cast<double>(q.d); }
+  __device__ void finalize(const double*) const {}
+};
+
+// FP32 Jacobi for the inner solves: the FP64 inverse diagonal (jacobi.hpp:
+// 27-35 on the FP64 values) rounded to float; exact zeros are counted.
+__global__ void inv_diag32_kernel(i64 n, const int* __restrict__ rp, const int* __restrict__ ci,
+                                  const double* __restrict__ v, float* __restrict__ inv32,
+                                  unsigned long long* zeros) {
+  const i64 i = blockIdx.x * static_cast<i64>(blockDim.x) + threadIdx.x;
+  if (i >= n) return;
+  int lo = rp[i], hi = rp[i + 1];
+  const int end = hi;
+  while (lo < hi) {
+    const int mid = lo + (hi - lo) / 2;
+    if (ci[mid] < i) lo = mid + 1; else hi = mid;
+  }
+  const double d = (lo < end && ci[lo] == i) ? v[lo] : 0.0;
+  if (d == 0.0) atomicAdd(zeros, 1ull);
+  inv32[i] = d == 0.0 ? 0.0f : static_cast<float>(__ddiv_rn(1.0, d));
+}
+
+static sk_status mixed_cg_solve(sk_matrix A, bool jacobi, const double* b, double* x,
+                                const sk_mixed_config* cfg, sk_mixed_summary* out, double* history,
+                                cudaStream_t st) {
+  const i64 n = A->nrow;
+  *out = sk_mixed_summary{};
+  using clk = std::chrono::steady_clock;
+  auto ms_since = [](clk::time_point t0) {
+    return std::chrono::duration<double, std::milli>(clk::now() - t0).count();
+  };
+  const auto t_setup = clk::now();
+  if (!f32_values(A)) {
+    sk_status s0 = sk_matrix_add_f32_values(A);
+    if (s0 != SK_OK) return s0;
+  }
+  // One workspace for the whole solve (allocated on the first call, reused
+  // after; the FP32 Jacobi is built once per handle):
+  //   [ inner FP32 CG region | d32 | inv32 ]  <- kept resident in L2
+  //   [ r32 | r64 | outer scalars, counters, reduction slots ]
+  const int cap = spmv_grid(A);
+  const size_t inner_bytes = (common_bytes(A, 5, static_cast<size_t>(n + 8) * 4, 0, 0) + 255) & ~size_t(255);
+  const size_t need = inner_bytes + 4096 + static_cast<size_t>(n + 64) * (8 + 4 + 4 + 4) + 4096 +
+                      static_cast<size_t>(cap) * kMaxRed * 8 + 1024;
+  const bool fresh = A->ws2_bytes < need;  // reused after the first call
+  if (fresh) {
+    if (A->ws2) {
+      cudaStreamSynchronize(st);
+      cudaFree(A->ws2);
+      A->ws2 = nullptr;
+    }
+    SK_CUDA(cudaMalloc(&A->ws2, need));
+    A->ws2_bytes = need;
+  }
+  char* inner_base = static_cast<char*>(A->ws2);
+  Carver cv{inner_base};
+  cv.off = inner_bytes;
+  float* d32 = cv.take<float>(static_cast<size_t>(n + 8) * 4);
+  float* inv32 = cv.take<float>(static_cast<size_t>(n + 8) * 4);
+  const size_t resident_bytes = cv.off;
+  float* r32 = cv.take<float>(static_cast<size_t>(n + 8) * 4);
+  double* r = cv.take<double>(static_cast<size_t>(n + 8) * 8);
+  Scalars* so = cv.take<Scalars>(sizeof(Scalars));
+  unsigned* cnt = cv.take<unsigned>(16);
+  double* partials = cv.take<double>(static_cast<size_t>(cap) * kMaxRed * 8);
+  SK_CUDA(cudaMemsetAsync(so, 0, sizeof(Scalars), st));
+  SK_CUDA(cudaMemsetAsync(cnt, 0, 16, st));
+  sk_precond_s jac32{};
+  if (jacobi) {
+    // built once per handle (ws2 keeps it): no allocation on later calls
+    if (fresh || !A->mixed_jacobi_ready) {
+      unsigned long long* zeros = reinterpret_cast<unsigned long long*>(cnt + 2);
+      SK_CUDA(cudaMemsetAsync(zeros, 0, 8, st));
+      SK_LAUNCH(inv_diag32_kernel, ceil_div(n, kThreads), kThreads, 0, st, n, A->csr.row_ptr, A->csr.col_ind,
+                static_cast<const double*>(A->csr.vals), inv32, zeros);
+      unsigned long long nz = 0;
+      SK_CUDA(cudaMemcpyAsync(&nz, zeros, 8, cudaMemcpyDeviceToHost, st));
+      SK_CUDA(cudaStreamSynchronize(st));
+      if (nz) return fail(SK_ZERO_DIAGONAL, "jacobi: zero diagonal entry");
+      A->mixed_jacobi_ready = true;
+    }
+    jac32.kind = 1;
+    jac32.A = A;
+    jac32.dtype = SK_F32;
+    jac32.n = n;
+    jac32.inv_diag = inv32;
+  }
+  RedWs ws{partials, cnt, cap};
+  double bnorm = 0;
+  {
+    // ||b|| in FP64
+    launch_vec(n, OpNormB<double>{b, so}, ws, nullptr, st);
+    Scalars h;
+    sk_status s1 = read_scalars(so, &h, st);
+    if (s1 != SK_OK) return s1;
+    bnorm = h.bnorm;
+  }
+  out->setup_ms = ms_since(t_setup);
+  sk_status status = SK_OK;
+  if (bnorm == 0.0) {
+    SK_CUDA(cudaMemsetAsync(x, 0, n * 8, st));
+    out->converged = 1;
+  } else {
+    sk_cg_config icfg{cfg->inner_tolerance, cfg->max_inner, cfg->max_inner, 0};
+    for (i64 outer = 0;; ++outer) {
+      auto t_outer = clk::now();
+      launch_spmv<double>(A, x, EpiResid64{b, r, so}, ws, nullptr, st);
+      Scalars h;
+      status = read_scalars(so, &h, st);
+      out->outer_ms += ms_since(t_outer);
+      if (status != SK_OK) break;
+      out->residual_norm = h.rnorm;
+      if (history && cfg->collect_residuals) history[outer] = h.rnorm;
+      out->outer_iterations = outer;
+      if (h.rnorm / bnorm < cfg->tolerance) {
+        out->converged = 1;
+        break;
+      }
+      if (outer >= cfg->max_outer) break;
+      launch_vec(n, OpScaleDown{r, r32, d32, 0.0}, ws, so, st);
+      // The last step needs only the remaining factor tol ||b|| / ||r||: its
+      // inner tolerance is tightened to half of that when that is below the
+      // configured one (floor 1e-7, about what FP32 CG can resolve), so that
+      // the refinement ends one step earlier instead of overshooting.
+      const double needed = cfg->tolerance * bnorm / h.rnorm;
+      icfg.tolerance = cfg->inner_tolerance;
+      if (cfg->adaptive_last_step && 0.5 * needed < cfg->inner_tolerance)
+        icfg.tolerance = std::max(0.5 * needed, 1e-7);
+      sk_summary is{};
+      auto t_inner = clk::now();
+      L2Window win(cfg->l2_window ? st : nullptr, inner_base, resident_bytes);
+      status = cg_solve<float>(A, jacobi ? &jac32 : nullptr, nullptr, r32, d32, &icfg, &is, nullptr, st,
+                               f32_values(A), inner_base);
+      win.release();
+      out->inner_ms += ms_since(t_inner);
+      if (status != SK_OK) break;
+      out->inner_iterations += is.computed_iterations;
+      t_outer = clk::now();
+      launch_vec(n, OpRefine{x, d32, 0.0}, ws, so, st);
+      out->outer_ms += ms_since(t_outer);
+    }
+  }
+  SK_CUDA(cudaStreamSynchronize(st));
+  return status;
 }
 
 }  // namespace sk
@@ -1064,3 +1361,18 @@ sk_status sk_fgmres_solve_host(sk_matrix A, sk_precond M, const void* b_host, vo
 }
 
 }  // extern "C"
+
+extern "C" sk_status sk_mixed_cg_solve(sk_matrix A, int32_t jacobi, const double* b_dev, double* x_dev,
+                                       const sk_mixed_config* cfg, sk_mixed_summary* out, double* history_host,
+                                       sk_stream s) {
+  sk_status st = check_solver_args(A, nullptr, nullptr, b_dev, x_dev);
+  if (st != SK_OK) return st;
+  SK_CHECK(cfg && out, SK_INVALID_ARG, "null config or summary");
+  SK_CHECK(A->dtype == SK_F64 && A->format == SK_CSR, SK_INVALID_ARG,
+           "the mixed-precision solver needs an FP64 CSR handle");
+  SK_CHECK(cfg->max_outer >= 0 && cfg->max_inner > 0, SK_INVALID_ARG, "bad iteration limits");
+  // The solve runs on the handle's own stream (an access-policy window needs
+  // a created stream), ordered after the caller's stream.
+  SK_CUDA(cudaStreamSynchronize(static_cast<cudaStream_t>(s)));
+  return mixed_cg_solve(A, jacobi != 0, b_dev, x_dev, cfg, out, history_host, A->stream);
+}

@@ -1,40 +1,68 @@
 // sk_vec.cuh -- one-pass element-wise kernels with fused, deterministic
 // grid reductions.  A pass is a functor Op with
 //   static constexpr int kNR;                 fused reductions
+//   struct In;                                the inputs of one element
 //   bool prepare(const Scalars*)              load scalars; false = skip
-//   void operator()(i64 i, double* red)      element i
+//   In load(i64 i)                            read element i's inputs
+//   void apply(i64 i, In const&, double* red) compute and store element i
 //   void finalize(const double* total)       last CTA, thread 0
-// and runs as vec_kernel<Op> over [0, n) with a grid that depends on n only
-// (so that the reduction tree, and hence the rounding, is reproducible).
+// vec_kernel<Op> gives each thread kUnroll elements (stride apart) and reads
+// all their inputs before any store, so that the loads are in flight
+// together (the stores could alias the inputs, so a fused load-compute-store
+// loop would serialize them).  The grid depends on n only, so the reduction
+// tree, and hence the rounding, is reproducible.
 #pragma once
 
 #include "sk_kernels.cuh"
 
 namespace sk {
 
+constexpr int kUnroll = 4;  // elements per thread per round (8 for small inputs)
+
+// One wave of 8 CTAs per SM at most (148 SMs on B200); the count depends
+// on n only.
 inline int vec_grid(i64 n) {
-  i64 g = (n + kThreads - 1) / kThreads;
+  i64 g = (n + kThreads * kUnroll - 1) / (kThreads * kUnroll);
   if (g > 148 * 8) g = 148 * 8;
   if (g < 1) g = 1;
   return static_cast<int>(g);
 }
 
 template <class Op>
-__global__ void __launch_bounds__(kThreads) vec_kernel(i64 n, Op op, RedWs ws, const Scalars* sc) {
+constexpr int vec_unroll() {
+  return sizeof(typename Op::In) <= 12 ? 2 * kUnroll : kUnroll;
+}
+
+template <class Op>
+__global__ void __launch_bounds__(kThreads, 4) vec_kernel(i64 n, Op op, RedWs ws, const Scalars* sc) {
   constexpr int NR = Op::kNR;
   if (!op.prepare(sc)) return;
   double red[NR > 0 ? NR : 1];
 #pragma unroll
   for (int j = 0; j < (NR > 0 ? NR : 1); ++j) red[j] = 0.0;
-  const i64 stride = static_cast<i64>(gridDim.x) * kThreads;
-  i64 i = static_cast<i64>(blockIdx.x) * kThreads + threadIdx.x;
-  for (; i + 3 * stride < n; i += 4 * stride) {
-    op(i, red);
-    op(i + stride, red);
-    op(i + 2 * stride, red);
-    op(i + 3 * stride, red);
+  // Each warp takes contiguous segments of 32 * U elements; lane l handles
+  // elements seg + 32 u + l.  The U elements of a thread are thus a
+  // compile-time distance apart (one address per array plus immediate
+  // offsets), and every load instruction reads 32 consecutive elements.
+  constexpr int U = vec_unroll<Op>();
+  constexpr i64 SEG = 32 * U;
+  const int lane = threadIdx.x & 31;
+  const i64 warp = (static_cast<i64>(blockIdx.x) * kThreads + threadIdx.x) >> 5;
+  const i64 nwarps = static_cast<i64>(gridDim.x) * (kThreads / 32);
+  for (i64 seg = warp * SEG; seg < n; seg += nwarps * SEG) {
+    const i64 i0 = seg + lane;
+    typename Op::In in[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const i64 i = i0 + 32 * u;
+      if (i < n) in[u] = op.load(i);
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const i64 i = i0 + 32 * u;
+      if (i < n) op.apply(i, in[u], red);
+    }
   }
-  for (; i < n; i += stride) op(i, red);
   if constexpr (NR > 0) {
     grid_reduce<NR>(red, ws, [&](const double* t) { op.finalize(t); });
   }
@@ -58,67 +86,64 @@ __global__ void scalar_kernel(Op op) {
 template <typename T>
 struct OpDot {
   static constexpr int kNR = 1;
+  struct In { T a, b; };
   const T* a;
   const T* b;
   double* out;
   __device__ bool prepare(const Scalars* sc) { return !solve_done(sc); }
-  __device__ void operator()(i64 i, double* red) const {
-    red[0] += static_cast<double>(mul(a[i], b[i]));
-  }
+  __device__ In load(i64 i) const { return {a[i], b[i]}; }
+  __device__ void apply(i64, In const& v, double* red) const { red[0] += static_cast<double>(mul(v.a, v.b)); }
   __device__ void finalize(const double* t) const { *out = t[0]; }
 };
 
 template <typename T>
 struct OpAxpy {  // y = alpha * x + y
   static constexpr int kNR = 0;
+  struct In { T x, y; };
   T alpha;
   const T* x;
   T* y;
   __device__ bool prepare(const Scalars* sc) { return !solve_done(sc); }
-  __device__ void operator()(i64 i, double*) const { y[i] = add(mul(alpha, x[i]), y[i]); }
+  __device__ In load(i64 i) const { return {x[i], y[i]}; }
+  __device__ void apply(i64 i, In const& v, double*) const { y[i] = add(mul(alpha, v.x), v.y); }
   __device__ void finalize(const double*) const {}
 };
 
 template <typename T>
 struct OpXpay {  // y = x + beta * y
   static constexpr int kNR = 0;
+  struct In { T x, y; };
   T beta;
   const T* x;
   T* y;
   __device__ bool prepare(const Scalars* sc) { return !solve_done(sc); }
-  __device__ void operator()(i64 i, double*) const { y[i] = add(x[i], mul(beta, y[i])); }
-  __device__ void finalize(const double*) const {}
-};
-
-template <typename T>
-struct OpScaleCopy {  // z = c * r
-  static constexpr int kNR = 0;
-  T c;
-  const T* r;
-  T* z;
-  __device__ bool prepare(const Scalars* sc) { return !solve_done(sc); }
-  __device__ void operator()(i64 i, double*) const { z[i] = mul(c, r[i]); }
+  __device__ In load(i64 i) const { return {x[i], y[i]}; }
+  __device__ void apply(i64 i, In const& v, double*) const { y[i] = add(v.x, mul(beta, v.y)); }
   __device__ void finalize(const double*) const {}
 };
 
 template <typename T>
 struct OpJacobi {  // z = inv_d * r   (jacobi.hpp:44-51)
   static constexpr int kNR = 0;
+  struct In { T d, r; };
   const T* inv_d;
   const T* r;
   T* z;
   __device__ bool prepare(const Scalars* sc) { return !solve_done(sc); }
-  __device__ void operator()(i64 i, double*) const { z[i] = mul(inv_d[i], r[i]); }
+  __device__ In load(i64 i) const { return {inv_d[i], r[i]}; }
+  __device__ void apply(i64 i, In const& v, double*) const { z[i] = mul(v.d, v.r); }
   __device__ void finalize(const double*) const {}
 };
 
 template <typename T>
 struct OpCopy {
   static constexpr int kNR = 0;
+  struct In { T a; };
   const T* a;
   T* b;
   __device__ bool prepare(const Scalars* sc) { return !solve_done(sc); }
-  __device__ void operator()(i64 i, double*) const { b[i] = a[i]; }
+  __device__ In load(i64 i) const { return {a[i]}; }
+  __device__ void apply(i64 i, In const& v, double*) const { b[i] = v.a; }
   __device__ void finalize(const double*) const {}
 };
 
@@ -126,23 +151,20 @@ struct OpCopy {
 // Chebyshev preconditioner pieces (chebyshev_preconditioner.hpp:98-169).
 // Abar v = (2 A v - (lmax + lmin) v) / (lmax - lmin).
 // ------------------------------------------------------------------
-template <typename T>
-struct ChebCoef {
-  T sum, diff;
-};
-
 // b_d = c_d r ; b_{d+1} = 0
 template <typename T>
 struct OpChebInit {
   static constexpr int kNR = 0;
+  struct In { T r; };
   T cd;
   const T* r;
   T* b_curr;
   T* b_prev;
   const Scalars* skip;
   __device__ bool prepare(const Scalars* sc) { return !solve_done(sc); }
-  __device__ void operator()(i64 i, double*) const {
-    b_curr[i] = mul(cd, r[i]);
+  __device__ In load(i64 i) const { return {r[i]}; }
+  __device__ void apply(i64 i, In const& v, double*) const {
+    b_curr[i] = mul(cd, v.r);
     b_prev[i] = T(0);
   }
   __device__ void finalize(const double*) const {}
@@ -182,11 +204,13 @@ struct EpiChebFinal {
 template <typename T>
 struct OpScaleCopySkip {  // z = c * r, skipped once the solve is done
   static constexpr int kNR = 0;
+  struct In { T r; };
   T c;
   const T* r;
   T* z;
   __device__ bool prepare(const Scalars* sc) { return !solve_done(sc); }
-  __device__ void operator()(i64 i, double*) const { z[i] = mul(c, r[i]); }
+  __device__ In load(i64 i) const { return {r[i]}; }
+  __device__ void apply(i64 i, In const& v, double*) const { z[i] = mul(c, v.r); }
   __device__ void finalize(const double*) const {}
 };
 

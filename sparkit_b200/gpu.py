@@ -325,6 +325,49 @@ def fgmres(b, x, cfg, op, preconditioner=identity):
                 b, x, Ad, c, cfg.max_iterations, cfg.collect_residuals)
 
 
+@dataclass
+class Mixed_config:
+    """FP32-inner / FP64-outer iterative refinement (sk_mixed_cg_solve)."""
+    tolerance: float = 1e-10
+    inner_tolerance: float = 1e-5
+    max_outer: int = 100
+    max_inner: int = 100000
+    collect_residuals: bool = False
+    adaptive_last_step: bool = True
+    l2_window: bool = True
+
+
+@dataclass
+class Mixed_summary:
+    residual_norm: float = 0.0
+    outer_iterations: int = 0
+    inner_iterations: int = 0
+    converged: bool = False
+    status: int = 0
+    residual_history: List[float] = field(default_factory=list)
+    setup_ms: float = 0.0
+    inner_ms: float = 0.0
+    outer_ms: float = 0.0
+
+
+def mixed_cg(b, x, cfg, op, jacobi_inner=True):
+    """Solves A x = b to cfg.tolerance on the true FP64 residual with FP32
+    CG inner solves (Jacobi-preconditioned unless jacobi_inner is False).
+    b and x are FP64 CUDA tensors (x holds the initial guess)."""
+    Ad = _op_matrix(op)
+    c = _lib.MixedConfig(cfg.tolerance, cfg.inner_tolerance, cfg.max_outer, cfg.max_inner,
+                         int(cfg.collect_residuals), int(cfg.adaptive_last_step), int(cfg.l2_window))
+    s = _lib.MixedSummary()
+    hist = np.zeros(cfg.max_outer + 2) if cfg.collect_residuals else None
+    check(lib().sk_mixed_cg_solve(Ad.handle, int(jacobi_inner), _ptr(b), _ptr(x), ctypes.byref(c), ctypes.byref(s),
+                                  _ptr(hist), _stream_of(b)))
+    out = Mixed_summary(s.residual_norm, s.outer_iterations, s.inner_iterations, bool(s.converged), s.status,
+                        [], s.setup_ms, s.inner_ms, s.outer_ms)
+    if hist is not None:
+        out.residual_history = hist[: s.outer_iterations + 1].tolist()
+    return out
+
+
 def device_count():
     n = ctypes.c_int()
     check(lib().sk_device_count(ctypes.byref(n)))

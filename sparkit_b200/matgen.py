@@ -196,3 +196,46 @@ def vector_laplacian_3d_bsr(nx, seed=0, coupling=0.1, dtype=np.float64):
     off = ~np.eye(3, dtype=bool)
     blk[d_idx] = np.where(off[None], coup[brow[d_idx]], blk[d_idx])
     return Block_sparse_row_matrix((3 * n, 3 * n), 3, 3, L.row_ptr(), bcol, blk.reshape(-1).astype(dtype))
+
+
+def gaussian_random_field(shape, sigma, corr_len, seed=0):
+    """Stationary Gaussian random field on a periodic grid: white noise
+    filtered in Fourier space by exp(-|k|^2 corr_len^2 / 2) (a Gaussian
+    covariance of length corr_len cells), shifted to mean 0 and scaled to
+    standard deviation sigma."""
+    rng = np.random.default_rng(seed)
+    w = rng.standard_normal(shape)
+    ks = np.meshgrid(*[2 * np.pi * np.fft.fftfreq(s) for s in shape], indexing="ij")
+    k2 = sum(k * k for k in ks)
+    g = np.real(np.fft.ifftn(np.fft.fftn(w) * np.exp(-0.5 * k2 * corr_len * corr_len)))
+    g -= g.mean()
+    g *= sigma / g.std()
+    return g
+
+
+def diffusion_3d_grf(n, sigma=2.0, corr_len=8.0, seed=0, dtype=np.float64):
+    """7-point finite-volume diffusion on an n^3 grid with cell coefficients
+    k = exp(g), g a Gaussian random field (sigma, corr_len cells).  Interior
+    faces take the harmonic mean of their two cells, boundary faces the cell
+    value (homogeneous Dirichlet): A_ii = sum of the cell's six face
+    coefficients, A_ij = -k_face.  SPD."""
+    g = gaussian_random_field((n, n, n), sigma, corr_len, seed)
+    kc = np.exp(g).reshape(-1)  # index = i + n*(j + n*k)
+    N = n ** 3
+    node = np.arange(N, dtype=np.int64)
+    i = node % n
+    j = (node // n) % n
+    kk = node // (n * n)
+    pl = n * n
+    offs = (-pl, -n, -1, 1, n, pl)
+    inside = (kk > 0, j > 0, i > 0, i + 1 < n, j + 1 < n, kk + 1 < n)
+    face = []
+    for off, ok in zip(offs, inside):
+        nb = np.where(ok, node + off, node)
+        kf = np.where(ok, 2.0 * kc * kc[nb] / (kc + kc[nb]), kc)
+        face.append(kf)
+    diag = sum(face)
+    cand = np.stack([node - pl, node - n, node - 1, node, node + 1, node + n, node + pl], axis=1)
+    valid = np.stack([inside[0], inside[1], inside[2], np.ones(N, bool), inside[3], inside[4], inside[5]], axis=1)
+    vals = np.stack([-face[0], -face[1], -face[2], diag, -face[3], -face[4], -face[5]], axis=1)
+    return _stencil_csr(N, cand, vals, valid, dtype)
