@@ -307,6 +307,60 @@ SK_API sk_status sk_mixed_cg_solve(sk_matrix A, int32_t jacobi,
                                    sk_mixed_summary* out, double* history_host,
                                    sk_stream s);
 
+/* ---------------------------------------------------------------- */
+/* Batched solves (no reference counterpart: the reference solves one */
+/* system per call; the comparison is a loop of the plain solver)     */
+/* ---------------------------------------------------------------- */
+
+typedef struct sk_batch_s* sk_batch;
+
+/* nsys independent SPD systems as the diagonal blocks of one CSR matrix
+ * (FP32 values): system s owns rows [sys_offsets[s], sys_offsets[s+1]) and
+ * every column index of those rows lies in the same range. */
+SK_API sk_status sk_batch_create(sk_batch* out, int64_t nsys,
+                                 const int64_t* sys_offsets,
+                                 const int64_t* row_ptr,
+                                 const int64_t* col_ind, const float* values);
+SK_API sk_status sk_batch_destroy(sk_batch B);
+
+typedef struct {
+  double tolerance;          /* FP64 true relative residual per system */
+  double inner_tolerance;    /* FP32 Jacobi-CG relative tolerance */
+  int64_t max_outer;
+  int64_t max_inner;
+  int32_t adaptive_last_step;
+  int32_t lanes_per_row;     /* 1, 2, 4 or 8 (from sk_batched_autotune) */
+  int32_t threads_per_cta;   /* 256, 512 or 1024 */
+} sk_batch_config;
+
+/* Device arrays of nsys entries each, written by the solve. */
+typedef struct {
+  int32_t* inner_iterations;
+  int32_t* outer_iterations;
+  double* relative_residual;
+  int32_t* converged;
+} sk_batch_results;
+
+/* Solves every system in one persistent launch (FP32 Jacobi-CG inside FP64
+ * iterative refinement, conjugate_gradient.hpp:122-312 per system), one CTA
+ * per system at a time taken from a longest-first queue.  The launch is
+ * captured into a CUDA graph and replayed while the pointers and settings
+ * stay the same.  b and x are FP64 device vectors over all rows; x holds the
+ * initial guesses and receives the solutions. */
+SK_API sk_status sk_batched_cg_solve(sk_batch B, const double* b_dev,
+                                     double* x_dev, const sk_batch_config* cfg,
+                                     sk_batch_results* res, sk_stream s);
+
+/* Times every (lanes_per_row, threads_per_cta) variant on the `sample`
+ * largest systems and returns the fastest; ms_out (may be NULL) receives
+ * sk_batched_variant_count() timings.  x is overwritten with zeros. */
+SK_API sk_status sk_batched_autotune(sk_batch B, const double* b_dev,
+                                     double* x_dev, const sk_batch_config* cfg,
+                                     sk_batch_results* res, int64_t sample,
+                                     int32_t* lanes_per_row,
+                                     int32_t* threads_per_cta, double* ms_out);
+SK_API int32_t sk_batched_variant_count(void);
+
 /* Host-buffer forms of the three solvers (b and x in host memory, copied
  * in and out inside the call): the drop-in boundary of the C++ overloads. */
 SK_API sk_status sk_cg_solve_host(sk_matrix A, sk_precond left, sk_precond right,

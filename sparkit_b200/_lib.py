@@ -61,6 +61,16 @@ class MixedSummary(ctypes.Structure):
                 ("outer_ms", c_dbl)]
 
 
+class BatchConfig(ctypes.Structure):
+    _fields_ = [("tolerance", c_dbl), ("inner_tolerance", c_dbl), ("max_outer", c_i64), ("max_inner", c_i64),
+                ("adaptive_last_step", c_i32), ("lanes_per_row", c_i32), ("threads_per_cta", c_i32)]
+
+
+class BatchResults(ctypes.Structure):
+    _fields_ = [("inner_iterations", c_vp), ("outer_iterations", c_vp), ("relative_residual", c_vp),
+                ("converged", c_vp)]
+
+
 class Summary(ctypes.Structure):
     _fields_ = [("residual_norm", c_dbl), ("computed_iterations", c_i64),
                 ("converged", c_i32), ("status", c_i32), ("history_length", c_i64)]
@@ -105,6 +115,12 @@ SIGNATURES = [
                          c_vp, c_vp]),
     ("sk_mixed_cg_solve", [c_vp, c_i32, c_vp, c_vp, ctypes.POINTER(MixedConfig), ctypes.POINTER(MixedSummary),
                            c_vp, c_vp]),
+    ("sk_batch_create", [ctypes.POINTER(c_vp), c_i64, c_vp, c_vp, c_vp, c_vp]),
+    ("sk_batch_destroy", [c_vp]),
+    ("sk_batched_cg_solve", [c_vp, c_vp, c_vp, ctypes.POINTER(BatchConfig), ctypes.POINTER(BatchResults), c_vp]),
+    ("sk_batched_autotune", [c_vp, c_vp, c_vp, ctypes.POINTER(BatchConfig), ctypes.POINTER(BatchResults), c_i64,
+                             ctypes.POINTER(c_i32), ctypes.POINTER(c_i32), c_vp]),
+    ("sk_batched_variant_count", []),
     ("sk_cg_solve_host", [c_vp, c_vp, c_vp, c_vp, c_vp, ctypes.POINTER(CgConfig), ctypes.POINTER(Summary),
                           c_vp]),
     ("sk_bicgstab_solve_host", [c_vp, c_vp, c_vp, c_vp, c_vp, ctypes.POINTER(BicgstabConfig),

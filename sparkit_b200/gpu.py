@@ -368,6 +368,83 @@ def mixed_cg(b, x, cfg, op, jacobi_inner=True):
     return out
 
 
+@dataclass
+class Batch_config:
+    """Settings of sk_batched_cg_solve."""
+    tolerance: float = 1e-10
+    inner_tolerance: float = 1e-5
+    max_outer: int = 30
+    max_inner: int = 20000
+    adaptive_last_step: bool = True
+    lanes_per_row: int = 1
+    threads_per_cta: int = 512
+
+
+class Batch:
+    """Many independent SPD systems (the diagonal blocks of one FP32 CSR
+    matrix) solved together on the device: one persistent launch, one CTA
+    per system, FP32 Jacobi-CG inside FP64 iterative refinement."""
+
+    def __init__(self, sys_offsets, row_ptr, col_ind, values):
+        sys_offsets = np.ascontiguousarray(sys_offsets, dtype=np.int64)
+        row_ptr = np.ascontiguousarray(row_ptr, dtype=np.int64)
+        col_ind = np.ascontiguousarray(col_ind, dtype=np.int64)
+        values = np.ascontiguousarray(values, dtype=np.float32)
+        h = ctypes.c_void_p()
+        check(lib().sk_batch_create(ctypes.byref(h), sys_offsets.size - 1, _ptr(sys_offsets), _ptr(row_ptr),
+                                    _ptr(col_ind), _ptr(values)))
+        self.handle = h
+        self.nsys = sys_offsets.size - 1
+        self.nrow = int(sys_offsets[-1])
+        self._res = None
+
+    def _results(self):
+        import torch
+        if self._res is None:
+            n = self.nsys
+            self._res = (torch.zeros(n, dtype=torch.int32, device="cuda"), torch.zeros(n, dtype=torch.int32, device="cuda"),
+                         torch.zeros(n, dtype=torch.float64, device="cuda"), torch.zeros(n, dtype=torch.int32, device="cuda"))
+        t = self._res
+        return _lib.BatchResults(_ptr(t[0]), _ptr(t[1]), _ptr(t[2]), _ptr(t[3])), t
+
+    @staticmethod
+    def _cfg(c):
+        return _lib.BatchConfig(c.tolerance, c.inner_tolerance, c.max_outer, c.max_inner, int(c.adaptive_last_step),
+                                c.lanes_per_row, c.threads_per_cta)
+
+    def autotune(self, b, x, cfg=None, sample=512):
+        """Times every (lanes_per_row, threads_per_cta) variant on the
+        `sample` largest systems; returns (lanes, threads, timings_ms)."""
+        cfg = cfg or Batch_config()
+        res, _ = self._results()
+        g, t = ctypes.c_int32(), ctypes.c_int32()
+        nvar = lib().sk_batched_variant_count()
+        ms = np.zeros(nvar)
+        check(lib().sk_batched_autotune(self.handle, _ptr(b), _ptr(x), ctypes.byref(self._cfg(cfg)), ctypes.byref(res),
+                                        int(sample), ctypes.byref(g), ctypes.byref(t), _ptr(ms)))
+        return g.value, t.value, ms
+
+    def solve(self, b, x, cfg=None):
+        """Solves all systems; returns per-system numpy arrays
+        (inner_iterations, outer_iterations, relative_residual, converged)."""
+        cfg = cfg or Batch_config()
+        res, t = self._results()
+        check(lib().sk_batched_cg_solve(self.handle, _ptr(b), _ptr(x), ctypes.byref(self._cfg(cfg)),
+                                        ctypes.byref(res), _stream_of(b)))
+        return tuple(a.cpu().numpy() for a in t)
+
+    def close(self):
+        if getattr(self, "handle", None) and not _lib.shutting_down():
+            lib().sk_batch_destroy(self.handle)
+        self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 def device_count():
     n = ctypes.c_int()
     check(lib().sk_device_count(ctypes.byref(n)))

@@ -239,3 +239,40 @@ def diffusion_3d_grf(n, sigma=2.0, corr_len=8.0, seed=0, dtype=np.float64):
     valid = np.stack([inside[0], inside[1], inside[2], np.ones(N, bool), inside[3], inside[4], inside[5]], axis=1)
     vals = np.stack([-face[0], -face[1], -face[2], diag, -face[3], -face[4], -face[5]], axis=1)
     return _stencil_csr(N, cand, vals, valid, dtype)
+
+
+def batched_spd_systems(count=4096, nmin=1000, nmax=65536, shift=(0.0, 0.5), seed=0):
+    """`count` independent SPD systems: each a 2-D 5-point or 3-D 7-point
+    Dirichlet Laplacian (seeded coin) plus a diagonal shift U[shift], with
+    n log-uniform in [nmin, nmax] rounded to a square or cubic grid.
+    Returns (sys_offsets, row_ptr, col_ind, values, kinds) of the
+    block-diagonal CSR matrix holding them (global row / column numbering,
+    float32 values)."""
+    rng = np.random.default_rng(seed)
+    offs = [0]
+    rps, cols, vals, kinds = [], [], [], []
+    nnz_base = 0
+    for _ in range(count):
+        n_target = float(np.exp(rng.uniform(np.log(nmin), np.log(nmax))))
+        three_d = bool(rng.integers(0, 2))
+        sft = rng.uniform(shift[0], shift[1])
+        if three_d:
+            g = max(2, int(round(n_target ** (1.0 / 3.0))))
+            L = laplacian_3d_dirichlet(g, diag=6.0 + sft)
+        else:
+            g = max(2, int(round(n_target ** 0.5)))
+            L = laplacian_2d_dirichlet(g)
+            v = L.values().copy()
+            rows = np.repeat(np.arange(L.shape()[0]), L.row_lengths())
+            v[L.col_ind() == rows] += sft
+            L = Compressed_row_matrix(L.shape(), L.row_ptr(), L.col_ind(), v)
+        n = L.shape()[0]
+        rps.append(L.row_ptr()[:-1] + nnz_base)
+        cols.append(L.col_ind() + offs[-1])
+        vals.append(L.values().astype(np.float32))
+        nnz_base += L.size()
+        offs.append(offs[-1] + n)
+        kinds.append(3 if three_d else 2)
+    row_ptr = np.concatenate(rps + [np.array([nnz_base], dtype=np.int64)])
+    return (np.array(offs, dtype=np.int64), row_ptr, np.concatenate(cols), np.concatenate(vals),
+            np.array(kinds, dtype=np.int8))
