@@ -361,6 +361,98 @@ SK_API sk_status sk_batched_autotune(sk_batch B, const double* b_dev,
                                      int32_t* threads_per_cta, double* ms_out);
 SK_API int32_t sk_batched_variant_count(void);
 
+/* ---------------------------------------------------------------- */
+/* Learned variable preconditioner for FGMRES (no reference           */
+/* counterpart: fgmres, sparkit/data/fgmres.hpp:452-470, accepts any   */
+/* callable as its variable preconditioner; this is one such callable */
+/* with the training that produces it)                                */
+/* ---------------------------------------------------------------- */
+
+/* A convolutional encoder-decoder over the 2-D grid of a 5-point matrix:
+ * nine 3x3 convolutions over four levels (16, 32, 64, 64 channels), BF16
+ * weights and activations, FP32 accumulation and FP32 master weights.
+ * It maps a residual to an approximation of the error.  Created with
+ * seeded He-initialised weights. */
+typedef struct sk_net_s* sk_net;
+SK_API sk_status sk_net_create(sk_net* out, uint64_t seed);
+SK_API sk_status sk_net_destroy(sk_net N);
+SK_API int64_t sk_net_param_count(void);
+/* Flat FP32 parameters, layer by layer: W[cout][9][cin] (tap 3 ky + kx
+ * reads pixel (y + ky - 1, x + kx - 1)) then b[cout]. */
+SK_API sk_status sk_net_get_params(sk_net N, float* host, int64_t capacity);
+SK_API sk_status sk_net_set_params(sk_net N, const float* host, int64_t count);
+/* Test hook: run the convolutions on mma.sync instead of tcgen05 (the two
+ * must agree; the tests compare them). */
+SK_API sk_status sk_net_set_legacy_mma(sk_net N, int32_t on);
+/* SK_TIMEOUT when a network kernel gave up a bounded wait (then clears). */
+SK_API sk_status sk_net_status(sk_net N);
+
+/* Training set of (residual, error) pairs on an nx x ny grid, stored FP32
+ * on the device, each tied to an instance (the coefficient planes of its
+ * matrix). */
+typedef struct sk_pairs_s* sk_pairs;
+SK_API sk_status sk_pairs_create(sk_pairs* out, int64_t nx, int64_t ny, int64_t capacity,
+                                 int32_t max_instances);
+SK_API sk_status sk_pairs_destroy(sk_pairs D);
+SK_API sk_status sk_pairs_count(sk_pairs D, int64_t* count);
+/* Registers the FP64 CSR 5-point matrix A of an nx x ny grid (row y*nx+x). */
+SK_API sk_status sk_pairs_add_instance(sk_pairs D, sk_matrix A, int32_t* instance);
+SK_API sk_status sk_pairs_add(sk_pairs D, int32_t instance, const double* r_dev,
+                              const double* e_dev, sk_stream s);
+/* Runs the plain Jacobi-FGMRES(restart) on A x = b from x = 0 one restart
+ * cycle at a time and adds (b - A x, xstar - x) after every cycle, for at
+ * most `cycles` cycles; xstar is the exact solution (b = A xstar). */
+SK_API sk_status sk_learned_harvest(sk_pairs D, int32_t instance, sk_matrix A, const double* b_dev,
+                                    const double* xstar_dev, int64_t restart, int64_t cycles,
+                                    int64_t* added);
+
+/* Adam on the loss
+ *   mean_b |A (y_b - e_b / s_b)|^2 / |r_b / s_b|^2 + mu |y_b - e_b / s_b|^2 / |e_b / s_b|^2
+ * (y_b the network's output for pair b, s_b the RMS of D^-1 r_b), batches
+ * drawn uniformly with the seed, learning rate cosine-decayed from lr to
+ * lr * lr_final_ratio. */
+typedef struct {
+  int64_t steps;
+  int32_t batch;
+  float lr;
+  float lr_final_ratio;
+  float beta1, beta2, eps;
+  double mu;
+  uint64_t seed;
+} sk_train_config;
+
+typedef struct {
+  double first_loss, last_loss;
+  double ms;  /* host wall time of the whole training */
+  int64_t steps;
+} sk_train_summary;
+
+SK_API sk_status sk_net_train(sk_net N, sk_pairs D, const sk_train_config* cfg,
+                              sk_train_summary* out, double* loss_history);
+/* Loss of one batch and its gradient (FP32, sk_net_param_count() values)
+ * without an update: the gradient check of the tests. */
+SK_API sk_status sk_net_loss_grad(sk_net N, sk_pairs D, const int32_t* pairs_host, int32_t batch,
+                                  double mu, double* loss, float* grad_host, int64_t capacity);
+
+/* The network as a preconditioner of the FP64 CSR 5-point matrix A on an
+ * nx x ny grid: z = s net(D^-1 r / s, off-diagonals / diagonal) with
+ * s = rms(D^-1 r).  Applied by sk_precond_apply and by FGMRES. */
+SK_API sk_status sk_learned_create(sk_precond* out, sk_matrix A, sk_net net, int64_t nx,
+                                   int64_t ny);
+/* The six coefficient planes (d, w, e, s, n, 1/d; FP32, 6 n values). */
+SK_API sk_status sk_learned_planes(sk_precond M, float* host, int64_t capacity);
+
+/* fgmres with M as the variable preconditioner and a fallback: after a
+ * restart cycle whose final residual estimate is above stall_ratio times
+ * its starting residual, the remaining cycles use `fallback` (Jacobi or
+ * Chebyshev).  *switched_at (may be NULL) receives the first cycle run with
+ * the fallback, or -1. */
+SK_API sk_status sk_fgmres_fallback_solve(sk_matrix A, sk_precond M, sk_precond fallback,
+                                          const double* b_dev, double* x_dev,
+                                          const sk_fgmres_config* cfg, double stall_ratio,
+                                          sk_summary* out, double* history_host,
+                                          int64_t* switched_at, sk_stream s);
+
 /* Host-buffer forms of the three solvers (b and x in host memory, copied
  * in and out inside the call): the drop-in boundary of the C++ overloads. */
 SK_API sk_status sk_cg_solve_host(sk_matrix A, sk_precond left, sk_precond right,

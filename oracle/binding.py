@@ -193,6 +193,76 @@ class Oracle:
         return self._solve("fgmres", A, [prec], b, x0, FgmresCfg(tol, restart, max_it, int(collect)), max_it,
                            prec_matrix)
 
+    # -------------------------------------------------------------- #
+    # Learned preconditioner network (sk_oracle_net.c)                #
+    # -------------------------------------------------------------- #
+
+    def net_param_count(self):
+        self.L.skon_param_count.restype = c_i64
+        return int(self.L.skon_param_count())
+
+    def net_apply(self, params, v, coef, H, W, round_bf16=True):
+        """z = s * net(features(v)); coef = grid_planes(A, H, W)."""
+        params = np.ascontiguousarray(params, dtype=np.float32)
+        v = np.ascontiguousarray(v, dtype=np.float64)
+        coef = np.ascontiguousarray(coef, dtype=np.float32)
+        z = np.zeros(H * W)
+        y = np.zeros(H * W)
+        self.L.skon_apply(ctypes.c_int(H), ctypes.c_int(W), _p(params), _p(v), _p(coef), ctypes.c_int(int(round_bf16)),
+                          _p(z), _p(y))
+        return z, y
+
+    def net_features(self, r, coef, B, H, W, round_bf16=True):
+        r = np.ascontiguousarray(r, dtype=np.float64)
+        coef = np.ascontiguousarray(coef, dtype=np.float32)
+        x = np.zeros(B * H * W * 8)
+        s = np.zeros(B)
+        self.L.skon_features(ctypes.c_int(B), ctypes.c_int(H), ctypes.c_int(W), _p(r), _p(coef),
+                             ctypes.c_int(int(round_bf16)), _p(x), _p(s))
+        return x.reshape(B, H, W, 8), s
+
+    def net_loss_grad(self, params, r, e, coef, B, H, W, mu=0.0, round_bf16=True, grad=True):
+        """Loss of a batch (r, e: B*H*W each; coef: B stacked grid_planes)
+        and its gradient with respect to the flat parameters."""
+        self.L.skon_loss_grad.restype = ctypes.c_double
+        params = np.ascontiguousarray(params, dtype=np.float32)
+        r = np.ascontiguousarray(r, dtype=np.float64)
+        e = np.ascontiguousarray(e, dtype=np.float64)
+        coef = np.ascontiguousarray(coef, dtype=np.float32)
+        g = np.zeros(self.net_param_count()) if grad else None
+        y = np.zeros(B * H * W)
+        loss = self.L.skon_loss_grad(ctypes.c_int(B), ctypes.c_int(H), ctypes.c_int(W), _p(params), _p(r), _p(e),
+                                     _p(coef), ctypes.c_double(mu), ctypes.c_int(int(round_bf16)), _p(g), _p(y))
+        return float(loss), g, y
+
+    def adam(self, p, m, v, g, lr, b1, b2, eps, t):
+        """In place on float32 arrays."""
+        self.L.skon_adam(c_i64(p.size), _p(p), _p(m), _p(v), _p(np.ascontiguousarray(g, dtype=np.float32)),
+                         ctypes.c_float(lr), ctypes.c_float(b1), ctypes.c_float(b2), ctypes.c_float(eps), c_i64(t))
+
+
+def grid_planes(A, H, W):
+    """The six coefficient planes of a 5-point matrix on an H x W grid (row
+    index y * W + x): diagonal, west, east, south, north (float32 of the
+    entries, 0 where the neighbour is missing) and float32(1 / diagonal)."""
+    n = H * W
+    rp, ci, va = A.row_ptr(), A.col_ind(), A.values().astype(np.float64)
+    rows = np.repeat(np.arange(n, dtype=np.int64), np.diff(rp))
+    off = ci - rows
+    planes = np.zeros((6, n), dtype=np.float32)
+    d64 = np.zeros(n)
+    for k, o in enumerate((0, -1, 1, -W, W)):
+        sel = off == o
+        if k == 1:
+            sel &= (rows % W) > 0
+        if k == 2:
+            sel &= (rows % W) < W - 1
+        planes[k, rows[sel]] = va[sel].astype(np.float32)
+        if k == 0:
+            d64[rows[sel]] = va[sel]
+    planes[5] = (1.0 / d64).astype(np.float32)
+    return planes
+
 
 class Reference:
     """The sparkit reference itself, compiled from its sources

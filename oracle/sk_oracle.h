@@ -118,6 +118,19 @@ void sko_set_dot_order(int mode);
 SKO_DECLARE(double, f64)
 SKO_DECLARE(float, f32)
 
+/* Learned preconditioner network (sk_oracle_net.c).  coef holds, per
+ * sample, six planes of H*W floats: diagonal, west, east, south, north
+ * coefficients and the inverse diagonal. */
+int64_t skon_param_count(void);
+void skon_features(int B, int H, int W, const double* r, const float* coef, int round_bf16, double* xin,
+                   double* scale);
+void skon_apply(int H, int W, const float* params, const double* v, const float* coef, int round_bf16,
+                double* z, double* y_out);
+double skon_loss_grad(int B, int H, int W, const float* params, const double* r, const double* e,
+                      const float* coef, double mu, int round_bf16, double* grad, double* y_out);
+void skon_adam(int64_t n, float* p, float* m, float* v, const float* g, float lr, float b1, float b2,
+               float eps, int64_t t);
+
 #ifdef __cplusplus
 }
 #endif

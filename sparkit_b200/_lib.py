@@ -61,6 +61,16 @@ class MixedSummary(ctypes.Structure):
                 ("outer_ms", c_dbl)]
 
 
+class TrainConfig(ctypes.Structure):
+    _fields_ = [("steps", c_i64), ("batch", c_i32), ("lr", ctypes.c_float), ("lr_final_ratio", ctypes.c_float),
+                ("beta1", ctypes.c_float), ("beta2", ctypes.c_float), ("eps", ctypes.c_float), ("mu", c_dbl),
+                ("seed", ctypes.c_uint64)]
+
+
+class TrainSummary(ctypes.Structure):
+    _fields_ = [("first_loss", c_dbl), ("last_loss", c_dbl), ("ms", c_dbl), ("steps", c_i64)]
+
+
 class BatchConfig(ctypes.Structure):
     _fields_ = [("tolerance", c_dbl), ("inner_tolerance", c_dbl), ("max_outer", c_i64), ("max_inner", c_i64),
                 ("adaptive_last_step", c_i32), ("lanes_per_row", c_i32), ("threads_per_cta", c_i32)]
@@ -121,6 +131,25 @@ SIGNATURES = [
     ("sk_batched_autotune", [c_vp, c_vp, c_vp, ctypes.POINTER(BatchConfig), ctypes.POINTER(BatchResults), c_i64,
                              ctypes.POINTER(c_i32), ctypes.POINTER(c_i32), c_vp]),
     ("sk_batched_variant_count", []),
+    ("sk_net_create", [ctypes.POINTER(c_vp), ctypes.c_uint64]),
+    ("sk_net_destroy", [c_vp]),
+    ("sk_net_param_count", []),
+    ("sk_net_get_params", [c_vp, c_vp, c_i64]),
+    ("sk_net_set_params", [c_vp, c_vp, c_i64]),
+    ("sk_net_set_legacy_mma", [c_vp, c_i32]),
+    ("sk_net_status", [c_vp]),
+    ("sk_pairs_create", [ctypes.POINTER(c_vp), c_i64, c_i64, c_i64, c_i32]),
+    ("sk_pairs_destroy", [c_vp]),
+    ("sk_pairs_count", [c_vp, P_i64]),
+    ("sk_pairs_add_instance", [c_vp, c_vp, ctypes.POINTER(c_i32)]),
+    ("sk_pairs_add", [c_vp, c_i32, c_vp, c_vp, c_vp]),
+    ("sk_learned_harvest", [c_vp, c_i32, c_vp, c_vp, c_vp, c_i64, c_i64, P_i64]),
+    ("sk_net_train", [c_vp, c_vp, ctypes.POINTER(TrainConfig), ctypes.POINTER(TrainSummary), c_vp]),
+    ("sk_net_loss_grad", [c_vp, c_vp, c_vp, c_i32, c_dbl, ctypes.POINTER(c_dbl), c_vp, c_i64]),
+    ("sk_learned_create", [ctypes.POINTER(c_vp), c_vp, c_vp, c_i64, c_i64]),
+    ("sk_learned_planes", [c_vp, c_vp, c_i64]),
+    ("sk_fgmres_fallback_solve", [c_vp, c_vp, c_vp, c_vp, c_vp, ctypes.POINTER(FgmresConfig), c_dbl,
+                                  ctypes.POINTER(Summary), c_vp, P_i64, c_vp]),
     ("sk_cg_solve_host", [c_vp, c_vp, c_vp, c_vp, c_vp, ctypes.POINTER(CgConfig), ctypes.POINTER(Summary),
                           c_vp]),
     ("sk_bicgstab_solve_host", [c_vp, c_vp, c_vp, c_vp, c_vp, ctypes.POINTER(BicgstabConfig),
@@ -163,7 +192,8 @@ def lib():
             for name, args in SIGNATURES:
                 fn = getattr(L, name)
                 fn.argtypes = args
-                fn.restype = ctypes.c_char_p if name in ("sk_version", "sk_last_error") else ctypes.c_int
+                fn.restype = (ctypes.c_char_p if name in ("sk_version", "sk_last_error")
+                              else c_i64 if name == "sk_net_param_count" else ctypes.c_int)
             _lib = L
     return _lib
 

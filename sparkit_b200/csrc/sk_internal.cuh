@@ -146,8 +146,10 @@ struct sk_matrix_s {
   sk::i64 spmv_bytes() const;
 };
 
+struct sk_net_s;
+
 struct sk_precond_s {
-  int kind;  // 1 = Jacobi, 2 = Chebyshev
+  int kind;  // 1 = Jacobi, 2 = Chebyshev, 3 = learned network
   sk_matrix A;
   sk_dtype dtype;
   sk::i64 n;
@@ -157,6 +159,11 @@ struct sk_precond_s {
   sk::i64 degree = 0;
   void* work = nullptr;  // Chebyshev: 3 n-vectors
   float* inv_diag32 = nullptr;  // FP32 copy for mixed precision
+  // learned (kind 3): the network and the matrix's coefficient planes on
+  // its grid_nx x grid_ny grid (d, w, e, s, n, 1/d; float)
+  sk_net_s* net = nullptr;
+  float* coef = nullptr;
+  sk::i64 grid_nx = 0, grid_ny = 0;
 };
 
 namespace sk {
@@ -192,6 +199,7 @@ struct Scalars {
   double rnorm;     // last residual norm recorded
   double tol;
   double aux;       // FGMRES: 1 / beta or 1 / h_{j+1,j}
+  double beta_cycle;  // FGMRES: ||r|| at the start of the current cycle
   long long iters;
   long long hist_len;
   long long max_iters;

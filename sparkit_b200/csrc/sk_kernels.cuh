@@ -149,13 +149,14 @@ __device__ __forceinline__ void cp_async_commit_wait_all() {
 
 // ------------------------------------------------------------------
 // CSR: one CTA per tile of rows (tiles[b] = {first row, first entry};
-// at most 256 rows and 2048 entries, or one longer row).  The tile's column
-// indices and values are copied into shared memory with cp.async as soon as
-// the CTA starts; then each row is summed by one thread in storage order
-// (bit-exact with the reference) -- the thread gathers x for its own row,
-// so for banded matrices a warp's gathers of the j-th neighbour are
-// coalesced -- or, in tiles holding a row longer than 32 entries, by L
-// lanes with strided partial sums and a shuffle tree.
+// at most 256 rows and 2048 entries, or one longer row).  Every thread
+// loads 8 of the tile's entries (coalesced, streaming) and gathers their x
+// values with all 16 loads in flight, so that the random gathers of skewed
+// matrices overlap instead of being walked row by row; the rounded products
+// go to shared memory.  Then each row is summed from there by one thread in
+// storage order (bit-exact with the reference), or, in tiles holding a row
+// longer than 32 entries, by L lanes with strided partial sums and a
+// shuffle tree.
 // ------------------------------------------------------------------
 template <typename T, class Epi>
 __global__ void __launch_bounds__(kThreads)
@@ -165,7 +166,6 @@ csr_spmv_kernel(const int* __restrict__ rp, const int* __restrict__ ci,
                 const unsigned char* __restrict__ lanes, Epi epi, RedWs ws,
                 const Scalars* sc) {
   constexpr int NR = Epi::kNR;
-  __shared__ __align__(16) int scol[kTileNnz + 8];
   __shared__ __align__(16) T sval[kTileNnz + 8];
   __shared__ int srp[kRowsMax + 1];
   if (solve_done(sc)) return;
@@ -188,38 +188,34 @@ csr_spmv_kernel(const int* __restrict__ rp, const int* __restrict__ ci,
     block_reduce<1>(acc);
     if (tid == 0) epi(r0, static_cast<T>(acc[0]), red);
   } else {
-    const int as = s & ~3;
-    const int ngroups = (((e + 3) & ~3) - as) >> 2;
-    for (int g = tid; g < ngroups; g += kThreads) {
-      cp_async16(scol + 4 * g, ci + as + 4 * g);
-      if constexpr (sizeof(T) == 8) {
-        cp_async16(sval + 4 * g, va + as + 4 * g);
-        cp_async16(sval + 4 * g + 2, va + as + 4 * g + 2);
-      } else {
-        cp_async16(sval + 4 * g, va + as + 4 * g);
+    // Every thread computes the products of entries s + tid + 256 j (j < 8:
+    // the loads of its 8 entries and their 8 gathers of x are in flight
+    // together) into shared memory; rows are then summed from there.
+    T* sprod = sval;
+    int cj[kTileNnz / kThreads];
+    T vj[kTileNnz / kThreads], xj[kTileNnz / kThreads];
+#pragma unroll
+    for (int j = 0; j < kTileNnz / kThreads; ++j) {
+      const int k = s + tid + j * kThreads;
+      if (k < e) {
+        cj[j] = __ldcs(ci + k);
+        vj[j] = __ldcs(va + k);
       }
     }
-    for (int t = tid; t <= nr; t += kThreads) srp[t] = __ldg(rp + r0 + t) - as;
-    cp_async_commit_wait_all();
+#pragma unroll
+    for (int j = 0; j < kTileNnz / kThreads; ++j)
+      if (s + tid + j * kThreads < e) xj[j] = __ldg(x + cj[j]);
+#pragma unroll
+    for (int j = 0; j < kTileNnz / kThreads; ++j)
+      if (s + tid + j * kThreads < e) sprod[tid + j * kThreads] = mul(vj[j], xj[j]);
+    for (int t = tid; t <= nr; t += kThreads) srp[t] = __ldg(rp + r0 + t) - s;
     __syncthreads();
     const int L = lanes[blockIdx.x];
     if (L == 1) {
       if (tid < nr) {
         const int a = srp[tid], b = srp[tid + 1];
         T sum = T(0);
-        for (int k = a; k < b; k += 8) {
-          T xv[8], vv[8];
-#pragma unroll
-          for (int j = 0; j < 8; ++j) {
-            if (k + j < b) {
-              xv[j] = __ldg(x + scol[k + j]);
-              vv[j] = sval[k + j];
-            }
-          }
-#pragma unroll
-          for (int j = 0; j < 8; ++j)
-            if (k + j < b) sum = add(sum, mul(vv[j], xv[j]));
-        }
+        for (int k = a; k < b; ++k) sum = add(sum, sprod[k]);
         epi(r0 + tid, sum, red);
       }
     } else {
@@ -233,19 +229,7 @@ csr_spmv_kernel(const int* __restrict__ rp, const int* __restrict__ ci,
         T sum = T(0);
         if (row < nr) {
           const int a = srp[row], b = srp[row + 1];
-          for (int k = a + lane; k < b; k += 4 * L) {
-            T xv[4], vv[4];
-#pragma unroll
-            for (int j = 0; j < 4; ++j) {
-              if (k + j * L < b) {
-                xv[j] = __ldg(x + scol[k + j * L]);
-                vv[j] = sval[k + j * L];
-              }
-            }
-#pragma unroll
-            for (int j = 0; j < 4; ++j)
-              if (k + j * L < b) sum = add(sum, mul(vv[j], xv[j]));
-          }
+          for (int k = a + lane; k < b; k += L) sum = add(sum, sprod[k]);
         }
         for (int off = L >> 1; off > 0; off >>= 1)
           sum = add(sum, __shfl_xor_sync(0xffffffffu, sum, off));

@@ -1,0 +1,17 @@
+// sk_learned.cuh -- entry points of the learned preconditioner used by the
+// preconditioner dispatch (sk_ops.cu) and the FGMRES driver.
+#pragma once
+
+#include "sk_internal.cuh"
+
+namespace sk {
+
+// z = s * net(features(v)) for an FP64 vector on the precond's grid.
+sk_status learned_apply(const sk_precond_s* M, const double* v, double* z, cudaStream_t st);
+// Frees the coefficient planes of a learned preconditioner.
+void learned_release(sk_precond_s* M);
+// Coefficient planes (d, w, e, s, n, 1/d) of a 5-point FP64 CSR matrix on
+// an nx x ny grid; SK_INVALID_ARG when the matrix is not such a stencil.
+sk_status grid_planes(sk_matrix A, int64_t nx, int64_t ny, float* coef, cudaStream_t st);
+
+}  // namespace sk

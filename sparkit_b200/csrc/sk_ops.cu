@@ -3,6 +3,7 @@
 #include <mutex>
 #include <vector>
 
+#include "sk_learned.cuh"
 #include "sk_vec.cuh"
 
 namespace sk {
@@ -86,6 +87,10 @@ static void precond_apply_t(const sk_precond_s* M, i64 n, const T* r, T* z, RedW
     launch_vec(n, OpCopy<T>{r, z}, ws, sc, st);
   } else if (M->kind == 1) {
     launch_vec(n, OpJacobi<T>{static_cast<const T*>(M->inv_diag), r, z}, ws, sc, st);
+  } else if (M->kind == 3) {
+    if constexpr (sizeof(T) == 8) {
+      if (learned_apply(M, r, z, st) != SK_OK) set_error("learned preconditioner apply failed");
+    }
   } else {
     chebyshev_apply_device<T>(M, r, z, static_cast<T*>(M->work), ws, sc, st);
   }
@@ -288,6 +293,12 @@ sk_status sk_precond_apply(sk_precond M, int64_t n, const void* r_dev, void* z_d
   cudaStream_t cs = M ? pick_stream(M->A, s) : static_cast<cudaStream_t>(s);
   // NULL preconditioner: identity on the FP64 path unless told otherwise.
   sk_dtype dt = M ? M->dtype : SK_F64;
+  if (M && M->kind == 3) {
+    sk_status ls = learned_apply(M, static_cast<const double*>(r_dev), static_cast<double*>(z_dev), cs);
+    if (ls != SK_OK) return ls;
+    SK_CUDA(cudaGetLastError());
+    return SK_OK;
+  }
   precond_apply_dispatch(M, dt, n, r_dev, z_dev, RedWs{}, nullptr, cs);
   SK_CUDA(cudaGetLastError());
   return SK_OK;
@@ -319,6 +330,7 @@ sk_status sk_precond_values(sk_precond M, void* host_out, int64_t capacity, int6
 sk_status sk_precond_destroy(sk_precond M) {
   if (!M) return SK_OK;
   // cudaFree waits for the device; the matrix M->A may already be gone.
+  if (M->kind == 3) learned_release(M);
   if (M->inv_diag) cudaFree(M->inv_diag);
   if (M->inv_diag32) cudaFree(M->inv_diag32);
   if (M->work) cudaFree(M->work);

@@ -743,6 +743,7 @@ struct EpiFgInit {
     for (int i = 0; i < m; ++i) sm.cs[i] = sm.sn[i] = 0.0;
     for (int i = 0; i <= m; ++i) sm.g[i] = 0.0;
     sm.g[0] = static_cast<double>(beta);
+    sc->beta_cycle = static_cast<double>(beta);
     sc->jfinal = 0;
     sc->done = 0;
     sc->beta0 = 0;
@@ -921,10 +922,15 @@ struct OpFgUpdateX {
   __device__ void finalize(const double*) const {}
 };
 
+// With `fallback` non-null, a restart cycle whose residual estimate ends
+// above stall_ratio times the cycle's starting residual switches the
+// preconditioner to `fallback` for the rest of the solve; *switched_at
+// receives the first cycle run with it (-1: never switched).
 template <typename T>
 static sk_status fgmres_solve(sk_matrix A, sk_precond M, const T* b, T* x,
                               const sk_fgmres_config* cfg, sk_summary* out, double* history_host,
-                              cudaStream_t st) {
+                              cudaStream_t st, sk_precond fallback = nullptr, double stall_ratio = 0.0,
+                              int64_t* switched_at = nullptr) {
   const i64 n = A->nrow;
   const int m = static_cast<int>(cfg->restart_dimension);
   SK_CHECK(m >= 1 && m <= 4096, SK_INVALID_ARG, "restart_dimension must be in [1, 4096]");
@@ -966,6 +972,8 @@ static sk_status fgmres_solve(sk_matrix A, sk_precond M, const T* b, T* x,
   h.hist_on = cfg->collect_residuals ? 1 : 0;
   if ((s = put_scalars(c.sc, h, st)) != SK_OK) return s;
   const int um1 = m + 1;
+  if (switched_at) *switched_at = -1;
+  int64_t cycle = 0;
   while (h.iters < cfg->max_iterations && !h.converged) {
     launch_spmv<T>(A, x, EpiFgInit<T>{b, V, c.sc, sm, m}, c.ws, nullptr, st);
     launch_vec(n, OpFgScale<T>{V, nullptr, T(0)}, c.ws, c.sc, st);
@@ -990,6 +998,11 @@ static sk_status fgmres_solve(sk_matrix A, sk_precond M, const T* b, T* x,
     launch_vec(n, OpFgUpdateX<T>{x, Z, ldv, sm.y, 0}, c.ws, c.sc, st);
     SK_CUDA(cudaGetLastError());
     if ((s = read_scalars(c.sc, &h, st)) != SK_OK) return s;
+    ++cycle;
+    if (fallback && M != fallback && !h.converged && h.rnorm > stall_ratio * h.beta_cycle) {
+      M = fallback;
+      if (switched_at) *switched_at = cycle;
+    }
   }
   return finish_summary(c, st, out, history_host);
 }
@@ -1336,6 +1349,21 @@ sk_status sk_fgmres_solve(sk_matrix A, sk_precond M, const void* b_dev, void* x_
                                 out, history_host, cs);
   return fgmres_solve<float>(A, M, static_cast<const float*>(b_dev), static_cast<float*>(x_dev), cfg, out,
                              history_host, cs);
+}
+
+sk_status sk_fgmres_fallback_solve(sk_matrix A, sk_precond M, sk_precond fallback, const double* b_dev,
+                                   double* x_dev, const sk_fgmres_config* cfg, double stall_ratio,
+                                   sk_summary* out, double* history_host, int64_t* switched_at, sk_stream s) {
+  sk_status st = check_solver_args(A, M, fallback, b_dev, x_dev);
+  if (st != SK_OK) return st;
+  SK_CHECK(cfg && out && M, SK_INVALID_ARG, "null config, summary or preconditioner");
+  SK_CHECK(A->dtype == SK_F64, SK_INVALID_ARG, "the fallback driver solves in FP64");
+  SK_CHECK(cfg->max_iterations >= 0, SK_INVALID_ARG, "negative max_iterations");
+  cudaStream_t cs = pick_stream(A, s);
+  st = fgmres_solve<double>(A, M, b_dev, x_dev, cfg, out, history_host, cs, fallback, stall_ratio, switched_at);
+  if (st != SK_OK) return st;
+  if (M->kind == 3) return sk_net_status(M->net);
+  return SK_OK;
 }
 
 sk_status sk_cg_solve_host(sk_matrix A, sk_precond left, sk_precond right, const void* b_host,

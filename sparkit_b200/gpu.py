@@ -368,6 +368,165 @@ def mixed_cg(b, x, cfg, op, jacobi_inner=True):
     return out
 
 
+# ------------------------------------------------------------------
+# Learned variable preconditioner of FGMRES (no reference counterpart:
+# fgmres.hpp:452-470 takes any callable as its variable preconditioner)
+# ------------------------------------------------------------------
+
+class Net:
+    """The convolutional encoder-decoder of the learned preconditioner
+    (sk_net_create): seeded He initialisation, FP32 master weights, BF16
+    copies for the tensor-core convolutions."""
+
+    def __init__(self, seed=0):
+        h = ctypes.c_void_p()
+        check(lib().sk_net_create(ctypes.byref(h), int(seed)))
+        self.handle = h
+
+    @staticmethod
+    def param_count():
+        return int(lib().sk_net_param_count())
+
+    def params(self):
+        out = np.empty(self.param_count(), dtype=np.float32)
+        check(lib().sk_net_get_params(self.handle, _ptr(out), out.size))
+        return out
+
+    def set_params(self, p):
+        p = np.ascontiguousarray(p, dtype=np.float32)
+        check(lib().sk_net_set_params(self.handle, _ptr(p), p.size))
+
+    def set_legacy_mma(self, on):
+        """Test hook: the convolutions on mma.sync instead of tcgen05."""
+        check(lib().sk_net_set_legacy_mma(self.handle, int(bool(on))))
+
+    def loss_grad(self, pairs, idx, mu=0.0):
+        """Loss of the batch of pair indices `idx` and its FP32 gradient."""
+        idx = np.ascontiguousarray(idx, dtype=np.int32)
+        loss = ctypes.c_double()
+        g = np.empty(self.param_count(), dtype=np.float32)
+        check(lib().sk_net_loss_grad(self.handle, pairs.handle, _ptr(idx), idx.size, float(mu), ctypes.byref(loss),
+                                     _ptr(g), g.size))
+        return loss.value, g
+
+    def train(self, pairs, cfg):
+        c = _lib.TrainConfig(cfg.steps, cfg.batch, cfg.lr, cfg.lr_final_ratio, cfg.beta1, cfg.beta2, cfg.eps,
+                             cfg.mu, cfg.seed)
+        s = _lib.TrainSummary()
+        hist = np.zeros(max(cfg.steps, 1))
+        check(lib().sk_net_train(self.handle, pairs.handle, ctypes.byref(c), ctypes.byref(s), _ptr(hist)))
+        return Train_summary(s.first_loss, s.last_loss, s.ms, s.steps, hist[: s.steps].tolist())
+
+    def close(self):
+        if getattr(self, "handle", None) and not _lib.shutting_down():
+            lib().sk_net_destroy(self.handle)
+        self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Pairs:
+    """(residual, error) training pairs on an nx x ny grid (sk_pairs_*)."""
+
+    def __init__(self, nx, ny, capacity, max_instances):
+        h = ctypes.c_void_p()
+        check(lib().sk_pairs_create(ctypes.byref(h), int(nx), int(ny), int(capacity), int(max_instances)))
+        self.handle, self.nx, self.ny = h, nx, ny
+
+    def add_instance(self, Ad):
+        i = ctypes.c_int32()
+        check(lib().sk_pairs_add_instance(self.handle, Ad.handle, ctypes.byref(i)))
+        return i.value
+
+    def add(self, instance, r, e):
+        check(lib().sk_pairs_add(self.handle, int(instance), _ptr(r), _ptr(e), _stream_of(r)))
+
+    def harvest(self, instance, Ad, b, xstar, restart=30, cycles=100):
+        """Pairs from the plain Jacobi-FGMRES(restart) run on Ad x = b from
+        x = 0, one per restart cycle (b, xstar: FP64 CUDA tensors)."""
+        n = ctypes.c_int64()
+        check(lib().sk_learned_harvest(self.handle, int(instance), Ad.handle, _ptr(b), _ptr(xstar), int(restart),
+                                       int(cycles), ctypes.byref(n)))
+        return n.value
+
+    def __len__(self):
+        n = ctypes.c_int64()
+        check(lib().sk_pairs_count(self.handle, ctypes.byref(n)))
+        return n.value
+
+    def close(self):
+        if getattr(self, "handle", None) and not _lib.shutting_down():
+            lib().sk_pairs_destroy(self.handle)
+        self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+@dataclass
+class Train_config:
+    steps: int = 1000
+    batch: int = 4
+    lr: float = 1e-3
+    lr_final_ratio: float = 0.1
+    beta1: float = 0.9
+    beta2: float = 0.999
+    eps: float = 1e-8
+    mu: float = 0.0
+    seed: int = 0
+
+
+@dataclass
+class Train_summary:
+    first_loss: float
+    last_loss: float
+    ms: float
+    steps: int
+    loss_history: List[float] = field(default_factory=list)
+
+
+class learned_preconditioner(_Precond):
+    """The trained network as the variable preconditioner of the FP64 CSR
+    5-point matrix Ad on an nx x ny grid (row y * nx + x)."""
+
+    def __init__(self, Ad, net, nx, ny):
+        h = ctypes.c_void_p()
+        check(lib().sk_learned_create(ctypes.byref(h), Ad.handle, net.handle, int(nx), int(ny)))
+        super().__init__(h, Ad, Ad.shape()[0])
+        self.net = net  # keeps the network alive
+
+    def planes(self):
+        out = np.empty(6 * self.n, dtype=np.float32)
+        check(lib().sk_learned_planes(self.handle, _ptr(out), out.size))
+        return out.reshape(6, self.n)
+
+
+def fgmres_fallback(b, x, cfg, op, preconditioner, fallback, stall_ratio=0.9):
+    """fgmres with a variable preconditioner and an automatic fallback:
+    after a restart cycle whose residual estimate stays above stall_ratio
+    times its start, the rest of the solve uses `fallback`.  b, x: FP64
+    CUDA tensors.  Returns (Summary, first cycle on the fallback or -1)."""
+    Ad = _op_matrix(op)
+    c = _lib.FgmresConfig(cfg.tolerance, cfg.restart_dimension, cfg.max_iterations, int(cfg.collect_residuals))
+    s = _lib.Summary()
+    sw = ctypes.c_int64()
+    hist = np.zeros(max(cfg.max_iterations, 1)) if cfg.collect_residuals else None
+    check(lib().sk_fgmres_fallback_solve(Ad.handle, _handle(preconditioner), _handle(fallback), _ptr(b), _ptr(x),
+                                         ctypes.byref(c), float(stall_ratio), ctypes.byref(s), _ptr(hist),
+                                         ctypes.byref(sw), _stream_of(b)))
+    out = Summary(s.residual_norm, s.computed_iterations, bool(s.converged), [], s.status)
+    if hist is not None:
+        out.iteration_residuals = hist[: s.history_length].tolist()
+    return out, sw.value
+
+
 @dataclass
 class Batch_config:
     """Settings of sk_batched_cg_solve."""

@@ -241,6 +241,83 @@ def diffusion_3d_grf(n, sigma=2.0, corr_len=8.0, seed=0, dtype=np.float64):
     return _stencil_csr(N, cand, vals, valid, dtype)
 
 
+def convdiff_2d_grf(n, sigma=1.0, corr_len=None, peclet=None, pe_range=(1.0, 100.0), seed=0,
+                    dtype=np.float64):
+    """2-D convection-diffusion on an n x n grid (row y * n + x),
+    finite-volume with first-order upwind convection and homogeneous
+    Dirichlet boundaries (the variable-coefficient generalisation of
+    matgen.hpp:276-330, whose constant-coefficient form has no boundary
+    terms).
+
+    * Diffusion k = exp(g) per cell, g a Gaussian random field (sigma,
+      correlation length corr_len cells, default n / 32); interior faces take
+      the harmonic mean of their two cells, boundary faces the cell value.
+    * Velocity from a seeded stream function psi on the cell corners (a
+      Gaussian random field of correlation length n / 8 times
+      sin(pi i / n) sin(pi j / n), so that it vanishes on the boundary):
+      u = d psi / dy on vertical faces, v = -d psi / dx on horizontal faces,
+      which is exactly divergence-free discretely and has no flow through
+      the boundary.
+    * Scale: the median cell Peclet number |u_f| / k_f over the interior
+      faces is `peclet`, drawn log-uniformly from pe_range when None.
+
+    Row P: A_PP = sum_f k_f + sum_f max(F_f, 0), A_PQ = -k_f + min(F_f, 0)
+    with F_f the outward flux through face f.  Returns (A, info) with the
+    Peclet target and the coefficient fields."""
+    rng = np.random.default_rng(seed)
+    if corr_len is None:
+        corr_len = max(n / 32.0, 1.0)
+    g = gaussian_random_field((n, n), sigma, corr_len, seed=int(rng.integers(1 << 31)))
+    kc = np.exp(g)  # [y, x]
+    psi = gaussian_random_field((n + 1, n + 1), 1.0, max(n / 8.0, 1.0), seed=int(rng.integers(1 << 31)))
+    w = np.sin(np.pi * np.arange(n + 1) / n)
+    psi = psi * w[:, None] * w[None, :]  # psi[b, a] at corner (x = a, y = b)
+    # vertical face between cells (x-1, y) and (x, y): x = 1..n-1 -> u[y, x]
+    u = psi[1:, :] - psi[:-1, :]       # [n, n+1]: face at corner column a, cell row y
+    v = -(psi[:, 1:] - psi[:, :-1])    # [n+1, n]: face at corner row b, cell column x
+    kx = 2.0 * kc[:, :-1] * kc[:, 1:] / (kc[:, :-1] + kc[:, 1:])  # interior vertical faces [n, n-1]
+    ky = 2.0 * kc[:-1, :] * kc[1:, :] / (kc[:-1, :] + kc[1:, :])  # interior horizontal faces [n-1, n]
+    pe_faces = np.concatenate([np.abs(u[:, 1:-1]).ravel() / kx.ravel(), np.abs(v[1:-1, :]).ravel() / ky.ravel()])
+    med = np.median(pe_faces)
+    if peclet is None:
+        peclet = float(np.exp(rng.uniform(np.log(pe_range[0]), np.log(pe_range[1]))))
+    scale = peclet / med if med > 0 else 0.0
+    u *= scale
+    v *= scale
+    N = n * n
+    diag = np.zeros((n, n))
+    offW = np.zeros((n, n))
+    offE = np.zeros((n, n))
+    offS = np.zeros((n, n))
+    offN = np.zeros((n, n))
+    # east faces of cells x = 0..n-2 (interior), flux out = u[:, x+1]
+    Fe = u[:, 1:-1]
+    diag[:, :-1] += kx + np.maximum(Fe, 0.0)
+    offE[:, :-1] = -kx + np.minimum(Fe, 0.0)
+    # west faces of cells x = 1..n-1, outward flux = -u[:, x]
+    Fw = -u[:, 1:-1]
+    diag[:, 1:] += kx + np.maximum(Fw, 0.0)
+    offW[:, 1:] = -kx + np.minimum(Fw, 0.0)
+    Fn = v[1:-1, :]
+    diag[:-1, :] += ky + np.maximum(Fn, 0.0)
+    offN[:-1, :] = -ky + np.minimum(Fn, 0.0)
+    Fs = -v[1:-1, :]
+    diag[1:, :] += ky + np.maximum(Fs, 0.0)
+    offS[1:, :] = -ky + np.minimum(Fs, 0.0)
+    # Dirichlet boundary faces: the cell coefficient
+    diag[:, 0] += kc[:, 0]
+    diag[:, -1] += kc[:, -1]
+    diag[0, :] += kc[0, :]
+    diag[-1, :] += kc[-1, :]
+    node = np.arange(N, dtype=np.int64)
+    r, c = node // n, node % n
+    cand = np.stack([node - n, node - 1, node, node + 1, node + n], axis=1)
+    valid = np.stack([r > 0, c > 0, np.ones(N, bool), c + 1 < n, r + 1 < n], axis=1)
+    vals = np.stack([offS.ravel(), offW.ravel(), diag.ravel(), offE.ravel(), offN.ravel()], axis=1)
+    A = _stencil_csr(N, cand, vals, valid, dtype)
+    return A, {"peclet": peclet, "k": kc, "u": u, "v": v}
+
+
 def batched_spd_systems(count=4096, nmin=1000, nmax=65536, shift=(0.0, 0.5), seed=0):
     """`count` independent SPD systems: each a 2-D 5-point or 3-D 7-point
     Dirichlet Laplacian (seeded coin) plus a diagonal shift U[shift], with
