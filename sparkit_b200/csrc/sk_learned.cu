@@ -46,6 +46,8 @@
 #include <chrono>
 #include <cmath>
 #include <cstring>
+#include <array>
+#include <map>
 #include <mutex>
 #include <random>
 #include <set>
@@ -200,6 +202,19 @@ __device__ __forceinline__ void mma16816(float (&d)[4], const uint32_t (&a)[4], 
 // ------------------------------------------------------------------
 // Convolution (forward, or input gradient with flipped weights)
 // ------------------------------------------------------------------
+__device__ __forceinline__ void unpack8(uint4 u, float (&f)[8]) {
+  const bf16* h = reinterpret_cast<const bf16*>(&u);
+#pragma unroll
+  for (int j = 0; j < 8; ++j) f[j] = __bfloat162float(h[j]);
+}
+__device__ __forceinline__ uint4 pack8(const float (&f)[8]) {
+  uint4 u;
+  bf16* h = reinterpret_cast<bf16*>(&u);
+#pragma unroll
+  for (int j = 0; j < 8; ++j) h[j] = __float2bfloat16_rn(f[j]);
+  return u;
+}
+
 enum ConvOut : int { OUT_BF16 = 0, OUT_F32 = 1, OUT_Z64 = 2 };
 
 struct ConvArgs {
@@ -210,33 +225,44 @@ struct ConvArgs {
   const bf16* mask;     // null: none; else out = 0 where mask <= 0 (same layout as out)
   int out_kind;
   bf16* out;            // OUT_BF16: [B][H][W][N]
+  bf16* pool_out;       // OUT_BF16, optional: 2x2 average of out, [B][H/2][W/2][N]
+  const bf16* up_skip;  // OUT_BF16, optional: up_out = up(out) + up_skip at [B][2H][2W][N]
+  bf16* up_out;
   float* outf;          // OUT_F32: channel 0 only, [B][H][W]
   double* outz;         // OUT_Z64: z = s[b] * (float)(acc0 + bias0)
   const double* scale;  // OUT_Z64: s per sample
   int* err;
 };
 
+// Thread = output pixel (x, y) of sample b with its N accumulators v.  All
+// threads of the CTA call it (the 2x2 pooling exchanges values between the
+// lanes of a warp: x + 1 is lane + 1, y + 1 is lane + 8).
 template <int N>
 __device__ __forceinline__ void conv_epilogue(ConvArgs const& a, int b, int y, int x, const float* v) {
-  if (y >= a.H || x >= a.W) return;
+  const bool valid = y < a.H && x < a.W;
   const i64 p = (static_cast<i64>(b) * a.H + y) * a.W + x;
   if (a.out_kind == OUT_F32) {
-    a.outf[p] = v[0] + (a.bias ? a.bias[0] : 0.0f);
+    if (valid) a.outf[p] = v[0] + (a.bias ? a.bias[0] : 0.0f);
     return;
   }
   if (a.out_kind == OUT_Z64) {
-    const float yv = v[0] + (a.bias ? a.bias[0] : 0.0f);
-    a.outz[p] = a.scale[b] * static_cast<double>(yv);
+    if (valid) {
+      const float yv = v[0] + (a.bias ? a.bias[0] : 0.0f);
+      a.outz[p] = a.scale[b] * static_cast<double>(yv);
+    }
     return;
   }
   uint4* dst = reinterpret_cast<uint4*>(a.out + p * N);
-  const uint4* msk = a.mask ? reinterpret_cast<const uint4*>(a.mask + p * N) : nullptr;
+  const uint4* msk = (a.mask && valid) ? reinterpret_cast<const uint4*>(a.mask + p * N) : nullptr;
+  const bool pool_writer = valid && ((x & 1) == 0) && ((y & 1) == 0);
+  const int h2 = a.H / 2, w2 = a.W / 2;
 #pragma unroll
   for (int c = 0; c < N / 8; ++c) {
     uint4 mv = msk ? msk[c] : make_uint4(0, 0, 0, 0);
     const bf16* mb = reinterpret_cast<const bf16*>(&mv);
     uint4 o;
     bf16* ob = reinterpret_cast<bf16*>(&o);
+    float r[8];
 #pragma unroll
     for (int j = 0; j < 8; ++j) {
       float t = v[c * 8 + j];
@@ -244,8 +270,33 @@ __device__ __forceinline__ void conv_epilogue(ConvArgs const& a, int b, int y, i
       if (a.relu) t = fmaxf(t, 0.0f);
       if (msk && !(__bfloat162float(mb[j]) > 0.0f)) t = 0.0f;
       ob[j] = __float2bfloat16_rn(t);
+      r[j] = __bfloat162float(ob[j]);
     }
-    dst[c] = o;
+    if (valid) dst[c] = o;
+    if (a.pool_out) {
+      float q[8];
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        const float r01 = __shfl_down_sync(0xffffffffu, r[j], 1);
+        const float r10 = __shfl_down_sync(0xffffffffu, r[j], 8);
+        const float r11 = __shfl_down_sync(0xffffffffu, r[j], 9);
+        q[j] = 0.25f * ((r[j] + r01) + (r10 + r11));
+      }
+      if (pool_writer)
+        reinterpret_cast<uint4*>(a.pool_out)[((static_cast<i64>(b) * h2 + y / 2) * w2 + x / 2) * (N / 8) + c] =
+            pack8(q);
+    }
+    if (a.up_out && valid) {
+#pragma unroll
+      for (int d = 0; d < 4; ++d) {
+        const i64 fp = (static_cast<i64>(b) * 2 * a.H + 2 * y + (d >> 1)) * (2 * a.W) + 2 * x + (d & 1);
+        float sk[8], u[8];
+        unpack8(reinterpret_cast<const uint4*>(a.up_skip)[fp * (N / 8) + c], sk);
+#pragma unroll
+        for (int j = 0; j < 8; ++j) u[j] = r[j] + sk[j];
+        reinterpret_cast<uint4*>(a.up_out)[fp * (N / 8) + c] = pack8(u);
+      }
+    }
   }
 }
 
@@ -542,59 +593,6 @@ __global__ void wgrad_reduce_kernel(const float* part, const float* bpart, int n
 // ------------------------------------------------------------------
 // Element-wise kernels over NHWC BF16 tensors (8 channels per thread)
 // ------------------------------------------------------------------
-__device__ __forceinline__ void unpack8(uint4 u, float (&f)[8]) {
-  const bf16* h = reinterpret_cast<const bf16*>(&u);
-#pragma unroll
-  for (int j = 0; j < 8; ++j) f[j] = __bfloat162float(h[j]);
-}
-__device__ __forceinline__ uint4 pack8(const float (&f)[8]) {
-  uint4 u;
-  bf16* h = reinterpret_cast<bf16*>(&u);
-#pragma unroll
-  for (int j = 0; j < 8; ++j) h[j] = __float2bfloat16_rn(f[j]);
-  return u;
-}
-
-// out[B][H/2][W/2][C] = avg of 2x2
-__global__ void pool_kernel(int B, int H, int W, int C, const bf16* in, bf16* out) {
-  const int h = H / 2, w = W / 2, cc = C / 8;
-  const i64 total = static_cast<i64>(B) * h * w * cc;
-  for (i64 i = blockIdx.x * static_cast<i64>(blockDim.x) + threadIdx.x; i < total;
-       i += static_cast<i64>(gridDim.x) * blockDim.x) {
-    const int c = static_cast<int>(i % cc);
-    const i64 pix = i / cc;
-    const int x = static_cast<int>(pix % w), y = static_cast<int>((pix / w) % h), b = static_cast<int>(pix / (static_cast<i64>(w) * h));
-    const uint4* src = reinterpret_cast<const uint4*>(in);
-    const i64 base = ((static_cast<i64>(b) * H + 2 * y) * W + 2 * x) * cc + c;
-    float p00[8], p01[8], p10[8], p11[8], o[8];
-    unpack8(src[base], p00);
-    unpack8(src[base + cc], p01);
-    unpack8(src[base + static_cast<i64>(W) * cc], p10);
-    unpack8(src[base + static_cast<i64>(W) * cc + cc], p11);
-#pragma unroll
-    for (int j = 0; j < 8; ++j) o[j] = 0.25f * ((p00[j] + p01[j]) + (p10[j] + p11[j]));
-    reinterpret_cast<uint4*>(out)[i] = pack8(o);
-  }
-}
-
-// out[B][H][W][C] = up(coarse) + skip
-__global__ void upadd_kernel(int B, int H, int W, int C, const bf16* coarse, const bf16* skip, bf16* out) {
-  const int cc = C / 8, h = H / 2, w = W / 2;
-  const i64 total = static_cast<i64>(B) * H * W * cc;
-  for (i64 i = blockIdx.x * static_cast<i64>(blockDim.x) + threadIdx.x; i < total;
-       i += static_cast<i64>(gridDim.x) * blockDim.x) {
-    const int c = static_cast<int>(i % cc);
-    const i64 pix = i / cc;
-    const int x = static_cast<int>(pix % W), y = static_cast<int>((pix / W) % H), b = static_cast<int>(pix / (static_cast<i64>(W) * H));
-    float a[8], s[8], o[8];
-    unpack8(reinterpret_cast<const uint4*>(coarse)[((static_cast<i64>(b) * h + y / 2) * w + x / 2) * cc + c], a);
-    unpack8(reinterpret_cast<const uint4*>(skip)[i], s);
-#pragma unroll
-    for (int j = 0; j < 8; ++j) o[j] = a[j] + s[j];
-    reinterpret_cast<uint4*>(out)[i] = pack8(o);
-  }
-}
-
 // g[B][H/2][W/2][C] = (act > 0) ? sum of the 4 fine gradients : 0
 __global__ void upadd_bwd_kernel(int B, int H, int W, int C, const bf16* dfine, const bf16* act, bf16* g) {
   const int h = H / 2, w = W / 2, cc = C / 8;
@@ -975,11 +973,29 @@ static sk_status make_map(CUtensorMap* m, const void* base, int B, int H, int W,
   return SK_OK;
 }
 
+// Encoded maps by (address, shape, box), so that repeated applies encode
+// nothing; the entries stay valid for as long as the buffer keeps its shape.
+struct MapCache {
+  std::map<std::array<long long, 7>, CUtensorMap> maps;
+  sk_status get(const void* base, int B, int H, int W, int C, int bw, int bh, CUtensorMap* out) {
+    const std::array<long long, 7> key{reinterpret_cast<long long>(base), B, H, W, C, bw, bh};
+    auto it = maps.find(key);
+    if (it != maps.end()) {
+      *out = it->second;
+      return SK_OK;
+    }
+    if (maps.size() > 512) maps.clear();
+    sk_status s = make_map(out, base, B, H, W, C, bw, bh);
+    if (s == SK_OK) maps.emplace(key, *out);
+    return s;
+  }
+};
+
 template <int CIN, int N, bool TC>
-static sk_status launch_conv(const void* in, ConvArgs const& a, cudaStream_t st) {
+static sk_status launch_conv(MapCache& mc, const void* in, ConvArgs const& a, cudaStream_t st) {
   using S = ConvSmem<CIN, N, TC>;
   CUtensorMap m;
-  sk_status s = make_map(&m, in, a.B, a.H, a.W, CIN, kHaloW, kHaloH);
+  sk_status s = mc.get(in, a.B, a.H, a.W, CIN, kHaloW, kHaloH, &m);
   if (s != SK_OK) return s;
   if (!attr_once(conv3x3_kernel<CIN, N, TC>, S::kBytes)) return fail(SK_CUDA_ERROR, "cudaFuncSetAttribute");
   dim3 grid(ceil_div(a.W, kTileW), ceil_div(a.H, kTileH), a.B);
@@ -989,9 +1005,9 @@ static sk_status launch_conv(const void* in, ConvArgs const& a, cudaStream_t st)
 }
 
 template <bool TC>
-static sk_status conv_dispatch(int cin, int n, const void* in, ConvArgs const& a, cudaStream_t st) {
+static sk_status conv_dispatch(MapCache& mc, int cin, int n, const void* in, ConvArgs const& a, cudaStream_t st) {
 #define SK_CONV_CASE(CI, NN) \
-  if (cin == CI && n == NN) return launch_conv<CI, NN, TC>(in, a, st);
+  if (cin == CI && n == NN) return launch_conv<CI, NN, TC>(mc, in, a, st);
   SK_CONV_CASE(8, 16)
   SK_CONV_CASE(16, 16)
   SK_CONV_CASE(16, 32)
@@ -1004,11 +1020,11 @@ static sk_status conv_dispatch(int cin, int n, const void* in, ConvArgs const& a
 }
 
 template <int CI, int CO>
-static sk_status launch_wgrad(const void* x, const void* g, WgradArgs a, int nctas, cudaStream_t st) {
+static sk_status launch_wgrad(MapCache& mc, const void* x, const void* g, WgradArgs a, int nctas, cudaStream_t st) {
   CUtensorMap xm, gm;
-  sk_status s = make_map(&xm, x, a.B, a.H, a.W, CI, kHaloW, kHaloH);
+  sk_status s = mc.get(x, a.B, a.H, a.W, CI, kHaloW, kHaloH, &xm);
   if (s != SK_OK) return s;
-  if ((s = make_map(&gm, g, a.B, a.H, a.W, CO, kTileW, kTileH)) != SK_OK) return s;
+  if ((s = mc.get(g, a.B, a.H, a.W, CO, kTileW, kTileH, &gm)) != SK_OK) return s;
   const int bytes = (CI / 8) * kPlaneStride + (CO / 8) * kGPlaneBytes + 64;
   if (!attr_once(wgrad_kernel<CI, CO>, bytes)) return fail(SK_CUDA_ERROR, "cudaFuncSetAttribute");
   SK_LAUNCH((wgrad_kernel<CI, CO>), dim3(nctas, 9), kConvThreads, bytes, st, xm, gm, a);
@@ -1016,10 +1032,10 @@ static sk_status launch_wgrad(const void* x, const void* g, WgradArgs a, int nct
   return SK_OK;
 }
 
-static sk_status wgrad_dispatch(int ci, int co, const void* x, const void* g, WgradArgs a, int nctas,
-                                cudaStream_t st) {
+static sk_status wgrad_dispatch(MapCache& mc, int ci, int co, const void* x, const void* g, WgradArgs a,
+                                int nctas, cudaStream_t st) {
 #define SK_WG_CASE(CI, CO) \
-  if (ci == CI && co == CO) return launch_wgrad<CI, CO>(x, g, a, nctas, st);
+  if (ci == CI && co == CO) return launch_wgrad<CI, CO>(mc, x, g, a, nctas, st);
   SK_WG_CASE(8, 16)
   SK_WG_CASE(16, 32)
   SK_WG_CASE(32, 64)
@@ -1058,6 +1074,7 @@ struct sk_net_s {
   long long step = 0;
   int legacy_mma = 0;  // cross-check hook: convolutions on mma.sync
   sk_status host_err = SK_OK;  // first failed apply inside a solver (sticky until read)
+  MapCache maps;
   int* err = nullptr;
   // activation / gradient workspace for one (B, H, W)
   int B = 0, H = 0, W = 0;
@@ -1171,7 +1188,7 @@ static sk_status conv_fwd(sk_net N, int l, const bf16* in, int H, int W, ConvArg
   a.wpk = N->wf[l];
   a.bias = bias_of(N, l);
   a.err = N->err;
-  return conv_dispatch<TC>(kCin[l], pad_n(kCout[l]), in, a, N->stream);
+  return conv_dispatch<TC>(N->maps, kCin[l], pad_n(kCout[l]), in, a, N->stream);
 }
 
 static sk_status run_conv(sk_net N, int l, const bf16* in, int H, int W, ConvArgs a) {
@@ -1193,8 +1210,8 @@ static sk_status run_dgrad(sk_net N, int l, const bf16* g, int H, int W, bf16* o
   a.out = out;
   a.err = N->err;
   const int cin = pad_n(kCout[l]);
-  return N->legacy_mma ? conv_dispatch<false>(cin, kCin[l], g, a, N->stream)
-                       : conv_dispatch<true>(cin, kCin[l], g, a, N->stream);
+  return N->legacy_mma ? conv_dispatch<false>(N->maps, cin, kCin[l], g, a, N->stream)
+                       : conv_dispatch<true>(N->maps, cin, kCin[l], g, a, N->stream);
 }
 
 static sk_status run_wgrad(sk_net N, int l, const bf16* x, const bf16* g, int H, int W) {
@@ -1210,7 +1227,7 @@ static sk_status run_wgrad(sk_net N, int l, const bf16* x, const bf16* g, int H,
   const int ntiles = a.ntiles_x * a.ntiles_y * a.B;
   const int nctas = std::min(N->wg_ctas / 9 + 1, ntiles);
   const int co = pad_n(kCout[l]);
-  sk_status s = wgrad_dispatch(kCin[l], co, x, g, a, nctas, N->stream);
+  sk_status s = wgrad_dispatch(N->maps, kCin[l], co, x, g, a, nctas, N->stream);
   if (s != SK_OK) return s;
   const int total = 9 * kCout[l] * kCin[l] + kCout[l];
   SK_LAUNCH(wgrad_reduce_kernel, ceil_div(total, 256), 256, 0, N->stream, N->part, N->bpart, nctas, co, kCin[l],
@@ -1219,40 +1236,30 @@ static sk_status run_wgrad(sk_net N, int l, const bf16* x, const bf16* g, int H,
   return SK_OK;
 }
 
-static void ew_launch_pool(sk_net N, int H, int W, int C, const bf16* in, bf16* out) {
-  const i64 n = static_cast<i64>(N->B) * (H / 2) * (W / 2) * (C / 8);
-  SK_LAUNCH(pool_kernel, ew_grid(n), 256, 0, N->stream, N->B, H, W, C, in, out);
-}
-static void ew_launch_upadd(sk_net N, int H, int W, int C, const bf16* c, const bf16* s, bf16* out) {
-  const i64 n = static_cast<i64>(N->B) * H * W * (C / 8);
-  SK_LAUNCH(upadd_kernel, ew_grid(n), 256, 0, N->stream, N->B, H, W, C, c, s, out);
-}
-
-// Forward pass from N->x0; the last layer writes per `last`.
+// Forward pass from N->x0; the last layer writes per `last`.  Pooling and
+// the upsample-and-add of the skip connections run in the epilogues of the
+// convolutions that produce their inputs.
 static sk_status net_forward(sk_net N, ConvArgs last) {
   const int H = N->H, W = N->W, H1 = H / 2, W1 = W / 2, H2 = H / 4, W2 = W / 4, H3 = H / 8, W3 = W / 8;
   sk_status s;
-  auto fwd = [&](int l, const bf16* in, int h, int w, bf16* out) {
+  auto fwd = [&](int l, const bf16* in, int h, int w, bf16* out, bf16* pool, const bf16* skip, bf16* up) {
     ConvArgs a{};
     a.relu = 1;
     a.out_kind = OUT_BF16;
     a.out = out;
+    a.pool_out = pool;
+    a.up_skip = skip;
+    a.up_out = up;
     return run_conv(N, l, in, h, w, a);
   };
-  if ((s = fwd(0, N->x0, H, W, N->e0)) != SK_OK) return s;
-  ew_launch_pool(N, H, W, 16, N->e0, N->p0);
-  if ((s = fwd(1, N->p0, H1, W1, N->e1)) != SK_OK) return s;
-  ew_launch_pool(N, H1, W1, 32, N->e1, N->p1);
-  if ((s = fwd(2, N->p1, H2, W2, N->e2)) != SK_OK) return s;
-  ew_launch_pool(N, H2, W2, 64, N->e2, N->p2);
-  if ((s = fwd(3, N->p2, H3, W3, N->e3)) != SK_OK) return s;
-  if ((s = fwd(4, N->e3, H3, W3, N->b3)) != SK_OK) return s;
-  ew_launch_upadd(N, H2, W2, 64, N->b3, N->e2, N->u2);
-  if ((s = fwd(5, N->u2, H2, W2, N->d2)) != SK_OK) return s;
-  ew_launch_upadd(N, H1, W1, 32, N->d2, N->e1, N->u1);
-  if ((s = fwd(6, N->u1, H1, W1, N->d1)) != SK_OK) return s;
-  ew_launch_upadd(N, H, W, 16, N->d1, N->e0, N->u0);
-  if ((s = fwd(7, N->u0, H, W, N->d0)) != SK_OK) return s;
+  if ((s = fwd(0, N->x0, H, W, N->e0, N->p0, nullptr, nullptr)) != SK_OK) return s;
+  if ((s = fwd(1, N->p0, H1, W1, N->e1, N->p1, nullptr, nullptr)) != SK_OK) return s;
+  if ((s = fwd(2, N->p1, H2, W2, N->e2, N->p2, nullptr, nullptr)) != SK_OK) return s;
+  if ((s = fwd(3, N->p2, H3, W3, N->e3, nullptr, nullptr, nullptr)) != SK_OK) return s;
+  if ((s = fwd(4, N->e3, H3, W3, N->b3, nullptr, N->e2, N->u2)) != SK_OK) return s;
+  if ((s = fwd(5, N->u2, H2, W2, N->d2, nullptr, N->e1, N->u1)) != SK_OK) return s;
+  if ((s = fwd(6, N->u1, H1, W1, N->d1, nullptr, N->e0, N->u0)) != SK_OK) return s;
+  if ((s = fwd(7, N->u0, H, W, N->d0, nullptr, nullptr, nullptr)) != SK_OK) return s;
   last.relu = 0;
   return run_conv(N, 8, N->d0, H, W, last);
 }
@@ -1381,6 +1388,27 @@ sk_status learned_apply(const sk_precond_s* M, const double* v, double* z, cudaS
   s = net_forward(N, last);
   if (s != SK_OK && N->host_err == SK_OK) N->host_err = s;
   return s;
+}
+
+template <bool TC>
+static sk_status conv_attrs() {
+  bool ok = attr_once(conv3x3_kernel<8, 16, TC>, ConvSmem<8, 16, TC>::kBytes) &&
+            attr_once(conv3x3_kernel<16, 16, TC>, ConvSmem<16, 16, TC>::kBytes) &&
+            attr_once(conv3x3_kernel<16, 32, TC>, ConvSmem<16, 32, TC>::kBytes) &&
+            attr_once(conv3x3_kernel<32, 16, TC>, ConvSmem<32, 16, TC>::kBytes) &&
+            attr_once(conv3x3_kernel<32, 64, TC>, ConvSmem<32, 64, TC>::kBytes) &&
+            attr_once(conv3x3_kernel<64, 32, TC>, ConvSmem<64, 32, TC>::kBytes) &&
+            attr_once(conv3x3_kernel<64, 64, TC>, ConvSmem<64, 64, TC>::kBytes);
+  return ok ? SK_OK : fail(SK_CUDA_ERROR, "cudaFuncSetAttribute");
+}
+
+sk_status learned_prepare(const sk_precond_s* M) {
+  sk_net N = M->net;
+  N->stream = nullptr;
+  sk_status s = net_workspace(N, 1, static_cast<int>(M->grid_ny), static_cast<int>(M->grid_nx));
+  if (s != SK_OK) return s;
+  SK_CUDA(cudaStreamSynchronize(nullptr));
+  return N->legacy_mma ? conv_attrs<false>() : conv_attrs<true>();
 }
 
 void learned_release(sk_precond_s* M) {

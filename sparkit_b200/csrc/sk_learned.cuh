@@ -8,6 +8,9 @@ namespace sk {
 
 // z = s * net(features(v)) for an FP64 vector on the precond's grid.
 sk_status learned_apply(const sk_precond_s* M, const double* v, double* z, cudaStream_t st);
+// Allocates everything an apply on M's grid needs and sets the kernels'
+// attributes, so that applies can then be captured into a CUDA graph.
+sk_status learned_prepare(const sk_precond_s* M);
 // Frees the coefficient planes of a learned preconditioner.
 void learned_release(sk_precond_s* M);
 // Coefficient planes (d, w, e, s, n, 1/d) of a 5-point FP64 CSR matrix on

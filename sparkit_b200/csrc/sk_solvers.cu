@@ -12,8 +12,10 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <map>
 #include <vector>
 
+#include "sk_learned.cuh"
 #include "sk_vec.cuh"
 
 namespace sk {
@@ -973,37 +975,102 @@ static sk_status fgmres_solve(sk_matrix A, sk_precond M, const T* b, T* x,
   if ((s = put_scalars(c.sc, h, st)) != SK_OK) return s;
   const int um1 = m + 1;
   if (switched_at) *switched_at = -1;
-  int64_t cycle = 0;
-  while (h.iters < cfg->max_iterations && !h.converged) {
-    launch_spmv<T>(A, x, EpiFgInit<T>{b, V, c.sc, sm, m}, c.ws, nullptr, st);
-    launch_vec(n, OpFgScale<T>{V, nullptr, T(0)}, c.ws, c.sc, st);
-    const i64 m_eff = std::min<i64>(m, cfg->max_iterations - h.iters);  // :241-244
+  // One restart cycle (compute_initial_residual .. update_solution) as a
+  // fixed sequence of launches: every pointer is the same from cycle to
+  // cycle, and a converged solve turns the remaining kernels into no-ops.
+  auto enqueue_cycle = [&](cudaStream_t q, int m_eff, sk_precond P) {
+    launch_spmv<T>(A, x, EpiFgInit<T>{b, V, c.sc, sm, m}, c.ws, nullptr, q);
+    launch_vec(n, OpFgScale<T>{V, nullptr, T(0)}, c.ws, c.sc, q);
     for (int j = 0; j < m_eff; ++j) {
       T* Vj = V + j * ldv;
       T* Vj1 = V + (j + 1) * ldv;
       T* Zj = Z + j * ldv;
-      if (!alias_z) precond_apply_dispatch(M, A->dtype, n, Vj, Zj, c.ws, c.sc, st);
-      launch_spmv<T>(A, Zj, EpiFgW<T>{Vj1, V, sm.H + j * um1}, c.ws, c.sc, st);
+      if (!alias_z) precond_apply_dispatch(P, A->dtype, n, Vj, Zj, c.ws, c.sc, q);
+      launch_spmv<T>(A, Zj, EpiFgW<T>{Vj1, V, sm.H + j * um1}, c.ws, c.sc, q);
       for (int i = 0; i <= j; ++i) {
         const T* vnext = i < j ? V + (i + 1) * ldv : nullptr;
         launch_vec(n, OpFgMgs<T>{Vj1, V + i * ldv, vnext, sm.H + i + j * um1, sm.H + (i + 1) + j * um1, T(0)},
-                   c.ws, c.sc, st);
+                   c.ws, c.sc, q);
       }
-      launch_vec(n, OpFgScale<T>{Vj1, sm.H + (j + 1) + j * um1, T(0)}, c.ws, c.sc, st);
+      launch_vec(n, OpFgScale<T>{Vj1, sm.H + (j + 1) + j * um1, T(0)}, c.ws, c.sc, q);
       g_launches.fetch_add(1, std::memory_order_relaxed);
-      scalar_kernel<<<1, 1, 0, st>>>(FgGivens<T>{c.sc, c.hist, sm, j, m});
+      scalar_kernel<<<1, 1, 0, q>>>(FgGivens<T>{c.sc, c.hist, sm, j, m});
     }
     g_launches.fetch_add(1, std::memory_order_relaxed);
-    scalar_kernel<<<1, 1, 0, st>>>(FgBackSub<T>{c.sc, sm, m});
-    launch_vec(n, OpFgUpdateX<T>{x, Z, ldv, sm.y, 0}, c.ws, c.sc, st);
-    SK_CUDA(cudaGetLastError());
-    if ((s = read_scalars(c.sc, &h, st)) != SK_OK) return s;
+    scalar_kernel<<<1, 1, 0, q>>>(FgBackSub<T>{c.sc, sm, m});
+    launch_vec(n, OpFgUpdateX<T>{x, Z, ldv, sm.y, 0}, c.ws, c.sc, q);
+  };
+  // Solves expected to run several cycles replay each cycle as a CUDA graph
+  // (one launch per cycle instead of ~m^2 / 2), captured on a created stream
+  // (the legacy stream cannot be captured; the caller's stream is drained
+  // first and this call returns after its last host read).
+  const bool graphs = cfg->max_iterations >= 3 * static_cast<i64>(m) && n >= 1;
+  cudaStream_t gs = st;
+  if (graphs && (st == nullptr || st == cudaStreamLegacy || st == cudaStreamPerThread)) {
+    SK_CUDA(cudaStreamSynchronize(st));
+    gs = A->stream;
+  }
+  struct Exec { cudaGraphExec_t exec = nullptr; i64 launches = 0; };
+  std::map<int, Exec> execs;  // by m_eff
+  auto drop_graphs = [&]() {
+    for (auto& kv : execs) cudaGraphExecDestroy(kv.second.exec);
+    execs.clear();
+  };
+  int64_t cycle = 0;
+  while (h.iters < cfg->max_iterations && !h.converged) {
+    const int m_eff = static_cast<int>(std::min<i64>(m, cfg->max_iterations - h.iters));  // :241-244
+    if (graphs) {
+      auto it = execs.find(m_eff);
+      if (it == execs.end()) {
+        if (M && M->kind == 3 && (s = learned_prepare(M)) != SK_OK) {
+          drop_graphs();
+          return s;
+        }
+        const i64 before = g_launches.load();
+        cudaGraph_t g = nullptr;
+        Exec e;
+        cudaError_t ce = cudaStreamBeginCapture(gs, cudaStreamCaptureModeThreadLocal);
+        if (ce == cudaSuccess) {
+          enqueue_cycle(gs, m_eff, M);
+          ce = cudaStreamEndCapture(gs, &g);
+        }
+        if (ce == cudaSuccess) ce = cudaGraphInstantiate(&e.exec, g, 0);
+        if (g) cudaGraphDestroy(g);
+        if (ce != cudaSuccess) {
+          drop_graphs();
+          return cuda_fail(ce, "FGMRES cycle capture");
+        }
+        e.launches = g_launches.load() - before;
+        g_launches.fetch_sub(e.launches);  // counted at each replay instead
+        it = execs.emplace(m_eff, e).first;
+      }
+      g_launches.fetch_add(it->second.launches);
+      cudaError_t ce = cudaGraphLaunch(it->second.exec, gs);
+      if (ce != cudaSuccess) {
+        drop_graphs();
+        return cuda_fail(ce, "cudaGraphLaunch");
+      }
+    } else {
+      enqueue_cycle(gs, m_eff, M);
+    }
+    cudaError_t le = cudaGetLastError();
+    if (le != cudaSuccess) {
+      drop_graphs();
+      return cuda_fail(le, "FGMRES cycle");
+    }
+    if ((s = read_scalars(c.sc, &h, gs)) != SK_OK) {
+      drop_graphs();
+      return s;
+    }
     ++cycle;
     if (fallback && M != fallback && !h.converged && h.rnorm > stall_ratio * h.beta_cycle) {
       M = fallback;
+      drop_graphs();
       if (switched_at) *switched_at = cycle;
     }
   }
+  drop_graphs();
+  st = gs;
   return finish_summary(c, st, out, history_host);
 }
 
