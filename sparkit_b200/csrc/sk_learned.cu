@@ -660,7 +660,7 @@ struct SampleSrc {
   }
 };
 
-constexpr int kRedBlocks = 64;  // CTAs per sample of the per-sample reductions
+constexpr int kRedBlocks = 256;  // CTAs per sample of the per-sample reductions
 
 // s[b] = sqrt(mean((r * invd)^2)); grid (kRedBlocks, B), block kThreads.
 __global__ void __launch_bounds__(kThreads) scale_kernel(SampleSrc src, double* partial, unsigned* counter,
@@ -668,8 +668,16 @@ __global__ void __launch_bounds__(kThreads) scale_kernel(SampleSrc src, double* 
   const int b = blockIdx.y;
   const float* cf = src.planes(b);
   double acc[1] = {0.0};
-  for (i64 p = blockIdx.x * static_cast<i64>(blockDim.x) + threadIdx.x; p < src.P;
-       p += static_cast<i64>(gridDim.x) * blockDim.x) {
+  const i64 stride = static_cast<i64>(gridDim.x) * blockDim.x;
+  i64 p = blockIdx.x * static_cast<i64>(blockDim.x) + threadIdx.x;
+  for (; p + 3 * stride < src.P; p += 4 * stride) {  // 4 independent loads in flight
+    double rt[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) rt[u] = src.r(b, p + u * stride) * static_cast<double>(cf[5 * src.P + p + u * stride]);
+#pragma unroll
+    for (int u = 0; u < 4; ++u) acc[0] += rt[u] * rt[u];
+  }
+  for (; p < src.P; p += stride) {
     const double rt = src.r(b, p) * static_cast<double>(cf[5 * src.P + p]);
     acc[0] += rt * rt;
   }
