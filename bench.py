@@ -325,19 +325,26 @@ def solver_runs(grid3):
     rp = float(np.linalg.norm(b - gpu.multiply(Gd, xd.cpu().numpy())) / np.linalg.norm(b))
     res["plain_fp64"] = {"ms": tp * 1e3, "iterations": sp.computed_iterations, "converged": sp.converged,
                          "true_rel_residual": rp}
-    for rep in range(3):
-        xd = torch.zeros_like(bd)
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        sm = gpu.mixed_cg(bd, xd, gpu.Mixed_config(1e-10, 1e-5, 100, 200000), gpu.spmv(Gd))
-        torch.cuda.synchronize()
-        tm = time.perf_counter() - t0
-        reps_m.append(tm * 1e3)
-    tm = min(reps_m[1:]) / 1e3
-    rm = float(np.linalg.norm(b - gpu.multiply(Gd, xd.cpu().numpy())) / np.linalg.norm(b))
-    res["mixed_fp32_fp64"] = {"ms": tm * 1e3, "outer": sm.outer_iterations, "inner_iterations": sm.inner_iterations,
-                              "converged": sm.converged, "true_rel_residual": rm}
-    res["speedup_mixed_vs_plain"] = tp / tm
+    variants = (("mixed_fp32_fp64", gpu.Mixed_config(1e-10, 1e-5, 100, 200000)),
+                ("mixed_per_step_kernels", gpu.Mixed_config(1e-10, 1e-5, 100, 200000, persistent=False)))
+    for name, mcfg in variants:
+        reps = []
+        for rep in range(3):
+            xd = torch.zeros_like(bd)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            sm = gpu.mixed_cg(bd, xd, mcfg, gpu.spmv(Gd))
+            torch.cuda.synchronize()
+            reps.append((time.perf_counter() - t0) * 1e3)
+        tm = min(reps[1:]) / 1e3
+        rm = float(np.linalg.norm(b - gpu.multiply(Gd, xd.cpu().numpy())) / np.linalg.norm(b))
+        res[name] = {"ms": tm * 1e3, "outer": sm.outer_iterations, "inner_iterations": sm.inner_iterations,
+                     "converged": sm.converged, "true_rel_residual": rm, "inner_ms": sm.inner_ms,
+                     "outer_ms": sm.outer_ms, "setup_ms": sm.setup_ms, "persistent": sm.persistent,
+                     "us_per_inner_iteration": sm.inner_ms * 1e3 / max(sm.inner_iterations, 1)}
+        reps_m.append({name: reps})
+        if name == "mixed_fp32_fp64":
+            res["speedup_mixed_vs_plain"] = tp / tm
     res["reps_ms"] = {"plain_fp64": reps_p, "mixed": reps_m, "reported": "best of the repetitions after the first"}
     res["n"] = n
     res["nnz"] = G.size()

@@ -288,6 +288,10 @@ typedef struct {
   int32_t l2_window;          /* keep the FP32 inner vectors resident in L2
                                  (a persisting access-policy window on the
                                  handle's stream, this process only) */
+  int32_t inner_kernel;       /* 0: each inner solve is one persistent
+                                 cooperative launch when the handle has its
+                                 SELL-32 copy (else per-step kernels);
+                                 1: one kernel per CG step */
 } sk_mixed_config;
 
 typedef struct {
@@ -299,6 +303,7 @@ typedef struct {
   double setup_ms;           /* host wall time: FP32 copies, Jacobi, ||b|| */
   double inner_ms;           /* host wall time in the FP32 inner solves */
   double outer_ms;           /* host wall time in the FP64 residual / update */
+  int32_t inner_kernel;      /* 0: persistent launch, 1: per-step kernels */
 } sk_mixed_summary;
 
 SK_API sk_status sk_mixed_cg_solve(sk_matrix A, int32_t jacobi,

@@ -52,13 +52,13 @@ class FgmresConfig(ctypes.Structure):
 class MixedConfig(ctypes.Structure):
     _fields_ = [("tolerance", c_dbl), ("inner_tolerance", c_dbl), ("max_outer", c_i64),
                 ("max_inner", c_i64), ("collect_residuals", c_i32), ("adaptive_last_step", c_i32),
-                ("l2_window", c_i32)]
+                ("l2_window", c_i32), ("inner_kernel", c_i32)]
 
 
 class MixedSummary(ctypes.Structure):
     _fields_ = [("residual_norm", c_dbl), ("outer_iterations", c_i64), ("inner_iterations", c_i64),
                 ("converged", c_i32), ("status", c_i32), ("setup_ms", c_dbl), ("inner_ms", c_dbl),
-                ("outer_ms", c_dbl)]
+                ("outer_ms", c_dbl), ("inner_kernel", c_i32)]
 
 
 class TrainConfig(ctypes.Structure):

@@ -17,6 +17,7 @@
 
 #include "sk_learned.cuh"
 #include "sk_vec.cuh"
+#include "sk_mixed.cuh"
 
 namespace sk {
 
@@ -1219,10 +1220,19 @@ static sk_status mixed_cg_solve(sk_matrix A, bool jacobi, const double* b, doubl
   // after; the FP32 Jacobi is built once per handle):
   //   [ inner FP32 CG region | d32 | inv32 ]  <- kept resident in L2
   //   [ r32 | r64 | outer scalars, counters, reduction slots ]
+  // The inner solve runs as one persistent launch (sk_mixed.cu) when the
+  // handle allows it, else as one kernel per CG step (cg_solve<float>).
+  const bool persistent = cfg->inner_kernel == 0 && inner_persistent_ok(A);
+  out->inner_kernel = persistent ? 0 : 1;
   const int cap = spmv_grid(A);
-  const size_t inner_bytes = (common_bytes(A, 5, static_cast<size_t>(n + 8) * 4, 0, 0) + 255) & ~size_t(255);
+  // persistent form: p, q and the inner residual in the first three
+  // vectors of the inner region
+  const size_t pstride = static_cast<size_t>((n + 8 + 63) / 64 * 64);
+  const size_t inner_bytes =
+      (std::max(common_bytes(A, 5, static_cast<size_t>(n + 8) * 4, 0, 0), 3 * pstride * 4) + 255) & ~size_t(255);
+  const size_t pscratch_bytes = (inner_persistent_scratch(A) + 255) & ~size_t(255);
   const size_t need = inner_bytes + 4096 + static_cast<size_t>(n + 64) * (8 + 4 + 4 + 4) + 4096 +
-                      static_cast<size_t>(cap) * kMaxRed * 8 + 1024;
+                      static_cast<size_t>(cap) * kMaxRed * 8 + 1024 + pscratch_bytes + 256;
   const bool fresh = A->ws2_bytes < need;  // reused after the first call
   if (fresh) {
     if (A->ws2) {
@@ -1244,6 +1254,10 @@ static sk_status mixed_cg_solve(sk_matrix A, bool jacobi, const double* b, doubl
   Scalars* so = cv.take<Scalars>(sizeof(Scalars));
   unsigned* cnt = cv.take<unsigned>(16);
   double* partials = cv.take<double>(static_cast<size_t>(cap) * kMaxRed * 8);
+  void* pscratch = cv.take<char>(pscratch_bytes);
+  float* pv = reinterpret_cast<float*>(inner_base);
+  float* qv = pv + pstride;
+  float* rv = qv + pstride;
   SK_CUDA(cudaMemsetAsync(so, 0, sizeof(Scalars), st));
   SK_CUDA(cudaMemsetAsync(cnt, 0, 16, st));
   sk_precond_s jac32{};
@@ -1298,7 +1312,7 @@ static sk_status mixed_cg_solve(sk_matrix A, bool jacobi, const double* b, doubl
         break;
       }
       if (outer >= cfg->max_outer) break;
-      launch_vec(n, OpScaleDown{r, r32, d32, 0.0}, ws, so, st);
+      launch_vec(n, OpScaleDown{r, persistent ? rv : r32, d32, 0.0}, ws, so, st);
       // The last step needs only the remaining factor tol ||b|| / ||r||: its
       // inner tolerance is tightened to half of that when that is below the
       // configured one (floor 1e-7, about what FP32 CG can resolve), so that
@@ -1310,8 +1324,16 @@ static sk_status mixed_cg_solve(sk_matrix A, bool jacobi, const double* b, doubl
       sk_summary is{};
       auto t_inner = clk::now();
       L2Window win(cfg->l2_window ? st : nullptr, inner_base, resident_bytes);
-      status = cg_solve<float>(A, jacobi ? &jac32 : nullptr, nullptr, r32, d32, &icfg, &is, nullptr, st,
-                               f32_values(A), inner_base);
+      if (persistent) {
+        InnerResult ir;
+        status = inner_cg_persistent(A, jacobi ? inv32 : nullptr, rv, d32, pv, qv, pscratch, icfg.tolerance,
+                                     icfg.max_iterations, st, &ir);
+        is.computed_iterations = ir.iterations;
+        is.converged = ir.converged;
+      } else {
+        status = cg_solve<float>(A, jacobi ? &jac32 : nullptr, nullptr, r32, d32, &icfg, &is, nullptr, st,
+                                 f32_values(A), inner_base);
+      }
       win.release();
       out->inner_ms += ms_since(t_inner);
       if (status != SK_OK) break;

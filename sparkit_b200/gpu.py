@@ -335,6 +335,7 @@ class Mixed_config:
     collect_residuals: bool = False
     adaptive_last_step: bool = True
     l2_window: bool = True
+    persistent: bool = True      # one cooperative launch per inner solve
 
 
 @dataclass
@@ -348,6 +349,7 @@ class Mixed_summary:
     setup_ms: float = 0.0
     inner_ms: float = 0.0
     outer_ms: float = 0.0
+    persistent: bool = False
 
 
 def mixed_cg(b, x, cfg, op, jacobi_inner=True):
@@ -356,13 +358,14 @@ def mixed_cg(b, x, cfg, op, jacobi_inner=True):
     b and x are FP64 CUDA tensors (x holds the initial guess)."""
     Ad = _op_matrix(op)
     c = _lib.MixedConfig(cfg.tolerance, cfg.inner_tolerance, cfg.max_outer, cfg.max_inner,
-                         int(cfg.collect_residuals), int(cfg.adaptive_last_step), int(cfg.l2_window))
+                         int(cfg.collect_residuals), int(cfg.adaptive_last_step), int(cfg.l2_window),
+                         0 if cfg.persistent else 1)
     s = _lib.MixedSummary()
     hist = np.zeros(cfg.max_outer + 2) if cfg.collect_residuals else None
     check(lib().sk_mixed_cg_solve(Ad.handle, int(jacobi_inner), _ptr(b), _ptr(x), ctypes.byref(c), ctypes.byref(s),
                                   _ptr(hist), _stream_of(b)))
     out = Mixed_summary(s.residual_norm, s.outer_iterations, s.inner_iterations, bool(s.converged), s.status,
-                        [], s.setup_ms, s.inner_ms, s.outer_ms)
+                        [], s.setup_ms, s.inner_ms, s.outer_ms, s.inner_kernel == 0)
     if hist is not None:
         out.residual_history = hist[: s.outer_iterations + 1].tolist()
     return out

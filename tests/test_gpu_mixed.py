@@ -42,3 +42,93 @@ def test_mixed_zero_rhs(gpu_lib):
     s = gpu.mixed_cg(bd, xd, gpu.Mixed_config(), gpu.spmv(Ad))
     torch.cuda.synchronize()
     assert s.converged and not xd.any()
+
+
+def _far_coupled_laplacian(m, shift, eps=0.05, extra=0):
+    """2-D Dirichlet Laplacian on m x m plus symmetric couplings -eps between
+    rows i and i + shift + 7 j, j = 0..extra (so rows hold up to 5 + 2 (extra
+    + 1) entries), with the diagonal raised to keep it diagonally dominant
+    (SPD)."""
+    from sparkit_b200.formats import Compressed_row_matrix
+    L = matgen.laplacian_2d_dirichlet(m)
+    n = L.shape()[0]
+    rp, ci, va = (np.asarray(a) for a in (L.row_ptr(), L.col_ind(), L.values()))
+    rows = np.repeat(np.arange(n), np.diff(rp))
+    va = np.where(ci == rows, va + 2 * eps * (extra + 1), va)
+    r_all, c_all, v_all = [rows], [ci], [va]
+    for j in range(extra + 1):
+        i = np.arange(n - shift - 7 * j)
+        r_all += [i, i + shift + 7 * j]
+        c_all += [i + shift + 7 * j, i]
+        v_all += [np.full(2 * i.size, -eps)]
+    r_all, c_all, v_all = np.concatenate(r_all), np.concatenate(c_all), np.concatenate(v_all)
+    order = np.lexsort((c_all, r_all))
+    r_all, c_all, v_all = r_all[order], c_all[order], v_all[order]
+    new_rp = np.zeros(n + 1, dtype=np.int64)
+    np.add.at(new_rp, r_all + 1, 1)
+    return Compressed_row_matrix((n, n), np.cumsum(new_rp), c_all.astype(np.int64), v_all)
+
+
+@pytest.mark.parametrize("jacobi", [True, False])
+def test_persistent_inner_matches_per_step(gpu_lib, oracle, jacobi):
+    """The persistent inner solve (one cooperative launch per outer step)
+    runs the per-step iteration; only the dot products' summation order
+    differs, so the FP32 iteration counts agree within 2% and both reach
+    the FP64 tolerance on the true residual."""
+    import torch
+    A = matgen.diffusion_3d_grf(32, sigma=2.0, corr_len=4.0, seed=2)
+    n = A.shape()[0]
+    b = matgen.uniform_vector(n, seed=4)
+    Ad = gpu.Device_matrix(A)
+    bd = torch.from_numpy(b).cuda()
+    res = {}
+    for persistent in (False, True):
+        xd = torch.zeros_like(bd)
+        cfg = gpu.Mixed_config(1e-10, 1e-5, 50, 100000, persistent=persistent)
+        s = gpu.mixed_cg(bd, xd, cfg, gpu.spmv(Ad), jacobi_inner=jacobi)
+        torch.cuda.synchronize()
+        rel = np.linalg.norm(b - oracle.spmv(A, xd.cpu().numpy())) / np.linalg.norm(b)
+        assert s.converged and rel < 1e-10, (persistent, s, rel)
+        assert s.persistent == persistent
+        res[persistent] = s
+    a, p = res[False].inner_iterations, res[True].inner_iterations
+    assert abs(a - p) <= max(2, 0.02 * a), (a, p)
+    assert res[False].outer_iterations == res[True].outer_iterations
+
+
+def test_persistent_inner_long_rows(gpu_lib, oracle):
+    """Rows longer than the slots staged per row (and far column offsets):
+    the persistent solve reads the rest straight from memory and still
+    reaches the tolerance in the per-step solve's iteration count."""
+    import torch
+    A = _far_coupled_laplacian(190, 33000, extra=6)
+    n = A.shape()[0]
+    b = matgen.uniform_vector(n, seed=6)
+    Ad = gpu.Device_matrix(A)
+    bd = torch.from_numpy(b).cuda()
+    its = {}
+    for persistent in (False, True):
+        xd = torch.zeros_like(bd)
+        s = gpu.mixed_cg(bd, xd, gpu.Mixed_config(1e-10, 1e-5, 50, 100000, persistent=persistent), gpu.spmv(Ad))
+        torch.cuda.synchronize()
+        rel = np.linalg.norm(b - oracle.spmv(A, xd.cpu().numpy())) / np.linalg.norm(b)
+        assert s.converged and rel < 1e-10, (s, rel)
+        assert s.persistent == persistent
+        its[persistent] = s.inner_iterations
+    assert abs(its[True] - its[False]) <= max(2, 0.02 * its[False]), its
+
+
+def test_persistent_inner_repeatable(gpu_lib):
+    """Deterministic reductions: two solves give the same bits."""
+    import torch
+    A = matgen.diffusion_3d_grf(24, sigma=2.0, corr_len=4.0, seed=3)
+    b = matgen.uniform_vector(A.shape()[0], seed=5)
+    Ad = gpu.Device_matrix(A)
+    bd = torch.from_numpy(b).cuda()
+    xs = []
+    for _ in range(2):
+        xd = torch.zeros_like(bd)
+        gpu.mixed_cg(bd, xd, gpu.Mixed_config(1e-10, 1e-5, 50, 100000), gpu.spmv(Ad))
+        torch.cuda.synchronize()
+        xs.append(xd.cpu().numpy())
+    assert np.array_equal(xs[0], xs[1])
