@@ -447,6 +447,23 @@ SK_API sk_status sk_learned_create(sk_precond* out, sk_matrix A, sk_net net, int
 /* The six coefficient planes (d, w, e, s, n, 1/d; FP32, 6 n values). */
 SK_API sk_status sk_learned_planes(sk_precond M, float* host, int64_t capacity);
 
+/* No reference counterpart (fgmres.hpp:96-428 accepts any callable as its
+ * variable preconditioner): a two-level preconditioner for the FP64 CSR
+ * matrix A on an nx x ny grid, with P piecewise constant over agg x agg
+ * aggregates of cells (agg divides nx and ny, at most 4096 aggregates) and
+ * Ac = P^T A P the Galerkin coarse operator, inverted at set-up (banded LU
+ * without pivoting; a zero pivot fails with SK_INVALID_ARG).
+ *   default:        z = S(r); z += P Ac^-1 P^T (r - A z)
+ *                   [SK_TWOLEVEL_POST_SMOOTH: z += S(r - A z)]
+ *   COARSE_FIRST:   z = P Ac^-1 P^T r; z += S(r - A z)
+ * S is `smoother` (Jacobi, Chebyshev or learned, FP64, not owned: destroy
+ * it after this one) or NULL (the coarse correction alone).  Applied by
+ * sk_precond_apply and by the FGMRES calls. */
+#define SK_TWOLEVEL_POST_SMOOTH 1
+#define SK_TWOLEVEL_COARSE_FIRST 2
+SK_API sk_status sk_twolevel_create(sk_precond* out, sk_matrix A, sk_precond smoother,
+                                    int64_t nx, int64_t ny, int64_t agg, int32_t flags);
+
 /* fgmres with M as the variable preconditioner and a fallback: after a
  * restart cycle whose final residual estimate is above stall_ratio times
  * its starting residual, the remaining cycles use `fallback` (Jacobi or

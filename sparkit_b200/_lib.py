@@ -148,6 +148,7 @@ SIGNATURES = [
     ("sk_net_loss_grad", [c_vp, c_vp, c_vp, c_i32, c_dbl, ctypes.POINTER(c_dbl), c_vp, c_i64]),
     ("sk_learned_create", [ctypes.POINTER(c_vp), c_vp, c_vp, c_i64, c_i64]),
     ("sk_learned_planes", [c_vp, c_vp, c_i64]),
+    ("sk_twolevel_create", [ctypes.POINTER(c_vp), c_vp, c_vp, c_i64, c_i64, c_i64, c_i32]),
     ("sk_fgmres_fallback_solve", [c_vp, c_vp, c_vp, c_vp, c_vp, ctypes.POINTER(FgmresConfig), c_dbl,
                                   ctypes.POINTER(Summary), c_vp, P_i64, c_vp]),
     ("sk_cg_solve_host", [c_vp, c_vp, c_vp, c_vp, c_vp, ctypes.POINTER(CgConfig), ctypes.POINTER(Summary),

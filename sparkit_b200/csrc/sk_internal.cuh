@@ -149,7 +149,7 @@ struct sk_matrix_s {
 struct sk_net_s;
 
 struct sk_precond_s {
-  int kind;  // 1 = Jacobi, 2 = Chebyshev, 3 = learned network
+  int kind;  // 1 = Jacobi, 2 = Chebyshev, 3 = learned network, 4 = two-level
   sk_matrix A;
   sk_dtype dtype;
   sk::i64 n;
@@ -164,6 +164,17 @@ struct sk_precond_s {
   sk_net_s* net = nullptr;
   float* coef = nullptr;
   sk::i64 grid_nx = 0, grid_ny = 0;
+  // two-level (kind 4): smoother (not owned), agg x agg aggregates of the
+  // grid, the dense inverse of the Galerkin coarse operator (coarse_n^2
+  // FP64, row-major) and work vectors
+  sk_precond_s* smoother = nullptr;
+  sk::i64 agg = 0, coarse_n = 0;
+  int post = 0, coarse_first = 0;
+  double* coarse_inv = nullptr;
+  double* tbuf = nullptr;
+  double* tbuf2 = nullptr;
+  double* rc = nullptr;
+  double* zc = nullptr;
 };
 
 namespace sk {

@@ -4,6 +4,7 @@
 #include <vector>
 
 #include "sk_learned.cuh"
+#include "sk_twolevel.cuh"
 #include "sk_vec.cuh"
 
 namespace sk {
@@ -91,6 +92,8 @@ static void precond_apply_t(const sk_precond_s* M, i64 n, const T* r, T* z, RedW
     if constexpr (sizeof(T) == 8) {
       if (learned_apply(M, r, z, st) != SK_OK) set_error("learned preconditioner apply failed");
     }
+  } else if (M->kind == 4) {
+    if constexpr (sizeof(T) == 8) twolevel_apply(M, r, z, ws, sc, st);
   } else {
     chebyshev_apply_device<T>(M, r, z, static_cast<T*>(M->work), ws, sc, st);
   }
@@ -301,6 +304,7 @@ sk_status sk_precond_apply(sk_precond M, int64_t n, const void* r_dev, void* z_d
   }
   precond_apply_dispatch(M, dt, n, r_dev, z_dev, RedWs{}, nullptr, cs);
   SK_CUDA(cudaGetLastError());
+  if (M && M->kind == 4 && M->smoother && M->smoother->kind == 3) return sk_net_status(M->smoother->net);
   return SK_OK;
 }
 
@@ -331,6 +335,7 @@ sk_status sk_precond_destroy(sk_precond M) {
   if (!M) return SK_OK;
   // cudaFree waits for the device; the matrix M->A may already be gone.
   if (M->kind == 3) learned_release(M);
+  if (M->kind == 4) twolevel_release(M);
   if (M->inv_diag) cudaFree(M->inv_diag);
   if (M->inv_diag32) cudaFree(M->inv_diag32);
   if (M->work) cudaFree(M->work);

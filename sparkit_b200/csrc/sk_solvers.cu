@@ -1023,7 +1023,8 @@ static sk_status fgmres_solve(sk_matrix A, sk_precond M, const T* b, T* x,
     if (graphs) {
       auto it = execs.find(m_eff);
       if (it == execs.end()) {
-        if (M && M->kind == 3 && (s = learned_prepare(M)) != SK_OK) {
+        const sk_precond_s* net_prec = M && M->kind == 4 ? M->smoother : M;
+        if (net_prec && net_prec->kind == 3 && (s = learned_prepare(net_prec)) != SK_OK) {
           drop_graphs();
           return s;
         }
@@ -1452,6 +1453,7 @@ sk_status sk_fgmres_fallback_solve(sk_matrix A, sk_precond M, sk_precond fallbac
   st = fgmres_solve<double>(A, M, b_dev, x_dev, cfg, out, history_host, cs, fallback, stall_ratio, switched_at);
   if (st != SK_OK) return st;
   if (M->kind == 3) return sk_net_status(M->net);
+  if (M->kind == 4 && M->smoother && M->smoother->kind == 3) return sk_net_status(M->smoother->net);
   return SK_OK;
 }
 

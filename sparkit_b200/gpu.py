@@ -511,6 +511,25 @@ class learned_preconditioner(_Precond):
         return out.reshape(6, self.n)
 
 
+class twolevel(_Precond):
+    """Smoother plus an exact coarse-grid correction (sk_twolevel_create),
+    P piecewise constant over agg x agg aggregates of the nx x ny grid and
+    Ac = P^T A P:
+      default:           z = S(r); z += P Ac^-1 P^T (r - A z)
+                         [post_smooth: z += S(r - A z)]
+      coarse_first:      z = P Ac^-1 P^T r; z += S(r - A z)
+    `smoother` is a jacobi, chebyshev_preconditioner or
+    learned_preconditioner of the same matrix, or None (coarse only)."""
+
+    def __init__(self, Ad, smoother, nx, ny, agg, post_smooth=False, coarse_first=False):
+        h = ctypes.c_void_p()
+        flags = (1 if post_smooth else 0) | (2 if coarse_first else 0)
+        check(lib().sk_twolevel_create(ctypes.byref(h), Ad.handle, smoother.handle if smoother else None, int(nx),
+                                       int(ny), int(agg), flags))
+        super().__init__(h, Ad, Ad.shape()[0])
+        self.smoother = smoother  # keeps the smoother alive
+
+
 def fgmres_fallback(b, x, cfg, op, preconditioner, fallback, stall_ratio=0.9):
     """fgmres with a variable preconditioner and an automatic fallback:
     after a restart cycle whose residual estimate stays above stall_ratio
