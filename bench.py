@@ -52,6 +52,10 @@ def parse():
     p.add_argument("--no-solvers", action="store_true")
     p.add_argument("--profile-solvers", action="store_true",
                    help="run 20 FP64 and 20 FP32 CG iterations on the GRF diffusion matrix (for ncu launch lists)")
+    p.add_argument("--profile-learned", action="store_true",
+                   help="apply the (untrained) learned preconditioner on 512^2 four times, for ncu")
+    p.add_argument("--profile-mixed", action="store_true",
+                   help="one mixed solve with 100 persistent FP32 inner iterations on the 128^3 GRF problem, for ncu")
     p.add_argument("--profile-formats", action="store_true",
                    help="run one product of every sweep format and precision (for ncu captures), no timing")
     return p.parse_args()
@@ -352,6 +356,98 @@ def solver_runs(grid3):
     return out
 
 
+def learned_runs(train_grid=128, instances=200, cycles=100, eval_grids=(128, 512)):
+    """c4: the learned FGMRES preconditioner.  (residual, error) pairs are
+    harvested from the plain Jacobi-FGMRES(30) runs (one pair per restart
+    cycle) on `instances` seeded convection-diffusion instances of
+    train_grid^2 (GRF diffusion sigma 1, divergence-free velocity, cell
+    Peclet log-uniform in [1, 100]); the network is trained on the GPU by
+    the library's own kernels.  Then FGMRES(30) to a 1e-8 relative residual
+    on held-out instances: single-level Jacobi, Chebyshev(8) (bounds from a
+    power iteration) and the learned preconditioner; at 512^2 also the
+    two-level forms (aggregation coarse correction) with Jacobi and with the
+    network as the smoother.  Times are wall times of the solve call with
+    inputs on the device; a solve that does not converge within its cap
+    reports its cap time and converged = false."""
+    import torch
+
+    from oracle.binding import Oracle
+    from sparkit_b200 import gpu, matgen
+    O = Oracle()
+    out = {}
+    m = train_grid
+    pairs = gpu.Pairs(m, m, instances * cycles, instances)
+    t0 = time.perf_counter()
+    for seed in range(instances):
+        Am = matgen.convdiff_2d_grf(m, seed=100 + seed)[0]
+        Amd = gpu.Device_matrix(Am)
+        inst = pairs.add_instance(Amd)
+        xs = np.random.default_rng(seed).uniform(-1, 1, m * m) if seed % 2 == 0 else \
+            matgen.gaussian_random_field((m, m), 1.0, m / 16, seed=seed).ravel()
+        pairs.harvest(inst, Amd, torch.from_numpy(O.spmv(Am, xs)).cuda(), torch.from_numpy(xs).cuda(), 30, cycles)
+        Amd.close()
+    torch.cuda.synchronize()
+    out["harvest"] = {"pairs": len(pairs), "grid": m, "instances": instances, "s": time.perf_counter() - t0}
+    net = gpu.Net(seed=1)
+    ts = net.train(pairs, gpu.Train_config(steps=2000, batch=8, lr=2e-3, mu=1.0, seed=3))
+    h = np.array(ts.loss_history)
+    out["train"] = {"steps": 2000, "batch": 8, "ms": ts.ms, "loss_first20": float(h[:20].mean()),
+                    "loss_last50": float(h[-50:].mean())}
+    pairs.close()
+
+    def run(M, Ad, A, b, maxit):
+        xd = torch.zeros_like(b)
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        s = gpu.fgmres(b, xd, gpu.Fgmres_config(1e-8, 30, maxit), gpu.spmv(Ad), M)
+        torch.cuda.synchronize()
+        ms = (time.perf_counter() - t1) * 1e3
+        bh = b.cpu().numpy()
+        rel = float(np.linalg.norm(bh - O.spmv(A, xd.cpu().numpy())) / np.linalg.norm(bh))
+        return {"iterations": s.computed_iterations, "converged": bool(s.converged), "ms": ms,
+                "true_rel_residual": rel, "cap": maxit}
+
+    def power_max(Ad, n, its=80):
+        v = torch.randn(n, dtype=torch.float64, device="cuda")
+        w = torch.empty_like(v)
+        lam = 0.0
+        for _ in range(its):
+            v /= v.norm()
+            Ad.spmv(v, w)
+            lam = float(torch.dot(v, w))
+            v, w = w, v
+        return lam
+
+    for g in eval_grids:
+        A, info = matgen.convdiff_2d_grf(g, seed=777)
+        Ad = gpu.Device_matrix(A)
+        b = torch.from_numpy(np.random.default_rng(3).uniform(-1, 1, g * g)).cuda()
+        J = gpu.jacobi(Ad)
+        lmax = power_max(Ad, g * g) * 1.05
+        L = gpu.learned_preconditioner(Ad, net, g, g)
+        big = g >= 512
+        r = {"grid": g, "peclet": info["peclet"],
+             "jacobi": run(J, Ad, A, b, 10000 if big else 6000),
+             "chebyshev8": run(gpu.chebyshev_preconditioner(Ad, lmax * 1e-2, lmax, 8), Ad, A, b,
+                               2500 if big else 1500),
+             "learned": run(L, Ad, A, b, 3000)}
+        if big:
+            agg = g // 64
+            r["twolevel_jacobi"] = run(gpu.twolevel(Ad, J, g, g, agg), Ad, A, b, 3000)
+            r["twolevel_learned"] = run(gpu.twolevel(Ad, L, g, g, agg, coarse_first=True), Ad, A, b, 3000)
+            r["twolevel_aggregates"] = [agg, (g // agg) ** 2]
+        plain = [r["jacobi"], r["chebyshev8"]]
+        lt = r["learned"]
+        if lt["converged"]:
+            best_plain = min(p["ms"] for p in plain)
+            r["learned_speedup_vs_plain"] = {
+                "value": best_plain / lt["ms"],
+                "lower_bound": not any(p["converged"] for p in plain),
+                "note": "plain solves that did not converge count with their cap time"}
+        out[f"grid{g}"] = r
+    return out
+
+
 def batched_runs(count=4096, loop_sample=64):
     """c5: `count` SPD systems (2-D 5-point / 3-D 7-point Laplacians plus a
     U[0, 0.5] shift, n log-uniform in [1k, 64k], FP32 CSR) solved to a 1e-10
@@ -467,6 +563,46 @@ def profile_formats(grid):
     return 0
 
 
+def profile_learned(grid=512, applies=4):
+    """The learned preconditioner's apply on the grid^2 convection-diffusion
+    matrix, `applies` times (the network's weights do not change the
+    kernels' work), for an ncu launch list or capture."""
+    import torch
+
+    from sparkit_b200 import gpu, matgen
+    torch.cuda.set_device(0)
+    A, _ = matgen.convdiff_2d_grf(grid, seed=999)
+    Ad = gpu.Device_matrix(A)
+    net = gpu.Net(seed=1)
+    M = gpu.learned_preconditioner(Ad, net, grid, grid)
+    v = torch.from_numpy(np.random.default_rng(0).standard_normal(grid * grid)).cuda()
+    z = torch.zeros_like(v)
+    for _ in range(applies):
+        M.apply(v, z)
+    torch.cuda.synchronize()
+    return 0
+
+
+def profile_mixed(grid, inner=100):
+    """One outer step of the mixed solver on the GRF diffusion problem with
+    `inner` persistent FP32 inner iterations, twice (warm-up, then the
+    captured one)."""
+    import torch
+
+    from sparkit_b200 import gpu, matgen
+    torch.cuda.set_device(0)
+    G = matgen.diffusion_3d_grf(grid, sigma=2.0, corr_len=8.0, seed=0)
+    Gd = gpu.Device_matrix(G)
+    Gd.add_f32_values()
+    b = torch.from_numpy(matgen.uniform_vector(G.shape()[0], seed=0)).cuda()
+    for _ in range(2):
+        x = torch.zeros_like(b)
+        s = gpu.mixed_cg(b, x, gpu.Mixed_config(1e-10, 1e-5, 1, inner), gpu.spmv(Gd))
+    torch.cuda.synchronize()
+    assert s.persistent and s.inner_iterations == inner
+    return 0
+
+
 def profile_solvers(grid):
     """A short plain FP64 Jacobi-CG (20 iterations) and a short mixed solve
     (one outer step of 20 FP32 iterations) for per-kernel launch lists."""
@@ -494,6 +630,10 @@ def main():
         return profile_formats(args.grid)
     if args.profile_solvers:
         return profile_solvers(args.grid)
+    if args.profile_learned:
+        return profile_learned()
+    if args.profile_mixed:
+        return profile_mixed(args.grid)
     import torch
     world, rank, local = dist_setup()
     if world > 1:
@@ -602,6 +742,7 @@ def main():
     if rank == 0 and world == 1 and not args.no_solvers:
         extra["solvers"] = solver_runs(args.grid)
         extra["solvers"]["c5_batched"] = batched_runs()
+        extra["solvers"]["c4_learned_fgmres"] = learned_runs()
 
     if rank == 0:
         line = {
