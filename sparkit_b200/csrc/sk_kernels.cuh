@@ -146,20 +146,29 @@ __device__ __forceinline__ void cp_async_commit_wait_all() {
   asm volatile("cp.async.commit_group;\n" ::: "memory");
   asm volatile("cp.async.wait_group 0;\n" ::: "memory");
 }
+// One element (4 or 8 bytes) global -> shared, asynchronously.
+template <typename T>
+__device__ __forceinline__ void cp_async_elem(T* smem, const T* gmem) {
+  static_assert(sizeof(T) == 4 || sizeof(T) == 8, "4- or 8-byte elements");
+  const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+  asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(s), "l"(gmem), "n"(sizeof(T)) : "memory");
+}
 
 // ------------------------------------------------------------------
 // CSR: one CTA per tile of rows (tiles[b] = {first row, first entry};
 // at most 256 rows and 2048 entries, or one longer row).  Every thread
-// loads 8 of the tile's entries (coalesced, streaming) and gathers their x
-// values with all 16 loads in flight, so that the random gathers of skewed
-// matrices overlap instead of being walked row by row; the rounded products
-// go to shared memory.  Then each row is summed from there by one thread in
-// storage order (bit-exact with the reference), or, in tiles holding a row
-// longer than 32 entries, by L lanes with strided partial sums and a
-// shuffle tree.
+// starts all of its work's loads at once: the tile's row pointers (one per
+// thread), the 8 values it owns straight into shared memory (cp.async, no
+// register held while in flight) and their 8 column indices; then the 8
+// gathers of x, so that the random gathers of skewed matrices overlap
+// instead of being walked row by row.  The rounded products replace the
+// values in shared memory.  Then each row is summed from there by one
+// thread in storage order (bit-exact with the reference), or, in tiles
+// holding a row longer than 32 entries, by L lanes with strided partial
+// sums and a shuffle tree.  Six CTAs share an SM (at most 40 registers).
 // ------------------------------------------------------------------
 template <typename T, class Epi>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, 6)
 csr_spmv_kernel(const int* __restrict__ rp, const int* __restrict__ ci,
                 const T* __restrict__ va, const T* __restrict__ x,
                 const int2* __restrict__ tiles,
@@ -188,27 +197,35 @@ csr_spmv_kernel(const int* __restrict__ rp, const int* __restrict__ ci,
     block_reduce<1>(acc);
     if (tid == 0) epi(r0, static_cast<T>(acc[0]), red);
   } else {
-    // Every thread computes the products of entries s + tid + 256 j (j < 8:
-    // the loads of its 8 entries and their 8 gathers of x are in flight
-    // together) into shared memory; rows are then summed from there.
+    // Thread tid owns entries s + tid + 256 j (j < 8).  Row 0 of the tile
+    // starts at s and row nr ends at e, so only rows 1..nr-1 need rp.
+    constexpr int J = kTileNnz / kThreads;
     T* sprod = sval;
-    int cj[kTileNnz / kThreads];
-    T vj[kTileNnz / kThreads], xj[kTileNnz / kThreads];
+    int rpv = 0;
+    if (tid > 0 && tid < nr) rpv = __ldg(rp + r0 + tid);
+    int cj[J];
 #pragma unroll
-    for (int j = 0; j < kTileNnz / kThreads; ++j) {
+    for (int j = 0; j < J; ++j) {
       const int k = s + tid + j * kThreads;
       if (k < e) {
+        cp_async_elem(sprod + tid + j * kThreads, va + k);
         cj[j] = __ldcs(ci + k);
-        vj[j] = __ldcs(va + k);
       }
     }
+    T xj[J];
 #pragma unroll
-    for (int j = 0; j < kTileNnz / kThreads; ++j)
+    for (int j = 0; j < J; ++j)
       if (s + tid + j * kThreads < e) xj[j] = __ldg(x + cj[j]);
+    cp_async_commit_wait_all();  // this thread's own values have landed
 #pragma unroll
-    for (int j = 0; j < kTileNnz / kThreads; ++j)
-      if (s + tid + j * kThreads < e) sprod[tid + j * kThreads] = mul(vj[j], xj[j]);
-    for (int t = tid; t <= nr; t += kThreads) srp[t] = __ldg(rp + r0 + t) - s;
+    for (int j = 0; j < J; ++j)
+      if (s + tid + j * kThreads < e) sprod[tid + j * kThreads] = mul(sprod[tid + j * kThreads], xj[j]);
+    if (tid == 0) {
+      srp[0] = 0;
+      srp[nr] = e - s;
+    } else if (tid < nr) {
+      srp[tid] = rpv - s;
+    }
     __syncthreads();
     const int L = lanes[blockIdx.x];
     if (L == 1) {
