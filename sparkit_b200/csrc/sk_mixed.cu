@@ -210,6 +210,13 @@ __device__ __forceinline__ double phase_spmv(PArgs const& a, int t0, int T) {
   row_fetch(a, lb, bb, 0, cb, vb);
   row_meta(a, ia + 2 * T, lc, bc);
   while (ia < a.n) {
+    // slots of row c (issued first, so that a wait on row b's indices
+    // below does not hold the HBM stream back), position of row d
+    int cc[kPU];
+    float vc[kPU];
+    row_fetch(a, lc, bc, 0, cc, vc);
+    int ld, bd;
+    row_meta(a, ia + 3 * T, ld, bd);
     // gathers of row b
     float gb[kPU];
 #pragma unroll
@@ -217,12 +224,6 @@ __device__ __forceinline__ double phase_spmv(PArgs const& a, int t0, int T) {
       if (j < lb) gb[j] = a.p[cb[j]];
     const int ib = ia + T;
     const float pb = ib < a.n ? a.p[ib] : 0.0f;
-    // slots of row c, position of row d
-    int cc[kPU];
-    float vc[kPU];
-    row_fetch(a, lc, bc, 0, cc, vc);
-    int ld, bd;
-    row_meta(a, ia + 3 * T, ld, bd);
     // sum of row a
     float sum = 0.0f;
 #pragma unroll
