@@ -235,6 +235,14 @@ typedef struct {
   int32_t collect_residuals;
 } sk_fgmres_config;
 
+/* Gmres_config<T>, sparkit/data/gmres.hpp:25-47 (the same fields) */
+typedef struct {
+  double tolerance;
+  int64_t restart_dimension;
+  int64_t max_iterations;
+  int32_t collect_residuals;
+} sk_gmres_config;
+
 /* CGSummary / Bicgstab_summary / Fgmres_summary
  * (conjugate_gradient.hpp:27-40, bicgstab.hpp:50-63, fgmres.hpp:55-68).
  * The per-iteration residual norms go to the caller's history buffer
@@ -268,6 +276,15 @@ SK_API sk_status sk_bicgstab_solve(sk_matrix A, sk_precond left, sk_precond righ
 SK_API sk_status sk_fgmres_solve(sk_matrix A, sk_precond M, const void* b_dev,
                           void* x_dev, const sk_fgmres_config* cfg,
                           sk_summary* out, double* history_host, sk_stream s);
+
+/* gmres(b, x, cfg, op, left, right) (sparkit/data/gmres.hpp:400-429):
+ * restarted GMRES(m) with M_L = left and M_R = right (NULL: identity).
+ * Convergence on |g_{j+1}| / ||b|| as in the reference (the residual of
+ * the left-preconditioned system over the unpreconditioned ||b||). */
+SK_API sk_status sk_gmres_solve(sk_matrix A, sk_precond left, sk_precond right,
+                                const void* b_dev, void* x_dev,
+                                const sk_gmres_config* cfg, sk_summary* out,
+                                double* history_host, sk_stream s);
 
 /* Mixed precision (no reference counterpart; the reference solves in one
  * value type): FP64 iterative refinement around conjugate_gradient
@@ -488,6 +505,10 @@ SK_API sk_status sk_bicgstab_solve_host(sk_matrix A, sk_precond left,
 SK_API sk_status sk_fgmres_solve_host(sk_matrix A, sk_precond M, const void* b_host,
                                void* x_host, const sk_fgmres_config* cfg,
                                sk_summary* out, double* history_host);
+SK_API sk_status sk_gmres_solve_host(sk_matrix A, sk_precond left, sk_precond right,
+                                     const void* b_host, void* x_host,
+                                     const sk_gmres_config* cfg, sk_summary* out,
+                                     double* history_host);
 
 #ifdef __cplusplus
 }

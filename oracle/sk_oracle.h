@@ -68,7 +68,8 @@ typedef struct {
   int32_t collect_residuals;
 } sko_krylov_config;
 
-/* Fgmres_config, sparkit/data/fgmres.hpp:25-47 */
+/* Fgmres_config, sparkit/data/fgmres.hpp:25-47; Gmres_config
+ * (gmres.hpp:25-47) has the same fields */
 typedef struct {
   double tolerance;
   int64_t restart_dimension;
@@ -109,7 +110,10 @@ typedef struct {
                         const sko_precond*, const T*, T*,                     \
                         const sko_krylov_config*, sko_summary*, double*);     \
   void sko_fgmres_##S(const sko_operator*, const sko_precond*, const T*, T*,  \
-                      const sko_fgmres_config*, sko_summary*, double*);
+                      const sko_fgmres_config*, sko_summary*, double*);       \
+  void sko_gmres_##S(const sko_operator*, const sko_precond*,                 \
+                     const sko_precond*, const T*, T*,                        \
+                     const sko_fgmres_config*, sko_summary*, double*);
 
 /* Summation order of the solvers' dot products: 0 = the reference's
  * sequential order (default), 1 = 256-element chunks added in order. */

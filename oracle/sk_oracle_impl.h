@@ -520,6 +520,136 @@ done:
   free(w); free(work);
 }
 
+/* ------------------------------------------------------------------ */
+/* Restarted GMRES(m) with left and right preconditioning              */
+/* Follows sparkit/data/gmres.hpp:106-396: M_L on the initial residual  */
+/* and on A z_j, M_R on v_j (z_j kept for the update), normalisation by */
+/* division (:230, :278), convergence on |g_{j+1}| / ||b|| (:202).      */
+/* One divergence, as for FGMRES: a zero initial residual norm (the     */
+/* reference divides by it) is treated as convergence.                  */
+/* ------------------------------------------------------------------ */
+void SKO_FN(sko_gmres_)(const sko_operator* A, const sko_precond* ML,
+                        const sko_precond* MR, const SKO_T* b, SKO_T* x,
+                        const sko_fgmres_config* cfg, sko_summary* out,
+                        double* history) {
+  int64_t n = A->nrow;
+  int64_t m = cfg->restart_dimension;
+  size_t vb = sizeof(SKO_T) * (size_t)(n + 1);
+  SKO_T* V = (SKO_T*)calloc((size_t)(m + 1), vb);
+  SKO_T* Z = (SKO_T*)calloc((size_t)(m > 0 ? m : 1), vb);
+  SKO_T* H = (SKO_T*)calloc((size_t)((m + 1) * m + 1), sizeof(SKO_T));
+  SKO_T* cs = (SKO_T*)calloc((size_t)(m + 1), sizeof(SKO_T));
+  SKO_T* sn = (SKO_T*)calloc((size_t)(m + 1), sizeof(SKO_T));
+  SKO_T* g = (SKO_T*)calloc((size_t)(m + 2), sizeof(SKO_T));
+  SKO_T* y = (SKO_T*)calloc((size_t)(m + 1), sizeof(SKO_T));
+  SKO_T* w = (SKO_T*)calloc(1, vb);
+  SKO_T* r0 = (SKO_T*)calloc(1, vb);
+  SKO_T* work = (SKO_T*)calloc(3, vb);
+  int64_t nhist = 0;
+  int64_t um1 = m + 1;
+  out->residual_norm = 0;
+  out->computed_iterations = 0;
+  out->converged = 0;
+  out->status = 0;
+  SKO_T bnorm = SKO_SQRT(SKO_FN(sko_dot_)(b, b, n)); /* :165 */
+  if (bnorm == (SKO_T)0) {
+    for (int64_t i = 0; i < n; ++i) x[i] = 0;
+    out->converged = 1;
+    goto done;
+  }
+  while (out->computed_iterations < cfg->max_iterations && !out->converged) {
+    /* compute_initial_residual :212-241 */
+    SKO_FN(sko_apply_op_)(A, x, w);
+    for (int64_t i = 0; i < n; ++i) r0[i] = b[i] - w[i];
+    SKO_FN(sko_apply_prec_)(ML, A, r0, V, n, work);
+    SKO_T beta = SKO_SQRT(SKO_FN(sko_dot_)(V, V, n));
+    if (beta == (SKO_T)0) {
+      out->residual_norm = 0;
+      out->converged = 1;
+      break;
+    }
+    for (int64_t i = 0; i < n; ++i) V[i] /= beta;
+    for (int64_t i = 0; i <= m; ++i) g[i] = 0;
+    g[0] = beta;
+    memset(Z, 0, vb * (size_t)m);
+    memset(H, 0, sizeof(SKO_T) * (size_t)((m + 1) * m)); /* :182-184 */
+    memset(cs, 0, sizeof(SKO_T) * (size_t)m);
+    memset(sn, 0, sizeof(SKO_T) * (size_t)m);
+    int64_t left = cfg->max_iterations - out->computed_iterations;
+    int64_t m_eff = m < left ? m : left; /* :186-187 */
+    int64_t j_final = 0;
+    for (int64_t j = 0; j < m_eff; ++j) {
+      SKO_T* Vj = V + j * (n + 1);
+      SKO_T* Vj1 = V + (j + 1) * (n + 1);
+      SKO_T* Zj = Z + j * (n + 1);
+      /* arnoldi_step :244-281 */
+      SKO_FN(sko_apply_prec_)(MR, A, Vj, Zj, n, work);
+      SKO_FN(sko_apply_op_)(A, Zj, w);
+      SKO_FN(sko_apply_prec_)(ML, A, w, Vj1, n, work);
+      for (int64_t i = 0; i <= j; ++i) {
+        SKO_T* Vi = V + i * (n + 1);
+        SKO_T h = SKO_FN(sko_dot_)(Vi, Vj1, n);
+        H[i + j * um1] = h;
+        for (int64_t k = 0; k < n; ++k) Vj1[k] -= h * Vi[k];
+      }
+      SKO_T hn = SKO_SQRT(SKO_FN(sko_dot_)(Vj1, Vj1, n));
+      H[j + 1 + j * um1] = hn;
+      if (hn > (SKO_T)0)
+        for (int64_t k = 0; k < n; ++k) Vj1[k] /= hn;
+      /* apply_givens_rotations :284-310, generate_givens :312-326 */
+      for (int64_t i = 0; i < j; ++i) {
+        SKO_T temp = cs[i] * H[i + j * um1] + sn[i] * H[i + 1 + j * um1];
+        H[i + 1 + j * um1] = -sn[i] * H[i + j * um1] + cs[i] * H[i + 1 + j * um1];
+        H[i + j * um1] = temp;
+      }
+      {
+        SKO_T a = H[j + j * um1];
+        SKO_T bb = H[j + 1 + j * um1];
+        if (bb == (SKO_T)0) { cs[j] = 1; sn[j] = 0; }
+        else if (a == (SKO_T)0) { cs[j] = 0; sn[j] = 1; }
+        else {
+          SKO_T rr = SKO_SQRT(a * a + bb * bb);
+          cs[j] = a / rr;
+          sn[j] = bb / rr;
+        }
+      }
+      H[j + j * um1] = cs[j] * H[j + j * um1] + sn[j] * H[j + 1 + j * um1];
+      H[j + 1 + j * um1] = 0;
+      {
+        SKO_T temp = cs[j] * g[j] + sn[j] * g[j + 1];
+        g[j + 1] = -sn[j] * g[j] + cs[j] * g[j + 1];
+        g[j] = temp;
+      }
+      out->computed_iterations += 1;
+      j_final = j;
+      SKO_T absres = SKO_FABS(g[j + 1]); /* :195-205 */
+      out->residual_norm = (double)absres;
+      if (history && cfg->collect_residuals) history[nhist++] = (double)absres;
+      if (absres / bnorm < (SKO_T)cfg->tolerance) {
+        out->converged = 1;
+        break;
+      }
+    }
+    /* form_solution :329-355 */
+    int64_t nj = j_final + 1;
+    for (int64_t ii = nj; ii > 0; --ii) {
+      int64_t i = ii - 1;
+      y[i] = g[i];
+      for (int64_t k = i + 1; k < nj; ++k) y[i] -= H[i + k * um1] * y[k];
+      y[i] /= H[i + i * um1];
+    }
+    for (int64_t i = 0; i < n; ++i) {
+      SKO_T sum = 0;
+      for (int64_t k = 0; k < nj; ++k) sum += Z[k * (n + 1) + i] * y[k];
+      x[i] += sum;
+    }
+  }
+done:
+  out->history_length = nhist;
+  free(V); free(Z); free(H); free(cs); free(sn); free(g); free(y);
+  free(w); free(r0); free(work);
+}
+
 #undef SKO_FN
 #undef SKO_CAT
 #undef SKO_CAT2

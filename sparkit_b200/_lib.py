@@ -123,6 +123,8 @@ SIGNATURES = [
                            ctypes.POINTER(Summary), c_vp, c_vp]),
     ("sk_fgmres_solve", [c_vp, c_vp, c_vp, c_vp, ctypes.POINTER(FgmresConfig), ctypes.POINTER(Summary),
                          c_vp, c_vp]),
+    ("sk_gmres_solve", [c_vp, c_vp, c_vp, c_vp, c_vp, ctypes.POINTER(FgmresConfig), ctypes.POINTER(Summary),
+                        c_vp, c_vp]),
     ("sk_mixed_cg_solve", [c_vp, c_i32, c_vp, c_vp, ctypes.POINTER(MixedConfig), ctypes.POINTER(MixedSummary),
                            c_vp, c_vp]),
     ("sk_batch_create", [ctypes.POINTER(c_vp), c_i64, c_vp, c_vp, c_vp, c_vp]),
@@ -157,6 +159,8 @@ SIGNATURES = [
                                 ctypes.POINTER(Summary), c_vp]),
     ("sk_fgmres_solve_host", [c_vp, c_vp, c_vp, c_vp, ctypes.POINTER(FgmresConfig), ctypes.POINTER(Summary),
                               c_vp]),
+    ("sk_gmres_solve_host", [c_vp, c_vp, c_vp, c_vp, c_vp, ctypes.POINTER(FgmresConfig), ctypes.POINTER(Summary),
+                             c_vp]),
 ]
 
 _lock = threading.Lock()

@@ -723,7 +723,42 @@ struct FgSmall {  // device arrays of one restart cycle
   double* sn;
   double* g;   // m+1
   double* y;   // m
+  double* zero;  // a constant 0 (the h of an MGS pass that only takes a dot)
 };
+
+// GMRES(m) (gmres.hpp:106-396) runs the FGMRES cycle with these changes:
+// the left preconditioner M_L on the initial residual and on A z_j
+// (:221-222, :253-254), and normalisation by division (:230, :278) where
+// fgmres.hpp multiplies by the reciprocal.  A Jacobi M_L is fused into the
+// product's epilogue; any other goes through the work vector `tmp`.
+template <typename T>
+struct GmLeft {
+  const sk_precond_s* L = nullptr;  // null: identity (FGMRES)
+  const T* linv = nullptr;          // Jacobi M_L: its inverse diagonal
+  T* tmp = nullptr;                 // other M_L: the vector before it
+  bool divide = false;              // GMRES normalisation
+};
+
+template <typename T>
+__device__ void fg_init_finalize(T beta, FgSmall const& sm, int m, Scalars* sc, bool divide) {
+  for (int i = 0; i < (m + 1) * m; ++i) sm.H[i] = 0.0;
+  for (int i = 0; i < m; ++i) sm.cs[i] = sm.sn[i] = 0.0;
+  for (int i = 0; i <= m; ++i) sm.g[i] = 0.0;
+  *sm.zero = 0.0;
+  sm.g[0] = static_cast<double>(beta);
+  sc->beta_cycle = static_cast<double>(beta);
+  sc->jfinal = 0;
+  sc->done = 0;
+  sc->beta0 = 0;
+  if (beta == T(0)) {
+    sc->beta0 = 1;
+    sc->converged = 1;
+    sc->done = 1;
+    sc->rnorm = 0.0;
+  } else {
+    sc->aux = divide ? static_cast<double>(beta) : static_cast<double>(T(1) / beta);
+  }
+}
 
 // compute_initial_residual (:207-224) and clear_hessenberg (:227-231).
 // A zero beta (the reference divides by it) ends the solve as converged.
@@ -735,29 +770,44 @@ struct EpiFgInit {
   Scalars* sc;
   FgSmall sm;
   int m;
+  const T* linv;  // Jacobi M_L (GMRES), else null
+  bool divide;
   __device__ void operator()(int row, T ax, double* red) const {
-    const T vi = sub(b[row], ax);
+    T vi = sub(b[row], ax);
+    if (linv) vi = mul(linv[row], vi);
     v0[row] = vi;
     red[0] += static_cast<double>(mul(vi, vi));
   }
   __device__ void finalize(const double* t) const {
-    const T beta = sqrt(static_cast<T>(t[0]));
-    for (int i = 0; i < (m + 1) * m; ++i) sm.H[i] = 0.0;
-    for (int i = 0; i < m; ++i) sm.cs[i] = sm.sn[i] = 0.0;
-    for (int i = 0; i <= m; ++i) sm.g[i] = 0.0;
-    sm.g[0] = static_cast<double>(beta);
-    sc->beta_cycle = static_cast<double>(beta);
-    sc->jfinal = 0;
-    sc->done = 0;
-    sc->beta0 = 0;
-    if (beta == T(0)) {
-      sc->beta0 = 1;
-      sc->converged = 1;
-      sc->done = 1;
-      sc->rnorm = 0.0;
-    } else {
-      sc->aux = static_cast<double>(T(1) / beta);
-    }
+    fg_init_finalize<T>(sqrt(static_cast<T>(t[0])), sm, m, sc, divide);
+  }
+};
+
+// tmp = b - A x (GMRES with a general M_L, before it is applied)
+template <typename T>
+struct EpiGmResid {
+  static constexpr int kNR = 0;
+  const T* b;
+  T* t;
+  __device__ void operator()(int row, T ax, double*) const { t[row] = sub(b[row], ax); }
+  __device__ void finalize(const double*) const {}
+};
+
+// beta = ||v0|| after a general M_L, and the cycle's initialisation.
+template <typename T>
+struct OpGmInitNorm {
+  static constexpr int kNR = 1;
+  const T* v0;
+  Scalars* sc;
+  FgSmall sm;
+  int m;
+  bool divide;
+  struct In { T v; };
+  __device__ bool prepare(const Scalars*) { return true; }
+  __device__ In load(i64 i) const { return {v0[i]}; }
+  __device__ void apply(i64, In const& q, double* red) const { red[0] += static_cast<double>(mul(q.v, q.v)); }
+  __device__ void finalize(const double* t) const {
+    fg_init_finalize<T>(sqrt(static_cast<T>(t[0])), sm, m, sc, divide);
   }
 };
 
@@ -769,6 +819,7 @@ struct OpFgScale {
   T* v;
   const double* hsrc;  // null: factor = aux; else factor = 1 / *hsrc if > 0
   T f;
+  bool divide;         // GMRES: v /= beta or v /= h (gmres.hpp:230, :278)
   __device__ bool prepare(const Scalars* s) {
     if (solve_done(s)) return false;
     if (!hsrc) {
@@ -777,12 +828,12 @@ struct OpFgScale {
     }
     const T h = static_cast<T>(*hsrc);
     if (!(h > T(0))) return false;  // :283
-    f = T(1) / h;
+    f = divide ? h : T(1) / h;
     return true;
   }
   struct In { T v; };
   __device__ In load(i64 i) const { return {v[i]}; }
-  __device__ void apply(i64 i, In const& q, double*) const { v[i] = mul(q.v, f); }
+  __device__ void apply(i64 i, In const& q, double*) const { v[i] = divide ? dvd(q.v, f) : mul(q.v, f); }
   __device__ void finalize(const double*) const {}
 };
 
@@ -793,7 +844,9 @@ struct EpiFgW {
   T* w;
   const T* v0;
   double* h_out;
+  const T* linv;  // Jacobi M_L (GMRES): w = M_L A z_j
   __device__ void operator()(int row, T val, double* red) const {
+    if (linv) val = mul(linv[row], val);
     w[row] = val;
     red[0] += static_cast<double>(mul(v0[row], val));
   }
@@ -929,19 +982,27 @@ struct OpFgUpdateX {
 // above stall_ratio times the cycle's starting residual switches the
 // preconditioner to `fallback` for the rest of the solve; *switched_at
 // receives the first cycle run with it (-1: never switched).
+//
+// With `left` non-null this is GMRES(m) (gmres.hpp:106-396): `left` is M_L
+// and M is M_R; the cycle applies M_L and normalises by division.
 template <typename T>
 static sk_status fgmres_solve(sk_matrix A, sk_precond M, const T* b, T* x,
                               const sk_fgmres_config* cfg, sk_summary* out, double* history_host,
                               cudaStream_t st, sk_precond fallback = nullptr, double stall_ratio = 0.0,
-                              int64_t* switched_at = nullptr) {
+                              int64_t* switched_at = nullptr, sk_precond left = nullptr, bool gmres = false) {
   const i64 n = A->nrow;
   const int m = static_cast<int>(cfg->restart_dimension);
   SK_CHECK(m >= 1 && m <= 4096, SK_INVALID_ARG, "restart_dimension must be in [1, 4096]");
   const i64 ld = n + 8 + 32;  // leading dimension of V and Z, 256-byte rounded below
   const i64 ldv = (ld * static_cast<i64>(sizeof(T)) + 255) / 256 * 256 / static_cast<i64>(sizeof(T));
   const bool alias_z = (M == nullptr);  // identity: Z_j = V_j
-  const i64 nvecs = (m + 1) + (alias_z ? 0 : m);
-  const size_t small_bytes = static_cast<size_t>((m + 1) * m + 4 * (m + 2)) * 8;
+  GmLeft<T> gl;
+  gl.L = left;
+  gl.divide = gmres;
+  if (left && left->kind == 1) gl.linv = static_cast<const T*>(left->inv_diag);
+  const bool general_left = left && left->kind != 1;
+  const i64 nvecs = (m + 1) + (alias_z ? 0 : m) + (general_left ? 1 : 0);
+  const size_t small_bytes = static_cast<size_t>((m + 1) * m + 4 * (m + 2) + 4) * 8;
   SolveCommon c;
   std::vector<char*> vv;
   char* extra = nullptr;
@@ -959,6 +1020,8 @@ static sk_status fgmres_solve(sk_matrix A, sk_precond M, const T* b, T* x,
   sm.sn = sm.cs + (m + 2);
   sm.g = sm.sn + (m + 2);
   sm.y = sm.g + (m + 2);
+  sm.zero = sm.y + (m + 2);
+  if (general_left) gl.tmp = V + ((m + 1) + (alias_z ? 0 : m)) * ldv;  // after V and Z
   *out = sk_summary{};
   double bnorm = 0;
   if ((s = norm_b<T>(b, n, c, st, &bnorm)) != SK_OK) return s;
@@ -980,20 +1043,32 @@ static sk_status fgmres_solve(sk_matrix A, sk_precond M, const T* b, T* x,
   // fixed sequence of launches: every pointer is the same from cycle to
   // cycle, and a converged solve turns the remaining kernels into no-ops.
   auto enqueue_cycle = [&](cudaStream_t q, int m_eff, sk_precond P) {
-    launch_spmv<T>(A, x, EpiFgInit<T>{b, V, c.sc, sm, m}, c.ws, nullptr, q);
-    launch_vec(n, OpFgScale<T>{V, nullptr, T(0)}, c.ws, c.sc, q);
+    if (general_left) {  // r0 = b - A x; v0 = M_L r0; beta = ||v0|| (:214-224)
+      launch_spmv<T>(A, x, EpiGmResid<T>{b, gl.tmp}, c.ws, nullptr, q);
+      precond_apply_dispatch(gl.L, A->dtype, n, gl.tmp, V, c.ws, nullptr, q);
+      launch_vec(n, OpGmInitNorm<T>{V, c.sc, sm, m, gl.divide}, c.ws, nullptr, q);
+    } else {
+      launch_spmv<T>(A, x, EpiFgInit<T>{b, V, c.sc, sm, m, gl.linv, gl.divide}, c.ws, nullptr, q);
+    }
+    launch_vec(n, OpFgScale<T>{V, nullptr, T(0), gl.divide}, c.ws, c.sc, q);
     for (int j = 0; j < m_eff; ++j) {
       T* Vj = V + j * ldv;
       T* Vj1 = V + (j + 1) * ldv;
       T* Zj = Z + j * ldv;
       if (!alias_z) precond_apply_dispatch(P, A->dtype, n, Vj, Zj, c.ws, c.sc, q);
-      launch_spmv<T>(A, Zj, EpiFgW<T>{Vj1, V, sm.H + j * um1}, c.ws, c.sc, q);
+      if (general_left) {  // v_{j+1} = M_L A z_j, then h_0j = <v_0, v_{j+1}>
+        launch_spmv<T>(A, Zj, EpiStore<T>{gl.tmp}, c.ws, c.sc, q);
+        precond_apply_dispatch(gl.L, A->dtype, n, gl.tmp, Vj1, c.ws, c.sc, q);
+        launch_vec(n, OpFgMgs<T>{Vj1, V, V, sm.zero, sm.H + j * um1, T(0)}, c.ws, c.sc, q);
+      } else {
+        launch_spmv<T>(A, Zj, EpiFgW<T>{Vj1, V, sm.H + j * um1, gl.linv}, c.ws, c.sc, q);
+      }
       for (int i = 0; i <= j; ++i) {
         const T* vnext = i < j ? V + (i + 1) * ldv : nullptr;
         launch_vec(n, OpFgMgs<T>{Vj1, V + i * ldv, vnext, sm.H + i + j * um1, sm.H + (i + 1) + j * um1, T(0)},
                    c.ws, c.sc, q);
       }
-      launch_vec(n, OpFgScale<T>{Vj1, sm.H + (j + 1) + j * um1, T(0)}, c.ws, c.sc, q);
+      launch_vec(n, OpFgScale<T>{Vj1, sm.H + (j + 1) + j * um1, T(0), gl.divide}, c.ws, c.sc, q);
       g_launches.fetch_add(1, std::memory_order_relaxed);
       scalar_kernel<<<1, 1, 0, q>>>(FgGivens<T>{c.sc, c.hist, sm, j, m});
     }
@@ -1023,10 +1098,12 @@ static sk_status fgmres_solve(sk_matrix A, sk_precond M, const T* b, T* x,
     if (graphs) {
       auto it = execs.find(m_eff);
       if (it == execs.end()) {
-        const sk_precond_s* net_prec = M && M->kind == 4 ? M->smoother : M;
-        if (net_prec && net_prec->kind == 3 && (s = learned_prepare(net_prec)) != SK_OK) {
-          drop_graphs();
-          return s;
+        for (const sk_precond_s* P : {static_cast<const sk_precond_s*>(M), static_cast<const sk_precond_s*>(left)}) {
+          const sk_precond_s* net_prec = P && P->kind == 4 ? P->smoother : P;
+          if (net_prec && net_prec->kind == 3 && (s = learned_prepare(net_prec)) != SK_OK) {
+            drop_graphs();
+            return s;
+          }
         }
         const i64 before = g_launches.load();
         cudaGraph_t g = nullptr;
@@ -1441,6 +1518,31 @@ sk_status sk_fgmres_solve(sk_matrix A, sk_precond M, const void* b_dev, void* x_
                              history_host, cs);
 }
 
+sk_status sk_gmres_solve(sk_matrix A, sk_precond left, sk_precond right, const void* b_dev, void* x_dev,
+                         const sk_gmres_config* cfg, sk_summary* out, double* history_host, sk_stream s) {
+  sk_status st = check_solver_args(A, left, right, b_dev, x_dev);
+  if (st != SK_OK) return st;
+  SK_CHECK(cfg && out, SK_INVALID_ARG, "null config or summary");
+  SK_CHECK(cfg->max_iterations >= 0, SK_INVALID_ARG, "negative max_iterations");
+  const sk_fgmres_config fc{cfg->tolerance, cfg->restart_dimension, cfg->max_iterations, cfg->collect_residuals};
+  cudaStream_t cs = pick_stream(A, s);
+  if (A->dtype == SK_F64)
+    st = fgmres_solve<double>(A, right, static_cast<const double*>(b_dev), static_cast<double*>(x_dev), &fc, out,
+                              history_host, cs, nullptr, 0.0, nullptr, left, true);
+  else
+    st = fgmres_solve<float>(A, right, static_cast<const float*>(b_dev), static_cast<float*>(x_dev), &fc, out,
+                             history_host, cs, nullptr, 0.0, nullptr, left, true);
+  if (st != SK_OK) return st;
+  for (sk_precond P : {left, right}) {
+    const sk_precond_s* net_prec = P && P->kind == 4 ? P->smoother : P;
+    if (net_prec && net_prec->kind == 3) {
+      sk_status ns = sk_net_status(net_prec->net);
+      if (ns != SK_OK) return ns;
+    }
+  }
+  return SK_OK;
+}
+
 sk_status sk_fgmres_fallback_solve(sk_matrix A, sk_precond M, sk_precond fallback, const double* b_dev,
                                    double* x_dev, const sk_fgmres_config* cfg, double stall_ratio,
                                    sk_summary* out, double* history_host, int64_t* switched_at, sk_stream s) {
@@ -1469,6 +1571,13 @@ sk_status sk_bicgstab_solve_host(sk_matrix A, sk_precond left, sk_precond right,
                                  double* history_host) {
   return host_wrapper<sk_bicgstab_config>(A, b_host, x_host, [&](void* bd, void* xd) {
     return sk_bicgstab_solve(A, left, right, bd, xd, cfg, out, history_host, A->stream);
+  });
+}
+
+sk_status sk_gmres_solve_host(sk_matrix A, sk_precond left, sk_precond right, const void* b_host, void* x_host,
+                              const sk_gmres_config* cfg, sk_summary* out, double* history_host) {
+  return host_wrapper<sk_gmres_config>(A, b_host, x_host, [&](void* bd, void* xd) {
+    return sk_gmres_solve(A, left, right, bd, xd, cfg, out, history_host, A->stream);
   });
 }
 

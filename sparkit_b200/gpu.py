@@ -326,6 +326,27 @@ def fgmres(b, x, cfg, op, preconditioner=identity):
 
 
 @dataclass
+class Gmres_config:
+    """Gmres_config<T> (gmres.hpp:25-47)."""
+    tolerance: float = 0.0
+    restart_dimension: int = 0
+    max_iterations: int = 0
+    collect_residuals: bool = False
+
+
+def gmres(b, x, cfg, op, left=identity, right=identity):
+    """gmres(bfirst, blast, xfirst, xlast, cfg, op, left, right)."""
+    Ad = _op_matrix(op)
+    c = _lib.FgmresConfig(cfg.tolerance, cfg.restart_dimension, cfg.max_iterations, int(cfg.collect_residuals))
+    L = lib()
+    return _run(lambda bp, xp, cp, sp, hp, st: L.sk_gmres_solve(Ad.handle, _handle(left), _handle(right), bp, xp,
+                                                                cp, sp, hp, st),
+                lambda bp, xp, cp, sp, hp: L.sk_gmres_solve_host(Ad.handle, _handle(left), _handle(right), bp, xp,
+                                                                 cp, sp, hp),
+                b, x, Ad, c, cfg.max_iterations, cfg.collect_residuals)
+
+
+@dataclass
 class Mixed_config:
     """FP32-inner / FP64-outer iterative refinement (sk_mixed_cg_solve)."""
     tolerance: float = 1e-10

@@ -110,6 +110,8 @@ def main():
                 runs.append(("cg_right", lambda: R.cg(A, b, np.zeros(n), 1e-12, 7, 500, right=spec, collect=True)))
             runs.append(("bicgstab", lambda: R.bicgstab(A, b, np.zeros(n), 1e-12, 500, left=spec, collect=True)))
             runs.append(("fgmres", lambda: R.fgmres(A, b, np.zeros(n), 1e-12, 5, 500, prec=spec, collect=True)))
+            runs.append(("gmres_left", lambda: R.gmres(A, b, np.zeros(n), 1e-12, 5, 500, left=spec, collect=True)))
+            runs.append(("gmres_right", lambda: R.gmres(A, b, np.zeros(n), 1e-12, 6, 500, right=spec, collect=True)))
             for rname, fn in runs:
                 x, s = fn()
                 key = f"{base}/{pname}/{rname}"

@@ -75,7 +75,9 @@ def test_solvers_against_reference(gpu_lib, golden, name, pname):
     spec = PRECS[pname]
     M = make_prec(spec, Ad)
     runs = {"bicgstab": lambda x: gpu.bicgstab(b, x, gpu.Bicgstab_config(1e-12, 500, True), gpu.spmv(Ad), M),
-            "fgmres": lambda x: gpu.fgmres(b, x, gpu.Fgmres_config(1e-12, 5, 500, True), gpu.spmv(Ad), M)}
+            "fgmres": lambda x: gpu.fgmres(b, x, gpu.Fgmres_config(1e-12, 5, 500, True), gpu.spmv(Ad), M),
+            "gmres_left": lambda x: gpu.gmres(b, x, gpu.Gmres_config(1e-12, 5, 500, True), gpu.spmv(Ad), left=M),
+            "gmres_right": lambda x: gpu.gmres(b, x, gpu.Gmres_config(1e-12, 6, 500, True), gpu.spmv(Ad), right=M)}
     if name in SPD:
         runs["cg_left"] = lambda x: gpu.conjugate_gradient(b, x, gpu.CGConfig(1e-12, 50, 500, True), gpu.spmv(Ad), M,
                                                            gpu.identity)
@@ -114,7 +116,7 @@ def test_config1_jacobi_cg(gpu_lib, oracle):
     assert np.linalg.norm(r) / np.linalg.norm(b) < 1e-9
 
 
-@pytest.mark.parametrize("solver", ["bicgstab", "fgmres"])
+@pytest.mark.parametrize("solver", ["bicgstab", "fgmres", "gmres_left", "gmres_right", "gmres_both"])
 @pytest.mark.parametrize("pname", ["none", "jacobi", "cheb"])
 def test_nonsymmetric_medium(gpu_lib, oracle, solver, pname):
     A = matgen.convection_diffusion_2d(48, 48, 1.0, 0.9, 0.5)
@@ -127,14 +129,42 @@ def test_nonsymmetric_medium(gpu_lib, oracle, solver, pname):
     if solver == "bicgstab":
         xr, sr = oracle.bicgstab(A, b, np.zeros(n), 1e-10, 3000, left=spec)
         s = gpu.bicgstab(b, x, gpu.Bicgstab_config(1e-10, 3000), gpu.spmv(Ad), M)
-    else:
+    elif solver == "fgmres":
         xr, sr = oracle.fgmres(A, b, np.zeros(n), 1e-10, 30, 3000, prec=spec)
         s = gpu.fgmres(b, x, gpu.Fgmres_config(1e-10, 30, 3000), gpu.spmv(Ad), M)
+    else:  # GMRES(30) with M on the left, the right or both sides
+        lspec = spec if solver in ("gmres_left", "gmres_both") else None
+        rspec = spec if solver in ("gmres_right", "gmres_both") else None
+        xr, sr = oracle.gmres(A, b, np.zeros(n), 1e-10, 30, 3000, left=lspec, right=rspec)
+        s = gpu.gmres(b, x, gpu.Gmres_config(1e-10, 30, 3000), gpu.spmv(Ad), left=M if lspec else gpu.identity,
+                      right=M if rspec else gpu.identity)
     assert s.converged == sr["converged"]
     assert iters_close(s.computed_iterations, sr["computed_iterations"], solver), (s.computed_iterations,
                                                                                    sr["computed_iterations"])
     if s.converged:
-        assert np.linalg.norm(b - oracle.spmv(A, x)) <= 1e-9 * np.linalg.norm(b)
+        # a left preconditioner makes the test act on M_L r: the true
+        # residual is then bounded through ||M_L^-1|| (diagonal 5.2 here)
+        bound = 1e-9 if solver in ("bicgstab", "fgmres", "gmres_right") or pname == "none" else 1e-8
+        assert np.linalg.norm(b - oracle.spmv(A, x)) <= bound * np.linalg.norm(b)
+
+
+def test_gmres_matches_oracle_history(gpu_lib, oracle):
+    """GMRES(m) step by step: the per-step residual estimates |g_{j+1}| of
+    the device solve follow the oracle's (which is bit-exact with the
+    reference) to the rounding of the dot products, on a restarted run
+    whose budget ends inside a cycle."""
+    A = matgen.convdiff_2d_grf(24, seed=3)[0]
+    n = A.shape()[0]
+    b = oracle.spmv(A, matgen.uniform_vector(n, seed=5))
+    Ad = gpu.Device_matrix(A)
+    J = gpu.jacobi(Ad)
+    x = np.zeros(n)
+    s = gpu.gmres(b, x, gpu.Gmres_config(1e-14, 8, 45, True), gpu.spmv(Ad), left=J, right=J)
+    xr, sr = oracle.gmres(A, b, np.zeros(n), 1e-14, 8, 45, left="jacobi", right="jacobi", collect=True)
+    assert s.computed_iterations == sr["computed_iterations"] == 45 and not s.converged
+    h, hr = np.array(s.iteration_residuals), np.array(sr["iteration_residuals"])
+    assert np.allclose(h, hr, rtol=1e-8, atol=0), np.max(np.abs(h - hr) / hr)
+    assert np.linalg.norm(x - xr) <= 1e-8 * np.linalg.norm(xr)
 
 
 def test_edge_cases(gpu_lib):
@@ -165,6 +195,17 @@ def test_edge_cases(gpu_lib):
     x = np.arange(1.0, 17.0)
     bb = gpu.multiply(Ad, x)
     s = gpu.fgmres(bb, x, gpu.Fgmres_config(1e-12, 5, 100), gpu.spmv(Ad))
+    assert s.converged and np.array_equal(x, np.arange(1.0, 17.0))
+    # GMRES: zero right-hand side, the budget, and an exact initial guess
+    # (gmres.hpp:218-231 divides by the zero norm; here it ends the solve)
+    J = gpu.jacobi(Ad)
+    x = np.ones(n)
+    s = gpu.gmres(np.zeros(n), x, gpu.Gmres_config(1e-12, 5, 100), gpu.spmv(Ad), left=J)
+    assert s.converged and s.computed_iterations == 0 and not x.any()
+    s = gpu.gmres(b, np.zeros(n), gpu.Gmres_config(1e-14, 5, 2), gpu.spmv(Ad), left=J, right=J)
+    assert not s.converged and s.computed_iterations == 2
+    x = np.arange(1.0, 17.0)
+    s = gpu.gmres(bb, x, gpu.Gmres_config(1e-12, 5, 100), gpu.spmv(Ad), right=J)
     assert s.converged and np.array_equal(x, np.arange(1.0, 17.0))
 
 

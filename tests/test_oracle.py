@@ -83,7 +83,9 @@ def test_solvers_match_reference_bitwise(oracle, golden, name, pname):
     b = golden[f"solve/{name}/b"]
     spec = PRECS[pname]
     runs = {"bicgstab": lambda: oracle.bicgstab(A, b, np.zeros(n), 1e-12, 500, left=spec, collect=True),
-            "fgmres": lambda: oracle.fgmres(A, b, np.zeros(n), 1e-12, 5, 500, prec=spec, collect=True)}
+            "fgmres": lambda: oracle.fgmres(A, b, np.zeros(n), 1e-12, 5, 500, prec=spec, collect=True),
+            "gmres_left": lambda: oracle.gmres(A, b, np.zeros(n), 1e-12, 5, 500, left=spec, collect=True),
+            "gmres_right": lambda: oracle.gmres(A, b, np.zeros(n), 1e-12, 6, 500, right=spec, collect=True)}
     if name in SPD:
         runs["cg_left"] = lambda: oracle.cg(A, b, np.zeros(n), 1e-12, 50, 500, left=spec, collect=True)
         runs["cg_right"] = lambda: oracle.cg(A, b, np.zeros(n), 1e-12, 7, 500, right=spec, collect=True)
@@ -125,6 +127,26 @@ def test_float_solvers_match_reference(oracle, reference):
         assert np.array_equal(x, xr) and s == sr
         x, s = oracle.fgmres(A, b, np.zeros(n, np.float32), 1e-5, 10, 1000, prec=spec, collect=True)
         xr, sr = reference.fgmres(A, b, np.zeros(n, np.float32), 1e-5, 10, 1000, prec=spec, collect=True)
+        assert np.array_equal(x, xr) and s == sr
+        x, s = oracle.gmres(A, b, np.zeros(n, np.float32), 1e-5, 10, 1000, left=spec, right=spec, collect=True)
+        xr, sr = reference.gmres(A, b, np.zeros(n, np.float32), 1e-5, 10, 1000, left=spec, right=spec,
+                                 collect=True)
+        assert np.array_equal(x, xr) and s == sr
+
+
+def test_gmres_edge_cases_match_reference(oracle, reference):
+    """gmres.hpp:164-176 and :186-187: zero right-hand side, a budget that
+    ends inside a restart cycle, and both preconditioners at once."""
+    A = matgen.convdiff_2d_grf(12, seed=3)[0]
+    n = A.shape()[0]
+    b = matgen.uniform_vector(n, seed=2)
+    x, s = oracle.gmres(A, np.zeros(n), np.ones(n), 1e-10, 5, 50, left="jacobi")
+    xr, sr = reference.gmres(A, np.zeros(n), np.ones(n), 1e-10, 5, 50, left="jacobi")
+    assert not x.any() and s["converged"] and s["computed_iterations"] == 0 and s == sr
+    for spec in ("jacobi", ("chebyshev", 0.2, 9.0, 4)):
+        x, s = oracle.gmres(A, b, np.zeros(n), 1e-14, 7, 23, left=spec, right=spec, collect=True)
+        xr, sr = reference.gmres(A, b, np.zeros(n), 1e-14, 7, 23, left=spec, right=spec, collect=True)
+        assert s["computed_iterations"] == 23 and not s["converged"]
         assert np.array_equal(x, xr) and s == sr
 
 
