@@ -235,6 +235,15 @@ typedef struct {
   int32_t collect_residuals;
 } sk_fgmres_config;
 
+/* Cgs_config<T> (sparkit/data/cgs.hpp:25-42) and Minres_config<T>
+ * (minres.hpp:25-45): tolerance, max_iterations, collect_residuals */
+typedef struct {
+  double tolerance;
+  int64_t max_iterations;
+  int32_t collect_residuals;
+} sk_cgs_config;
+typedef sk_cgs_config sk_minres_config;
+
 /* Gmres_config<T>, sparkit/data/gmres.hpp:25-47 (the same fields) */
 typedef struct {
   double tolerance;
@@ -285,6 +294,21 @@ SK_API sk_status sk_gmres_solve(sk_matrix A, sk_precond left, sk_precond right,
                                 const void* b_dev, void* x_dev,
                                 const sk_gmres_config* cfg, sk_summary* out,
                                 double* history_host, sk_stream s);
+
+/* cgs(b, x, cfg, op, left, right) (sparkit/data/cgs.hpp:374-395):
+ * conjugate gradient squared; each step spends two matrix-vector products
+ * and counts as two iterations, as in the reference. */
+SK_API sk_status sk_cgs_solve(sk_matrix A, sk_precond left, sk_precond right,
+                              const void* b_dev, void* x_dev, const sk_cgs_config* cfg,
+                              sk_summary* out, double* history_host, sk_stream s);
+
+/* minres(b, x, cfg, op, left, right) (sparkit/data/minres.hpp:397-418):
+ * preconditioned MINRES with M = M_R M_L, for symmetric A (and SPD M);
+ * convergence on the recurrence's |phi_bar| / ||b||. */
+SK_API sk_status sk_minres_solve(sk_matrix A, sk_precond left, sk_precond right,
+                                 const void* b_dev, void* x_dev,
+                                 const sk_minres_config* cfg, sk_summary* out,
+                                 double* history_host, sk_stream s);
 
 /* Mixed precision (no reference counterpart; the reference solves in one
  * value type): FP64 iterative refinement around conjugate_gradient
@@ -505,6 +529,13 @@ SK_API sk_status sk_bicgstab_solve_host(sk_matrix A, sk_precond left,
 SK_API sk_status sk_fgmres_solve_host(sk_matrix A, sk_precond M, const void* b_host,
                                void* x_host, const sk_fgmres_config* cfg,
                                sk_summary* out, double* history_host);
+SK_API sk_status sk_cgs_solve_host(sk_matrix A, sk_precond left, sk_precond right,
+                                   const void* b_host, void* x_host, const sk_cgs_config* cfg,
+                                   sk_summary* out, double* history_host);
+SK_API sk_status sk_minres_solve_host(sk_matrix A, sk_precond left, sk_precond right,
+                                      const void* b_host, void* x_host,
+                                      const sk_minres_config* cfg, sk_summary* out,
+                                      double* history_host);
 SK_API sk_status sk_gmres_solve_host(sk_matrix A, sk_precond left, sk_precond right,
                                      const void* b_host, void* x_host,
                                      const sk_gmres_config* cfg, sk_summary* out,

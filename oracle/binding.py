@@ -210,6 +210,14 @@ class Oracle:
         return self._solve("gmres", A, [left, right], b, x0, FgmresCfg(tol, restart, max_it, int(collect)), max_it,
                            prec_matrix)
 
+    def cgs(self, A, b, x0, tol, max_it, left=None, right=None, collect=False, prec_matrix=None):
+        return self._solve("cgs", A, [left, right], b, x0, KrylovCfg(tol, max_it, int(collect)), max_it + 2,
+                           prec_matrix)
+
+    def minres(self, A, b, x0, tol, max_it, left=None, right=None, collect=False, prec_matrix=None):
+        return self._solve("minres", A, [left, right], b, x0, KrylovCfg(tol, max_it, int(collect)), max_it + 2,
+                           prec_matrix)
+
     # -------------------------------------------------------------- #
     # Learned preconditioner network (sk_oracle_net.c)                #
     # -------------------------------------------------------------- #
@@ -499,6 +507,31 @@ class Reference:
         if rc == -1:
             raise ValueError("jacobi: zero diagonal entry")
         return x, s.as_dict(hist)
+
+    def _krylov2(self, name, A, b, x0, tol, max_it, left, right, collect):
+        h = self.csr_handle(A)
+        lk, lmin, lmax, deg = self._pk(left)
+        rk, rmin, rmax, rdeg = self._pk(right)
+        if rk == 2:
+            lmin, lmax, deg = rmin, rmax, rdeg
+        b = np.ascontiguousarray(b, dtype=A.dtype)
+        x = np.array(x0, dtype=A.dtype, copy=True)
+        hist = np.zeros(max_it + 4)
+        s = Summary()
+        rc = getattr(self.L, f"ref_{name}_{_sfx(A.dtype)}")(c_vp(h), _p(b), _p(x), ctypes.c_double(tol),
+                                                           c_i64(max_it), int(collect), lk, rk,
+                                                           ctypes.c_double(lmin), ctypes.c_double(lmax), c_i64(deg),
+                                                           ctypes.byref(s), _p(hist))
+        self.destroy(h, A.dtype)
+        if rc == -1:
+            raise ValueError("jacobi: zero diagonal entry")
+        return x, s.as_dict(hist)
+
+    def cgs(self, A, b, x0, tol, max_it, left=None, right=None, collect=False):
+        return self._krylov2("cgs", A, b, x0, tol, max_it, left, right, collect)
+
+    def minres(self, A, b, x0, tol, max_it, left=None, right=None, collect=False):
+        return self._krylov2("minres", A, b, x0, tol, max_it, left, right, collect)
 
     # generators of the reference's tests ----------------------------
     def _gen(self, name, dtype, *args):

@@ -12,8 +12,9 @@
 // (conversions.hpp:427, :524, :641), jacobi / jacobi_apply (jacobi.hpp:27,
 // :44), chebyshev_preconditioner / _apply (chebyshev_preconditioner.hpp:46,
 // :98), conjugate_gradient (conjugate_gradient.hpp:347), bicgstab
-// (bicgstab.hpp:391), fgmres (fgmres.hpp:459), gmres (gmres.hpp:408) and
-// the matrix generators of matgen.hpp used by the reference's solver tests.
+// (bicgstab.hpp:391), fgmres (fgmres.hpp:459), gmres (gmres.hpp:408), cgs
+// (cgs.hpp:374), minres (minres.hpp:397) and the matrix generators of
+// matgen.hpp used by the reference's solver tests.
 
 #include <algorithm>
 #include <chrono>
@@ -34,6 +35,8 @@
 #include <sparkit/data/conversions.hpp>
 #include <sparkit/data/fgmres.hpp>
 #include <sparkit/data/gmres.hpp>
+#include <sparkit/data/cgs.hpp>
+#include <sparkit/data/minres.hpp>
 #include <sparkit/data/jacobi.hpp>
 #include <sparkit/data/matgen.hpp>
 #include <sparkit/data/sparse_blas.hpp>
@@ -246,6 +249,24 @@ namespace {
     return 0;
   }
 
+  // cgs (cgs.hpp:374) and minres (minres.hpp:397): the bicgstab signature
+  template <typename T, typename Cfg, typename F>
+  int krylov2(Handle<T> const* A, i64 n, T const* b, T* x, double tol,
+              i64 max_it, int collect, int lk, int rk, double lmin,
+              double lmax, i64 deg, Summary* out, double* history, F solve) {
+    Prec<T> L, R;
+    int e = setup_prec(L, A, lk, lmin, lmax, deg);
+    if (e) return e;
+    e = setup_prec(R, A, rk, lmin, lmax, deg);
+    if (e) return e;
+    std::vector<T> bv(b, b + n), xv(x, x + n);
+    Cfg cfg{static_cast<T>(tol), max_it, collect != 0};
+    auto s = solve(bv, xv, cfg, L, R);
+    std::copy(xv.begin(), xv.end(), x);
+    fill_summary<decltype(s), T>(out, s, history);
+    return 0;
+  }
+
 } // namespace
 
 #define REF_API extern "C" __attribute__((visibility("default")))
@@ -402,6 +423,29 @@ namespace {
     auto* A = static_cast<Handle<T>*>(h);                                      \
     return gmres<T>(A, A->nrow(), b, x, tol, restart, max_it, collect, lk, rk, \
                     lmin, lmax, deg, out, hist);                               \
+  }                                                                            \
+  REF_API int ref_cgs_##S(void* h, T const* b, T* x, double tol, i64 max_it,   \
+                          int collect, int lk, int rk, double lmin,            \
+                          double lmax, i64 deg, Summary* out, double* hist) {  \
+    auto* A = static_cast<Handle<T>*>(h);                                      \
+    return krylov2<T, sd::Cgs_config<T>>(                                      \
+      A, A->nrow(), b, x, tol, max_it, collect, lk, rk, lmin, lmax, deg, out,  \
+      hist, [&](auto& bv, auto& xv, auto cfg, auto& L, auto& R) {              \
+        return sd::cgs(bv.begin(), bv.end(), xv.begin(), xv.end(), cfg,        \
+                       Op<T>{A}, std::cref(L), std::cref(R));                  \
+      });                                                                      \
+  }                                                                            \
+  REF_API int ref_minres_##S(void* h, T const* b, T* x, double tol,            \
+                             i64 max_it, int collect, int lk, int rk,          \
+                             double lmin, double lmax, i64 deg, Summary* out,  \
+                             double* hist) {                                   \
+    auto* A = static_cast<Handle<T>*>(h);                                      \
+    return krylov2<T, sd::Minres_config<T>>(                                   \
+      A, A->nrow(), b, x, tol, max_it, collect, lk, rk, lmin, lmax, deg, out,  \
+      hist, [&](auto& bv, auto& xv, auto cfg, auto& L, auto& R) {              \
+        return sd::minres(bv.begin(), bv.end(), xv.begin(), xv.end(), cfg,     \
+                          Op<T>{A}, std::cref(L), std::cref(R));               \
+      });                                                                      \
   }                                                                            \
   REF_API void* ref_poisson_2d_##S(i64 nx, i64 ny, double shift) {             \
     return wrap_csr<T>(sd::poisson_2d<T>(nx, ny, static_cast<T>(shift)));      \

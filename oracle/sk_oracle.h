@@ -61,7 +61,8 @@ typedef struct {
   int32_t collect_residuals;
 } sko_cg_config;
 
-/* Bicgstab_config, sparkit/data/bicgstab.hpp:25-42 */
+/* Bicgstab_config, sparkit/data/bicgstab.hpp:25-42; Cgs_config
+ * (cgs.hpp:25-42) and Minres_config (minres.hpp:25-45) have the same fields */
 typedef struct {
   double tolerance;
   int64_t max_iterations;
@@ -113,7 +114,13 @@ typedef struct {
                       const sko_fgmres_config*, sko_summary*, double*);       \
   void sko_gmres_##S(const sko_operator*, const sko_precond*,                 \
                      const sko_precond*, const T*, T*,                        \
-                     const sko_fgmres_config*, sko_summary*, double*);
+                     const sko_fgmres_config*, sko_summary*, double*);        \
+  void sko_cgs_##S(const sko_operator*, const sko_precond*,                   \
+                   const sko_precond*, const T*, T*,                          \
+                   const sko_krylov_config*, sko_summary*, double*);          \
+  void sko_minres_##S(const sko_operator*, const sko_precond*,                \
+                      const sko_precond*, const T*, T*,                       \
+                      const sko_krylov_config*, sko_summary*, double*);
 
 /* Summation order of the solvers' dot products: 0 = the reference's
  * sequential order (default), 1 = 256-element chunks added in order. */

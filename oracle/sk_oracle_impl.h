@@ -650,6 +650,193 @@ done:
   free(w); free(r0); free(work);
 }
 
+/* ------------------------------------------------------------------ */
+/* Conjugate gradient squared with left and right preconditioning      */
+/* Follows sparkit/data/cgs.hpp:106-395 step for step (two matrix-     */
+/* vector products per step, counted as two iterations; rho_new == 0   */
+/* leaves the directions as they are, as the reference does).          */
+/* ------------------------------------------------------------------ */
+void SKO_FN(sko_cgs_)(const sko_operator* A, const sko_precond* ML,
+                      const sko_precond* MR, const SKO_T* b, SKO_T* x,
+                      const sko_krylov_config* cfg, sko_summary* out,
+                      double* history) {
+  int64_t n = A->nrow;
+  size_t vb = sizeof(SKO_T) * (size_t)(n + 1);
+  SKO_T* r = (SKO_T*)calloc(1, vb);
+  SKO_T* r_hat = (SKO_T*)calloc(1, vb);
+  SKO_T* p = (SKO_T*)calloc(1, vb);
+  SKO_T* u = (SKO_T*)calloc(1, vb);
+  SKO_T* q = (SKO_T*)calloc(1, vb);
+  SKO_T* q_hat = (SKO_T*)calloc(1, vb);
+  SKO_T* u_hat = (SKO_T*)calloc(1, vb);
+  SKO_T* p_hat = (SKO_T*)calloc(1, vb);
+  SKO_T* tmp = (SKO_T*)calloc(1, vb);
+  SKO_T* work = (SKO_T*)calloc(3, vb);
+  int64_t nhist = 0;
+  out->residual_norm = 0;
+  out->computed_iterations = 0;
+  out->converged = 0;
+  out->status = 0;
+  SKO_T bnorm = SKO_SQRT(SKO_FN(sko_dot_)(b, b, n)); /* :168 */
+  if (bnorm == (SKO_T)0) {
+    for (int64_t i = 0; i < n; ++i) x[i] = 0;
+    out->converged = 1;
+    goto done;
+  }
+  SKO_FN(sko_apply_op_)(A, x, tmp); /* compute_initial_residual :191-198 */
+  for (int64_t i = 0; i < n; ++i) r[i] = b[i] - tmp[i];
+  memcpy(r_hat, r, vb); /* :201-209 */
+  memcpy(p, r, vb);
+  memcpy(u, r, vb);
+  SKO_T rho = SKO_FN(sko_dot_)(r_hat, r, n);
+  while (out->computed_iterations < cfg->max_iterations && !out->converged) {
+    /* cgs_step :212-232 */
+    SKO_FN(sko_apply_prec_)(ML, A, p, tmp, n, work); /* compute_q_hat :235-239 */
+    SKO_FN(sko_apply_prec_)(MR, A, tmp, p_hat, n, work);
+    SKO_FN(sko_apply_op_)(A, p_hat, q_hat);
+    SKO_T alpha = rho / SKO_FN(sko_dot_)(r_hat, q_hat, n); /* :242-244 */
+    for (int64_t i = 0; i < n; ++i) q[i] = u[i] - alpha * q_hat[i]; /* :247-252 */
+    for (int64_t i = 0; i < n; ++i) u_hat[i] = u[i] + q[i];          /* :255-260 */
+    SKO_FN(sko_apply_prec_)(ML, A, u_hat, tmp, n, work);             /* :263-266 */
+    SKO_FN(sko_apply_prec_)(MR, A, tmp, p_hat, n, work);
+    for (int64_t i = 0; i < n; ++i) x[i] += alpha * p_hat[i];        /* :269-275 */
+    SKO_FN(sko_apply_op_)(A, p_hat, tmp);                            /* :278-284 */
+    for (int64_t i = 0; i < n; ++i) r[i] -= alpha * tmp[i];
+    out->computed_iterations += 2;
+    SKO_T r_norm = SKO_SQRT(SKO_FN(sko_dot_)(r, r, n)); /* check_convergence :287-298 */
+    out->residual_norm = (double)r_norm;
+    if (history && cfg->collect_residuals) history[nhist++] = (double)r_norm;
+    if (r_norm / bnorm < (SKO_T)cfg->tolerance) {
+      out->converged = 1;
+      break;
+    }
+    SKO_T rho_new = SKO_FN(sko_dot_)(r_hat, r, n);
+    if (rho_new == (SKO_T)0) continue;
+    SKO_T beta = rho_new / rho;
+    for (int64_t i = 0; i < n; ++i) u[i] = r[i] + beta * q[i]; /* :301-309 */
+    for (int64_t i = 0; i < n; ++i) p[i] = u[i] + beta * (q[i] + beta * p[i]);
+    rho = rho_new;
+  }
+done:
+  out->history_length = nhist;
+  free(r); free(r_hat); free(p); free(u); free(q); free(q_hat); free(u_hat);
+  free(p_hat); free(tmp); free(work);
+}
+
+/* ------------------------------------------------------------------ */
+/* MINRES with left and right preconditioning                          */
+/* Follows sparkit/data/minres.hpp:106-418 step for step, including    */
+/* its two exits: rho == 0 in apply_givens_rotations (:265-286) marks  */
+/* convergence but the step still updates x with the previous step's   */
+/* rho, delta and phi before check_convergence (:300-309) decides      */
+/* again; beta_new == 0 skips rotate_state (:311-325), so the next step */
+/* repeats on the same Lanczos vectors.                                 */
+/* ------------------------------------------------------------------ */
+void SKO_FN(sko_minres_)(const sko_operator* A, const sko_precond* ML,
+                         const sko_precond* MR, const SKO_T* b, SKO_T* x,
+                         const sko_krylov_config* cfg, sko_summary* out,
+                         double* history) {
+  int64_t n = A->nrow;
+  size_t vb = sizeof(SKO_T) * (size_t)(n + 1);
+  SKO_T* v_prev = (SKO_T*)calloc(1, vb);
+  SKO_T* v = (SKO_T*)calloc(1, vb);
+  SKO_T* z = (SKO_T*)calloc(1, vb);
+  SKO_T* w = (SKO_T*)calloc(1, vb);
+  SKO_T* tmp = (SKO_T*)calloc(1, vb);
+  SKO_T* d_prev = (SKO_T*)calloc(1, vb);
+  SKO_T* d = (SKO_T*)calloc(1, vb);
+  SKO_T* work = (SKO_T*)calloc(3, vb);
+  int64_t nhist = 0;
+  SKO_T beta = 0, alpha = 0, epsilon = 0, delta = 0, rho = 0, phi = 0, phi_bar = 0;
+  SKO_T cs_prev = 0, sn_prev = 0, cs = 0, sn = 0, cs_new = 0, sn_new = 0;
+  out->residual_norm = 0;
+  out->computed_iterations = 0;
+  out->converged = 0;
+  out->status = 0;
+  SKO_T bnorm = SKO_SQRT(SKO_FN(sko_dot_)(b, b, n)); /* :170 */
+  if (bnorm == (SKO_T)0) {
+    for (int64_t i = 0; i < n; ++i) x[i] = 0;
+    out->converged = 1;
+    goto done;
+  }
+  /* compute_initial_residual :184-217 */
+  SKO_FN(sko_apply_op_)(A, x, w);
+  for (int64_t i = 0; i < n; ++i) v[i] = b[i] - w[i];
+  SKO_FN(sko_apply_prec_)(ML, A, v, tmp, n, work);
+  SKO_FN(sko_apply_prec_)(MR, A, tmp, z, n, work);
+  beta = SKO_SQRT(SKO_FN(sko_dot_)(v, z, n));
+  if (beta == (SKO_T)0) {
+    out->converged = 1;
+    goto done;
+  }
+  {
+    SKO_T inv_beta = (SKO_T)1 / beta;
+    for (int64_t i = 0; i < n; ++i) v[i] = v[i] * inv_beta;
+    for (int64_t i = 0; i < n; ++i) z[i] = z[i] * inv_beta;
+  }
+  phi_bar = beta;
+  cs_prev = 1; sn_prev = 0; cs = 1; sn = 0;
+  while (out->computed_iterations < cfg->max_iterations && !out->converged) {
+    /* minres_step :225-234; lanczos_step :237-247 */
+    SKO_FN(sko_apply_op_)(A, z, w);
+    alpha = SKO_FN(sko_dot_)(z, w, n);
+    for (int64_t i = 0; i < n; ++i) w[i] -= alpha * v[i] + beta * v_prev[i];
+    /* precondition_lanczos :250-262 */
+    SKO_FN(sko_apply_prec_)(ML, A, w, tmp, n, work);
+    SKO_FN(sko_apply_prec_)(MR, A, tmp, v_prev, n, work);
+    SKO_T beta_new = SKO_SQRT(SKO_FN(sko_dot_)(w, v_prev, n));
+    /* apply_givens_rotations :265-286 */
+    epsilon = sn_prev * beta;
+    {
+      SKO_T delta_1 = cs_prev * beta;
+      SKO_T delta_l = cs * delta_1 + sn * alpha;
+      SKO_T rho_bar = -sn * delta_1 + cs * alpha;
+      SKO_T rho_l = SKO_SQRT(rho_bar * rho_bar + beta_new * beta_new);
+      if (rho_l == (SKO_T)0) {
+        out->converged = 1;
+      } else {
+        cs_new = rho_bar / rho_l;
+        sn_new = beta_new / rho_l;
+        phi = cs_new * phi_bar;
+        phi_bar = -sn_new * phi_bar;
+        rho = rho_l;
+        delta = delta_l;
+      }
+    }
+    /* update_solution :288-297 */
+    for (int64_t i = 0; i < n; ++i) {
+      SKO_T d_old = d[i];
+      d_prev[i] = (z[i] - delta * d[i] - epsilon * d_prev[i]) / rho;
+      d[i] = d_prev[i];
+      d_prev[i] = d_old;
+      x[i] += phi * d[i];
+    }
+    {
+      SKO_T res = SKO_FABS(phi_bar); /* check_convergence :300-309 */
+      out->residual_norm = (double)res;
+      out->converged = res / bnorm < (SKO_T)cfg->tolerance;
+      if (history && cfg->collect_residuals) history[nhist++] = (double)res;
+    }
+    out->computed_iterations += 1;
+    if (out->converged || beta_new == (SKO_T)0) continue;
+    {
+      SKO_T inv_beta_new = (SKO_T)1 / beta_new; /* rotate_state :311-325 */
+      for (int64_t i = 0; i < n; ++i) {
+        SKO_T v_old = v[i];
+        z[i] = v_prev[i] * inv_beta_new;
+        v_prev[i] = v_old;
+        v[i] = w[i] * inv_beta_new;
+      }
+      cs_prev = cs; sn_prev = sn; cs = cs_new; sn = sn_new;
+      beta = beta_new;
+    }
+  }
+done:
+  out->history_length = nhist;
+  free(v_prev); free(v); free(z); free(w); free(tmp); free(d_prev); free(d);
+  free(work);
+}
+
 #undef SKO_FN
 #undef SKO_CAT
 #undef SKO_CAT2

@@ -125,6 +125,10 @@ SIGNATURES = [
                          c_vp, c_vp]),
     ("sk_gmres_solve", [c_vp, c_vp, c_vp, c_vp, c_vp, ctypes.POINTER(FgmresConfig), ctypes.POINTER(Summary),
                         c_vp, c_vp]),
+    ("sk_cgs_solve", [c_vp, c_vp, c_vp, c_vp, c_vp, ctypes.POINTER(BicgstabConfig), ctypes.POINTER(Summary),
+                      c_vp, c_vp]),
+    ("sk_minres_solve", [c_vp, c_vp, c_vp, c_vp, c_vp, ctypes.POINTER(BicgstabConfig), ctypes.POINTER(Summary),
+                         c_vp, c_vp]),
     ("sk_mixed_cg_solve", [c_vp, c_i32, c_vp, c_vp, ctypes.POINTER(MixedConfig), ctypes.POINTER(MixedSummary),
                            c_vp, c_vp]),
     ("sk_batch_create", [ctypes.POINTER(c_vp), c_i64, c_vp, c_vp, c_vp, c_vp]),
@@ -161,6 +165,10 @@ SIGNATURES = [
                               c_vp]),
     ("sk_gmres_solve_host", [c_vp, c_vp, c_vp, c_vp, c_vp, ctypes.POINTER(FgmresConfig), ctypes.POINTER(Summary),
                              c_vp]),
+    ("sk_cgs_solve_host", [c_vp, c_vp, c_vp, c_vp, c_vp, ctypes.POINTER(BicgstabConfig), ctypes.POINTER(Summary),
+                           c_vp]),
+    ("sk_minres_solve_host", [c_vp, c_vp, c_vp, c_vp, c_vp, ctypes.POINTER(BicgstabConfig),
+                              ctypes.POINTER(Summary), c_vp]),
 ]
 
 _lock = threading.Lock()

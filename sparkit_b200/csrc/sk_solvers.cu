@@ -1153,6 +1153,564 @@ static sk_status fgmres_solve(sk_matrix A, sk_precond M, const T* b, T* x,
   return finish_summary(c, st, out, history_host);
 }
 
+// ==================================================================
+// Preconditioner pair of CGS and MINRES: out = M_R (M_L in), applied in
+// that order as cgs.hpp:235-239 / minres.hpp:190-191 do.  Identity and
+// Jacobi on both sides fuse into one element-wise pass.
+// ==================================================================
+template <typename T>
+struct OpLR {
+  static constexpr int kNR = 0;
+  const T* invl;  // null: identity
+  const T* invr;
+  const T* in;
+  T* out;
+  struct In { T v, l, r; };
+  __device__ bool prepare(const Scalars* sc) { return !solve_done(sc); }
+  __device__ In load(i64 i) const { return {in[i], invl ? invl[i] : T(0), invr ? invr[i] : T(0)}; }
+  __device__ void apply(i64 i, In const& q, double*) const {
+    T v = q.v;
+    if (invl) v = mul(q.l, v);
+    if (invr) v = mul(q.r, v);
+    out[i] = v;
+  }
+  __device__ void finalize(const double*) const {}
+};
+
+template <typename T>
+struct LRPair {
+  const sk_precond_s* L;
+  const sk_precond_s* R;
+  const T* invl = nullptr;
+  const T* invr = nullptr;
+  bool fused = false;  // both sides identity or Jacobi
+  LRPair(const sk_precond_s* l, const sk_precond_s* r) : L(l), R(r) {
+    const bool lf = !l || l->kind == 1, rf = !r || r->kind == 1;
+    fused = lf && rf;
+    if (l && l->kind == 1) invl = static_cast<const T*>(l->inv_diag);
+    if (r && r->kind == 1) invr = static_cast<const T*>(r->inv_diag);
+  }
+};
+
+template <typename T>
+static void apply_lr(LRPair<T> const& lr, i64 n, const T* in, T* tmp, T* out, SolveCommon const& c,
+                     cudaStream_t st) {
+  const sk_dtype dt = sizeof(T) == 8 ? SK_F64 : SK_F32;
+  if (lr.fused) {
+    launch_vec(n, OpLR<T>{lr.invl, lr.invr, in, out}, c.ws, c.sc, st);
+    return;
+  }
+  precond_apply_dispatch(lr.L, dt, n, in, tmp, c.ws, c.sc, st);
+  precond_apply_dispatch(lr.R, dt, n, tmp, out, c.ws, c.sc, st);
+}
+
+// ==================================================================
+// CGS, cgs.hpp:106-395
+// ==================================================================
+
+// compute_initial_residual (:191-198), initialize_shadow_residual and
+// initialize_search_directions (:201-209), rho = <r_hat, r> (:178).
+template <typename T>
+struct EpiCgsInit {
+  static constexpr int kNR = 1;
+  const T* b;
+  T *r, *r_hat, *p, *u;
+  Scalars* sc;
+  __device__ void operator()(int row, T ax, double* red) const {
+    const T ri = sub(b[row], ax);
+    r[row] = r_hat[row] = p[row] = u[row] = ri;
+    red[0] += static_cast<double>(mul(ri, ri));
+  }
+  __device__ void finalize(const double* t) const { sc->rho = static_cast<double>(static_cast<T>(t[0])); }
+};
+
+// compute_q_hat's product (:235-239) and compute_alpha (:242-244)
+template <typename T>
+struct EpiCgsQhat {
+  static constexpr int kNR = 1;
+  T* q_hat;
+  const T* r_hat;
+  Scalars* sc;
+  __device__ void operator()(int row, T v, double* red) const {
+    q_hat[row] = v;
+    red[0] += static_cast<double>(mul(r_hat[row], v));
+  }
+  __device__ void finalize(const double* t) const {
+    sc->alpha = static_cast<double>(static_cast<T>(sc->rho) / static_cast<T>(t[0]));
+  }
+};
+
+// compute_q (:247-252), compute_u_hat (:255-260); with a fusable
+// preconditioner pair also apply_preconditioner_to_u_hat (:263-266) and
+// update_solution (:269-275).
+template <typename T>
+struct OpCgsQ {
+  static constexpr int kNR = 0;
+  const T* u;
+  const T* q_hat;
+  T* q;
+  T* u_hat;   // written when not fused
+  T* p_hat;   // fused: p_hat = M_R M_L u_hat, x += alpha p_hat
+  T* x;
+  const T* invl;
+  const T* invr;
+  bool fused;
+  T alpha;
+  struct In { T u, qh, x, l, r; };
+  __device__ bool prepare(const Scalars* s) {
+    if (solve_done(s)) return false;
+    alpha = static_cast<T>(s->alpha);
+    return true;
+  }
+  __device__ In load(i64 i) const {
+    return {u[i], q_hat[i], fused ? x[i] : T(0), fused && invl ? invl[i] : T(0), fused && invr ? invr[i] : T(0)};
+  }
+  __device__ void apply(i64 i, In const& v, double*) const {
+    const T qi = sub(v.u, mul(alpha, v.qh));
+    q[i] = qi;
+    T uh = add(v.u, qi);
+    if (!fused) {
+      u_hat[i] = uh;
+      return;
+    }
+    if (invl) uh = mul(v.l, uh);
+    if (invr) uh = mul(v.r, uh);
+    p_hat[i] = uh;
+    x[i] = add(v.x, mul(alpha, uh));
+  }
+  __device__ void finalize(const double*) const {}
+};
+
+// update_solution (:269-275) after a general preconditioner pair
+template <typename T>
+struct OpCgsX {
+  static constexpr int kNR = 0;
+  T* x;
+  const T* p_hat;
+  T alpha;
+  struct In { T x, p; };
+  __device__ bool prepare(const Scalars* s) {
+    if (solve_done(s)) return false;
+    alpha = static_cast<T>(s->alpha);
+    return true;
+  }
+  __device__ In load(i64 i) const { return {x[i], p_hat[i]}; }
+  __device__ void apply(i64 i, In const& v, double*) const { x[i] = add(v.x, mul(alpha, v.p)); }
+  __device__ void finalize(const double*) const {}
+};
+
+// compute_residual_update (:278-284), check_convergence (:287-298), and
+// rho_new = <r_hat, r> with its zero test and beta (:224-231).
+template <typename T>
+struct EpiCgsR {
+  static constexpr int kNR = 2;
+  T* r;
+  const T* r_hat;
+  Scalars* sc;
+  double* hist;
+  __device__ void operator()(int row, T ax, double* red) const {
+    const T ri = sub(r[row], mul(static_cast<T>(sc->alpha), ax));
+    r[row] = ri;
+    red[0] += static_cast<double>(mul(ri, ri));
+    red[1] += static_cast<double>(mul(r_hat[row], ri));
+  }
+  __device__ void finalize(const double* t) const {
+    sc->iters += 2;
+    const T rn = sqrt(static_cast<T>(t[0]));
+    record(sc, hist, static_cast<double>(rn));
+    if (rn / static_cast<T>(sc->bnorm) < static_cast<T>(sc->tol)) {
+      sc->converged = 1;
+      sc->done = 1;
+      return;
+    }
+    const T rho_new = static_cast<T>(t[1]);
+    if (rho_new == T(0)) {
+      sc->skip = 1;
+    } else {
+      sc->skip = 0;
+      sc->beta = static_cast<double>(rho_new / static_cast<T>(sc->rho));
+      sc->rho = static_cast<double>(rho_new);
+    }
+    if (sc->iters >= sc->max_iters) sc->done = 1;
+  }
+};
+
+// update_search_directions (:301-309)
+template <typename T>
+struct OpCgsDir {
+  static constexpr int kNR = 0;
+  const T* r;
+  const T* q;
+  T* u;
+  T* p;
+  T beta;
+  struct In { T r, q, p; };
+  __device__ bool prepare(const Scalars* s) {
+    if (solve_done(s) || s->skip) return false;
+    beta = static_cast<T>(s->beta);
+    return true;
+  }
+  __device__ In load(i64 i) const { return {r[i], q[i], p[i]}; }
+  __device__ void apply(i64 i, In const& v, double*) const {
+    const T ui = add(v.r, mul(beta, v.q));
+    u[i] = ui;
+    p[i] = add(ui, mul(beta, add(v.q, mul(beta, v.p))));
+  }
+  __device__ void finalize(const double*) const {}
+};
+
+template <typename T>
+static sk_status cgs_solve(sk_matrix A, sk_precond L, sk_precond R, const T* b, T* x, const sk_cgs_config* cfg,
+                           sk_summary* out, double* history_host, cudaStream_t st) {
+  const i64 n = A->nrow;
+  const size_t vb = static_cast<size_t>(n + 8) * sizeof(T);
+  SolveCommon c;
+  std::vector<char*> vv;
+  const i64 hist_cap = cfg->collect_residuals ? cfg->max_iterations / 2 + 4 : 0;
+  sk_status s = carve_common(A, st, 9, vb, 0, hist_cap, &c, &vv, nullptr);
+  if (s != SK_OK) return s;
+  T *r = (T*)vv[0], *r_hat = (T*)vv[1], *p = (T*)vv[2], *u = (T*)vv[3], *q = (T*)vv[4], *q_hat = (T*)vv[5],
+    *u_hat = (T*)vv[6], *p_hat = (T*)vv[7], *tmp = (T*)vv[8];
+  *out = sk_summary{};
+  double bnorm = 0;
+  if ((s = norm_b<T>(b, n, c, st, &bnorm)) != SK_OK) return s;
+  if (bnorm == 0.0) {  // :168-172
+    SK_CUDA(cudaMemsetAsync(x, 0, n * sizeof(T), st));
+    SK_CUDA(cudaStreamSynchronize(st));
+    out->converged = 1;
+    return SK_OK;
+  }
+  Scalars h{};
+  h.bnorm = bnorm;
+  h.tol = cfg->tolerance;
+  h.max_iters = cfg->max_iterations;
+  h.hist_on = cfg->collect_residuals ? 1 : 0;
+  h.done = cfg->max_iterations <= 0 ? 1 : 0;
+  if ((s = put_scalars(c.sc, h, st)) != SK_OK) return s;
+  launch_spmv<T>(A, x, EpiCgsInit<T>{b, r, r_hat, p, u, c.sc}, c.ws, nullptr, st);
+  const LRPair<T> lr(L, R);
+  i64 steps = 0, chunk = 4;
+  while (!h.done) {
+    for (i64 j = 0; j < chunk; ++j, ++steps) {  // cgs_step (:212-232)
+      apply_lr<T>(lr, n, p, tmp, p_hat, c, st);
+      launch_spmv<T>(A, p_hat, EpiCgsQhat<T>{q_hat, r_hat, c.sc}, c.ws, c.sc, st);
+      launch_vec(n, OpCgsQ<T>{u, q_hat, q, u_hat, p_hat, x, lr.invl, lr.invr, lr.fused, T(0)}, c.ws, c.sc, st);
+      if (!lr.fused) {
+        apply_lr<T>(lr, n, u_hat, tmp, p_hat, c, st);
+        launch_vec(n, OpCgsX<T>{x, p_hat, T(0)}, c.ws, c.sc, st);
+      }
+      launch_spmv<T>(A, p_hat, EpiCgsR<T>{r, r_hat, c.sc, c.hist}, c.ws, c.sc, st);
+      launch_vec(n, OpCgsDir<T>{r, q, u, p, T(0)}, c.ws, c.sc, st);
+    }
+    SK_CUDA(cudaGetLastError());
+    if ((s = read_scalars(c.sc, &h, st)) != SK_OK) return s;
+    chunk = std::min<i64>(chunk * 2, 32);
+  }
+  return finish_summary(c, st, out, history_host);
+}
+
+// ==================================================================
+// MINRES, minres.hpp:106-418
+// ==================================================================
+
+struct MinScalars {  // the solver's recurrence scalars, in T (stored as double)
+  double alpha, beta, eps, delta, rho, phi, phi_bar, cs_prev, sn_prev, cs, sn, cs_new, sn_new, inv_bn;
+  int rotate;   // this step rotates the Lanczos vectors (:230-233)
+  int pending;  // update_solution of the step just run is still to be applied
+};
+
+// compute_initial_residual (:184-217): v = b - A x; z = M_R M_L v
+// (fused pair) and beta = sqrt(<v, z>).
+template <typename T>
+__device__ void min_init_finalize(T beta, Scalars* sc, MinScalars* ms) {
+  if (beta == T(0)) {
+    sc->converged = 1;
+    sc->done = 1;
+    return;
+  }
+  ms->beta = static_cast<double>(beta);
+  ms->inv_bn = static_cast<double>(T(1) / beta);
+  ms->phi_bar = static_cast<double>(beta);
+  ms->cs_prev = 1.0;
+  ms->sn_prev = 0.0;
+  ms->cs = 1.0;
+  ms->sn = 0.0;
+}
+
+template <typename T>
+struct EpiMinInit {
+  static constexpr int kNR = 1;
+  const T* b;
+  T* v;
+  T* z;  // fused pair: z = M_R M_L v
+  const T* invl;
+  const T* invr;
+  bool fused;
+  Scalars* sc;
+  MinScalars* ms;
+  __device__ void operator()(int row, T ax, double* red) const {
+    const T vi = sub(b[row], ax);
+    v[row] = vi;
+    if (!fused) return;
+    T zi = vi;
+    if (invl) zi = mul(invl[row], zi);
+    if (invr) zi = mul(invr[row], zi);
+    z[row] = zi;
+    red[0] += static_cast<double>(mul(vi, zi));
+  }
+  __device__ void finalize(const double* t) const {
+    if (fused) min_init_finalize<T>(sqrt(static_cast<T>(t[0])), sc, ms);
+  }
+};
+
+// beta = sqrt(<v, z>) after a general preconditioner pair
+template <typename T>
+struct OpMinInitDot {
+  static constexpr int kNR = 1;
+  const T* v;
+  const T* z;
+  Scalars* sc;
+  MinScalars* ms;
+  struct In { T v, z; };
+  __device__ bool prepare(const Scalars*) { return true; }
+  __device__ In load(i64 i) const { return {v[i], z[i]}; }
+  __device__ void apply(i64, In const& q, double* red) const { red[0] += static_cast<double>(mul(q.v, q.z)); }
+  __device__ void finalize(const double* t) const { min_init_finalize<T>(sqrt(static_cast<T>(t[0])), sc, ms); }
+};
+
+// v *= 1 / beta, z *= 1 / beta (:207-214)
+template <typename T>
+struct OpMinScale {
+  static constexpr int kNR = 0;
+  T* v;
+  T* z;
+  const MinScalars* ms;
+  T f;
+  struct In { T v, z; };
+  __device__ bool prepare(const Scalars* s) {
+    if (solve_done(s)) return false;
+    f = static_cast<T>(ms->inv_bn);
+    return true;
+  }
+  __device__ In load(i64 i) const { return {v[i], z[i]}; }
+  __device__ void apply(i64 i, In const& q, double*) const {
+    v[i] = mul(q.v, f);
+    z[i] = mul(q.z, f);
+  }
+  __device__ void finalize(const double*) const {}
+};
+
+// lanczos_step's product w = A z and alpha = <z, w> (:237-241)
+template <typename T>
+struct EpiMinW {
+  static constexpr int kNR = 1;
+  T* w;
+  const T* z;
+  MinScalars* ms;
+  __device__ void operator()(int row, T val, double* red) const {
+    w[row] = val;
+    red[0] += static_cast<double>(mul(z[row], val));
+  }
+  __device__ void finalize(const double* t) const { ms->alpha = static_cast<double>(static_cast<T>(t[0])); }
+};
+
+// apply_givens_rotations (:265-286), check_convergence (:300-309), the
+// step count (:231) and the scalar half of rotate_state (:320-324), from
+// beta_new; the vector half runs in OpMinUpdate.
+template <typename T>
+__device__ void min_step_finalize(T beta_new, Scalars* sc, MinScalars* ms, double* hist) {
+  const T beta = static_cast<T>(ms->beta), alpha = static_cast<T>(ms->alpha);
+  const T cs_prev = static_cast<T>(ms->cs_prev), sn_prev = static_cast<T>(ms->sn_prev);
+  const T cs = static_cast<T>(ms->cs), sn = static_cast<T>(ms->sn);
+  ms->eps = static_cast<double>(mul(sn_prev, beta));
+  const T delta_1 = mul(cs_prev, beta);
+  const T delta = add(mul(cs, delta_1), mul(sn, alpha));
+  const T rho_bar = add(mul(-sn, delta_1), mul(cs, alpha));
+  const T rho = sqrt(add(mul(rho_bar, rho_bar), mul(beta_new, beta_new)));
+  if (rho != T(0)) {  // else rho, delta and phi keep the previous step's values
+    const T cs_new = dvd(rho_bar, rho), sn_new = dvd(beta_new, rho);
+    const T phi_bar = static_cast<T>(ms->phi_bar);
+    ms->cs_new = static_cast<double>(cs_new);
+    ms->sn_new = static_cast<double>(sn_new);
+    ms->phi = static_cast<double>(mul(cs_new, phi_bar));
+    ms->phi_bar = static_cast<double>(mul(-sn_new, phi_bar));
+    ms->rho = static_cast<double>(rho);
+    ms->delta = static_cast<double>(delta);
+  }
+  ms->pending = 1;
+  const T res = fabs(static_cast<T>(ms->phi_bar));
+  record(sc, hist, static_cast<double>(res));
+  const bool conv = res / static_cast<T>(sc->bnorm) < static_cast<T>(sc->tol);
+  sc->converged = conv ? 1 : 0;
+  sc->iters += 1;
+  ms->rotate = (!conv && beta_new != T(0)) ? 1 : 0;
+  if (ms->rotate) {
+    ms->inv_bn = static_cast<double>(T(1) / beta_new);
+    ms->cs_prev = ms->cs;
+    ms->sn_prev = ms->sn;
+    ms->cs = ms->cs_new;
+    ms->sn = ms->sn_new;
+    ms->beta = static_cast<double>(beta_new);
+  }
+  if (conv || sc->iters >= sc->max_iters) sc->done = 1;
+}
+
+// w -= alpha v + beta v_prev (:244-246); with a fusable pair also
+// precondition_lanczos (:250-262): v_prev = M_R M_L w, beta_new.
+template <typename T>
+struct OpMinLanczos {
+  static constexpr int kNR = 1;
+  T* w;
+  const T* v;
+  T* vp;
+  const T* invl;
+  const T* invr;
+  bool fused;
+  Scalars* sc;
+  MinScalars* ms;
+  double* hist;
+  T alpha, beta;
+  struct In { T w, v, vp, l, r; };
+  __device__ bool prepare(const Scalars* s) {
+    if (solve_done(s)) return false;
+    alpha = static_cast<T>(ms->alpha);
+    beta = static_cast<T>(ms->beta);
+    return true;
+  }
+  __device__ In load(i64 i) const {
+    return {w[i], v[i], vp[i], fused && invl ? invl[i] : T(0), fused && invr ? invr[i] : T(0)};
+  }
+  __device__ void apply(i64 i, In const& q, double* red) const {
+    const T wi = sub(q.w, add(mul(alpha, q.v), mul(beta, q.vp)));
+    w[i] = wi;
+    if (!fused) return;
+    T zi = wi;
+    if (invl) zi = mul(q.l, zi);
+    if (invr) zi = mul(q.r, zi);
+    vp[i] = zi;
+    red[0] += static_cast<double>(mul(wi, zi));
+  }
+  __device__ void finalize(const double* t) const {
+    if (fused) min_step_finalize<T>(sqrt(static_cast<T>(t[0])), sc, ms, hist);
+  }
+};
+
+// beta_new = sqrt(<w, v_prev>) after a general preconditioner pair
+template <typename T>
+struct OpMinDot {
+  static constexpr int kNR = 1;
+  const T* w;
+  const T* vp;
+  Scalars* sc;
+  MinScalars* ms;
+  double* hist;
+  struct In { T w, vp; };
+  __device__ bool prepare(const Scalars* s) { return !solve_done(s); }
+  __device__ In load(i64 i) const { return {w[i], vp[i]}; }
+  __device__ void apply(i64, In const& q, double* red) const { red[0] += static_cast<double>(mul(q.w, q.vp)); }
+  __device__ void finalize(const double* t) const { min_step_finalize<T>(sqrt(static_cast<T>(t[0])), sc, ms, hist); }
+};
+
+// update_solution (:288-297) and the vector half of rotate_state
+// (:311-319).  Runs for the step just taken even when it converged (the
+// reference updates x before it tests), hence its own `pending` gate,
+// cleared by its finalize.
+template <typename T>
+struct OpMinUpdate {
+  static constexpr int kNR = 1;
+  T *d, *dp, *x, *z, *v, *vp;
+  const T* w;
+  MinScalars* ms;
+  T delta, eps, rho, phi, inv_bn;
+  int rotate;
+  struct In { T d, dp, x, z, v, vp, w; };
+  __device__ bool prepare(const Scalars*) {
+    if (!*reinterpret_cast<const volatile int*>(&ms->pending)) return false;
+    delta = static_cast<T>(ms->delta);
+    eps = static_cast<T>(ms->eps);
+    rho = static_cast<T>(ms->rho);
+    phi = static_cast<T>(ms->phi);
+    inv_bn = static_cast<T>(ms->inv_bn);
+    rotate = ms->rotate;
+    return true;
+  }
+  __device__ In load(i64 i) const { return {d[i], dp[i], x[i], z[i], v[i], vp[i], rotate ? w[i] : T(0)}; }
+  __device__ void apply(i64 i, In const& q, double* red) const {
+    const T dn = dvd(sub(sub(q.z, mul(delta, q.d)), mul(eps, q.dp)), rho);
+    d[i] = dn;
+    dp[i] = q.d;
+    x[i] = add(q.x, mul(phi, dn));
+    if (rotate) {
+      z[i] = mul(q.vp, inv_bn);
+      vp[i] = q.v;
+      v[i] = mul(q.w, inv_bn);
+    }
+    red[0] += 0.0;
+  }
+  __device__ void finalize(const double*) const { ms->pending = 0; }
+};
+
+template <typename T>
+static sk_status minres_solve(sk_matrix A, sk_precond L, sk_precond R, const T* b, T* x,
+                              const sk_minres_config* cfg, sk_summary* out, double* history_host,
+                              cudaStream_t st) {
+  const i64 n = A->nrow;
+  const size_t vb = static_cast<size_t>(n + 8) * sizeof(T);
+  SolveCommon c;
+  std::vector<char*> vv;
+  char* extra = nullptr;
+  const i64 hist_cap = cfg->collect_residuals ? cfg->max_iterations + 2 : 0;
+  sk_status s = carve_common(A, st, 7, vb, sizeof(MinScalars) + 256, hist_cap, &c, &vv, &extra);
+  if (s != SK_OK) return s;
+  T *vp = (T*)vv[0], *v = (T*)vv[1], *z = (T*)vv[2], *w = (T*)vv[3], *tmp = (T*)vv[4], *dp = (T*)vv[5],
+    *d = (T*)vv[6];
+  MinScalars* ms = reinterpret_cast<MinScalars*>(extra);
+  *out = sk_summary{};
+  double bnorm = 0;
+  if ((s = norm_b<T>(b, n, c, st, &bnorm)) != SK_OK) return s;
+  if (bnorm == 0.0) {  // :170-174
+    SK_CUDA(cudaMemsetAsync(x, 0, n * sizeof(T), st));
+    SK_CUDA(cudaStreamSynchronize(st));
+    out->converged = 1;
+    return SK_OK;
+  }
+  Scalars h{};
+  h.bnorm = bnorm;
+  h.tol = cfg->tolerance;
+  h.max_iters = cfg->max_iterations;
+  h.hist_on = cfg->collect_residuals ? 1 : 0;
+  if ((s = put_scalars(c.sc, h, st)) != SK_OK) return s;
+  SK_CUDA(cudaMemsetAsync(ms, 0, sizeof(MinScalars), st));
+  for (T* vec : {vp, d, dp}) SK_CUDA(cudaMemsetAsync(vec, 0, n * sizeof(T), st));  // :144-158
+  const LRPair<T> lr(L, R);
+  launch_spmv<T>(A, x, EpiMinInit<T>{b, v, z, lr.invl, lr.invr, lr.fused, c.sc, ms}, c.ws, nullptr, st);
+  if (!lr.fused) {
+    apply_lr<T>(lr, n, v, tmp, z, c, st);
+    launch_vec(n, OpMinInitDot<T>{v, z, c.sc, ms}, c.ws, nullptr, st);
+  }
+  launch_vec(n, OpMinScale<T>{v, z, ms, T(0)}, c.ws, c.sc, st);
+  SK_CUDA(cudaGetLastError());
+  if ((s = read_scalars(c.sc, &h, st)) != SK_OK) return s;
+  if (!h.done && cfg->max_iterations <= 0) h.done = 1;
+  i64 chunk = 4;
+  while (!h.done) {
+    for (i64 j = 0; j < chunk; ++j) {  // minres_step (:225-234)
+      launch_spmv<T>(A, z, EpiMinW<T>{w, z, ms}, c.ws, c.sc, st);
+      launch_vec(n, OpMinLanczos<T>{w, v, vp, lr.invl, lr.invr, lr.fused, c.sc, ms, c.hist, T(0), T(0)}, c.ws,
+                 c.sc, st);
+      if (!lr.fused) {
+        apply_lr<T>(lr, n, w, tmp, vp, c, st);
+        launch_vec(n, OpMinDot<T>{w, vp, c.sc, ms, c.hist}, c.ws, c.sc, st);
+      }
+      launch_vec(n, OpMinUpdate<T>{d, dp, x, z, v, vp, w, ms, T(0), T(0), T(0), T(0), T(0), 0}, c.ws, nullptr, st);
+    }
+    SK_CUDA(cudaGetLastError());
+    if ((s = read_scalars(c.sc, &h, st)) != SK_OK) return s;
+    chunk = std::min<i64>(chunk * 2, 32);
+  }
+  return finish_summary(c, st, out, history_host);
+}
+
 // Keeps [base, base + bytes) resident in L2 for the kernels of stream `st`
 // while it lives: a persisting access-policy window on the stream and a
 // persisting set-aside of the same size (both settings of this process's
@@ -1543,6 +2101,32 @@ sk_status sk_gmres_solve(sk_matrix A, sk_precond left, sk_precond right, const v
   return SK_OK;
 }
 
+sk_status sk_cgs_solve(sk_matrix A, sk_precond left, sk_precond right, const void* b_dev, void* x_dev,
+                       const sk_cgs_config* cfg, sk_summary* out, double* history_host, sk_stream s) {
+  sk_status st = check_solver_args(A, left, right, b_dev, x_dev);
+  if (st != SK_OK) return st;
+  SK_CHECK(cfg && out, SK_INVALID_ARG, "null config or summary");
+  cudaStream_t cs = pick_stream(A, s);
+  if (A->dtype == SK_F64)
+    return cgs_solve<double>(A, left, right, static_cast<const double*>(b_dev), static_cast<double*>(x_dev), cfg,
+                             out, history_host, cs);
+  return cgs_solve<float>(A, left, right, static_cast<const float*>(b_dev), static_cast<float*>(x_dev), cfg, out,
+                          history_host, cs);
+}
+
+sk_status sk_minres_solve(sk_matrix A, sk_precond left, sk_precond right, const void* b_dev, void* x_dev,
+                          const sk_minres_config* cfg, sk_summary* out, double* history_host, sk_stream s) {
+  sk_status st = check_solver_args(A, left, right, b_dev, x_dev);
+  if (st != SK_OK) return st;
+  SK_CHECK(cfg && out, SK_INVALID_ARG, "null config or summary");
+  cudaStream_t cs = pick_stream(A, s);
+  if (A->dtype == SK_F64)
+    return minres_solve<double>(A, left, right, static_cast<const double*>(b_dev), static_cast<double*>(x_dev),
+                                cfg, out, history_host, cs);
+  return minres_solve<float>(A, left, right, static_cast<const float*>(b_dev), static_cast<float*>(x_dev), cfg, out,
+                             history_host, cs);
+}
+
 sk_status sk_fgmres_fallback_solve(sk_matrix A, sk_precond M, sk_precond fallback, const double* b_dev,
                                    double* x_dev, const sk_fgmres_config* cfg, double stall_ratio,
                                    sk_summary* out, double* history_host, int64_t* switched_at, sk_stream s) {
@@ -1578,6 +2162,20 @@ sk_status sk_gmres_solve_host(sk_matrix A, sk_precond left, sk_precond right, co
                               const sk_gmres_config* cfg, sk_summary* out, double* history_host) {
   return host_wrapper<sk_gmres_config>(A, b_host, x_host, [&](void* bd, void* xd) {
     return sk_gmres_solve(A, left, right, bd, xd, cfg, out, history_host, A->stream);
+  });
+}
+
+sk_status sk_cgs_solve_host(sk_matrix A, sk_precond left, sk_precond right, const void* b_host, void* x_host,
+                            const sk_cgs_config* cfg, sk_summary* out, double* history_host) {
+  return host_wrapper<sk_cgs_config>(A, b_host, x_host, [&](void* bd, void* xd) {
+    return sk_cgs_solve(A, left, right, bd, xd, cfg, out, history_host, A->stream);
+  });
+}
+
+sk_status sk_minres_solve_host(sk_matrix A, sk_precond left, sk_precond right, const void* b_host, void* x_host,
+                               const sk_minres_config* cfg, sk_summary* out, double* history_host) {
+  return host_wrapper<sk_minres_config>(A, b_host, x_host, [&](void* bd, void* xd) {
+    return sk_minres_solve(A, left, right, bd, xd, cfg, out, history_host, A->stream);
   });
 }
 

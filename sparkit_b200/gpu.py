@@ -313,6 +313,42 @@ def bicgstab(b, x, cfg, op, left=identity, right=identity):
                 b, x, Ad, c, cfg.max_iterations + 2, cfg.collect_residuals)
 
 
+@dataclass
+class Cgs_config:
+    """Cgs_config<T> (cgs.hpp:25-42)."""
+    tolerance: float = 0.0
+    max_iterations: int = 0
+    collect_residuals: bool = False
+
+
+@dataclass
+class Minres_config:
+    """Minres_config<T> (minres.hpp:25-45)."""
+    tolerance: float = 0.0
+    max_iterations: int = 0
+    collect_residuals: bool = False
+
+
+def _krylov2(name, b, x, cfg, op, left, right, max_hist):
+    Ad = _op_matrix(op)
+    c = _lib.BicgstabConfig(cfg.tolerance, cfg.max_iterations, int(cfg.collect_residuals))
+    L = lib()
+    dev, host = getattr(L, f"sk_{name}_solve"), getattr(L, f"sk_{name}_solve_host")
+    return _run(lambda bp, xp, cp, sp, hp, st: dev(Ad.handle, _handle(left), _handle(right), bp, xp, cp, sp, hp, st),
+                lambda bp, xp, cp, sp, hp: host(Ad.handle, _handle(left), _handle(right), bp, xp, cp, sp, hp),
+                b, x, Ad, c, max_hist, cfg.collect_residuals)
+
+
+def cgs(b, x, cfg, op, left=identity, right=identity):
+    """cgs(bfirst, blast, xfirst, xlast, cfg, op, left, right)."""
+    return _krylov2("cgs", b, x, cfg, op, left, right, cfg.max_iterations // 2 + 4)
+
+
+def minres(b, x, cfg, op, left=identity, right=identity):
+    """minres(bfirst, blast, xfirst, xlast, cfg, op, left, right)."""
+    return _krylov2("minres", b, x, cfg, op, left, right, cfg.max_iterations + 2)
+
+
 def fgmres(b, x, cfg, op, preconditioner=identity):
     """fgmres(bfirst, blast, xfirst, xlast, cfg, op, preconditioner)."""
     Ad = _op_matrix(op)

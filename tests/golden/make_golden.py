@@ -112,6 +112,9 @@ def main():
             runs.append(("fgmres", lambda: R.fgmres(A, b, np.zeros(n), 1e-12, 5, 500, prec=spec, collect=True)))
             runs.append(("gmres_left", lambda: R.gmres(A, b, np.zeros(n), 1e-12, 5, 500, left=spec, collect=True)))
             runs.append(("gmres_right", lambda: R.gmres(A, b, np.zeros(n), 1e-12, 6, 500, right=spec, collect=True)))
+            runs.append(("cgs", lambda: R.cgs(A, b, np.zeros(n), 1e-12, 500, left=spec, collect=True)))
+            if name in spd:
+                runs.append(("minres", lambda: R.minres(A, b, np.zeros(n), 1e-12, 500, left=spec, collect=True)))
             for rname, fn in runs:
                 x, s = fn()
                 key = f"{base}/{pname}/{rname}"

@@ -28,12 +28,12 @@ def make_prec(spec, Ad):
 
 
 def iters_close(a, b, solver="cg"):
-    """+-2% (at least 1) for CG and FGMRES.  BiCGSTAB's count moves with the
-    summation order of its dot products even on the CPU (the reference
-    re-run with chunked sums shifts by ~2%, test_oracle.py records it), and
-    the GPU sums in a tree, so its band is +-12%; its solutions are checked
-    through the true residual instead."""
-    frac = 0.12 if solver == "bicgstab" else 0.02
+    """+-2% (at least 1) for CG, FGMRES, GMRES and MINRES.  BiCGSTAB's and
+    CGS's counts move with the summation order of their dot products even on
+    the CPU (the reference re-run with chunked sums shifts by ~2%,
+    test_oracle.py records it), and the GPU sums in a tree, so their band is
+    +-12%; their solutions are checked through the true residual instead."""
+    frac = 0.12 if solver in ("bicgstab", "cgs") else 0.02
     return abs(a - b) <= max(1, int(np.ceil(frac * b)))
 
 
@@ -77,8 +77,10 @@ def test_solvers_against_reference(gpu_lib, golden, name, pname):
     runs = {"bicgstab": lambda x: gpu.bicgstab(b, x, gpu.Bicgstab_config(1e-12, 500, True), gpu.spmv(Ad), M),
             "fgmres": lambda x: gpu.fgmres(b, x, gpu.Fgmres_config(1e-12, 5, 500, True), gpu.spmv(Ad), M),
             "gmres_left": lambda x: gpu.gmres(b, x, gpu.Gmres_config(1e-12, 5, 500, True), gpu.spmv(Ad), left=M),
-            "gmres_right": lambda x: gpu.gmres(b, x, gpu.Gmres_config(1e-12, 6, 500, True), gpu.spmv(Ad), right=M)}
+            "gmres_right": lambda x: gpu.gmres(b, x, gpu.Gmres_config(1e-12, 6, 500, True), gpu.spmv(Ad), right=M),
+            "cgs": lambda x: gpu.cgs(b, x, gpu.Cgs_config(1e-12, 500, True), gpu.spmv(Ad), left=M)}
     if name in SPD:
+        runs["minres"] = lambda x: gpu.minres(b, x, gpu.Minres_config(1e-12, 500, True), gpu.spmv(Ad), left=M)
         runs["cg_left"] = lambda x: gpu.conjugate_gradient(b, x, gpu.CGConfig(1e-12, 50, 500, True), gpu.spmv(Ad), M,
                                                            gpu.identity)
         runs["cg_right"] = lambda x: gpu.conjugate_gradient(b, x, gpu.CGConfig(1e-12, 7, 500, True), gpu.spmv(Ad),
@@ -90,8 +92,11 @@ def test_solvers_against_reference(gpu_lib, golden, name, pname):
         ref_iters = int(golden[f"{key}/iters"])
         assert s.converged == bool(golden[f"{key}/converged"]), key
         assert iters_close(s.computed_iterations, ref_iters, rname), (key, s.computed_iterations, ref_iters)
-        # one recorded residual per iteration (CG, FGMRES) or per half step (BiCGSTAB)
-        if rname != "bicgstab":
+        # one recorded residual per iteration (CG, FGMRES, GMRES, MINRES),
+        # per half step (BiCGSTAB) or per two-product step (CGS)
+        if rname == "cgs":
+            assert len(s.iteration_residuals) == (s.computed_iterations + 1) // 2, key
+        elif rname != "bicgstab":
             assert len(s.iteration_residuals) == s.computed_iterations, key
         if s.converged:
             xr = golden[f"{key}/x"]
@@ -146,6 +151,55 @@ def test_nonsymmetric_medium(gpu_lib, oracle, solver, pname):
         # residual is then bounded through ||M_L^-1|| (diagonal 5.2 here)
         bound = 1e-9 if solver in ("bicgstab", "fgmres", "gmres_right") or pname == "none" else 1e-8
         assert np.linalg.norm(b - oracle.spmv(A, x)) <= bound * np.linalg.norm(b)
+
+
+@pytest.mark.parametrize("pname", ["none", "jacobi", "cheb"])
+@pytest.mark.parametrize("side", ["left", "right"])
+def test_cgs_minres_medium(gpu_lib, oracle, pname, side):
+    """CGS on the 48 x 48 convection-diffusion problem and MINRES on the
+    64 x 64 Dirichlet Laplacian (symmetric, as MINRES requires), against the
+    oracle (bit-exact with the reference): the same decision, iteration
+    counts in band, and the true residual."""
+    spec = {"none": None, "jacobi": "jacobi", "cheb": ("chebyshev", 0.2, 9.5, 8)}[pname]
+    kw = {"left": spec} if side == "left" else {"right": spec}
+    for solver, A in (("cgs", matgen.convection_diffusion_2d(48, 48, 1.0, 0.9, 0.5)),
+                      ("minres", matgen.laplacian_2d_dirichlet(64))):
+        n = A.shape()[0]
+        b = oracle.spmv(A, matgen.uniform_vector(n, seed=2))
+        Ad = gpu.Device_matrix(A)
+        M = make_prec(spec, Ad)
+        x = np.zeros(n)
+        xr, sr = getattr(oracle, solver)(A, b, np.zeros(n), 1e-10, 3000, **kw)
+        cfg = gpu.Cgs_config(1e-10, 3000) if solver == "cgs" else gpu.Minres_config(1e-10, 3000)
+        gkw = {side: M}
+        s = getattr(gpu, solver)(b, x, cfg, gpu.spmv(Ad), **gkw)
+        assert s.converged == sr["converged"], (solver, s, sr)
+        assert iters_close(s.computed_iterations, sr["computed_iterations"], solver), (
+            solver, s.computed_iterations, sr["computed_iterations"])
+        if s.converged:
+            # CGS tests its recursive residual, which drifts from the true one
+            # by rounding (the oracle's own true residual is the yardstick)
+            rel_ref = np.linalg.norm(b - oracle.spmv(A, xr)) / np.linalg.norm(b)
+            bound = max(1e-9, 50 * rel_ref) if solver == "cgs" else 1e-9
+            assert np.linalg.norm(b - oracle.spmv(A, x)) <= bound * np.linalg.norm(b), (solver, rel_ref)
+
+
+def test_minres_matches_oracle_history(gpu_lib, oracle):
+    """MINRES step by step on an SPD problem with a Jacobi pair: the
+    per-step |phi_bar| of the device solve follow the oracle's to the
+    rounding of the dot products (to 1e-6), and the budget ends the solve."""
+    A = matgen.diffusion_3d_grf(10, sigma=1.0, corr_len=3.0, seed=4)
+    n = A.shape()[0]
+    b = matgen.uniform_vector(n, seed=6)
+    Ad = gpu.Device_matrix(A)
+    J = gpu.jacobi(Ad)
+    x = np.zeros(n)
+    s = gpu.minres(b, x, gpu.Minres_config(1e-15, 40, True), gpu.spmv(Ad), left=J)
+    xr, sr = oracle.minres(A, b, np.zeros(n), 1e-15, 40, left="jacobi", collect=True)
+    assert s.computed_iterations == sr["computed_iterations"] == 40 and not s.converged
+    h, hr = np.array(s.iteration_residuals), np.array(sr["iteration_residuals"])
+    assert np.allclose(h, hr, rtol=1e-6, atol=0), np.max(np.abs(h - hr) / hr)
+    assert np.linalg.norm(x - xr) <= 1e-6 * np.linalg.norm(xr)
 
 
 def test_gmres_matches_oracle_history(gpu_lib, oracle):
@@ -207,6 +261,16 @@ def test_edge_cases(gpu_lib):
     x = np.arange(1.0, 17.0)
     s = gpu.gmres(bb, x, gpu.Gmres_config(1e-12, 5, 100), gpu.spmv(Ad), right=J)
     assert s.converged and np.array_equal(x, np.arange(1.0, 17.0))
+    # CGS and MINRES: zero right-hand side and budgets (a CGS step spends
+    # two products, so a budget of 3 ends after the second step)
+    for fn, cfg in ((gpu.cgs, gpu.Cgs_config), (gpu.minres, gpu.Minres_config)):
+        x = np.ones(n)
+        s = fn(np.zeros(n), x, cfg(1e-12, 100), gpu.spmv(Ad), left=J)
+        assert s.converged and s.computed_iterations == 0 and not x.any()
+    s = gpu.cgs(b, np.zeros(n), gpu.Cgs_config(1e-15, 3), gpu.spmv(Ad))
+    assert not s.converged and s.computed_iterations == 4
+    s = gpu.minres(b, np.zeros(n), gpu.Minres_config(1e-15, 3), gpu.spmv(Ad), right=J)
+    assert not s.converged and s.computed_iterations == 3
 
 
 def test_device_resident_solve(gpu_lib, oracle):
