@@ -111,6 +111,36 @@ SK_API sk_status sk_bsr_create(sk_matrix* out, int64_t nrow, int64_t ncol,
                         const int64_t* row_ptr, const int64_t* col_ind,
                         const void* values, sk_dtype dtype);
 
+/* Conversions built on the device from a CSR handle (its dtype kept; the
+ * CSR col_ind sorted within each row, as every reference CSR is).  The new
+ * handle holds exactly what sk_ell_create / sk_jad_create / sk_bsr_create
+ * would build from the reference's conversion of the same matrix.
+ *   to_ellpack(Compressed_row_matrix<T>)          conversions.hpp:427-467
+ *   to_jagged_diagonal(Compressed_row_matrix<T>)  conversions.hpp:641-691
+ *     (rows by decreasing length, ties by row index:
+ *      Jagged_diagonal_sparsity_Impl.cpp:41-47)
+ *   to_block_sparse_row(csr, block_rows, block_cols) conversions.hpp:524-577 */
+SK_API sk_status sk_ell_from_csr(sk_matrix* out, sk_matrix csr);
+SK_API sk_status sk_jad_from_csr(sk_matrix* out, sk_matrix csr);
+SK_API sk_status sk_bsr_from_csr(sk_matrix* out, sk_matrix csr,
+                          int64_t block_rows, int64_t block_cols);
+
+/* The reference's accessors row_ptr() / col_ind() / values() / perm() /
+ * jdiag() (Compressed_row_matrix.hpp, Ellpack_matrix.hpp,
+ * Jagged_diagonal_matrix.hpp, Block_sparse_row_matrix.hpp) as host copies
+ * of a handle, sized by sk_matrix_info:
+ *   CSR  row_ptr[nrow+1], col_ind[nnz], values[nnz]
+ *   ELL  col_ind[nrow*width] row-major with -1 past each row, values alike
+ *   JAD  perm[nrow] (written only when width > 0: an empty reference JAD
+ *        holds none), jdiag[width+1], col_ind[nnz], values[nnz]
+ *   BSR  row_ptr[ceil(nrow/block_rows)+1], col_ind[width],
+ *        values[width*block_rows*block_cols] */
+SK_API sk_status sk_csr_export(sk_matrix A, int64_t* row_ptr, int64_t* col_ind, void* values);
+SK_API sk_status sk_ell_export(sk_matrix A, int64_t* col_ind, void* values);
+SK_API sk_status sk_jad_export(sk_matrix A, int64_t* perm, int64_t* jdiag,
+                        int64_t* col_ind, void* values);
+SK_API sk_status sk_bsr_export(sk_matrix A, int64_t* row_ptr, int64_t* col_ind, void* values);
+
 SK_API sk_status sk_matrix_destroy(sk_matrix A);
 
 /* info[0..7] = format, dtype, nrow, ncol, nnz (stored entries), width

@@ -101,6 +101,13 @@ SIGNATURES = [
     ("sk_ell_create", [ctypes.POINTER(c_vp), c_i64, c_i64, c_i64, c_vp, c_vp, ctypes.c_int]),
     ("sk_jad_create", [ctypes.POINTER(c_vp), c_i64, c_i64, c_i64, c_vp, c_vp, c_vp, c_vp, ctypes.c_int]),
     ("sk_bsr_create", [ctypes.POINTER(c_vp), c_i64, c_i64, c_i64, c_i64, c_vp, c_vp, c_vp, ctypes.c_int]),
+    ("sk_ell_from_csr", [ctypes.POINTER(c_vp), c_vp]),
+    ("sk_jad_from_csr", [ctypes.POINTER(c_vp), c_vp]),
+    ("sk_bsr_from_csr", [ctypes.POINTER(c_vp), c_vp, c_i64, c_i64]),
+    ("sk_csr_export", [c_vp, c_vp, c_vp, c_vp]),
+    ("sk_ell_export", [c_vp, c_vp, c_vp]),
+    ("sk_jad_export", [c_vp, c_vp, c_vp, c_vp, c_vp]),
+    ("sk_bsr_export", [c_vp, c_vp, c_vp, c_vp]),
     ("sk_matrix_destroy", [c_vp]),
     ("sk_matrix_info", [c_vp, P_i64]),
     ("sk_matrix_add_f32_values", [c_vp]),

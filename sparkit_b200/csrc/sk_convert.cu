@@ -1,0 +1,728 @@
+// sk_convert.cu -- the ELLPACK, jagged-diagonal and BSR handles built on the
+// device from a device-resident CSR handle (the reference builds them on the
+// host with sorts over int64 index lists, conversions.hpp:427-691), and the
+// export of every handle back to the reference's host arrays.
+//
+// Every conversion is a handful of streaming passes over the CSR arrays:
+//   ELL  width = longest row (a max reduction), then one thread per row
+//        writes its slots; a warp stores one slot of 32 rows as one segment.
+//   JAD  rows ordered by decreasing length, ties by row index (a stable LSD
+//        radix sort on the key maxlen - len, 8 bits per pass: one pass when
+//        every row is shorter than 256), the diagonal widths from the sorted
+//        lengths, then one thread per permuted row writes its diagonals.
+//   BSR  a group of lanes per block row merges the sorted block columns of
+//        its rows, once to count the blocks and once to fill them.
+#include <algorithm>
+#include <climits>
+#include <vector>
+
+#include "sk_internal.cuh"
+
+namespace sk {
+namespace {
+
+constexpr int kScanTile = 4096;   // scan: items per CTA (256 threads x 16)
+constexpr int kRadixTile = 4096;  // radix sort: keys per CTA (16 rounds of 256)
+
+// ------------------------------------------------------------------
+// Temporary device buffers of one conversion
+// ------------------------------------------------------------------
+struct Temps {
+  std::vector<void*> p;
+  ~Temps() {
+    for (void* q : p) cudaFree(q);
+  }
+  template <typename V>
+  sk_status get(V** out, i64 count) {
+    void* q = nullptr;
+    cudaError_t e = cudaMalloc(&q, static_cast<size_t>(std::max<i64>(count, 1) + 8) * sizeof(V));
+    if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc");
+    p.push_back(q);
+    *out = static_cast<V*>(q);
+    return SK_OK;
+  }
+};
+
+// ------------------------------------------------------------------
+// Row lengths and their maximum
+// ------------------------------------------------------------------
+__global__ void row_len_kernel(const int* __restrict__ rp, i64 n, int* __restrict__ len,
+                               int* __restrict__ maxlen) {
+  int m = 0;
+  i64 i = blockIdx.x * static_cast<i64>(blockDim.x) + threadIdx.x;
+  const i64 stride = static_cast<i64>(gridDim.x) * blockDim.x;
+  for (; i < n; i += stride) {
+    const int l = rp[i + 1] - rp[i];
+    if (len) len[i] = l;
+    m = max(m, l);
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0 && m > 0) atomicMax(maxlen, m);
+}
+
+static sk_status max_row_length(const int* rp, i64 n, int* len, int* dmax, cudaStream_t st, int* out) {
+  SK_CUDA(cudaMemsetAsync(dmax, 0, sizeof(int), st));
+  if (n > 0) SK_LAUNCH(row_len_kernel, grid_for(n), kThreads, 0, st, rp, n, len, dmax);
+  SK_CUDA(cudaMemcpyAsync(out, dmax, sizeof(int), cudaMemcpyDeviceToHost, st));
+  SK_CUDA(cudaStreamSynchronize(st));
+  return SK_OK;
+}
+
+// ------------------------------------------------------------------
+// Exclusive scan to int64 (reduce, scan the tile sums, scan the tiles)
+// ------------------------------------------------------------------
+// Block-wide exclusive scan of one value per thread; returns the block total.
+__device__ i64 block_excl_scan(i64 v, i64* excl, i64* warp_tot) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  i64 inc = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const i64 t = __shfl_up_sync(0xffffffffu, inc, o);
+    if (lane >= o) inc += t;
+  }
+  if (lane == 31) warp_tot[warp] = inc;
+  __syncthreads();
+  if (warp == 0) {
+    const int nw = blockDim.x >> 5;
+    i64 w = lane < nw ? warp_tot[lane] : 0;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const i64 t = __shfl_up_sync(0xffffffffu, w, o);
+      if (lane >= o) w += t;
+    }
+    if (lane < nw) warp_tot[lane] = w;  // inclusive over warps
+  }
+  __syncthreads();
+  const i64 before = warp > 0 ? warp_tot[warp - 1] : 0;
+  *excl = before + inc - v;
+  const i64 total = warp_tot[(blockDim.x >> 5) - 1];
+  __syncthreads();
+  return total;
+}
+
+template <typename In>
+__global__ void __launch_bounds__(kThreads) scan_sums_kernel(const In* __restrict__ in, i64 n,
+                                                             i64* __restrict__ sums) {
+  __shared__ i64 wt[kThreads / 32];
+  const i64 base = static_cast<i64>(blockIdx.x) * kScanTile;
+  i64 s = 0;
+  for (int r = 0; r < kScanTile / kThreads; ++r) {
+    const i64 i = base + r * kThreads + threadIdx.x;
+    if (i < n) s += static_cast<i64>(in[i]);
+  }
+  i64 excl;
+  const i64 tot = block_excl_scan(s, &excl, wt);
+  if (threadIdx.x == 0) sums[blockIdx.x] = tot;
+}
+
+// In-place exclusive scan of the tile sums by one CTA.
+__global__ void __launch_bounds__(1024) scan_single_kernel(i64* __restrict__ v, i64 n) {
+  __shared__ i64 wt[32];
+  i64 carry = 0;
+  for (i64 base = 0; base < n; base += blockDim.x) {
+    const i64 i = base + threadIdx.x;
+    const i64 x = i < n ? v[i] : 0;
+    i64 excl;
+    const i64 tot = block_excl_scan(x, &excl, wt);
+    if (i < n) v[i] = carry + excl;
+    carry += tot;
+  }
+}
+
+// out[i] = offset of the tile + exclusive scan inside it; out[n] = total.
+template <typename In>
+__global__ void __launch_bounds__(kThreads) scan_tiles_kernel(const In* __restrict__ in, i64 n,
+                                                              const i64* __restrict__ tile_off,
+                                                              i64* __restrict__ out) {
+  __shared__ i64 buf[kScanTile];
+  __shared__ i64 wt[kThreads / 32];
+  const i64 base = static_cast<i64>(blockIdx.x) * kScanTile;
+  for (int r = 0; r < kScanTile / kThreads; ++r) {
+    const int j = r * kThreads + threadIdx.x;
+    buf[j] = base + j < n ? static_cast<i64>(in[base + j]) : 0;
+  }
+  __syncthreads();
+  constexpr int kPer = kScanTile / kThreads;
+  i64 s = 0;
+  for (int k = 0; k < kPer; ++k) s += buf[threadIdx.x * kPer + k];
+  i64 excl;
+  const i64 tot = block_excl_scan(s, &excl, wt);
+  i64 run = tile_off[blockIdx.x] + excl;
+  for (int k = 0; k < kPer; ++k) {
+    const i64 x = buf[threadIdx.x * kPer + k];
+    buf[threadIdx.x * kPer + k] = run;
+    run += x;
+  }
+  __syncthreads();
+  for (int r = 0; r < kScanTile / kThreads; ++r) {
+    const int j = r * kThreads + threadIdx.x;
+    if (base + j < n) out[base + j] = buf[j];
+  }
+  if (base + kScanTile >= n && threadIdx.x == 0) out[n] = tile_off[blockIdx.x] + tot;
+}
+
+// out[0..n] = exclusive scan of in[0..n) with the total at out[n].
+template <typename In>
+static sk_status exclusive_scan(const In* in, i64 n, i64* out, Temps& tmp, cudaStream_t st) {
+  if (n == 0) {
+    SK_CUDA(cudaMemsetAsync(out, 0, sizeof(i64), st));
+    return SK_OK;
+  }
+  const i64 nt = (n + kScanTile - 1) / kScanTile;
+  i64* sums = nullptr;
+  sk_status s = tmp.get(&sums, nt);
+  if (s != SK_OK) return s;
+  SK_LAUNCH(scan_sums_kernel<In>, static_cast<unsigned>(nt), kThreads, 0, st, in, n, sums);
+  SK_LAUNCH(scan_single_kernel, 1, 1024, 0, st, sums, nt);
+  SK_LAUNCH(scan_tiles_kernel<In>, static_cast<unsigned>(nt), kThreads, 0, st, in, n, sums, out);
+  SK_CUDA(cudaGetLastError());
+  return SK_OK;
+}
+
+__global__ void narrow_i64_kernel(const i64* __restrict__ in, i64 n, int* __restrict__ out) {
+  i64 i = blockIdx.x * static_cast<i64>(blockDim.x) + threadIdx.x;
+  const i64 stride = static_cast<i64>(gridDim.x) * blockDim.x;
+  for (; i < n; i += stride) out[i] = static_cast<int>(in[i]);
+}
+
+// ------------------------------------------------------------------
+// Stable LSD radix sort of (key, index) pairs, 8 bits per pass
+// ------------------------------------------------------------------
+__global__ void __launch_bounds__(kThreads) radix_hist_kernel(const unsigned* __restrict__ keys, i64 n,
+                                                              int shift, int* __restrict__ hist,
+                                                              i64 ntiles) {
+  __shared__ int cnt[256];
+  cnt[threadIdx.x] = 0;
+  __syncthreads();
+  const i64 base = static_cast<i64>(blockIdx.x) * kRadixTile;
+  for (int r = 0; r < kRadixTile / kThreads; ++r) {
+    const i64 i = base + r * kThreads + threadIdx.x;
+    if (i < n) atomicAdd(&cnt[(keys[i] >> shift) & 255u], 1);
+  }
+  __syncthreads();
+  hist[threadIdx.x * ntiles + blockIdx.x] = cnt[threadIdx.x];
+}
+
+// Keys of one tile go out in position order within each digit: round by
+// round, warp by warp within a round, lane by lane within a warp.
+__global__ void __launch_bounds__(kThreads) radix_scatter_kernel(
+    const unsigned* __restrict__ kin, const int* __restrict__ vin, unsigned* __restrict__ kout,
+    int* __restrict__ vout, i64 n, int shift, const i64* __restrict__ off, i64 ntiles) {
+  __shared__ int run[256];
+  __shared__ int wcnt[kThreads / 32][256];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  run[tid] = 0;
+#pragma unroll
+  for (int w = 0; w < kThreads / 32; ++w) wcnt[w][tid] = 0;
+  __syncthreads();
+  const unsigned lt = (1u << lane) - 1u;
+  const i64 base = static_cast<i64>(blockIdx.x) * kRadixTile;
+  for (int r = 0; r < kRadixTile / kThreads; ++r) {
+    const i64 i = base + r * kThreads + tid;
+    const bool valid = i < n;
+    const unsigned key = valid ? kin[i] : 0u;
+    const int d = valid ? static_cast<int>((key >> shift) & 255u) : 256;
+    const unsigned peers = __match_any_sync(0xffffffffu, d);
+    const int lrank = __popc(peers & lt);
+    if (valid && lane == __ffs(peers) - 1) wcnt[warp][d] = __popc(peers);
+    __syncthreads();
+    if (valid) {
+      int pos = run[d] + lrank;
+      for (int w = 0; w < warp; ++w) pos += wcnt[w][d];
+      const i64 dst = off[static_cast<i64>(d) * ntiles + blockIdx.x] + pos;
+      kout[dst] = key;
+      vout[dst] = vin ? vin[i] : static_cast<int>(i);
+    }
+    __syncthreads();
+    int s = 0;
+#pragma unroll
+    for (int w = 0; w < kThreads / 32; ++w) {
+      s += wcnt[w][tid];
+      wcnt[w][tid] = 0;
+    }
+    run[tid] += s;
+    __syncthreads();
+  }
+}
+
+// Sorts keys[0..n) (values <= maxkey) stably; on return *keys_out and
+// *idx_out hold the sorted keys and the original positions (either the
+// input buffers or the scratch ones).
+static sk_status stable_radix_sort(unsigned* keys, unsigned* keys2, int* idx, int* idx2, i64 n,
+                                   unsigned maxkey, Temps& tmp, cudaStream_t st, unsigned** keys_out,
+                                   int** idx_out) {
+  const i64 ntiles = (n + kRadixTile - 1) / kRadixTile;
+  int* hist = nullptr;
+  i64* off = nullptr;
+  sk_status s;
+  if ((s = tmp.get(&hist, 256 * ntiles)) != SK_OK) return s;
+  if ((s = tmp.get(&off, 256 * ntiles + 1)) != SK_OK) return s;
+  unsigned *ka = keys, *kb = keys2;
+  int *va = nullptr, *vb = idx;
+  int shift = 0;
+  do {
+    SK_LAUNCH(radix_hist_kernel, static_cast<unsigned>(ntiles), kThreads, 0, st, ka, n, shift, hist, ntiles);
+    if ((s = exclusive_scan(hist, 256 * ntiles, off, tmp, st)) != SK_OK) return s;
+    SK_LAUNCH(radix_scatter_kernel, static_cast<unsigned>(ntiles), kThreads, 0, st, ka, va, kb, vb, n, shift,
+              off, ntiles);
+    SK_CUDA(cudaGetLastError());
+    std::swap(ka, kb);
+    va = vb;
+    vb = (vb == idx) ? idx2 : idx;
+    shift += 8;
+  } while (shift < 32 && (maxkey >> shift) != 0);
+  *keys_out = ka;
+  *idx_out = va;
+  return SK_OK;
+}
+
+// ------------------------------------------------------------------
+// CSR -> ELL
+// ------------------------------------------------------------------
+// One thread per slot row i < ld: entry k of row i to k * ld + i, the
+// slots past the row's length (and the rows past nrow) zero.
+template <typename T>
+__global__ void csr_to_ell_kernel(i64 n, i64 ld, i64 width, const int* __restrict__ rp,
+                                  const int* __restrict__ ci, const T* __restrict__ va,
+                                  int* __restrict__ col, T* __restrict__ val, int* __restrict__ rowlen) {
+  const i64 i = blockIdx.x * static_cast<i64>(blockDim.x) + threadIdx.x;
+  if (i >= ld) return;
+  int a = 0, len = 0;
+  if (i < n) {
+    a = rp[i];
+    len = rp[i + 1] - a;
+    rowlen[i] = len;
+  }
+  for (i64 k = 0; k < width; ++k) {
+    const bool in = k < len;
+    col[k * ld + i] = in ? ci[a + k] : 0;
+    val[k * ld + i] = in ? va[a + k] : T(0);
+  }
+}
+
+// ------------------------------------------------------------------
+// CSR -> JAD
+// ------------------------------------------------------------------
+__global__ void jad_keys_kernel(const int* __restrict__ len, i64 n, unsigned maxlen,
+                                unsigned* __restrict__ keys) {
+  i64 i = blockIdx.x * static_cast<i64>(blockDim.x) + threadIdx.x;
+  const i64 stride = static_cast<i64>(gridDim.x) * blockDim.x;
+  for (; i < n; i += stride) keys[i] = maxlen - static_cast<unsigned>(len[i]);
+}
+
+// perm, plen from the sorted keys; width[k] = rows longer than k, written
+// by the last sorted row of at least k + 1 entries.
+__global__ void jad_perm_kernel(const unsigned* __restrict__ skeys, const int* __restrict__ sidx, i64 n,
+                                unsigned maxlen, int* __restrict__ perm, int* __restrict__ plen,
+                                int* __restrict__ width) {
+  i64 p = blockIdx.x * static_cast<i64>(blockDim.x) + threadIdx.x;
+  const i64 stride = static_cast<i64>(gridDim.x) * blockDim.x;
+  for (; p < n; p += stride) {
+    const int l = static_cast<int>(maxlen - skeys[p]);
+    const int next = p + 1 < n ? static_cast<int>(maxlen - skeys[p + 1]) : 0;
+    perm[p] = sidx[p];
+    plen[p] = l;
+    for (int k = next; k < l; ++k) width[k] = static_cast<int>(p + 1);
+  }
+}
+
+// One thread per permuted row p: entry k of row perm[p] to jdiag[k] + p.
+template <typename T>
+__global__ void csr_to_jad_kernel(i64 n, const int* __restrict__ perm, const int* __restrict__ plen,
+                                  const int* __restrict__ jdiag, const int* __restrict__ rp,
+                                  const int* __restrict__ ci, const T* __restrict__ va,
+                                  int* __restrict__ col, T* __restrict__ val) {
+  i64 p = blockIdx.x * static_cast<i64>(blockDim.x) + threadIdx.x;
+  const i64 stride = static_cast<i64>(gridDim.x) * blockDim.x;
+  for (; p < n; p += stride) {
+    const int a = rp[perm[p]], l = plen[p];
+    for (int k = 0; k < l; ++k) {
+      const i64 dst = static_cast<i64>(__ldg(jdiag + k)) + p;
+      col[dst] = ci[a + k];
+      val[dst] = va[a + k];
+    }
+  }
+}
+
+__global__ void iota_kernel(int* __restrict__ p, i64 n) {
+  i64 i = blockIdx.x * static_cast<i64>(blockDim.x) + threadIdx.x;
+  const i64 stride = static_cast<i64>(gridDim.x) * blockDim.x;
+  for (; i < n; i += stride) p[i] = static_cast<int>(i);
+}
+
+// ------------------------------------------------------------------
+// CSR -> BSR
+// ------------------------------------------------------------------
+// A group of G lanes (a power of two, G >= min(br, 32)) per block row; lane
+// gl of the group holds rows gl, gl + G, ... (at most 8) of the block row.
+// Each step takes the smallest block column at the heads of the rows (a
+// min over the group), then every lane moves past its entries in that
+// block column, which FILL scatters into the block.
+constexpr int kBsrRowsPerLane = 8;
+
+template <typename T, bool FILL>
+__global__ void __launch_bounds__(kThreads) csr_to_bsr_kernel(
+    i64 nrow, i64 nbr, int br, int bc, int G, const int* __restrict__ rp, const int* __restrict__ ci,
+    const T* __restrict__ va, int* __restrict__ cnt, const i64* __restrict__ brp, int* __restrict__ bcol,
+    T* __restrict__ bval) {
+  const int lane = threadIdx.x & 31;
+  const i64 warp_id = (blockIdx.x * static_cast<i64>(blockDim.x) + threadIdx.x) >> 5;
+  const int gpw = 32 / G;
+  const int g = lane / G, gl = lane - g * G;
+  const i64 I = warp_id * gpw + g;
+  const bool active = I < nbr;
+  int pos[kBsrRowsPerLane], end[kBsrRowsPerLane];
+#pragma unroll
+  for (int j = 0; j < kBsrRowsPerLane; ++j) {
+    const int lr = gl + G * j;
+    const i64 r = I * br + lr;
+    if (active && lr < br && r < nrow) {
+      pos[j] = rp[r];
+      end[j] = rp[r + 1];
+    } else {
+      pos[j] = end[j] = 0;
+    }
+  }
+  const i64 bsz = static_cast<i64>(br) * bc;
+  const i64 first = (FILL && active) ? brp[I] : 0;
+  int count = 0;
+  for (;;) {
+    int h = INT_MAX;
+#pragma unroll
+    for (int j = 0; j < kBsrRowsPerLane; ++j)
+      if (pos[j] < end[j]) h = min(h, ci[pos[j]] / bc);
+    for (int o = G >> 1; o > 0; o >>= 1) h = min(h, __shfl_xor_sync(0xffffffffu, h, o));
+    if (!__any_sync(0xffffffffu, h != INT_MAX)) break;
+    if (h == INT_MAX) continue;
+    const i64 blk = first + count;
+    if (FILL && gl == 0) bcol[blk] = h;
+#pragma unroll
+    for (int j = 0; j < kBsrRowsPerLane; ++j) {
+      while (pos[j] < end[j]) {
+        const int c = ci[pos[j]];
+        if (c / bc != h) break;
+        if (FILL) bval[blk * bsz + static_cast<i64>(gl + G * j) * bc + (c - h * bc)] = va[pos[j]];
+        ++pos[j];
+      }
+    }
+    ++count;
+  }
+  if (!FILL && active && gl == 0) cnt[I] = count;
+}
+
+// ------------------------------------------------------------------
+// Exports (device layout -> the reference's host arrays)
+// ------------------------------------------------------------------
+__global__ void widen_kernel(const int* __restrict__ in, i64 n, long long* __restrict__ out) {
+  i64 i = blockIdx.x * static_cast<i64>(blockDim.x) + threadIdx.x;
+  const i64 stride = static_cast<i64>(gridDim.x) * blockDim.x;
+  for (; i < n; i += stride) out[i] = in[i];
+}
+
+// Row-major slots g0 .. g0 + count of the reference's ELL layout: -1 and 0
+// past each row's length (Ellpack_sparsity_Impl.cpp:35-37).
+template <typename T>
+__global__ void ell_export_kernel(i64 g0, i64 count, i64 width, i64 ld, const int* __restrict__ col,
+                                  const T* __restrict__ val, const int* __restrict__ rowlen,
+                                  long long* __restrict__ ocol, T* __restrict__ oval) {
+  i64 t = blockIdx.x * static_cast<i64>(blockDim.x) + threadIdx.x;
+  const i64 stride = static_cast<i64>(gridDim.x) * blockDim.x;
+  for (; t < count; t += stride) {
+    const i64 g = g0 + t, i = g / width, k = g - i * width;
+    const bool in = k < rowlen[i];
+    ocol[t] = in ? col[k * ld + i] : -1;
+    oval[t] = in ? val[k * ld + i] : T(0);
+  }
+}
+
+static sk_status download_indices(const int* dev, i64 count, int64_t* host, cudaStream_t st) {
+  if (count == 0) return SK_OK;
+  SK_CHECK(host, SK_INVALID_ARG, "null output array");
+  Temps tmp;
+  long long* stage = nullptr;
+  const i64 chunk = std::min(count, kChunk);
+  sk_status s = tmp.get(&stage, chunk);
+  if (s != SK_OK) return s;
+  for (i64 off = 0; off < count; off += chunk) {
+    const i64 c = std::min(chunk, count - off);
+    SK_LAUNCH(widen_kernel, grid_for(c), kThreads, 0, st, dev + off, c, stage);
+    SK_CUDA(cudaMemcpyAsync(host + off, stage, c * sizeof(long long), cudaMemcpyDeviceToHost, st));
+    SK_CUDA(cudaStreamSynchronize(st));
+  }
+  return SK_OK;
+}
+
+static sk_status download_values(const void* dev, i64 count, sk_dtype dt, void* host, cudaStream_t st) {
+  if (count == 0) return SK_OK;
+  SK_CHECK(host, SK_INVALID_ARG, "null output array");
+  SK_CUDA(cudaMemcpyAsync(host, dev, count * vbytes(dt), cudaMemcpyDeviceToHost, st));
+  SK_CUDA(cudaStreamSynchronize(st));
+  return SK_OK;
+}
+
+static sk_status check_source(sk_matrix* out, sk_matrix csr) {
+  SK_CHECK(out, SK_INVALID_ARG, "null output handle");
+  *out = nullptr;
+  SK_CHECK(csr, SK_INVALID_ARG, "null CSR handle");
+  SK_CHECK(csr->format == SK_CSR, SK_INVALID_ARG, "the source handle must be CSR");
+  SK_CUDA(cudaSetDevice(csr->device));
+  SK_CUDA(cudaStreamSynchronize(csr->stream));
+  return SK_OK;
+}
+
+template <typename T>
+static sk_status ell_from_csr(sk_matrix A, sk_matrix C) {
+  cudaStream_t st = A->stream;
+  const i64 n = C->nrow;
+  Temps tmp;
+  int* dmax = nullptr;
+  sk_status s;
+  if ((s = tmp.get(&dmax, 1)) != SK_OK) return s;
+  int width = 0;
+  if ((s = max_row_length(C->csr.row_ptr, n, nullptr, dmax, st, &width)) != SK_OK) return s;
+  const i64 ld = (n + 31) / 32 * 32 + 96;  // the slot stride of sk_ell_create
+  A->ell.width = width;
+  A->ell.ld = ld;
+  A->nnz = C->nnz;
+  const i64 stored = ld * width;
+  void *col = nullptr, *va = nullptr, *rl = nullptr;
+  if ((s = dev_alloc(A, &col, (stored + 8) * 4)) != SK_OK) return s;
+  if ((s = dev_alloc(A, &va, (stored + 8) * sizeof(T))) != SK_OK) return s;
+  if ((s = dev_alloc(A, &rl, (n + 8) * 4)) != SK_OK) return s;
+  A->ell.col = static_cast<int*>(col);
+  A->ell.vals = va;
+  A->ell.rowlen = static_cast<int*>(rl);
+  if (n > 0)
+    SK_LAUNCH(csr_to_ell_kernel<T>, ceil_div(ld, kThreads), kThreads, 0, st, n, ld, static_cast<i64>(width),
+              C->csr.row_ptr, C->csr.col_ind, static_cast<const T*>(C->csr.vals), A->ell.col,
+              static_cast<T*>(va), A->ell.rowlen);
+  SK_CUDA(cudaGetLastError());
+  SK_CUDA(cudaStreamSynchronize(st));
+  return SK_OK;
+}
+
+template <typename T>
+static sk_status jad_from_csr(sk_matrix A, sk_matrix C) {
+  cudaStream_t st = A->stream;
+  const i64 n = C->nrow, nnz = C->nnz;
+  Temps tmp;
+  sk_status s;
+  int *len = nullptr, *dmax = nullptr;
+  if ((s = tmp.get(&len, n)) != SK_OK) return s;
+  if ((s = tmp.get(&dmax, 1)) != SK_OK) return s;
+  int maxlen = 0;
+  if ((s = max_row_length(C->csr.row_ptr, n, len, dmax, st, &maxlen)) != SK_OK) return s;
+  const i64 njd = nnz > 0 ? maxlen : 0;
+  A->nnz = nnz;
+  A->jad.njd = njd;
+  void *pm = nullptr, *jd = nullptr, *ci = nullptr, *va = nullptr, *pl = nullptr;
+  if ((s = dev_alloc(A, &pm, (n + 8) * 4)) != SK_OK) return s;
+  if ((s = dev_alloc(A, &jd, (njd + 8) * 4)) != SK_OK) return s;
+  if ((s = dev_alloc(A, &ci, (nnz + 8) * 4)) != SK_OK) return s;
+  if ((s = dev_alloc(A, &va, (nnz + 8) * sizeof(T))) != SK_OK) return s;
+  if ((s = dev_alloc(A, &pl, (n + 8) * 4 + 64)) != SK_OK) return s;
+  A->jad.perm = static_cast<int*>(pm);
+  A->jad.jdiag = static_cast<int*>(jd);
+  A->jad.col = static_cast<int*>(ci);
+  A->jad.vals = va;
+  A->jad.plen = static_cast<int*>(pl);
+  if (njd == 0) {
+    // An empty matrix: no diagonals (Jagged_diagonal_sparsity_Impl.cpp:28-31);
+    // the identity order serves the product, every row sums to zero.
+    SK_CUDA(cudaMemsetAsync(jd, 0, 4, st));
+    SK_CUDA(cudaMemsetAsync(pl, 0, (n + 8) * 4, st));
+    if (n > 0) SK_LAUNCH(iota_kernel, grid_for(n), kThreads, 0, st, A->jad.perm, n);
+    SK_CUDA(cudaGetLastError());
+    SK_CUDA(cudaStreamSynchronize(st));
+    return SK_OK;
+  }
+  unsigned *k1 = nullptr, *k2 = nullptr, *sk = nullptr;
+  int *i1 = nullptr, *i2 = nullptr, *si = nullptr, *width = nullptr;
+  i64* jd64 = nullptr;
+  if ((s = tmp.get(&k1, n)) != SK_OK) return s;
+  if ((s = tmp.get(&k2, n)) != SK_OK) return s;
+  if ((s = tmp.get(&i1, n)) != SK_OK) return s;
+  if ((s = tmp.get(&i2, n)) != SK_OK) return s;
+  if ((s = tmp.get(&width, njd)) != SK_OK) return s;
+  if ((s = tmp.get(&jd64, njd + 1)) != SK_OK) return s;
+  SK_LAUNCH(jad_keys_kernel, grid_for(n), kThreads, 0, st, len, n, static_cast<unsigned>(maxlen), k1);
+  if ((s = stable_radix_sort(k1, k2, i1, i2, n, static_cast<unsigned>(maxlen), tmp, st, &sk, &si)) != SK_OK)
+    return s;
+  SK_LAUNCH(jad_perm_kernel, grid_for(n), kThreads, 0, st, sk, si, n, static_cast<unsigned>(maxlen),
+            A->jad.perm, A->jad.plen, width);
+  if ((s = exclusive_scan(width, njd, jd64, tmp, st)) != SK_OK) return s;
+  SK_LAUNCH(narrow_i64_kernel, grid_for(njd + 1), kThreads, 0, st, jd64, njd + 1, A->jad.jdiag);
+  SK_LAUNCH(csr_to_jad_kernel<T>, grid_for(n), kThreads, 0, st, n, A->jad.perm, A->jad.plen, A->jad.jdiag,
+            C->csr.row_ptr, C->csr.col_ind, static_cast<const T*>(C->csr.vals), A->jad.col, static_cast<T*>(va));
+  SK_CUDA(cudaGetLastError());
+  SK_CUDA(cudaStreamSynchronize(st));
+  return SK_OK;
+}
+
+template <typename T>
+static sk_status bsr_from_csr(sk_matrix A, sk_matrix C, int br, int bc) {
+  cudaStream_t st = A->stream;
+  const i64 n = C->nrow;
+  const i64 nbr = (n + br - 1) / br;
+  const i64 bsz = static_cast<i64>(br) * bc;
+  auto& b = A->bsr;
+  b.br = br;
+  b.bc = bc;
+  b.nbr = nbr;
+  b.nbr_mult = n / br;
+  Temps tmp;
+  sk_status s;
+  int* cnt = nullptr;
+  i64* rp64 = nullptr;
+  if ((s = tmp.get(&cnt, nbr)) != SK_OK) return s;
+  if ((s = tmp.get(&rp64, nbr + 1)) != SK_OK) return s;
+  int G = 1;
+  while (G < br && G < 32) G <<= 1;
+  const i64 warps = (nbr + (32 / G) - 1) / (32 / G);
+  const int grid = ceil_div(warps * 32, kThreads);
+  if (nbr > 0)
+    SK_LAUNCH((csr_to_bsr_kernel<T, false>), grid, kThreads, 0, st, n, nbr, br, bc, G, C->csr.row_ptr,
+              C->csr.col_ind, static_cast<const T*>(C->csr.vals), cnt, nullptr, nullptr, nullptr);
+  if ((s = exclusive_scan(cnt, nbr, rp64, tmp, st)) != SK_OK) return s;
+  std::vector<int64_t> rp(static_cast<size_t>(nbr) + 1);
+  SK_CUDA(cudaMemcpyAsync(rp.data(), rp64, (nbr + 1) * sizeof(i64), cudaMemcpyDeviceToHost, st));
+  SK_CUDA(cudaStreamSynchronize(st));
+  const i64 nblocks = rp[static_cast<size_t>(nbr)];
+  SK_CHECK(nblocks * bsz < (i64(1) << 31) - 16, SK_INDEX_OVERFLOW, "block values do not fit int32");
+  b.nblocks = nblocks;
+  A->nnz = nblocks * bsz;
+  void *drp = nullptr, *dci = nullptr, *dva = nullptr;
+  if ((s = dev_alloc(A, &drp, (nbr + 8) * 4)) != SK_OK) return s;
+  if ((s = dev_alloc(A, &dci, (nblocks + 8) * 4)) != SK_OK) return s;
+  if ((s = dev_alloc(A, &dva, (nblocks * bsz + 8) * sizeof(T))) != SK_OK) return s;
+  SK_CUDA(cudaMemsetAsync(dva, 0, (nblocks * bsz + 8) * sizeof(T), st));
+  b.row_ptr = static_cast<int*>(drp);
+  b.col = static_cast<int*>(dci);
+  b.vals = dva;
+  SK_LAUNCH(narrow_i64_kernel, grid_for(nbr + 1), kThreads, 0, st, rp64, nbr + 1, b.row_ptr);
+  if (nbr > 0)
+    SK_LAUNCH((csr_to_bsr_kernel<T, true>), grid, kThreads, 0, st, n, nbr, br, bc, G, C->csr.row_ptr,
+              C->csr.col_ind, static_cast<const T*>(C->csr.vals), nullptr, rp64, b.col, static_cast<T*>(dva));
+  SK_CUDA(cudaGetLastError());
+  // the product's partition of block rows into CTA tiles is a greedy walk
+  // over the block row pointers, taken on the host copy above
+  std::vector<int> part;
+  bsr_partition(rp.data(), nbr, br, bsz, part);
+  b.nparts = static_cast<int>(part.size()) - 1;
+  if ((s = upload_vector(A, part, &b.part, st)) != SK_OK) return s;
+  if ((s = build_bsr_sell(A, rp.data(), st)) != SK_OK) return s;
+  SK_CUDA(cudaStreamSynchronize(st));
+  return SK_OK;
+}
+
+}  // namespace
+}  // namespace sk
+
+using namespace sk;
+
+extern "C" {
+
+sk_status sk_ell_from_csr(sk_matrix* out, sk_matrix csr) {
+  sk_status s = check_source(out, csr);
+  if (s != SK_OK) return s;
+  if ((s = new_handle(out, SK_ELL, csr->dtype, csr->nrow, csr->ncol)) != SK_OK) return s;
+  HandleGuard guard{out};
+  s = csr->dtype == SK_F64 ? ell_from_csr<double>(*out, csr) : ell_from_csr<float>(*out, csr);
+  if (s != SK_OK) return s;
+  guard.ok = true;
+  return SK_OK;
+}
+
+sk_status sk_jad_from_csr(sk_matrix* out, sk_matrix csr) {
+  sk_status s = check_source(out, csr);
+  if (s != SK_OK) return s;
+  if ((s = new_handle(out, SK_JAD, csr->dtype, csr->nrow, csr->ncol)) != SK_OK) return s;
+  HandleGuard guard{out};
+  s = csr->dtype == SK_F64 ? jad_from_csr<double>(*out, csr) : jad_from_csr<float>(*out, csr);
+  if (s != SK_OK) return s;
+  guard.ok = true;
+  return SK_OK;
+}
+
+sk_status sk_bsr_from_csr(sk_matrix* out, sk_matrix csr, int64_t block_rows, int64_t block_cols) {
+  sk_status s = check_source(out, csr);
+  if (s != SK_OK) return s;
+  SK_CHECK(block_rows >= 1 && block_cols >= 1 && block_rows <= kThreads &&
+               block_rows * block_cols <= kBsrTileVals,
+           SK_INVALID_ARG, "block shape must be >= 1, block_rows <= 256, block size <= 4096");
+  if ((s = new_handle(out, SK_BSR, csr->dtype, csr->nrow, csr->ncol)) != SK_OK) return s;
+  HandleGuard guard{out};
+  const int br = static_cast<int>(block_rows), bc = static_cast<int>(block_cols);
+  s = csr->dtype == SK_F64 ? bsr_from_csr<double>(*out, csr, br, bc) : bsr_from_csr<float>(*out, csr, br, bc);
+  if (s != SK_OK) return s;
+  guard.ok = true;
+  return SK_OK;
+}
+
+sk_status sk_csr_export(sk_matrix A, int64_t* row_ptr, int64_t* col_ind, void* values) {
+  SK_CHECK(A && A->format == SK_CSR, SK_INVALID_ARG, "not a CSR handle");
+  cudaStream_t st = A->stream;
+  SK_CUDA(cudaStreamSynchronize(st));
+  sk_status s;
+  if ((s = download_indices(A->csr.row_ptr, A->nrow + 1, row_ptr, st)) != SK_OK) return s;
+  if ((s = download_indices(A->csr.col_ind, A->nnz, col_ind, st)) != SK_OK) return s;
+  return download_values(A->csr.vals, A->nnz, A->dtype, values, st);
+}
+
+sk_status sk_ell_export(sk_matrix A, int64_t* col_ind, void* values) {
+  SK_CHECK(A && A->format == SK_ELL, SK_INVALID_ARG, "not an ELL handle");
+  cudaStream_t st = A->stream;
+  SK_CUDA(cudaStreamSynchronize(st));
+  const i64 slots = A->nrow * A->ell.width;
+  if (slots == 0) return SK_OK;
+  SK_CHECK(col_ind && values, SK_INVALID_ARG, "null output array");
+  const size_t V = vbytes(A->dtype);
+  Temps tmp;
+  long long* stage = nullptr;
+  char* vstage = nullptr;
+  const i64 chunk = std::min(slots, kChunk);
+  sk_status s;
+  if ((s = tmp.get(&stage, chunk)) != SK_OK) return s;
+  if ((s = tmp.get(&vstage, chunk * static_cast<i64>(V))) != SK_OK) return s;
+  for (i64 off = 0; off < slots; off += chunk) {
+    const i64 c = std::min(chunk, slots - off);
+    if (A->dtype == SK_F64)
+      SK_LAUNCH(ell_export_kernel<double>, grid_for(c), kThreads, 0, st, off, c, A->ell.width, A->ell.ld,
+                A->ell.col, static_cast<const double*>(A->ell.vals), A->ell.rowlen, stage,
+                reinterpret_cast<double*>(vstage));
+    else
+      SK_LAUNCH(ell_export_kernel<float>, grid_for(c), kThreads, 0, st, off, c, A->ell.width, A->ell.ld,
+                A->ell.col, static_cast<const float*>(A->ell.vals), A->ell.rowlen, stage,
+                reinterpret_cast<float*>(vstage));
+    SK_CUDA(cudaMemcpyAsync(col_ind + off, stage, c * sizeof(long long), cudaMemcpyDeviceToHost, st));
+    SK_CUDA(cudaMemcpyAsync(static_cast<char*>(values) + off * V, vstage, c * V, cudaMemcpyDeviceToHost, st));
+    SK_CUDA(cudaStreamSynchronize(st));
+  }
+  return SK_OK;
+}
+
+sk_status sk_jad_export(sk_matrix A, int64_t* perm, int64_t* jdiag, int64_t* col_ind, void* values) {
+  SK_CHECK(A && A->format == SK_JAD, SK_INVALID_ARG, "not a JAD handle");
+  SK_CHECK(jdiag, SK_INVALID_ARG, "null jdiag");
+  cudaStream_t st = A->stream;
+  SK_CUDA(cudaStreamSynchronize(st));
+  sk_status s;
+  if (A->jad.njd > 0 && (s = download_indices(A->jad.perm, A->nrow, perm, st)) != SK_OK) return s;
+  if ((s = download_indices(A->jad.jdiag, A->jad.njd + 1, jdiag, st)) != SK_OK) return s;
+  if ((s = download_indices(A->jad.col, A->nnz, col_ind, st)) != SK_OK) return s;
+  return download_values(A->jad.vals, A->nnz, A->dtype, values, st);
+}
+
+sk_status sk_bsr_export(sk_matrix A, int64_t* row_ptr, int64_t* col_ind, void* values) {
+  SK_CHECK(A && A->format == SK_BSR, SK_INVALID_ARG, "not a BSR handle");
+  cudaStream_t st = A->stream;
+  SK_CUDA(cudaStreamSynchronize(st));
+  const auto& b = A->bsr;
+  sk_status s;
+  if ((s = download_indices(b.row_ptr, b.nbr + 1, row_ptr, st)) != SK_OK) return s;
+  if ((s = download_indices(b.col, b.nblocks, col_ind, st)) != SK_OK) return s;
+  return download_values(b.vals, b.nblocks * b.br * b.bc, A->dtype, values, st);
+}
+
+}  // extern "C"

@@ -135,12 +135,11 @@ __global__ void to_float_kernel(const T* __restrict__ in, float* __restrict__ ou
   for (; i < n; i += stride) out[i] = static_cast<float>(in[i]);
 }
 
-static int grid_for(i64 n) {
+int grid_for(i64 n) {
   i64 g = (n + kThreads - 1) / kThreads;
   return static_cast<int>(std::max<i64>(1, std::min<i64>(g, 148 * 32)));
 }
 
-constexpr i64 kChunk = i64(1) << 23;  // staging elements per upload step
 
 // Copies count int64 host indices to int32 device memory, checking range.
 static sk_status upload_indices(const int64_t* host, i64 count, int* dev, long long lo,
@@ -174,8 +173,6 @@ static sk_status upload_indices(const int64_t* host, i64 count, int* dev, long l
                                        " index value(s) outside the valid int32 range");
   return SK_OK;
 }
-
-static size_t vbytes(sk_dtype dt) { return dt == SK_F64 ? 8 : 4; }
 
 // Row-block partition of a CSR row_ptr for csr_spmv_kernel: blocks of at
 // most kRowsMax rows and kTileNnz entries, or one row longer than a tile.
@@ -213,7 +210,7 @@ static void csr_partition(const int64_t* rp, i64 n, std::vector<int>& part,
 // BSR block-row partition: at most kThreads / br block rows and a tile's
 // worth of block values per CTA; a longer block row gets a CTA alone (the
 // kernel then walks it tile by tile).
-static void bsr_partition(const int64_t* rp, i64 nbr, i64 br, i64 bsz, std::vector<int>& part) {
+void bsr_partition(const int64_t* rp, i64 nbr, i64 br, i64 bsz, std::vector<int>& part) {
   part.clear();
   part.push_back(0);
   i64 max_rows = std::max<i64>(1, kThreads / br);
@@ -231,17 +228,7 @@ static void bsr_partition(const int64_t* rp, i64 nbr, i64 br, i64 bsz, std::vect
   }
 }
 
-template <typename V>
-static sk_status upload_vector(sk_matrix A, const std::vector<V>& h, V** dev, cudaStream_t st) {
-  void* p = nullptr;
-  sk_status s = dev_alloc(A, &p, h.size() * sizeof(V) + 64);
-  if (s != SK_OK) return s;
-  *dev = static_cast<V*>(p);
-  if (!h.empty()) SK_CUDA(cudaMemcpyAsync(p, h.data(), h.size() * sizeof(V), cudaMemcpyHostToDevice, st));
-  return SK_OK;
-}
-
-static sk_status new_handle(sk_matrix* out, sk_format f, sk_dtype dt, i64 nrow, i64 ncol) {
+sk_status new_handle(sk_matrix* out, sk_format f, sk_dtype dt, i64 nrow, i64 ncol) {
   SK_CHECK(out != nullptr, SK_INVALID_ARG, "null output handle");
   *out = nullptr;
   SK_CHECK(dt == SK_F64 || dt == SK_F32, SK_INVALID_ARG, "dtype must be SK_F64 or SK_F32");
@@ -268,7 +255,7 @@ static sk_status new_handle(sk_matrix* out, sk_format f, sk_dtype dt, i64 nrow, 
   return SK_OK;
 }
 
-static void destroy_handle(sk_matrix A) {
+void destroy_handle(sk_matrix A) {
   if (!A) return;
   if (A->stream) cudaStreamSynchronize(A->stream);
   for (void* p : A->allocations) cudaFree(p);
@@ -278,17 +265,6 @@ static void destroy_handle(sk_matrix A) {
   if (A->stream) cudaStreamDestroy(A->stream);
   delete A;
 }
-
-struct HandleGuard {
-  sk_matrix* slot;
-  bool ok = false;
-  ~HandleGuard() {
-    if (!ok && slot && *slot) {
-      destroy_handle(*slot);
-      *slot = nullptr;
-    }
-  }
-};
 
 // Adds the SELL-32 copy of a CSR handle when every row has at most
 // kSellMaxRow entries and the padding stays within a quarter of nnz.
@@ -336,7 +312,7 @@ static sk_status build_sell(sk_matrix A, const int64_t* rp, cudaStream_t st_) {
 
 // Adds the sliced copy of a 2x2 or 3x3 BSR handle when every block row has
 // at most kSellMaxRow blocks and the padding stays within a quarter.
-static sk_status build_bsr_sell(sk_matrix A, const int64_t* rp, cudaStream_t st_) {
+sk_status build_bsr_sell(sk_matrix A, const int64_t* rp, cudaStream_t st_) {
   auto& B = A->bsr;
   if (!((B.br == 3 && B.bc == 3) || (B.br == 2 && B.bc == 2))) return SK_OK;
   const i64 nbr = B.nbr;

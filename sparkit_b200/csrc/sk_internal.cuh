@@ -226,4 +226,46 @@ struct Scalars {
 };
 inline int ceil_div(i64 a, i64 b) { return static_cast<int>((a + b - 1) / b); }
 
+// ------------------------------------------------------------------
+// Handle construction, shared by the uploads of host arrays (sk_core.cu)
+// and the conversions on the device (sk_convert.cu)
+// ------------------------------------------------------------------
+constexpr i64 kChunk = i64(1) << 23;  // staging elements per host copy step
+
+inline size_t vbytes(sk_dtype dt) { return dt == SK_F64 ? 8 : 4; }
+
+// Grid of a grid-stride kernel over n elements: at most 32 CTAs per SM.
+int grid_for(i64 n);
+
+// A new handle of format f on the current device, with its own stream.
+sk_status new_handle(sk_matrix* out, sk_format f, sk_dtype dt, i64 nrow, i64 ncol);
+void destroy_handle(sk_matrix A);
+
+// Destroys a half-built handle when its constructor returns early.
+struct HandleGuard {
+  sk_matrix* slot;
+  bool ok = false;
+  ~HandleGuard() {
+    if (!ok && slot && *slot) {
+      destroy_handle(*slot);
+      *slot = nullptr;
+    }
+  }
+};
+
+template <typename V>
+sk_status upload_vector(sk_matrix A, const std::vector<V>& h, V** dev, cudaStream_t st) {
+  void* p = nullptr;
+  sk_status s = dev_alloc(A, &p, h.size() * sizeof(V) + 64);
+  if (s != SK_OK) return s;
+  *dev = static_cast<V*>(p);
+  if (!h.empty()) SK_CUDA(cudaMemcpyAsync(p, h.data(), h.size() * sizeof(V), cudaMemcpyHostToDevice, st));
+  return SK_OK;
+}
+
+// BSR block-row partition of the product kernel (host row pointers) and
+// the sliced copy of 2x2 / 3x3 handles.
+void bsr_partition(const int64_t* rp, i64 nbr, i64 br, i64 bsz, std::vector<int>& part);
+sk_status build_bsr_sell(sk_matrix A, const int64_t* rp, cudaStream_t st);
+
 }  // namespace sk

@@ -99,9 +99,45 @@ class Device_matrix:
         self.handle = h
         self.dtype = dt
         self._shape = (n, m)
+        self._block = (A.block_rows(), A.block_cols()) if isinstance(A, Block_sparse_row_matrix) else None
+
+    @classmethod
+    def _wrap(cls, h, dtype, shape, block=None):
+        self = cls.__new__(cls)
+        self.handle = h
+        self.dtype = np.dtype(dtype)
+        self._shape = tuple(shape)
+        self._block = block
+        return self
 
     def shape(self):
         return self._shape
+
+    def to_host(self):
+        """The handle as the reference's host object, read back from the
+        device (sk_csr_export / sk_ell_export / sk_jad_export /
+        sk_bsr_export)."""
+        inf = self.info()
+        n, m = self._shape
+        fmt, nnz, w = inf["format"], inf["nnz"], inf["width"]
+        z = lambda k, dt=np.int64: np.zeros(k, dtype=dt)
+        if fmt == 0:
+            rp, ci, va = z(n + 1), z(nnz), z(nnz, self.dtype)
+            check(lib().sk_csr_export(self.handle, _ptr(rp), _ptr(ci), _ptr(va)))
+            return Compressed_row_matrix((n, m), rp, ci, va)
+        if fmt == 1:
+            ci, va = z(n * w), z(n * w, self.dtype)
+            check(lib().sk_ell_export(self.handle, _ptr(ci), _ptr(va)))
+            return Ellpack_matrix((n, m), w, ci, va)
+        if fmt == 2:
+            pm, jd, ci, va = z(n if w else 0), z(w + 1), z(nnz), z(nnz, self.dtype)
+            check(lib().sk_jad_export(self.handle, _ptr(pm), _ptr(jd), _ptr(ci), _ptr(va)))
+            return Jagged_diagonal_matrix((n, m), pm, jd, ci, va)
+        br, bc = self._block
+        nbr = (n + br - 1) // br
+        rp, ci, va = z(nbr + 1), z(w), z(w * br * bc, self.dtype)
+        check(lib().sk_bsr_export(self.handle, _ptr(rp), _ptr(ci), _ptr(va)))
+        return Block_sparse_row_matrix((n, m), br, bc, rp, ci, va)
 
     def info(self):
         """dict of sk_matrix_info: format, dtype, nrow, ncol, nnz, width,
@@ -135,6 +171,31 @@ class Device_matrix:
             self.close()
         except Exception:
             pass
+
+
+def _convert(fn, Ad, *args, block=None):
+    h = ctypes.c_void_p()
+    check(fn(ctypes.byref(h), Ad.handle, *args))
+    return Device_matrix._wrap(h, Ad.dtype, Ad.shape(), block)
+
+
+def to_ellpack(Ad):
+    """to_ellpack(Compressed_row_matrix) (conversions.hpp:427-467), built on
+    the device from a CSR handle: sk_ell_from_csr."""
+    return _convert(lib().sk_ell_from_csr, Ad)
+
+
+def to_jagged_diagonal(Ad):
+    """to_jagged_diagonal(Compressed_row_matrix) (conversions.hpp:641-691)
+    on the device: sk_jad_from_csr."""
+    return _convert(lib().sk_jad_from_csr, Ad)
+
+
+def to_block_sparse_row(Ad, block_rows, block_cols):
+    """to_block_sparse_row(csr, block_rows, block_cols)
+    (conversions.hpp:524-577) on the device: sk_bsr_from_csr."""
+    return _convert(lib().sk_bsr_from_csr, Ad, int(block_rows), int(block_cols),
+                    block=(int(block_rows), int(block_cols)))
 
 
 def multiply(Ad, x):

@@ -7,7 +7,7 @@ oracle/build_ref.sh).  Run from the repository root:
 Outputs
   reference_outputs.npz  -- inputs and reference outputs, keyed by case:
       SpMV of every format (reference conversions + multiply) on seeded
-      matrices, Jacobi inverse diagonals, Chebyshev coefficients and applies,
+      matrices, the conversions' own arrays, Jacobi inverse diagonals, Chebyshev coefficients and applies,
       and CG / BiCGSTAB / FGMRES solutions, summaries and residual histories
       on the matrices of the reference's solver tests.
 known_answers.json (hand-written, not generated) holds the known-answer
@@ -26,6 +26,10 @@ from sparkit_b200 import matgen  # noqa: E402
 from sparkit_b200.formats import Compressed_row_matrix  # noqa: E402
 
 OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "reference_outputs.npz")
+
+# block shapes of the conversion fixtures: square, rectangular, blocks that
+# do not divide the matrix, and block rows taller than a warp
+CONVERT_BLOCKS = ((1, 1), (2, 2), (3, 3), (2, 3), (1, 4), (4, 4), (5, 7), (33, 2), (64, 1))
 
 
 def spmv_matrices():
@@ -73,6 +77,26 @@ def main():
             out[f"{tag}/y_jad"] = R.spmv(Ad, x, "jad")
             for br, bc in ((2, 2), (3, 3), (2, 3)):
                 out[f"{tag}/y_bsr{br}{bc}"] = R.spmv(Ad, x, "bsr", (br, bc))
+    # the reference's own conversions (FP64), the input of the device-side
+    # construction tests; the ELL of longrow_3000 (7.8M padded slots) is
+    # left out, its layout is the CSR padded to the longest row
+    convs = dict(spmv_matrices())
+    convs["empty_5x4"] = Compressed_row_matrix((5, 4), np.zeros(6, np.int64), np.zeros(0, np.int64), np.zeros(0))
+    for name, A in convs.items():
+        tag = f"convert/{name}"
+        lens = np.diff(A.row_ptr())
+        if A.shape()[0] * int(lens.max()) <= 200000:
+            E = R.to_ellpack(A)
+            out[f"{tag}/ell/width"] = np.array(E.max_nnz_per_row())
+            out[f"{tag}/ell/col_ind"] = E.col_ind()
+            out[f"{tag}/ell/values"] = E.values()
+        J = R.to_jagged_diagonal(A)
+        for f in ("perm", "jdiag", "col_ind", "values"):
+            out[f"{tag}/jad/{f}"] = getattr(J, f)()
+        for br, bc in CONVERT_BLOCKS:
+            B = R.to_block_sparse_row(A, br, bc)
+            for f in ("row_ptr", "col_ind", "values"):
+                out[f"{tag}/bsr{br}x{bc}/{f}"] = getattr(B, f)()
     # preconditioners
     P = matgen.poisson_2d(8, 8, 0.5)
     out["jacobi/poisson8/inv_d"] = R.jacobi(P)
