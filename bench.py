@@ -56,6 +56,9 @@ def parse():
                    help="apply the (untrained) learned preconditioner on 512^2 four times, for ncu")
     p.add_argument("--profile-mixed", action="store_true",
                    help="one mixed solve with 100 persistent FP32 inner iterations on the 128^3 GRF problem, for ncu")
+    p.add_argument("--no-convert", action="store_true")
+    p.add_argument("--profile-convert", action="store_true",
+                   help="each device format conversion once (for an ncu launch list)")
     p.add_argument("--profile-formats", action="store_true",
                    help="run one product of every sweep format and precision (for ncu captures), no timing")
     return p.parse_args()
@@ -260,6 +263,103 @@ def sweep(stream, grid):
     out["zipf_csr_f64"] = {"gbs": Zd.info()["spmv_bytes"] / ms / 1e6, "us": ms * 1e3, "nnz": Z.size(),
                            "mean_row": Z.size() / Z.shape()[0]}
     return out
+
+
+def _timed_convert(make, reps=7):
+    """Median wall time of a synchronous device conversion (after one
+    untimed call), the median device time of its kernels (events around
+    them, sk_matrix_build_ms) and the info of the handle it built."""
+    import torch
+    make().close()
+    ts, ds = [], []
+    for _ in range(reps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        h = make()
+        ts.append(time.perf_counter() - t0)
+        ds.append(h.build_ms())
+        info = h.info()
+        h.close()
+    return float(np.median(ts)), float(np.median(ds)), info
+
+
+def convert_bytes(fmt, n, nnz, vbytes, info, block=None):
+    """Algorithmic bytes of one conversion: the CSR read once, the new
+    layout written once (ELL with its slot stride and padding)."""
+    read = 4 * (n + 1) + nnz * (4 + vbytes)
+    if fmt == "ell":
+        ld = (n + 31) // 32 * 32 + 96
+        return read + ld * info["width"] * (4 + vbytes) + 4 * n
+    if fmt == "jad":
+        return read + 8 * n + 4 * (info["width"] + 1) + nnz * (4 + vbytes)
+    br, bc = block
+    nbr = (n + br - 1) // br
+    return read + 4 * (nbr + 1) + info["width"] * (4 + br * bc * vbytes)
+
+
+def convert_cases(grid):
+    from sparkit_b200 import matgen
+    A = matgen.laplacian_3d_dirichlet(grid)
+    V = matgen.vector_laplacian_3d_bsr_csr(grid, seed=1)
+    Z = matgen.zipf_random(1_000_000, s=1.5, cap=2048, seed=0)
+    # (tag, matrix, format, block, rows of the reference's sample)
+    return [("lap3d_ell", A, "ell", None, 1 << 18), ("lap3d_jad", A, "jad", None, 1 << 18),
+            ("vec3_bsr33", V, "bsr", (3, 3), 3 << 17), ("zipf_jad", Z, "jad", None, 25_000),
+            ("zipf_ell", Z, "ell", None, 25_000)]
+
+
+def convert_runs(grid):
+    """Device-side construction of the sweep's layouts from CSR handles
+    (sk_ell_from_csr / sk_jad_from_csr / sk_bsr_from_csr), FP64: the
+    synchronous call (allocation, kernels, the scalars read back) and the
+    device time of its kernels, as CSR entries converted per second, and
+    the algorithmic GB/s of the kernels; beside each, the compiled
+    reference's own host conversion on a row sample of the same matrix
+    (one core)."""
+    from oracle.binding import Reference, reference_available
+    from sparkit_b200 import formats, gpu
+    peak, _ = measured_peak()
+    ref = Reference() if reference_available() else None
+    out = {}
+    for tag, M, fmt, blk, rows in convert_cases(grid):
+        Cd = gpu.Device_matrix(M)
+        make = {"ell": lambda: gpu.to_ellpack(Cd), "jad": lambda: gpu.to_jagged_diagonal(Cd),
+                "bsr": lambda: gpu.to_block_sparse_row(Cd, *blk)}[fmt]
+        secs, dev_ms, info = _timed_convert(make)
+        Cd.close()
+        n, nnz = M.shape()[0], M.size()
+        nbytes = convert_bytes(fmt, n, nnz, 8, info, blk)
+        dev_s = dev_ms * 1e-3
+        row = {"call_ms": secs * 1e3, "device_ms": dev_ms, "nnz": nnz, "width": info["width"],
+               "mnnz_per_s": nnz / secs / 1e6, "device_mnnz_per_s": nnz / dev_s / 1e6,
+               "device_gbs": nbytes / dev_s / 1e9, "frac_of_measured_peak": nbytes / dev_s / 1e9 / peak,
+               "bytes_model": nbytes}
+        if ref is not None:
+            rp = M.row_ptr()[: rows + 1].copy()
+            S = formats.Compressed_row_matrix((rows, M.shape()[1]), rp, M.col_ind()[: rp[-1]],
+                                              M.values()[: rp[-1]])
+            rs = ref.convert_seconds(S, fmt, blk or (3, 3))
+            row["cpu_reference"] = {"mnnz_per_s": S.size() / rs / 1e6, "s": rs, "cores": 1, "kind": "reference",
+                                    "sample": f"rows 0..{rows} ({S.size()} entries)"}
+            row["speedup_vs_reference"] = row["mnnz_per_s"] / row["cpu_reference"]["mnnz_per_s"]
+        out[tag] = row
+    return out
+
+
+def profile_convert(grid):
+    """Each device conversion once, for an ncu launch list."""
+    import torch
+
+    from sparkit_b200 import gpu
+    torch.cuda.set_device(0)
+    for tag, M, fmt, blk, _ in convert_cases(grid):
+        Cd = gpu.Device_matrix(M)
+        h = {"ell": lambda: gpu.to_ellpack(Cd), "jad": lambda: gpu.to_jagged_diagonal(Cd),
+             "bsr": lambda: gpu.to_block_sparse_row(Cd, *blk)}[fmt]()
+        h.close()
+        Cd.close()
+    torch.cuda.synchronize()
+    return 0
 
 
 def solver_runs(grid3):
@@ -628,6 +728,8 @@ def main():
         return run_reference(args)
     if args.profile_formats:
         return profile_formats(args.grid)
+    if args.profile_convert:
+        return profile_convert(args.grid)
     if args.profile_solvers:
         return profile_solvers(args.grid)
     if args.profile_learned:
@@ -739,6 +841,8 @@ def main():
     if rank == 0 and world == 1 and not args.no_sweep:
         Ad.close()
         extra["sweep"] = sweep(stream, args.grid)
+    if rank == 0 and world == 1 and not args.no_convert:
+        extra["convert"] = convert_runs(args.grid)
     if rank == 0 and world == 1 and not args.no_solvers:
         extra["solvers"] = solver_runs(args.grid)
         extra["solvers"]["c5_batched"] = batched_runs()

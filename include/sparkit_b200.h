@@ -124,6 +124,10 @@ SK_API sk_status sk_ell_from_csr(sk_matrix* out, sk_matrix csr);
 SK_API sk_status sk_jad_from_csr(sk_matrix* out, sk_matrix csr);
 SK_API sk_status sk_bsr_from_csr(sk_matrix* out, sk_matrix csr,
                           int64_t block_rows, int64_t block_cols);
+/* Device time in ms of the kernels that built a handle on the device (the
+ * conversions above; host allocations between them not counted; the BSR
+ * sliced product copy not counted); 0 for handles uploaded from the host. */
+SK_API sk_status sk_matrix_build_ms(sk_matrix A, double* ms);
 
 /* The reference's accessors row_ptr() / col_ind() / values() / perm() /
  * jdiag() (Compressed_row_matrix.hpp, Ellpack_matrix.hpp,

@@ -369,6 +369,25 @@ class Reference:
         self.destroy(e, A.dtype)
         return Block_sparse_row_matrix((n, m), br, bc, rp, ci, va)
 
+    def convert_seconds(self, A, fmt, block=(3, 3)):
+        """Wall time of the reference's own conversion of A (CSR) to fmt:
+        the CSR handle is built before and the result destroyed after the
+        timed call."""
+        import time
+        s = _sfx(A.dtype)
+        h = self.csr_handle(A)
+        t0 = time.perf_counter()
+        if fmt == "ell":
+            e = getattr(self.L, f"ref_to_ellpack_{s}")(c_vp(h))
+        elif fmt == "jad":
+            e = getattr(self.L, f"ref_to_jagged_diagonal_{s}")(c_vp(h))
+        else:
+            e = getattr(self.L, f"ref_to_block_sparse_row_{s}")(c_vp(h), c_i64(block[0]), c_i64(block[1]))
+        secs = time.perf_counter() - t0
+        self.destroy(e, A.dtype)
+        self.destroy(h, A.dtype)
+        return secs
+
     def _handle_any(self, A):
         """Reference handle of A in its own format (built through the
         reference's conversion from CSR, which the format tests pin)."""

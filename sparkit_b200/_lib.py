@@ -104,6 +104,7 @@ SIGNATURES = [
     ("sk_ell_from_csr", [ctypes.POINTER(c_vp), c_vp]),
     ("sk_jad_from_csr", [ctypes.POINTER(c_vp), c_vp]),
     ("sk_bsr_from_csr", [ctypes.POINTER(c_vp), c_vp, c_i64, c_i64]),
+    ("sk_matrix_build_ms", [c_vp, ctypes.POINTER(c_dbl)]),
     ("sk_csr_export", [c_vp, c_vp, c_vp, c_vp]),
     ("sk_ell_export", [c_vp, c_vp, c_vp]),
     ("sk_jad_export", [c_vp, c_vp, c_vp, c_vp, c_vp]),

@@ -143,6 +143,7 @@ struct sk_matrix_s {
   void* ws2 = nullptr;  // second workspace (outer loop of the mixed solver)
   size_t ws2_bytes = 0;
   bool mixed_jacobi_ready = false;  // FP32 inverse diagonal held in ws2
+  double build_ms = 0;  // device time of the kernels that built the handle on the device
   sk::i64 spmv_bytes() const;
 };
 

@@ -147,6 +147,13 @@ class Device_matrix:
         keys = ("format", "dtype", "nrow", "ncol", "nnz", "width", "device_bytes", "spmv_bytes")
         return dict(zip(keys, list(arr)))
 
+    def build_ms(self):
+        """Device time of the kernels that built this handle on the device
+        (sk_matrix_build_ms); 0.0 for a handle uploaded from the host."""
+        v = ctypes.c_double()
+        check(lib().sk_matrix_build_ms(self.handle, ctypes.byref(v)))
+        return v.value
+
     def add_f32_values(self):
         check(lib().sk_matrix_add_f32_values(self.handle))
 

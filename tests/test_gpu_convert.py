@@ -66,6 +66,7 @@ def test_converted_handles_multiply_like_uploaded_ones(gpu_lib, golden, name):
         for dev, host in pairs:
             up = gpu.Device_matrix(host)
             assert dev.info()["nnz"] == up.info()["nnz"] and dev.info()["width"] == up.info()["width"]
+            assert dev.build_ms() > 0.0 and up.build_ms() == 0.0
             _same(gpu.multiply(dev, x), gpu.multiply(up, x))
 
 
