@@ -59,6 +59,29 @@ class Summary(ctypes.Structure):
 
 
 
+class LanczosCfg(ctypes.Structure):
+    _fields_ = [("num_eigenvalues", c_i64), ("krylov_dimension", c_i64), ("tolerance", ctypes.c_double),
+                ("max_restarts", c_i64), ("target", ctypes.c_int32), ("collect_residuals", ctypes.c_int32)]
+
+
+class LanczosOut(ctypes.Structure):
+    _fields_ = [("count", c_i64), ("computed_restarts", c_i64), ("converged_count", c_i64),
+                ("residual_count", c_i64), ("restart_residuals_count", c_i64), ("converged", ctypes.c_int32)]
+
+    def as_dict(self, ev, vecs, res, rr):
+        d = dict(eigenvalues=ev[: self.count].copy(), residual_norms=res[: self.residual_count].copy(),
+                 computed_restarts=self.computed_restarts, converged_count=self.converged_count,
+                 converged=bool(self.converged), restart_residuals=rr[: self.restart_residuals_count].copy())
+        if vecs is not None:
+            d["eigenvectors"] = vecs[: self.count].copy()
+        return d
+
+
+# Eigen_target (eigen_target.hpp:13-20)
+EIGEN_TARGETS = ("largest_magnitude", "smallest_magnitude", "largest_algebraic", "smallest_algebraic",
+                 "largest_real", "smallest_real")
+
+
 def _pad_to_blocks(x, bc):
     """x followed by zeros up to a whole number of bc-wide block columns."""
     m = -(-x.size // int(bc)) * int(bc)
@@ -217,6 +240,50 @@ class Oracle:
     def minres(self, A, b, x0, tol, max_it, left=None, right=None, collect=False, prec_matrix=None):
         return self._solve("minres", A, [left, right], b, x0, KrylovCfg(tol, max_it, int(collect)), max_it + 2,
                            prec_matrix)
+
+    # -------------------------------------------------------------- #
+    # Lanczos and the eigenvalue estimates (sk_oracle_lanczos.h)       #
+    # -------------------------------------------------------------- #
+
+    def tridiagonal_eigen(self, d, e, tol=1e-15, max_iterations=None, vectors=True):
+        """tridiagonal_eigen (dense_tridiagonal_eigen.hpp:58): unsorted
+        eigenvalues and, per eigenvalue, its eigenvector (rows)."""
+        d = np.array(d, dtype=np.float64)
+        e = np.array(e, dtype=np.float64)
+        n = d.size
+        Q = np.zeros((n, n)) if vectors else None
+        maxit = 30 * n if max_iterations is None else max_iterations
+        self.L.sko_tridiagonal_eigen_f64(c_i64(n), _p(d), _p(e), ctypes.c_double(tol), c_i64(maxit), _p(Q))
+        return d, Q
+
+    def lanczos(self, A, nev=1, m=20, tol=1e-10, max_restarts=10, target="largest_algebraic", collect=False,
+                vectors=False):
+        """lanczos(n, cfg, multiply(A)) (lanczos.hpp:495)."""
+        op, keep = self._operator(A)
+        n = A.shape()[0]
+        ev = np.zeros(max(nev, 1), A.dtype)
+        res = np.zeros(max(nev, 1), A.dtype)
+        vecs = np.zeros((max(nev, 1), n), A.dtype) if vectors else None
+        rr = np.zeros(max_restarts + 2)
+        cfg = LanczosCfg(nev, m, tol, max_restarts, EIGEN_TARGETS.index(target), int(collect))
+        out = LanczosOut()
+        getattr(self.L, f"sko_lanczos_{_sfx(A.dtype)}")(ctypes.byref(op), ctypes.byref(cfg), _p(ev), _p(vecs),
+                                                       _p(res), _p(rr), ctypes.byref(out))
+        return out.as_dict(ev, vecs, res, rr)
+
+    def eigenvalue_bounds(self, A, num_iter=30):
+        """estimate_eigenvalue_bounds (conditioning.hpp:132): (lmin, lmax)."""
+        op, keep = self._operator(A)
+        out = np.zeros(2, A.dtype)
+        getattr(self.L, f"sko_eigenvalue_bounds_{_sfx(A.dtype)}")(ctypes.byref(op), c_i64(num_iter), _p(out))
+        return out[0], out[1]
+
+    def spectral_radius(self, A, num_iter=20):
+        """estimate_spectral_radius (conditioning.hpp:112)."""
+        op, keep = self._operator(A)
+        f = getattr(self.L, f"sko_spectral_radius_{_sfx(A.dtype)}")
+        f.restype = ctypes.c_double if A.dtype == np.float64 else ctypes.c_float
+        return f(ctypes.byref(op), c_i64(num_iter))
 
     # -------------------------------------------------------------- #
     # Learned preconditioner network (sk_oracle_net.c)                #
@@ -387,6 +454,37 @@ class Reference:
         self.destroy(e, A.dtype)
         self.destroy(h, A.dtype)
         return secs
+
+    def lanczos(self, A, nev=1, m=20, tol=1e-10, max_restarts=10, target="largest_algebraic", collect=False,
+                vectors=False):
+        h = self.csr_handle(A)
+        n = A.shape()[0]
+        ev = np.zeros(max(nev, 1), A.dtype)
+        res = np.zeros(max(nev, 1), A.dtype)
+        vecs = np.zeros((max(nev, 1), n), A.dtype) if vectors else None
+        rr = np.zeros(max_restarts + 2)
+        out = LanczosOut()
+        getattr(self.L, f"ref_lanczos_{_sfx(A.dtype)}")(c_vp(h), c_i64(nev), c_i64(m), ctypes.c_double(tol),
+                                                       c_i64(max_restarts), EIGEN_TARGETS.index(target),
+                                                       int(collect), _p(ev), _p(vecs), _p(res), _p(rr),
+                                                       ctypes.byref(out))
+        self.destroy(h, A.dtype)
+        return out.as_dict(ev, vecs, res, rr)
+
+    def eigenvalue_bounds(self, A, num_iter=30):
+        h = self.csr_handle(A)
+        out = np.zeros(2, A.dtype)
+        getattr(self.L, f"ref_eigenvalue_bounds_{_sfx(A.dtype)}")(c_vp(h), c_i64(num_iter), _p(out))
+        self.destroy(h, A.dtype)
+        return out[0], out[1]
+
+    def spectral_radius(self, A, num_iter=20):
+        h = self.csr_handle(A)
+        f = getattr(self.L, f"ref_spectral_radius_{_sfx(A.dtype)}")
+        f.restype = ctypes.c_double
+        v = f(c_vp(h), c_i64(num_iter))
+        self.destroy(h, A.dtype)
+        return A.dtype.type(v)
 
     def _handle_any(self, A):
         """Reference handle of A in its own format (built through the

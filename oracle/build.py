@@ -14,7 +14,8 @@ REF_SO = os.path.join(HERE, "_ref", "libsparkit_ref.so")
 
 
 def build_oracle(force=False):
-    src = [os.path.join(HERE, f) for f in ("sk_oracle.c", "sk_oracle_net.c", "sk_oracle_impl.h", "sk_oracle.h")]
+    src = [os.path.join(HERE, f) for f in ("sk_oracle.c", "sk_oracle_net.c", "sk_oracle_impl.h", "sk_oracle_lanczos.h",
+                                         "sk_oracle.h")]
     if not force and os.path.exists(ORACLE_SO) and all(
         os.path.getmtime(ORACLE_SO) >= os.path.getmtime(s) for s in src
     ):

@@ -13,7 +13,9 @@
 // :44), chebyshev_preconditioner / _apply (chebyshev_preconditioner.hpp:46,
 // :98), conjugate_gradient (conjugate_gradient.hpp:347), bicgstab
 // (bicgstab.hpp:391), fgmres (fgmres.hpp:459), gmres (gmres.hpp:408), cgs
-// (cgs.hpp:374), minres (minres.hpp:397) and the matrix generators of
+// (cgs.hpp:374), minres (minres.hpp:397), lanczos (lanczos.hpp:495),
+// estimate_spectral_radius / estimate_eigenvalue_bounds (conditioning.hpp:112,
+// :132) and the matrix generators of
 // matgen.hpp used by the reference's solver tests.
 
 #include <algorithm>
@@ -37,6 +39,8 @@
 #include <sparkit/data/gmres.hpp>
 #include <sparkit/data/cgs.hpp>
 #include <sparkit/data/minres.hpp>
+#include <sparkit/data/conditioning.hpp>
+#include <sparkit/data/lanczos.hpp>
 #include <sparkit/data/jacobi.hpp>
 #include <sparkit/data/matgen.hpp>
 #include <sparkit/data/sparse_blas.hpp>
@@ -175,6 +179,37 @@ namespace {
       std::copy(y.begin(), y.end(), out);
     }
   };
+
+  // The scalars of Lanczos_result<T> (lanczos.hpp:39-47).
+  struct LanczosOut {
+    i64 count, computed_restarts, converged_count, residual_count, restart_residuals_count;
+    int converged;
+  };
+
+  template <typename T>
+  void lanczos_run(Handle<T> const* A, i64 nev, i64 m, double tol, i64 max_restarts, int target,
+                   int collect, T* eigenvalues, T* eigenvectors, T* residual_norms,
+                   double* restart_residuals, LanczosOut* out) {
+    sd::Lanczos_config<T> cfg{nev, m, static_cast<T>(tol), max_restarts,
+                              static_cast<sd::Eigen_target>(target), collect != 0};
+    auto r = sd::lanczos<T>(A->nrow(), cfg, Op<T>{A});
+    out->count = static_cast<i64>(r.eigenvalues.size());
+    out->computed_restarts = r.computed_restarts;
+    out->converged_count = r.converged_count;
+    out->residual_count = static_cast<i64>(r.residual_norms.size());
+    out->restart_residuals_count = static_cast<i64>(r.restart_residuals.size());
+    out->converged = r.converged ? 1 : 0;
+    for (std::size_t k = 0; k < r.eigenvalues.size(); ++k) {
+      eigenvalues[k] = r.eigenvalues[k];
+      if (eigenvectors)
+        std::copy(r.eigenvectors[k].begin(), r.eigenvectors[k].end(),
+                  eigenvectors + k * A->nrow());
+    }
+    for (std::size_t k = 0; k < r.residual_norms.size(); ++k) residual_norms[k] = r.residual_norms[k];
+    if (restart_residuals)
+      for (std::size_t k = 0; k < r.restart_residuals.size(); ++k)
+        restart_residuals[k] = static_cast<double>(r.restart_residuals[k]);
+  }
 
   template <typename T>
   int cg(Handle<T> const* A, i64 n, T const* b, T* x, double tol,
@@ -446,6 +481,23 @@ namespace {
         return sd::minres(bv.begin(), bv.end(), xv.begin(), xv.end(), cfg,     \
                           Op<T>{A}, std::cref(L), std::cref(R));               \
       });                                                                      \
+  }                                                                            \
+  REF_API void ref_lanczos_##S(void* h, i64 nev, i64 m, double tol, i64 maxr,  \
+                              int target, int collect, T* ev, T* evec,         \
+                              T* res, double* rr, LanczosOut* out) {           \
+    lanczos_run<T>(static_cast<Handle<T>*>(h), nev, m, tol, maxr, target,      \
+                   collect, ev, evec, res, rr, out);                           \
+  }                                                                            \
+  REF_API void ref_eigenvalue_bounds_##S(void* h, i64 num_iter, T* out2) {     \
+    auto* A = static_cast<Handle<T>*>(h);                                      \
+    auto p = sd::estimate_eigenvalue_bounds<T>(A->nrow(), Op<T>{A}, num_iter); \
+    out2[0] = p.first;                                                         \
+    out2[1] = p.second;                                                        \
+  }                                                                            \
+  REF_API double ref_spectral_radius_##S(void* h, i64 num_iter) {              \
+    auto* A = static_cast<Handle<T>*>(h);                                      \
+    return static_cast<double>(                                                \
+      sd::estimate_spectral_radius<T>(A->nrow(), Op<T>{A}, num_iter));         \
   }                                                                            \
   REF_API void* ref_poisson_2d_##S(i64 nx, i64 ny, double shift) {             \
     return wrap_csr<T>(sd::poisson_2d<T>(nx, ny, static_cast<T>(shift)));      \

@@ -3,9 +3,10 @@
  *
  * TEST INFRASTRUCTURE ONLY.  This is a plain-C restatement of the sparkit
  * reference's sequential algorithms (SpMV over CSR / ELLPACK / jagged
- * diagonal / BSR, Jacobi and Chebyshev preconditioners, CG, BiCGSTAB and
- * FGMRES), used by the tests, the smoke check and the CPU-baseline leg of
- * the benchmark to check the CUDA library.  The product never links it.
+ * diagonal / BSR, Jacobi and Chebyshev preconditioners, CG, BiCGSTAB,
+ * FGMRES, GMRES, CGS, MINRES, and the Lanczos eigenvalue estimates), used
+ * by the tests, the smoke check and the CPU-baseline leg of the benchmark
+ * to check the CUDA library.  The product never links it.
  *
  * Parity pinning: tests/test_oracle.py checks every routine here against
  * the known-answer vectors of the reference's own Catch2 tests
@@ -120,7 +121,34 @@ typedef struct {
                    const sko_krylov_config*, sko_summary*, double*);          \
   void sko_minres_##S(const sko_operator*, const sko_precond*,                \
                       const sko_precond*, const T*, T*,                       \
-                      const sko_krylov_config*, sko_summary*, double*);
+                      const sko_krylov_config*, sko_summary*, double*);       \
+  void sko_tridiagonal_eigen_##S(int64_t, T*, T*, T, int64_t, T*);            \
+  void sko_lanczos_##S(const sko_operator*, const sko_lanczos_config*, T*,    \
+                       T*, T*, double*, sko_lanczos_result*);                 \
+  T sko_spectral_radius_##S(const sko_operator*, int64_t);                    \
+  void sko_eigenvalue_bounds_##S(const sko_operator*, int64_t, T*);
+
+/* Lanczos_config<T> (lanczos.hpp:25-33); target in Eigen_target order
+ * (eigen_target.hpp:13-20: largest_magnitude, smallest_magnitude,
+ * largest_algebraic, smallest_algebraic, largest_real, smallest_real). */
+typedef struct {
+  int64_t num_eigenvalues;
+  int64_t krylov_dimension;
+  double tolerance;
+  int64_t max_restarts;
+  int32_t target;
+  int32_t collect_residuals;
+} sko_lanczos_config;
+
+/* The scalars of Lanczos_result<T> (lanczos.hpp:39-47). */
+typedef struct {
+  int64_t count;                   /* eigenvalues returned */
+  int64_t computed_restarts;
+  int64_t converged_count;
+  int64_t residual_count;          /* residual_norms written */
+  int64_t restart_residuals_count; /* restart_residuals written */
+  int32_t converged;
+} sko_lanczos_result;
 
 /* Summation order of the solvers' dot products: 0 = the reference's
  * sequential order (default), 1 = 256-element chunks added in order. */

@@ -59,6 +59,31 @@ def spmv_matrices():
     return mats
 
 
+LANCZOS_TARGETS = ("largest_magnitude", "smallest_magnitude", "largest_algebraic", "smallest_algebraic")
+
+
+def eigen_matrices():
+    """Symmetric matrices for the eigenvalue estimates: definite, an
+    indefinite shifted Laplacian, n below the Krylov dimension, and 2 I,
+    whose first Lanczos residual is exactly zero (the reference rejects
+    shapes below 2 x 2, Shape.cpp:8-10)."""
+    from sparkit_b200.formats import Compressed_row_matrix as C
+    L = matgen.laplacian_2d_dirichlet(10)
+    n = L.shape()[0]
+    lens = np.diff(L.row_ptr())
+    rows = np.repeat(np.arange(n), lens)
+    vals = L.values() - 3.0 * (rows == L.col_ind())  # spectrum in (-3, 5)
+    return {
+        "lap2d_24": matgen.laplacian_2d_dirichlet(24),
+        "grid16": matgen.poisson_2d(4, 4, 5.0),
+        "tridiag50": matgen.tridiagonal_matrix(50, -1.0, 4.0, -1.0),
+        "lap3d_6": matgen.laplacian_3d_dirichlet(6),
+        "indef_100": C((n, n), L.row_ptr(), L.col_ind(), vals),
+        "tridiag5": matgen.tridiagonal_matrix(5, -1.0, 2.0, -1.0),
+        "twoI_4x4": C((4, 4), np.arange(5), np.arange(4), np.full(4, 2.0)),
+    }
+
+
 def main():
     R = Reference()
     out = {}
@@ -97,6 +122,23 @@ def main():
             B = R.to_block_sparse_row(A, br, bc)
             for f in ("row_ptr", "col_ind", "values"):
                 out[f"{tag}/bsr{br}x{bc}/{f}"] = getattr(B, f)()
+    # Lanczos and the eigenvalue estimates (conditioning.hpp:112, :132;
+    # lanczos.hpp:495) on symmetric matrices, FP64 and FP32; "twoI_4x4" (2 I)
+    # takes the zero-beta random restart (lanczos.hpp:184-186)
+    for name, A in eigen_matrices().items():
+        for dt in (np.float64, np.float32):
+            Ad = A.astype(dt)
+            tag = f"eigen/{name}/{np.dtype(dt).name}"
+            out[f"{tag}/bounds"] = np.array(R.eigenvalue_bounds(Ad), dtype=dt)
+            out[f"{tag}/radius"] = np.array(R.spectral_radius(Ad), dtype=dt)
+            for target in LANCZOS_TARGETS:
+                r = R.lanczos(Ad, nev=3, m=12, tol=1e-8, max_restarts=5, target=target, collect=True,
+                              vectors=True)
+                key = f"{tag}/lanczos/{target}"
+                for k in ("eigenvalues", "residual_norms", "restart_residuals", "eigenvectors"):
+                    out[f"{key}/{k}"] = r[k]
+                out[f"{key}/scalars"] = np.array([r["computed_restarts"], r["converged_count"],
+                                                  int(r["converged"])])
     # preconditioners
     P = matgen.poisson_2d(8, 8, 0.5)
     out["jacobi/poisson8/inv_d"] = R.jacobi(P)

@@ -187,6 +187,51 @@ def test_cgs_minres_match_reference(oracle, reference):
         assert s["computed_iterations"] == (8 if fn == "cgs" else 7)
 
 
+@pytest.mark.parametrize("dtype", ["float64", "float32"])
+def test_eigen_estimates_match_reference_fixtures(oracle, golden, dtype):
+    """lanczos / estimate_eigenvalue_bounds / estimate_spectral_radius
+    (lanczos.hpp:495, conditioning.hpp:112, :132): the oracle reproduces the
+    reference's eigenvalues, residual norms, restart residuals, Ritz vectors
+    and counts bit for bit, for every target, FP64 and FP32 (the start
+    vectors come from the reference's own mt19937 sequence)."""
+    from tests.golden.make_golden import LANCZOS_TARGETS, eigen_matrices
+    dt = np.dtype(dtype)
+    for name, A in eigen_matrices().items():
+        Ad = A.astype(dt)
+        tag = f"eigen/{name}/{dtype}"
+        assert np.array_equal(np.array(oracle.eigenvalue_bounds(Ad), dtype=dt), golden[f"{tag}/bounds"]), name
+        assert np.array_equal(np.array(oracle.spectral_radius(Ad), dtype=dt), golden[f"{tag}/radius"]), name
+        for target in LANCZOS_TARGETS:
+            r = oracle.lanczos(Ad, nev=3, m=12, tol=1e-8, max_restarts=5, target=target, collect=True,
+                               vectors=True)
+            key = f"{tag}/lanczos/{target}"
+            for k in ("eigenvalues", "residual_norms", "restart_residuals", "eigenvectors"):
+                assert np.array_equal(r[k], golden[f"{key}/{k}"]), (name, target, k)
+            assert [r["computed_restarts"], r["converged_count"], int(r["converged"])] == \
+                golden[f"{key}/scalars"].tolist(), (name, target)
+
+
+def test_eigen_estimates_match_reference(oracle, reference):
+    """Beyond the fixtures, against the compiled reference: other Krylov
+    dimensions and restart budgets (0 restarts: no convergence check), the
+    remaining targets, and the bounds of the 3D Laplacian against the
+    exact extreme eigenvalues 6 -+ 6 cos(pi / 9)."""
+    A = matgen.laplacian_3d_dirichlet(8)
+    for kw in (dict(nev=1, m=31, tol=1e-10, max_restarts=10, target="largest_real"),
+               dict(nev=2, m=8, tol=1e-12, max_restarts=0, target="smallest_real"),
+               dict(nev=4, m=20, tol=1e-6, max_restarts=3, target="smallest_magnitude")):
+        r = oracle.lanczos(A, collect=True, vectors=True, **kw)
+        rr = reference.lanczos(A, collect=True, vectors=True, **kw)
+        for k in ("eigenvalues", "residual_norms", "restart_residuals", "eigenvectors"):
+            assert np.array_equal(r[k], rr[k]), (kw, k)
+        assert (r["computed_restarts"], r["converged_count"], r["converged"]) == \
+            (rr["computed_restarts"], rr["converged_count"], rr["converged"])
+    lo, hi = oracle.eigenvalue_bounds(A)
+    assert (lo, hi) == reference.eigenvalue_bounds(A)
+    exact = 6 * np.cos(np.pi / 9)
+    assert abs(hi - (6 + exact)) < 1e-8 and abs(lo - (6 - exact)) < 1e-6
+
+
 def test_generators_match_reference(reference):
     pairs = [(matgen.poisson_2d(4, 4, 5.0), reference.poisson_2d(4, 4, 5.0)),
              (matgen.poisson_2d(5, 3), reference.poisson_2d(5, 3)),
