@@ -57,6 +57,9 @@ def parse():
     p.add_argument("--profile-mixed", action="store_true",
                    help="one mixed solve with 100 persistent FP32 inner iterations on the 128^3 GRF problem, for ncu")
     p.add_argument("--no-convert", action="store_true")
+    p.add_argument("--no-eigen", action="store_true")
+    p.add_argument("--profile-eigen", action="store_true",
+                   help="one sk_eigenvalue_bounds on the grid^3 Laplacian (for an ncu launch list)")
     p.add_argument("--profile-convert", action="store_true",
                    help="each device format conversion once (for an ncu launch list)")
     p.add_argument("--profile-formats", action="store_true",
@@ -358,6 +361,54 @@ def profile_convert(grid):
              "bsr": lambda: gpu.to_block_sparse_row(Cd, *blk)}[fmt]()
         h.close()
         Cd.close()
+    torch.cuda.synchronize()
+    return 0
+
+
+def eigen_runs(grid):
+    """estimate_eigenvalue_bounds (conditioning.hpp:132, two Lanczos passes
+    of Krylov dimension 31, up to 10 restarts each) through
+    sk_eigenvalue_bounds on the grid^3 and 48^3 Dirichlet Laplacians: wall
+    time of the synchronous call (its restart decisions read two scalars
+    per Lanczos step back to the host), median of 3 after one warm-up;
+    beside it the compiled reference's own estimate on the 48^3 matrix (one
+    core)."""
+    from oracle.binding import Reference, reference_available
+    from sparkit_b200 import gpu, matgen
+    out = {}
+    for g in (grid, 48):
+        A = matgen.laplacian_3d_dirichlet(g)
+        Ad = gpu.Device_matrix(A)
+        gpu.estimate_eigenvalue_bounds(Ad)
+        ts = []
+        for _ in range(3):
+            t0 = time.perf_counter()
+            lo, hi = gpu.estimate_eigenvalue_bounds(Ad)
+            ts.append(time.perf_counter() - t0)
+        c = 6 * np.cos(np.pi / (g + 1))
+        row = {"n": A.shape()[0], "ms": float(np.median(ts)) * 1e3, "lambda_min": lo, "lambda_max": hi,
+               "exact": [6 - c, 6 + c]}
+        if g == 48 and reference_available():
+            R = Reference()
+            t0 = time.perf_counter()
+            rb = R.eigenvalue_bounds(A)
+            rs = time.perf_counter() - t0
+            row["cpu_reference"] = {"s": rs, "cores": 1, "kind": "reference", "lambda_min": float(rb[0]),
+                                    "lambda_max": float(rb[1])}
+            row["speedup_vs_reference"] = rs / (row["ms"] * 1e-3)
+        out[f"lap3d_{g}"] = row
+        Ad.close()
+    return out
+
+
+def profile_eigen(grid):
+    """One sk_eigenvalue_bounds on the grid^3 Laplacian, for an ncu launch list."""
+    import torch
+
+    from sparkit_b200 import gpu, matgen
+    torch.cuda.set_device(0)
+    Ad = gpu.Device_matrix(matgen.laplacian_3d_dirichlet(grid))
+    gpu.estimate_eigenvalue_bounds(Ad)
     torch.cuda.synchronize()
     return 0
 
@@ -730,6 +781,8 @@ def main():
         return profile_formats(args.grid)
     if args.profile_convert:
         return profile_convert(args.grid)
+    if args.profile_eigen:
+        return profile_eigen(args.grid)
     if args.profile_solvers:
         return profile_solvers(args.grid)
     if args.profile_learned:
@@ -843,6 +896,8 @@ def main():
         extra["sweep"] = sweep(stream, args.grid)
     if rank == 0 and world == 1 and not args.no_convert:
         extra["convert"] = convert_runs(args.grid)
+    if rank == 0 and world == 1 and not args.no_eigen:
+        extra["eigen_bounds"] = eigen_runs(args.grid)
     if rank == 0 and world == 1 and not args.no_solvers:
         extra["solvers"] = solver_runs(args.grid)
         extra["solvers"]["c5_batched"] = batched_runs()

@@ -211,6 +211,74 @@ SK_API sk_status sk_jacobi_create(sk_precond* out, sk_matrix A);
 SK_API sk_status sk_chebyshev_create(sk_precond* out, sk_matrix A, double lambda_min,
                               double lambda_max, int64_t degree);
 
+/* ---------------------------------------------------------------- */
+/* Eigenvalue estimates (symmetric matrices)                         */
+/* ---------------------------------------------------------------- */
+
+/* Eigen_target (sparkit/data/eigen_target.hpp:13-20). */
+typedef enum {
+  SK_LARGEST_MAGNITUDE = 0,
+  SK_SMALLEST_MAGNITUDE = 1,
+  SK_LARGEST_ALGEBRAIC = 2,
+  SK_SMALLEST_ALGEBRAIC = 3,
+  SK_LARGEST_REAL = 4,
+  SK_SMALLEST_REAL = 5
+} sk_eigen_target;
+
+/* Lanczos_config<T> (sparkit/data/lanczos.hpp:25-33); target is an
+ * sk_eigen_target. */
+typedef struct {
+  int64_t num_eigenvalues;
+  int64_t krylov_dimension;
+  double tolerance;
+  int64_t max_restarts;
+  int32_t target;
+  int32_t collect_residuals;
+} sk_lanczos_config;
+
+/* The scalars of Lanczos_result<T> (lanczos.hpp:39-47): count eigenvalues
+ * (min(num_eigenvalues, krylov_dimension, n)), residual_count residual
+ * norms of the last convergence test (0 when max_restarts is 0),
+ * restart_residuals_count entries of restart_residuals (collect only). */
+typedef struct {
+  int64_t count;
+  int64_t computed_restarts;
+  int64_t converged_count;
+  int64_t residual_count;
+  int64_t restart_residuals_count;
+  int32_t converged;
+  int32_t status;
+} sk_lanczos_summary;
+
+/* lanczos(n, cfg, op) with op = multiply(A) (lanczos.hpp:495-503), A square
+ * and symmetric, any format.  Host outputs: eigenvalues[count],
+ * residual_norms[count] and restart_residuals[max_restarts] (each may be
+ * NULL).  eigenvectors_dev (may be NULL): count device vectors of nrow
+ * entries of A's dtype, one after another.  The n-length work runs on the
+ * device; the tridiagonal eigensolve and restart arithmetic on the host.
+ * The reorthogonalisation is the reference's modified Gram-Schmidt. */
+SK_API sk_status sk_lanczos(sk_matrix A, const sk_lanczos_config* cfg, double* eigenvalues,
+                     double* residual_norms, double* restart_residuals,
+                     void* eigenvectors_dev, sk_lanczos_summary* out, sk_stream stream);
+
+/* estimate_spectral_radius(n, multiply(A), num_iter) (conditioning.hpp:112-126;
+ * the reference's default num_iter is 20).  This and sk_eigenvalue_bounds
+ * reorthogonalise by block Gram-Schmidt (the same to rounding for the one
+ * extreme eigenvalue they estimate). */
+SK_API sk_status sk_spectral_radius(sk_matrix A, int64_t num_iter, double* rho);
+
+/* estimate_eigenvalue_bounds(n, multiply(A), num_iter)
+ * (conditioning.hpp:132-168; default num_iter 30): two Lanczos passes,
+ * largest and smallest algebraic. */
+SK_API sk_status sk_eigenvalue_bounds(sk_matrix A, int64_t num_iter, double* lambda_min,
+                               double* lambda_max);
+
+/* chebyshev_preconditioner(A, lambda_min, lambda_max, degree) with the
+ * bounds from sk_eigenvalue_bounds(A, num_iter); bounds (may be NULL)
+ * receives them. */
+SK_API sk_status sk_chebyshev_create_auto(sk_precond* out, sk_matrix A, int64_t degree,
+                                   int64_t num_iter, double bounds[2]);
+
 /* z = M^{-1} r on device vectors: jacobi_apply (jacobi.hpp:44-51) or
  * chebyshev_preconditioner_apply (chebyshev_preconditioner.hpp:98-169).
  * A NULL precond is the identity (a copy). */

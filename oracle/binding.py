@@ -131,7 +131,8 @@ class Oracle:
         return op, keep
 
     def set_dot_order(self, mode):
-        """0: the reference's sequential dot products; 1: chunked order."""
+        """0: the reference's sequential dot products; 1: chunked order;
+        2: reversed order."""
         self.L.sko_set_dot_order(int(mode))
 
     def spmv(self, A, x):

@@ -12,7 +12,8 @@
 
 #define SKO_PI 3.141592653589793238462643383279502884
 
-/* 0: reference order (sequential); 1: chunked order (sensitivity studies). */
+/* 0: reference order (sequential); 1: chunked order; 2: reversed order
+ * (1 and 2: sensitivity studies). */
 static int sko_dot_order = 0;
 void sko_set_dot_order(int mode) { sko_dot_order = mode; }
 

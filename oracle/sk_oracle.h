@@ -151,7 +151,8 @@ typedef struct {
 } sko_lanczos_result;
 
 /* Summation order of the solvers' dot products: 0 = the reference's
- * sequential order (default), 1 = 256-element chunks added in order. */
+ * sequential order (default), 1 = 256-element chunks added in order,
+ * 2 = sequential from the last element (sensitivity studies). */
 void sko_set_dot_order(int mode);
 
 SKO_DECLARE(double, f64)

@@ -237,6 +237,11 @@ static void SKO_FN(sko_apply_prec_)(const sko_precond* M, const sko_operator* A,
  * to measure how sensitive a solver's iteration count is to the summation
  * order (the GPU sums in a fixed tree). */
 static SKO_T SKO_FN(sko_dot_)(const SKO_T* a, const SKO_T* b, int64_t n) {
+  if (sko_dot_order == 2) {
+    SKO_T s = 0;
+    for (int64_t i = n; i > 0; --i) s += a[i - 1] * b[i - 1];
+    return s;
+  }
   if (sko_dot_order == 1) {
     SKO_T total = 0;
     for (int64_t c = 0; c < n; c += 256) {

@@ -86,6 +86,17 @@ class Summary(ctypes.Structure):
                 ("converged", c_i32), ("status", c_i32), ("history_length", c_i64)]
 
 
+class LanczosConfig(ctypes.Structure):
+    _fields_ = [("num_eigenvalues", c_i64), ("krylov_dimension", c_i64), ("tolerance", c_dbl),
+                ("max_restarts", c_i64), ("target", c_i32), ("collect_residuals", c_i32)]
+
+
+class LanczosSummary(ctypes.Structure):
+    _fields_ = [("count", c_i64), ("computed_restarts", c_i64), ("converged_count", c_i64),
+                ("residual_count", c_i64), ("restart_residuals_count", c_i64), ("converged", c_i32),
+                ("status", c_i32)]
+
+
 # (name, argtypes) of every exported function, in header order.
 SIGNATURES = [
     ("sk_version", []),
@@ -121,6 +132,11 @@ SIGNATURES = [
     ("sk_xpay", [ctypes.c_int, c_i64, c_vp, c_dbl, c_vp, c_vp]),
     ("sk_jacobi_create", [ctypes.POINTER(c_vp), c_vp]),
     ("sk_chebyshev_create", [ctypes.POINTER(c_vp), c_vp, c_dbl, c_dbl, c_i64]),
+    ("sk_lanczos", [c_vp, ctypes.POINTER(LanczosConfig), c_vp, c_vp, c_vp, c_vp, ctypes.POINTER(LanczosSummary),
+                    c_vp]),
+    ("sk_spectral_radius", [c_vp, c_i64, ctypes.POINTER(c_dbl)]),
+    ("sk_eigenvalue_bounds", [c_vp, c_i64, ctypes.POINTER(c_dbl), ctypes.POINTER(c_dbl)]),
+    ("sk_chebyshev_create_auto", [ctypes.POINTER(c_vp), c_vp, c_i64, c_i64, c_vp]),
     ("sk_precond_apply", [c_vp, c_i64, c_vp, c_vp, c_vp]),
     ("sk_precond_values", [c_vp, c_vp, c_i64, P_i64]),
     ("sk_precond_destroy", [c_vp]),

@@ -277,6 +277,65 @@ class chebyshev_preconditioner(_Precond):
         self.lambda_min, self.lambda_max, self.degree = lambda_min, lambda_max, degree
 
 
+class chebyshev_preconditioner_auto(chebyshev_preconditioner):
+    """chebyshev_preconditioner(A, lambda_min, lambda_max, degree) with the
+    bounds from estimate_eigenvalue_bounds(A, num_iter) (conditioning.hpp:132),
+    computed on the device (sk_chebyshev_create_auto)."""
+
+    def __init__(self, Ad, degree, num_iter=30):
+        h = ctypes.c_void_p()
+        b = np.zeros(2)
+        check(lib().sk_chebyshev_create_auto(ctypes.byref(h), Ad.handle, int(degree), int(num_iter), _ptr(b)))
+        _Precond.__init__(self, h, Ad, Ad.shape()[0])
+        self.lambda_min, self.lambda_max, self.degree = float(b[0]), float(b[1]), degree
+
+
+# Eigen_target (eigen_target.hpp:13-20)
+EIGEN_TARGETS = ("largest_magnitude", "smallest_magnitude", "largest_algebraic", "smallest_algebraic",
+                 "largest_real", "smallest_real")
+
+
+def lanczos(Ad, nev=1, m=20, tol=1e-10, max_restarts=10, target="largest_algebraic", collect=False,
+            vectors=False):
+    """lanczos(n, Lanczos_config, multiply(A)) (lanczos.hpp:495-503) on the
+    device: a dict of the Lanczos_result fields (eigenvectors as a device
+    tensor of shape (count, n) when vectors=True)."""
+    import torch
+    n = Ad.shape()[0]
+    cfg = _lib.LanczosConfig(int(nev), int(m), float(tol), int(max_restarts), EIGEN_TARGETS.index(target),
+                             int(collect))
+    ev = np.zeros(max(int(nev), 1))
+    res = np.zeros(max(int(nev), 1))
+    rr = np.zeros(int(max_restarts) + 2)
+    vecs = torch.zeros((max(int(nev), 1), n), dtype=torch.float64 if Ad.dtype == np.float64 else torch.float32,
+                       device="cuda") if vectors else None
+    out = _lib.LanczosSummary()
+    st = _stream_of(vecs) if vecs is not None else None
+    check(lib().sk_lanczos(Ad.handle, ctypes.byref(cfg), _ptr(ev), _ptr(res), _ptr(rr),
+                           _ptr(vecs) if vecs is not None else None, ctypes.byref(out), st))
+    d = dict(eigenvalues=ev[: out.count].astype(Ad.dtype), residual_norms=res[: out.residual_count].astype(Ad.dtype),
+             restart_residuals=rr[: out.restart_residuals_count], computed_restarts=out.computed_restarts,
+             converged_count=out.converged_count, converged=bool(out.converged))
+    if vecs is not None:
+        d["eigenvectors"] = vecs[: out.count]
+    return d
+
+
+def estimate_spectral_radius(Ad, num_iter=20):
+    """estimate_spectral_radius(n, multiply(A), num_iter) (conditioning.hpp:112)."""
+    v = ctypes.c_double()
+    check(lib().sk_spectral_radius(Ad.handle, int(num_iter), ctypes.byref(v)))
+    return v.value
+
+
+def estimate_eigenvalue_bounds(Ad, num_iter=30):
+    """estimate_eigenvalue_bounds(n, multiply(A), num_iter)
+    (conditioning.hpp:132): (lambda_min, lambda_max)."""
+    lo, hi = ctypes.c_double(), ctypes.c_double()
+    check(lib().sk_eigenvalue_bounds(Ad.handle, int(num_iter), ctypes.byref(lo), ctypes.byref(hi)))
+    return lo.value, hi.value
+
+
 def chebyshev_apply_noalloc(Ad, lambda_min, lambda_max, degree, r, z, stream=None):
     """z = p(A) r like chebyshev_preconditioner(Ad, ...).apply(r, z), for
     callers that cannot allocate device memory at apply time: no handle is
