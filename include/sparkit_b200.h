@@ -145,6 +145,32 @@ SK_API sk_status sk_jad_export(sk_matrix A, int64_t* perm, int64_t* jdiag,
                         int64_t* col_ind, void* values);
 SK_API sk_status sk_bsr_export(sk_matrix A, int64_t* row_ptr, int64_t* col_ind, void* values);
 
+/* read_matrix_market<T>(path) followed by to_compressed_row
+ * (sparkit/data/matrix_market.hpp:45-115, matrix_market.cpp:28-87,
+ * Coordinate_matrix.hpp:36-41) into a device CSR handle of dtype.  As the
+ * reference: a case-insensitive banner; coordinate format only; real,
+ * integer and pattern fields (pattern entries are 1); comment and empty
+ * lines skipped before the size line; exactly nnz entry lines with 1-based
+ * indices; a symmetric file's off-diagonal entries mirrored (skew-symmetric
+ * and hermitian files read as stored); the last of duplicate entries kept;
+ * a side of 1 or less rejected ("invalid matrix shape").  Unlike the
+ * reference, a malformed or out-of-range entry line, or fewer than nnz of
+ * them, is an error.  The entry lines are parsed by `threads` host threads
+ * (0: all cores); mirroring, sorting, de-duplication and the row pointers
+ * run on the device.  Errors: SK_INVALID_ARG with the reason in
+ * sk_last_error(). */
+SK_API sk_status sk_matrix_market_read(sk_matrix* out, const char* path, sk_dtype dtype,
+                                int32_t threads);
+SK_API sk_status sk_matrix_market_read_buffer(sk_matrix* out, const char* text, int64_t length,
+                                       sk_dtype dtype, int32_t threads);
+
+/* write_matrix_market(path, A) (matrix_market.hpp:119-150) of a CSR handle:
+ * the banner "%%MatrixMarket matrix coordinate real general", the size line
+ * and one "row col value" line per entry.  precision 0 prints values as the
+ * reference's ostream does (6 significant digits); 17 round-trips FP64. */
+SK_API sk_status sk_matrix_market_write(sk_matrix A, const char* path, int32_t precision,
+                                 int32_t threads);
+
 SK_API sk_status sk_matrix_destroy(sk_matrix A);
 
 /* info[0..7] = format, dtype, nrow, ncol, nnz (stored entries), width

@@ -120,6 +120,9 @@ SIGNATURES = [
     ("sk_ell_export", [c_vp, c_vp, c_vp]),
     ("sk_jad_export", [c_vp, c_vp, c_vp, c_vp, c_vp]),
     ("sk_bsr_export", [c_vp, c_vp, c_vp, c_vp]),
+    ("sk_matrix_market_read", [ctypes.POINTER(c_vp), ctypes.c_char_p, ctypes.c_int, c_i32]),
+    ("sk_matrix_market_read_buffer", [ctypes.POINTER(c_vp), ctypes.c_char_p, c_i64, ctypes.c_int, c_i32]),
+    ("sk_matrix_market_write", [c_vp, ctypes.c_char_p, c_i32, c_i32]),
     ("sk_matrix_destroy", [c_vp]),
     ("sk_matrix_info", [c_vp, P_i64]),
     ("sk_matrix_add_f32_values", [c_vp]),

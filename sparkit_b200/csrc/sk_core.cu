@@ -357,6 +357,23 @@ sk_status build_bsr_sell(sk_matrix A, const int64_t* rp, cudaStream_t st_) {
   return SK_OK;
 }
 
+// The product's tables of a CSR handle whose arrays are on the device:
+// the row-block partition and its tiles, and the SELL-32 copy, all from the
+// host copy of the row pointers.
+sk_status csr_finish(sk_matrix A, const int64_t* row_ptr, cudaStream_t st_) {
+  sk_status st;
+  std::vector<int> part;
+  std::vector<unsigned char> lanes;
+  csr_partition(row_ptr, A->nrow, part, lanes);
+  A->csr.nparts = static_cast<int>(part.size()) - 1;
+  std::vector<int2> tiles(part.size());
+  for (size_t b = 0; b < part.size(); ++b)
+    tiles[b] = make_int2(part[b], static_cast<int>(row_ptr[part[b]]));
+  if ((st = upload_vector(A, tiles, &A->csr.tiles, st_)) != SK_OK) return st;
+  if ((st = upload_vector(A, lanes, &A->csr.lanes, st_)) != SK_OK) return st;
+  return build_sell(A, row_ptr, st_);
+}
+
 }  // namespace sk
 
 using namespace sk;
@@ -449,16 +466,7 @@ sk_status sk_csr_create(sk_matrix* out, int64_t nrow, int64_t ncol, const int64_
   if ((st = upload_indices(col_ind, nnz, A->csr.col_ind, 0, ncol, false, st_, "col_ind")) != SK_OK)
     return st;
   if (nnz) SK_CUDA(cudaMemcpyAsync(va, values, nnz * V, cudaMemcpyHostToDevice, st_));
-  std::vector<int> part;
-  std::vector<unsigned char> lanes;
-  csr_partition(row_ptr, nrow, part, lanes);
-  A->csr.nparts = static_cast<int>(part.size()) - 1;
-  std::vector<int2> tiles(part.size());
-  for (size_t b = 0; b < part.size(); ++b)
-    tiles[b] = make_int2(part[b], static_cast<int>(row_ptr[part[b]]));
-  if ((st = upload_vector(A, tiles, &A->csr.tiles, st_)) != SK_OK) return st;
-  if ((st = upload_vector(A, lanes, &A->csr.lanes, st_)) != SK_OK) return st;
-  if ((st = build_sell(A, row_ptr, st_)) != SK_OK) return st;
+  if ((st = csr_finish(A, row_ptr, st_)) != SK_OK) return st;
   SK_CUDA(cudaStreamSynchronize(st_));
   guard.ok = true;
   return SK_OK;

@@ -264,6 +264,10 @@ sk_status upload_vector(sk_matrix A, const std::vector<V>& h, V** dev, cudaStrea
   return SK_OK;
 }
 
+// The product's tables of a CSR handle whose row_ptr / col_ind / vals are
+// already on the device, from the host copy of its row pointers.
+sk_status csr_finish(sk_matrix A, const int64_t* row_ptr, cudaStream_t st);
+
 // BSR block-row partition of the product kernel (host row pointers) and
 // the sliced copy of 2x2 / 3x3 handles.
 void bsr_partition(const int64_t* rp, i64 nbr, i64 br, i64 bsz, std::vector<int>& part);

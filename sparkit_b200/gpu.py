@@ -205,6 +205,28 @@ def to_block_sparse_row(Ad, block_rows, block_cols):
                     block=(int(block_rows), int(block_cols)))
 
 
+def read_matrix_market(source, dtype=np.float64, threads=0):
+    """read_matrix_market<T>(path) followed by to_compressed_row
+    (matrix_market.hpp:45-115) into a device CSR handle.  `source` is a path,
+    or bytes holding the file's text.  Errors raise SkError with the reason."""
+    dt = np.dtype(dtype)
+    h = ctypes.c_void_p()
+    if isinstance(source, (bytes, bytearray)):
+        buf = bytes(source)
+        check(lib().sk_matrix_market_read_buffer(ctypes.byref(h), buf, len(buf), _dtype_code(dt), int(threads)))
+    else:
+        check(lib().sk_matrix_market_read(ctypes.byref(h), str(source).encode(), _dtype_code(dt), int(threads)))
+    arr = (ctypes.c_int64 * 8)()
+    check(lib().sk_matrix_info(h, arr))
+    return Device_matrix._wrap(h, dt, (arr[2], arr[3]))
+
+
+def write_matrix_market(Ad, path, precision=0, threads=0):
+    """write_matrix_market(path, A) (matrix_market.hpp:119-150) of a CSR
+    handle; precision 0 prints 6 significant digits as the reference does."""
+    check(lib().sk_matrix_market_write(Ad.handle, str(path).encode(), int(precision), int(threads)))
+
+
 def multiply(Ad, x):
     """multiply(A, span<T const>) -> vector<T>, host in / host out."""
     x = np.ascontiguousarray(x, dtype=Ad.dtype)
