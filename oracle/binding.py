@@ -82,6 +82,15 @@ EIGEN_TARGETS = ("largest_magnitude", "smallest_magnitude", "largest_algebraic",
                  "largest_real", "smallest_real")
 
 
+class MmCsr(ctypes.Structure):
+    _fields_ = [("nrow", c_i64), ("ncol", c_i64), ("nnz", c_i64), ("row_ptr", c_vp), ("col_ind", c_vp),
+                ("values", c_vp), ("err", ctypes.c_char * 256)]
+
+
+class MatrixMarketError(ValueError):
+    """The reason a Matrix Market text was rejected."""
+
+
 def _pad_to_blocks(x, bc):
     """x followed by zeros up to a whole number of bc-wide block columns."""
     m = -(-x.size // int(bc)) * int(bc)
@@ -241,6 +250,44 @@ class Oracle:
     def minres(self, A, b, x0, tol, max_it, left=None, right=None, collect=False, prec_matrix=None):
         return self._solve("minres", A, [left, right], b, x0, KrylovCfg(tol, max_it, int(collect)), max_it + 2,
                            prec_matrix)
+
+    # -------------------------------------------------------------- #
+    # Matrix Market (sk_oracle_mm.c)                                   #
+    # -------------------------------------------------------------- #
+
+    def mm_read(self, text, dtype=np.float64):
+        """read_matrix_market<T> + to_compressed_row on the text (bytes)."""
+        dt = np.dtype(dtype)
+        text = bytes(text)
+        m = MmCsr()
+        rc = getattr(self.L, f"sko_mm_read_{_sfx(dt)}")(text, c_i64(len(text)), ctypes.byref(m))
+        if rc:
+            raise MatrixMarketError(m.err.decode())
+        try:
+            rp = np.ctypeslib.as_array(ctypes.cast(m.row_ptr, ctypes.POINTER(c_i64)), (m.nrow + 1,)).copy()
+            ci = (np.ctypeslib.as_array(ctypes.cast(m.col_ind, ctypes.POINTER(c_i64)), (m.nnz,)).copy()
+                  if m.nnz else np.zeros(0, np.int64))
+            ct = ctypes.c_double if dt == np.float64 else ctypes.c_float
+            va = (np.ctypeslib.as_array(ctypes.cast(m.values, ctypes.POINTER(ct)), (m.nnz,)).copy()
+                  if m.nnz else np.zeros(0, dt))
+        finally:
+            self.L.sko_mm_free(ctypes.byref(m))
+        return Compressed_row_matrix((m.nrow, m.ncol), rp, ci, va)
+
+    def mm_write(self, A):
+        """write_matrix_market of a CSR matrix, as bytes."""
+        n, mcol = A.shape()
+        f = getattr(self.L, f"sko_mm_write_{_sfx(A.dtype)}")
+        f.restype = c_vp
+        ln = c_i64()
+        rp = np.ascontiguousarray(A.row_ptr(), np.int64)
+        ci = np.ascontiguousarray(A.col_ind(), np.int64)
+        va = np.ascontiguousarray(A.values())
+        ptr = f(c_i64(n), c_i64(mcol), _p(rp), _p(ci), _p(va), ctypes.byref(ln))
+        try:
+            return ctypes.string_at(ptr, ln.value)
+        finally:
+            self.L.sko_free(c_vp(ptr))
 
     # -------------------------------------------------------------- #
     # Lanczos and the eigenvalue estimates (sk_oracle_lanczos.h)       #
@@ -455,6 +502,31 @@ class Reference:
         self.destroy(e, A.dtype)
         self.destroy(h, A.dtype)
         return secs
+
+    def mm_read(self, text, dtype=np.float64):
+        """The reference's read_matrix_market<T> + to_compressed_row."""
+        dt = np.dtype(dtype)
+        text = bytes(text)
+        f = getattr(self.L, f"ref_mm_read_{_sfx(dt)}")
+        f.restype = c_vp
+        err = ctypes.create_string_buffer(512)
+        h = f(text, c_i64(len(text)), err, c_i64(512))
+        if not h:
+            raise MatrixMarketError(err.value.decode())
+        A = self.export_csr(h, dt)
+        self.destroy(h, dt)
+        return A
+
+    def mm_write(self, A):
+        """The reference's write_matrix_market of a CSR matrix, as bytes."""
+        h = self.csr_handle(A)
+        f = getattr(self.L, f"ref_mm_write_{_sfx(A.dtype)}")
+        f.restype = c_i64
+        n = f(c_vp(h), None, c_i64(0))
+        buf = ctypes.create_string_buffer(int(n) + 1)
+        f(c_vp(h), buf, c_i64(n))
+        self.destroy(h, A.dtype)
+        return buf.raw[:n]
 
     def lanczos(self, A, nev=1, m=20, tol=1e-10, max_restarts=10, target="largest_algebraic", collect=False,
                 vectors=False):

@@ -17,7 +17,11 @@ set -euo pipefail
 HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
 REF_ROOT="${REF_ROOT:-/root/reference}"
 OUT="$HERE/_ref"
-CXX="${CXX:-g++}"
+# The g++ on PATH, not $CXX: a toolchain that links libstdc++ statically
+# gives the library a private iostream state, which crashes the reference's
+# istream-based Matrix Market reader once another libstdc++ (numpy's) is in
+# the process.  REF_CXX overrides.
+CXX="${REF_CXX:-g++}"
 
 if [ ! -f "$REF_ROOT/sparkit/config.hpp.in" ]; then
   echo "build_ref.sh: reference sources not found at $REF_ROOT; skipping" >&2

@@ -15,7 +15,8 @@
 // (bicgstab.hpp:391), fgmres (fgmres.hpp:459), gmres (gmres.hpp:408), cgs
 // (cgs.hpp:374), minres (minres.hpp:397), lanczos (lanczos.hpp:495),
 // estimate_spectral_radius / estimate_eigenvalue_bounds (conditioning.hpp:112,
-// :132) and the matrix generators of
+// :132), read_matrix_market / write_matrix_market (matrix_market.hpp:45,
+// :119) and the matrix generators of
 // matgen.hpp used by the reference's solver tests.
 
 #include <algorithm>
@@ -41,6 +42,9 @@
 #include <sparkit/data/minres.hpp>
 #include <sparkit/data/conditioning.hpp>
 #include <sparkit/data/lanczos.hpp>
+#include <sparkit/data/matrix_market.hpp>
+#include <cstdio>
+#include <sstream>
 #include <sparkit/data/jacobi.hpp>
 #include <sparkit/data/matgen.hpp>
 #include <sparkit/data/sparse_blas.hpp>
@@ -481,6 +485,26 @@ namespace {
         return sd::minres(bv.begin(), bv.end(), xv.begin(), xv.end(), cfg,     \
                           Op<T>{A}, std::cref(L), std::cref(R));               \
       });                                                                      \
+  }                                                                            \
+  REF_API void* ref_mm_read_##S(char const* text, i64 len, char* err,          \
+                                i64 errcap) {                                  \
+    try {                                                                      \
+      std::istringstream is{std::string(text, static_cast<std::size_t>(len))}; \
+      auto coo = sd::read_matrix_market<T>(is);                                \
+      return wrap_csr<T>(sd::to_compressed_row(coo));                          \
+    } catch (std::exception const& ex) {                                       \
+      std::snprintf(err, static_cast<std::size_t>(errcap), "%s", ex.what());   \
+      return nullptr;                                                          \
+    }                                                                          \
+  }                                                                            \
+  REF_API i64 ref_mm_write_##S(void* h, char* buf, i64 cap) {                  \
+    std::ostringstream os;                                                     \
+    sd::write_matrix_market(os, *static_cast<Handle<T>*>(h)->csr);             \
+    auto str = os.str();                                                       \
+    if (buf && cap > 0)                                                        \
+      std::memcpy(buf, str.data(),                                             \
+                  std::min<std::size_t>(str.size(), static_cast<std::size_t>(cap))); \
+    return static_cast<i64>(str.size());                                       \
   }                                                                            \
   REF_API void ref_lanczos_##S(void* h, i64 nev, i64 m, double tol, i64 maxr,  \
                               int target, int collect, T* ev, T* evec,         \

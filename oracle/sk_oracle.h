@@ -4,7 +4,8 @@
  * TEST INFRASTRUCTURE ONLY.  This is a plain-C restatement of the sparkit
  * reference's sequential algorithms (SpMV over CSR / ELLPACK / jagged
  * diagonal / BSR, Jacobi and Chebyshev preconditioners, CG, BiCGSTAB,
- * FGMRES, GMRES, CGS, MINRES, and the Lanczos eigenvalue estimates), used
+ * FGMRES, GMRES, CGS, MINRES, the Lanczos eigenvalue estimates and the
+ * Matrix Market reader and writer), used
  * by the tests, the smoke check and the CPU-baseline leg of the benchmark
  * to check the CUDA library.  The product never links it.
  *
@@ -149,6 +150,25 @@ typedef struct {
   int64_t restart_residuals_count; /* restart_residuals written */
   int32_t converged;
 } sko_lanczos_result;
+
+/* A CSR matrix read from Matrix Market text (sk_oracle_mm.c); the arrays
+ * are malloc'd (sko_mm_free); err holds the reason when reading fails. */
+typedef struct {
+  int64_t nrow, ncol, nnz;
+  int64_t* row_ptr;
+  int64_t* col_ind;
+  void* values;
+  char err[256];
+} sko_mm_csr;
+
+int sko_mm_read_f64(const char* text, int64_t len, sko_mm_csr* out);
+int sko_mm_read_f32(const char* text, int64_t len, sko_mm_csr* out);
+void sko_mm_free(sko_mm_csr* m);
+char* sko_mm_write_f64(int64_t nrow, int64_t ncol, const int64_t* rp, const int64_t* ci, const double* v,
+                       int64_t* len);
+char* sko_mm_write_f32(int64_t nrow, int64_t ncol, const int64_t* rp, const int64_t* ci, const float* v,
+                       int64_t* len);
+void sko_free(void* p);
 
 /* Summation order of the solvers' dot products: 0 = the reference's
  * sequential order (default), 1 = 256-element chunks added in order,

@@ -18,6 +18,9 @@
 #include <atomic>
 #include <cctype>
 #include <charconv>
+#include <cmath>
+#include <cstdlib>
+#include <limits>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -100,13 +103,25 @@ bool parse_int(const char*& p, const char* e, long long* v) {
 }
 
 // istream >> T for a real: leading whitespace, then the decimal form
-// (std::from_chars rounds correctly, like the strtod behind istream).
+// (std::from_chars rounds correctly, like the strtod behind istream).  A
+// value beyond the type's range reads as libstdc++'s num_get reads it: an
+// overflow as the largest finite value of its sign, an underflow as
+// strtod's (strtof's) zero or subnormal.
 template <typename T>
 bool parse_real(const char*& p, const char* e, T* v) {
   while (p < e && is_space(*p)) ++p;
   if (p < e && *p == '+') ++p;
   auto r = std::from_chars(p, e, *v, std::chars_format::general);
-  if (r.ec != std::errc()) return false;
+  if (r.ec == std::errc::result_out_of_range) {
+    char buf[128];
+    const size_t n = std::min<size_t>(static_cast<size_t>(r.ptr - p), sizeof(buf) - 1);
+    std::memcpy(buf, p, n);
+    buf[n] = 0;
+    const double d = sizeof(T) == 4 ? static_cast<double>(std::strtof(buf, nullptr)) : std::strtod(buf, nullptr);
+    *v = std::isinf(d) ? std::copysign(std::numeric_limits<T>::max(), static_cast<T>(d)) : static_cast<T>(d);
+  } else if (r.ec != std::errc()) {
+    return false;
+  }
   p = r.ptr;
   return true;
 }

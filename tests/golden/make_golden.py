@@ -7,7 +7,8 @@ oracle/build_ref.sh).  Run from the repository root:
 Outputs
   reference_outputs.npz  -- inputs and reference outputs, keyed by case:
       SpMV of every format (reference conversions + multiply) on seeded
-      matrices, the conversions' own arrays, Jacobi inverse diagonals, Chebyshev coefficients and applies,
+      matrices, the conversions' own arrays, Matrix Market texts read and
+      written, Jacobi inverse diagonals, Chebyshev coefficients and applies,
       and CG / BiCGSTAB / FGMRES solutions, summaries and residual histories
       on the matrices of the reference's solver tests.
 known_answers.json (hand-written, not generated) holds the known-answer
@@ -84,6 +85,45 @@ def eigen_matrices():
     }
 
 
+def mm_texts():
+    """Seeded Matrix Market texts for the reader's fixtures: comments and a
+    blank line before the size line, duplicate entries (the last one wins),
+    symmetric files with diagonals and duplicates, skew-symmetric (read as
+    stored), pattern, signed integers, CRLF line ends, extreme and
+    oddly written reals, and 17-digit values."""
+    rng = np.random.default_rng(21)
+    out = {}
+
+    def body(entries, fmt):
+        return "".join(fmt(*e) for e in entries)
+
+    n, m, k = 200, 150, 3000
+    r, c = rng.integers(1, n + 1, k), rng.integers(1, m + 1, k)
+    r[-40:], c[-40:] = r[:40], c[:40]  # duplicates of earlier entries
+    v = rng.standard_normal(k) * 10.0 ** rng.integers(-8, 8, k)
+    out["general_dup"] = ("%%MatrixMarket matrix coordinate real general\n% seeded\n\n%\n"
+                          f"{n} {m} {k}\n" + body(zip(r, c, v), lambda a, b, x: f"{a} {b} {x:.17g}\n"))
+    n, k = 120, 900
+    r, c = rng.integers(1, n + 1, k), rng.integers(1, n + 1, k)
+    r, c = np.maximum(r, c), np.minimum(r, c)  # lower triangle
+    r[:60] = c[:60]  # diagonal entries
+    r[-30:], c[-30:] = r[60:90], c[60:90]
+    v = rng.uniform(-1, 1, k)
+    out["symmetric_dup"] = (f"%%MatrixMarket matrix coordinate real symmetric\n{n} {n} {k}\n" +
+                            body(zip(r, c, v), lambda a, b, x: f"{a} {b} {x:.17g}\n"))
+    out["skew"] = ("%%MatrixMarket matrix coordinate real skew-symmetric\n5 5 4\n2 1 1.5\n3 1 -2\n"
+                   "4 2 3.25\n5 4 0.5\n")
+    out["pattern_sym"] = "%%MatrixMarket matrix coordinate pattern symmetric\n4 4 5\n1 1\n2 1\n3 2\n4 4\n4 1\n"
+    out["integer_signed"] = ("%%MatrixMarket matrix coordinate integer general\n4 3 5\n1 1 -7\n2 3 +12\n"
+                             "4 2 0\n3 1 123456789\n1 1 9\n")
+    out["crlf"] = "%%MatrixMarket matrix coordinate real general\r\n3 3 3\r\n1 1 1.5\r\n2 3 -2.25\r\n3 2 1e3\r\n"
+    out["odd_reals"] = ("%%MatrixMarket matrix coordinate real general\n3 4 11\n1 1 1e-300\n1 2 5e-324\n"
+                        "1 3 1.7976931348623157e308\n1 4 -0.0\n2 1 1.\n2 2 .5\n2 3 +3\n3 1 1E5\n"
+                        "3 4 0.1000000000000000055511151231257827\n3 3 -1e400\n3 2 1e-400\n")
+    out["tabs_and_spaces"] = "%%MatrixMarket matrix coordinate real general\n  3\t3  2\n\t1   1\t2.5  \n 3 3 -1\n"
+    return out
+
+
 def main():
     R = Reference()
     out = {}
@@ -139,6 +179,20 @@ def main():
                     out[f"{key}/{k}"] = r[k]
                 out[f"{key}/scalars"] = np.array([r["computed_restarts"], r["converged_count"],
                                                   int(r["converged"])])
+    # Matrix Market: the reference's read_matrix_market + to_compressed_row
+    # on seeded texts (both value types), and its write_matrix_market of the
+    # results
+    for name, text in mm_texts().items():
+        raw = text.encode()
+        out[f"mm/{name}/text"] = np.frombuffer(raw, dtype=np.uint8)
+        for dt in (np.float64, np.float32):
+            M = R.mm_read(raw, dt)
+            tag = f"mm/{name}/{np.dtype(dt).name}"
+            out[f"{tag}/shape"] = np.array(M.shape())
+            out[f"{tag}/row_ptr"] = M.row_ptr()
+            out[f"{tag}/col_ind"] = M.col_ind()
+            out[f"{tag}/values"] = M.values()
+            out[f"{tag}/written"] = np.frombuffer(R.mm_write(M), dtype=np.uint8)
     # preconditioners
     P = matgen.poisson_2d(8, 8, 0.5)
     out["jacobi/poisson8/inv_d"] = R.jacobi(P)

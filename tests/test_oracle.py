@@ -254,6 +254,87 @@ def test_fp32_lanczos_depends_on_summation_order(oracle):
     assert max(abs(f0[0] - f2[0]), abs(f0[1] - f2[1])) > 0.1
 
 
+def _dense(shape, entries):
+    D = np.zeros(shape)
+    for r, c, v in entries:
+        D[int(r), int(c)] = v
+    return D
+
+
+def _csr_dense(A):
+    D = np.zeros(A.shape())
+    rp, ci, va = A.row_ptr(), A.col_ind(), A.values()
+    for r in range(A.shape()[0]):
+        D[r, ci[rp[r]:rp[r + 1]]] = va[rp[r]:rp[r + 1]]
+    return D
+
+
+def test_matrix_market_known_answers(oracle, known):
+    """The reference's own Catch2 cases for read_matrix_market,
+    parse_banner and write_matrix_market (matrix_market_test.cpp)."""
+    from oracle.binding import MatrixMarketError
+    from tests.helpers import csr_from_entries
+    mm = known["matrix_market"]
+    for case in mm["read"]:
+        A = oracle.mm_read(case["text"].encode())
+        assert A.shape() == tuple(case["shape"]), case["source"]
+        assert np.array_equal(_csr_dense(A), _dense(case["shape"], case["entries"])), case["source"]
+    for case in mm["rejected"]:
+        with pytest.raises(MatrixMarketError):
+            oracle.mm_read(case["text"].encode())
+    for case in mm["write"]:
+        A = csr_from_entries(tuple(case["shape"]), case["entries"])
+        assert oracle.mm_write(A) == case["text"].encode(), case["source"]
+
+
+def _same_bits(a, b):
+    a, b = np.asarray(a), np.asarray(b)
+    return a.dtype == b.dtype and a.shape == b.shape and np.array_equal(a.view(np.uint8), b.view(np.uint8))
+
+
+@pytest.mark.parametrize("dtype", ["float64", "float32"])
+def test_matrix_market_matches_reference_fixtures(oracle, golden, dtype):
+    """read_matrix_market + to_compressed_row on seeded texts (duplicates,
+    symmetric, skew, pattern, signed integers, CRLF, out-of-range reals)
+    and write_matrix_market of the result, against the compiled
+    reference's outputs, bit for bit (the sign of zero included)."""
+    from tests.golden.make_golden import mm_texts
+    for name in mm_texts():
+        tag = f"mm/{name}/{dtype}"
+        A = oracle.mm_read(bytes(golden[f"mm/{name}/text"]), np.dtype(dtype))
+        assert A.shape() == tuple(golden[f"{tag}/shape"]), name
+        for f in ("row_ptr", "col_ind", "values"):
+            assert _same_bits(getattr(A, f)(), golden[f"{tag}/{f}"]), (name, f)
+        assert oracle.mm_write(A) == bytes(golden[f"{tag}/written"]), name
+
+
+def test_matrix_market_matches_reference_live(oracle, reference):
+    """Beyond the fixtures, against the compiled reference itself: seeded
+    random files of every symmetry and field, FP64 and FP32."""
+    rng = np.random.default_rng(5)
+    for trial in range(12):
+        n, m = int(rng.integers(2, 40)), int(rng.integers(2, 40))
+        sym = ["general", "symmetric", "skew-symmetric", "hermitian"][trial % 4]
+        field = ["real", "integer", "pattern"][trial % 3]
+        if sym != "general":
+            m = n
+        k = int(rng.integers(0, 3 * n))
+        r, c = rng.integers(1, n + 1, k), rng.integers(1, m + 1, k)
+        if sym != "general":
+            r, c = np.maximum(r, c), np.minimum(r, c)
+        vals = rng.standard_normal(k) * 10.0 ** rng.integers(-5, 5, k)
+        lines = [f"%%MatrixMarket matrix coordinate {field} {sym}", f"{n} {m} {k}"]
+        for a, b, v in zip(r, c, vals):
+            lines.append(f"{a} {b}" if field == "pattern" else
+                         f"{a} {b} {int(v * 100)}" if field == "integer" else f"{a} {b} {v:.17g}")
+        text = ("\n".join(lines) + "\n").encode()
+        for dt in (np.float64, np.float32):
+            A, B = oracle.mm_read(text, dt), reference.mm_read(text, dt)
+            for f in ("row_ptr", "col_ind", "values"):
+                assert _same_bits(getattr(A, f)(), getattr(B, f)()), (trial, sym, field, f)
+            assert oracle.mm_write(A) == reference.mm_write(B)
+
+
 def test_generators_match_reference(reference):
     pairs = [(matgen.poisson_2d(4, 4, 5.0), reference.poisson_2d(4, 4, 5.0)),
              (matgen.poisson_2d(5, 3), reference.poisson_2d(5, 3)),
