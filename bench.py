@@ -58,6 +58,7 @@ def parse():
                    help="one mixed solve with 100 persistent FP32 inner iterations on the 128^3 GRF problem, for ncu")
     p.add_argument("--no-convert", action="store_true")
     p.add_argument("--no-eigen", action="store_true")
+    p.add_argument("--no-mm", action="store_true")
     p.add_argument("--profile-eigen", action="store_true",
                    help="one sk_eigenvalue_bounds on the grid^3 Laplacian (for an ncu launch list)")
     p.add_argument("--profile-convert", action="store_true",
@@ -411,6 +412,52 @@ def profile_eigen(grid):
     gpu.estimate_eigenvalue_bounds(Ad)
     torch.cuda.synchronize()
     return 0
+
+
+def mm_runs(grid):
+    """Matrix Market file -> device CSR handle (sk_matrix_market_read, all
+    host cores parsing, the assembly on the device) for the grid^3
+    Laplacian written with 17 significant digits: wall time of the call
+    (median of 3 after one warm-up, the file in the page cache), text MB/s
+    and entries/s; beside it the compiled reference's read_matrix_market +
+    to_compressed_row on the file's first 262,144 entry lines (one core)."""
+    import tempfile
+
+    from oracle.binding import Reference, reference_available
+    from sparkit_b200 import gpu, matgen
+    A = matgen.laplacian_3d_dirichlet(grid)
+    nnz = A.size()
+    out = {"nnz": nnz, "threads": os.cpu_count()}
+    with tempfile.TemporaryDirectory() as d:
+        path = os.path.join(d, "lap.mtx")
+        Ad = gpu.Device_matrix(A)
+        t0 = time.perf_counter()
+        gpu.write_matrix_market(Ad, path, precision=17)
+        out["write_ms"] = (time.perf_counter() - t0) * 1e3
+        Ad.close()
+        size = os.path.getsize(path)
+        gpu.read_matrix_market(path).close()
+        ts = []
+        for _ in range(3):
+            t0 = time.perf_counter()
+            B = gpu.read_matrix_market(path)
+            ts.append(time.perf_counter() - t0)
+            B.close()
+        secs = float(np.median(ts))
+        out.update({"file_mb": size / 1e6, "read_ms": secs * 1e3, "mb_per_s": size / secs / 1e6,
+                    "mentries_per_s": nnz / secs / 1e6})
+        if reference_available():
+            sample = 1 << 18
+            with open(path, "rb") as f:
+                lines = f.read().split(b"\n")
+            head = lines[1].split()
+            text = b"\n".join([lines[0], b" ".join([head[0], head[1], str(sample).encode()])] +
+                               lines[2:2 + sample]) + b"\n"
+            rs = Reference().mm_read_seconds(text)
+            out["cpu_reference"] = {"s": rs, "mentries_per_s": sample / rs / 1e6, "cores": 1, "kind": "reference",
+                                    "sample": f"the first {sample} entry lines of the same file"}
+            out["speedup_vs_reference"] = out["mentries_per_s"] / out["cpu_reference"]["mentries_per_s"]
+    return out
 
 
 def solver_runs(grid3):
@@ -898,6 +945,8 @@ def main():
         extra["convert"] = convert_runs(args.grid)
     if rank == 0 and world == 1 and not args.no_eigen:
         extra["eigen_bounds"] = eigen_runs(args.grid)
+    if rank == 0 and world == 1 and not args.no_mm:
+        extra["matrix_market"] = mm_runs(args.grid)
     if rank == 0 and world == 1 and not args.no_solvers:
         extra["solvers"] = solver_runs(args.grid)
         extra["solvers"]["c5_batched"] = batched_runs()

@@ -517,6 +517,23 @@ class Reference:
         self.destroy(h, dt)
         return A
 
+    def mm_read_seconds(self, text, dtype=np.float64):
+        """Wall time of the reference's read_matrix_market + to_compressed_row
+        on the text (the arrays are not copied out)."""
+        import time
+        dt = np.dtype(dtype)
+        text = bytes(text)
+        f = getattr(self.L, f"ref_mm_read_{_sfx(dt)}")
+        f.restype = c_vp
+        err = ctypes.create_string_buffer(512)
+        t0 = time.perf_counter()
+        h = f(text, c_i64(len(text)), err, c_i64(512))
+        secs = time.perf_counter() - t0
+        if not h:
+            raise MatrixMarketError(err.value.decode())
+        self.destroy(h, dt)
+        return secs
+
     def mm_write(self, A):
         """The reference's write_matrix_market of a CSR matrix, as bytes."""
         h = self.csr_handle(A)

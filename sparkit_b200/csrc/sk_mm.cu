@@ -4,9 +4,9 @@
 // banner: matrix_market.cpp:28-87) followed by to_compressed_row of the
 // resulting Coordinate_matrix (Coordinate_matrix.hpp:36-41: a map keyed by
 // (row, column), so the last of duplicate entries wins, then sorted):
-//   host threads   split the entry lines at line boundaries and parse them
-//                  with std::from_chars (correctly rounded, as the
-//                  reference's istream >> T);
+//   host threads   split the (memory-mapped) text at line boundaries and
+//                  parse their pieces with std::from_chars (correctly
+//                  rounded, as the reference's istream >> T);
 //   device         mirrors the entries of a symmetric file, sorts the
 //                  (row, column) keys with a stable LSD radix sort, keeps
 //                  the last entry of every key and builds the row pointers:
@@ -26,6 +26,11 @@
 #include <string>
 #include <thread>
 #include <vector>
+
+#include <fcntl.h>
+#include <sys/mman.h>
+#include <sys/stat.h>
+#include <unistd.h>
 
 #include "sk_sort.cuh"
 
@@ -137,7 +142,7 @@ const char* line_end(const char* p, const char* e) {
 // 0-based keys row * ncol + col in file order, each mirrored entry of a
 // symmetric file right after its original (matrix_market.hpp:104-106).
 template <typename T>
-__global__ void mm_keys_kernel(i64 nnz, const long long* __restrict__ rows, const long long* __restrict__ cols,
+__global__ void mm_keys_kernel(i64 nnz, const int* __restrict__ rows, const int* __restrict__ cols,
                                const T* __restrict__ vals, const i64* __restrict__ mirror_before, i64 ncol,
                                unsigned long long* __restrict__ keys, T* __restrict__ vexp) {
   i64 k = blockIdx.x * static_cast<i64>(blockDim.x) + threadIdx.x;
@@ -155,8 +160,8 @@ __global__ void mm_keys_kernel(i64 nnz, const long long* __restrict__ rows, cons
   }
 }
 
-__global__ void mm_mirror_flags_kernel(i64 nnz, const long long* __restrict__ rows,
-                                       const long long* __restrict__ cols, int* __restrict__ flag) {
+__global__ void mm_mirror_flags_kernel(i64 nnz, const int* __restrict__ rows, const int* __restrict__ cols,
+                                       int* __restrict__ flag) {
   i64 k = blockIdx.x * static_cast<i64>(blockDim.x) + threadIdx.x;
   const i64 stride = static_cast<i64>(gridDim.x) * blockDim.x;
   for (; k < nnz; k += stride) flag[k] = rows[k] != cols[k] ? 1 : 0;
@@ -242,7 +247,10 @@ sk_status mm_read(sk_matrix* out, const char* text, i64 len, sk_dtype dt, int th
   // skew-symmetric and hermitian files are read as stored (:99-100)
   const bool symmetric = symmetry == MM_SYMMETRIC;
 
-  // -- host: the nnz entry lines, split among threads at line boundaries
+  // -- host: the entry lines, split among threads at line boundaries; each
+  // thread parses its piece into its own arrays (first touch in parallel),
+  // a prefix over the pieces' line counts places them, and the lines past
+  // the first nnz are ignored, as the reference never reads them
   int nt = threads > 0 ? threads : static_cast<int>(std::thread::hardware_concurrency());
   nt = std::max(1, std::min({nt, 64, static_cast<int>((end - data) / (1 << 20)) + 1}));
   std::vector<const char*> cut(static_cast<size_t>(nt) + 1);
@@ -253,54 +261,48 @@ sk_status mm_read(sk_matrix* out, const char* text, i64 len, sk_dtype dt, int th
     const char* q = line_end(c, end);
     cut[t] = q < end ? q + 1 : end;
   }
-  auto run = [&](auto fn) {
-    std::vector<std::thread> pool;
-    for (int t = 1; t < nt; ++t) pool.emplace_back(fn, t);
-    fn(0);
-    for (auto& th : pool) th.join();
+  struct Piece {
+    std::vector<int> r, c;
+    std::vector<T> v;
+    i64 bad = -1;  // first malformed line of the piece
   };
-  // lines in each piece (a final line without '\n' counts)
-  std::vector<i64> nlines(static_cast<size_t>(nt), 0);
-  run([&](int t) {
-    i64 c = 0;
-    for (const char* q = cut[t]; q < cut[t + 1];) {
-      const char* e2 = line_end(q, cut[t + 1]);
-      ++c;
-      q = e2 < cut[t + 1] ? e2 + 1 : cut[t + 1];
-    }
-    nlines[t] = c;
-  });
+  std::vector<Piece> piece(static_cast<size_t>(nt));
+  {
+    std::vector<std::thread> pool;
+    auto parse = [&](int t) {
+      Piece& P = piece[t];
+      const size_t guess = static_cast<size_t>(cut[t + 1] - cut[t]) / 16 + 16;
+      P.r.reserve(guess);
+      P.c.reserve(guess);
+      P.v.reserve(guess);
+      for (const char* q = cut[t]; q < cut[t + 1];) {
+        const char* e2 = line_end(q, cut[t + 1]);
+        const char* r = q;
+        long long a = 0, b = 0;
+        T v = T(1);  // pattern entries are 1 (:90-92)
+        bool ok = parse_int(r, e2, &a) && parse_int(r, e2, &b) && (pattern || parse_real<T>(r, e2, &v));
+        ok = ok && a >= 1 && a <= rows && b >= 1 && b <= cols;
+        if (!ok && P.bad < 0) P.bad = static_cast<i64>(P.r.size());
+        P.r.push_back(ok ? static_cast<int>(a) : 1);
+        P.c.push_back(ok ? static_cast<int>(b) : 1);
+        P.v.push_back(v);
+        q = e2 < cut[t + 1] ? e2 + 1 : cut[t + 1];
+      }
+    };
+    for (int t = 1; t < nt; ++t) pool.emplace_back(parse, t);
+    parse(0);
+    for (auto& th : pool) th.join();
+  }
   std::vector<i64> first(static_cast<size_t>(nt) + 1, 0);
-  for (int t = 0; t < nt; ++t) first[t + 1] = first[t] + nlines[t];
+  for (int t = 0; t < nt; ++t) first[t + 1] = first[t] + static_cast<i64>(piece[t].r.size());
   if (first[nt] < nnz)
     return fail(SK_INVALID_ARG, "matrix market: unexpected end of input (" + std::to_string(first[nt]) + " of " +
                                     std::to_string(nnz) + " entry lines)");
-  std::vector<long long> hr(static_cast<size_t>(nnz)), hc(static_cast<size_t>(nnz));
-  std::vector<T> hv(static_cast<size_t>(nnz));
-  std::atomic<long long> bad{-1};
-  run([&](int t) {
-    i64 L = first[t];
-    for (const char* q = cut[t]; q < cut[t + 1] && L < nnz; ++L) {
-      const char* e2 = line_end(q, cut[t + 1]);
-      const char* r = q;
-      long long a = 0, b = 0;
-      T v = T(1);  // pattern entries are 1 (:90-92)
-      bool ok = parse_int(r, e2, &a) && parse_int(r, e2, &b) && (pattern || parse_real<T>(r, e2, &v));
-      ok = ok && a >= 1 && a <= rows && b >= 1 && b <= cols;
-      if (!ok) {
-        long long cur = bad.load();
-        while ((cur < 0 || L < cur) && !bad.compare_exchange_weak(cur, L)) {
-        }
-      }
-      hr[L] = a;
-      hc[L] = b;
-      hv[L] = v;
-      q = e2 < cut[t + 1] ? e2 + 1 : cut[t + 1];
-    }
-  });
-  if (bad.load() >= 0)
-    return fail(SK_INVALID_ARG, "matrix market: entry line " + std::to_string(bad.load() + 1) + " is not 'row col" +
-                                    (pattern ? "" : " value") + "' with 1-based indices in range");
+  for (int t = 0; t < nt; ++t)
+    if (piece[t].bad >= 0 && first[t] + piece[t].bad < nnz)
+      return fail(SK_INVALID_ARG, "matrix market: entry line " + std::to_string(first[t] + piece[t].bad + 1) +
+                                      " is not 'row col" + (pattern ? "" : " value") +
+                                      "' with 1-based indices in range");
 
   // -- device: mirror, sort, keep the last of each key, row pointers
   if ((s = new_handle(out, SK_CSR, dt, rows, cols)) != SK_OK) return s;
@@ -308,15 +310,17 @@ sk_status mm_read(sk_matrix* out, const char* text, i64 len, sk_dtype dt, int th
   sk_matrix A = *out;
   cudaStream_t st = A->stream;
   Temps tmp(st);
-  long long *dr = nullptr, *dc = nullptr;
+  int *dr = nullptr, *dc = nullptr;
   T* dv = nullptr;
   if ((s = tmp.get(&dr, nnz)) != SK_OK) return s;
   if ((s = tmp.get(&dc, nnz)) != SK_OK) return s;
   if ((s = tmp.get(&dv, nnz)) != SK_OK) return s;
-  if (nnz) {
-    SK_CUDA(cudaMemcpyAsync(dr, hr.data(), nnz * sizeof(long long), cudaMemcpyHostToDevice, st));
-    SK_CUDA(cudaMemcpyAsync(dc, hc.data(), nnz * sizeof(long long), cudaMemcpyHostToDevice, st));
-    SK_CUDA(cudaMemcpyAsync(dv, hv.data(), nnz * sizeof(T), cudaMemcpyHostToDevice, st));
+  for (int t = 0; t < nt; ++t) {
+    const i64 cnt = std::min<i64>(static_cast<i64>(piece[t].r.size()), nnz - first[t]);
+    if (cnt <= 0) break;
+    SK_CUDA(cudaMemcpyAsync(dr + first[t], piece[t].r.data(), cnt * sizeof(int), cudaMemcpyHostToDevice, st));
+    SK_CUDA(cudaMemcpyAsync(dc + first[t], piece[t].c.data(), cnt * sizeof(int), cudaMemcpyHostToDevice, st));
+    SK_CUDA(cudaMemcpyAsync(dv + first[t], piece[t].v.data(), cnt * sizeof(T), cudaMemcpyHostToDevice, st));
   }
   i64 nexp = nnz;
   i64* mirror_before = nullptr;
@@ -446,19 +450,25 @@ sk_status sk_matrix_market_read_buffer(sk_matrix* out, const char* text, int64_t
 sk_status sk_matrix_market_read(sk_matrix* out, const char* path, sk_dtype dtype, int32_t threads) {
   SK_CHECK(out && path, SK_INVALID_ARG, "null argument");
   *out = nullptr;
-  FILE* f = std::fopen(path, "rb");
-  if (!f) return fail(SK_INVALID_ARG, std::string("matrix market: cannot open file: ") + path);
-  std::vector<char> text;
-  if (std::fseek(f, 0, SEEK_END) == 0) {
-    const long sz = std::ftell(f);
-    if (sz > 0) text.reserve(static_cast<size_t>(sz));
-    std::fseek(f, 0, SEEK_SET);
+  const int fd = ::open(path, O_RDONLY);
+  if (fd < 0) return fail(SK_INVALID_ARG, std::string("matrix market: cannot open file: ") + path);
+  struct stat sb;
+  if (::fstat(fd, &sb) != 0) {
+    ::close(fd);
+    return fail(SK_INVALID_ARG, std::string("matrix market: cannot read file: ") + path);
   }
-  char chunk[1 << 16];
-  size_t got;
-  while ((got = std::fread(chunk, 1, sizeof(chunk), f)) > 0) text.insert(text.end(), chunk, chunk + got);
-  std::fclose(f);
-  return read_any(out, text.data(), static_cast<i64>(text.size()), dtype, threads);
+  const size_t len = static_cast<size_t>(sb.st_size);
+  if (len == 0) {
+    ::close(fd);
+    return read_any(out, "", 0, dtype, threads);
+  }
+  // the page cache mapped read-only: no copy of the text
+  void* m = ::mmap(nullptr, len, PROT_READ, MAP_PRIVATE, fd, 0);
+  ::close(fd);
+  if (m == MAP_FAILED) return fail(SK_INVALID_ARG, std::string("matrix market: cannot map file: ") + path);
+  sk_status s = read_any(out, static_cast<const char*>(m), static_cast<i64>(len), dtype, threads);
+  ::munmap(m, len);
+  return s;
 }
 
 sk_status sk_matrix_market_write(sk_matrix A, const char* path, int32_t precision, int32_t threads) {
