@@ -460,6 +460,75 @@ def mm_runs(grid):
     return out
 
 
+def krylov_runs():
+    """GMRES(30), CGS and BiCGSTAB with a left Jacobi preconditioner on the
+    256^2 upwind convection-diffusion problem, MINRES and CG with Jacobi on
+    the 48^3 Dirichlet Laplacian, all to 1e-10: wall time of the host-array
+    call (b and x copied in and out; median of 3 after one warm-up) beside
+    the compiled reference's own solver on the same problem (one core); and
+    the device solvers alone on the 1024^2 / 128^3 versions."""
+    from oracle.binding import Reference, reference_available
+    from sparkit_b200 import gpu, matgen
+    ref = Reference() if reference_available() else None
+
+    def spec(n, A, b):
+        Ad = gpu.Device_matrix(A)
+        J = gpu.jacobi(Ad)
+        op = gpu.spmv(Ad)
+        maxit = 40000
+        return {
+            "gmres30": (lambda x: gpu.gmres(b, x, gpu.Gmres_config(1e-10, 30, maxit), op, left=J),
+                        lambda: ref.gmres(A, b, np.zeros(n), 1e-10, 30, maxit, left="jacobi")),
+            "cgs": (lambda x: gpu.cgs(b, x, gpu.Cgs_config(1e-10, maxit), op, left=J),
+                    lambda: ref.cgs(A, b, np.zeros(n), 1e-10, maxit, left="jacobi")),
+            "bicgstab": (lambda x: gpu.bicgstab(b, x, gpu.Bicgstab_config(1e-10, maxit), op, J),
+                         lambda: ref.bicgstab(A, b, np.zeros(n), 1e-10, maxit, left="jacobi")),
+            "minres": (lambda x: gpu.minres(b, x, gpu.Minres_config(1e-10, maxit), op, left=J),
+                       lambda: ref.minres(A, b, np.zeros(n), 1e-10, maxit, left="jacobi")),
+            "cg": (lambda x: gpu.conjugate_gradient(b, x, gpu.CGConfig(1e-10, maxit, maxit), op, J, gpu.identity),
+                   lambda: ref.cg(A, b, np.zeros(n), 1e-10, maxit, maxit, left="jacobi")),
+        }, Ad
+
+    def timed(fn, n):
+        fn(np.zeros(n))
+        ts, s = [], None
+        for _ in range(3):
+            x = np.zeros(n)
+            t0 = time.perf_counter()
+            s = fn(x)
+            ts.append(time.perf_counter() - t0)
+        return float(np.median(ts)), s, x
+
+    out = {}
+    problems = [("convdiff_256sq", matgen.convection_diffusion_2d(256, 256, 1.0, 0.9, 0.5), ("gmres30", "cgs", "bicgstab"), True),
+                ("lap3d_48", matgen.laplacian_3d_dirichlet(48), ("minres", "cg"), True),
+                ("convdiff_1024sq", matgen.convection_diffusion_2d(1024, 1024, 1.0, 0.9, 0.5), ("gmres30", "cgs", "bicgstab"),
+                 False),
+                ("lap3d_128", matgen.laplacian_3d_dirichlet(128), ("minres", "cg"), False)]
+    from oracle.binding import Oracle
+    orc = Oracle()  # the true residual check
+    for pname, A, solvers, with_ref in problems:
+        n = A.shape()[0]
+        b = orc.spmv(A, matgen.uniform_vector(n, seed=2))
+        fns, Ad = spec(n, A, b)
+        for sname in solvers:
+            g, r = fns[sname]
+            secs, st, x = timed(g, n)
+            rel = float(np.linalg.norm(b - orc.spmv(A, x)) / np.linalg.norm(b))
+            row = {"n": n, "ms": secs * 1e3, "iterations": st.computed_iterations, "converged": bool(st.converged),
+                   "true_rel_residual": rel, "us_per_iteration": secs * 1e6 / max(st.computed_iterations, 1)}
+            if with_ref and ref is not None:
+                t0 = time.perf_counter()
+                _, rs = r()
+                rsec = time.perf_counter() - t0
+                row["cpu_reference"] = {"s": rsec, "iterations": rs["computed_iterations"],
+                                        "converged": bool(rs["converged"]), "cores": 1, "kind": "reference"}
+                row["speedup_vs_reference"] = rsec / secs
+            out[f"{pname}/{sname}"] = row
+        Ad.close()
+    return out
+
+
 def solver_runs(grid3):
     """Time-to-solution of the solver configurations (wall time of the
     solve call, inputs resident on the device, one warm-up solve first).
@@ -951,6 +1020,7 @@ def main():
         extra["solvers"] = solver_runs(args.grid)
         extra["solvers"]["c5_batched"] = batched_runs()
         extra["solvers"]["c4_learned_fgmres"] = learned_runs()
+        extra["solvers"]["krylov"] = krylov_runs()
 
     if rank == 0:
         line = {
