@@ -200,7 +200,12 @@ SK_API sk_status sk_spmv_f32(sk_matrix A, const float* x_dev, float* y_dev,
 
 /* The drop-in form of multiply(A, span<T const>) -> std::vector<T>: x is
  * a host array of ncol values, y a host array of nrow values.  Copies x in,
- * runs the product and copies y out (synchronous). */
+ * runs the product and copies y out (synchronous).  A CSR product with at
+ * least 8 MiB of y is pipelined in row chunks: each chunk's product starts
+ * once the prefix of x its columns reach is on the device, and its rows of
+ * y are copied out while later pieces of x still arrive (page-locked host
+ * buffers let the two copy directions overlap).  The result is the same as
+ * sk_spmv's, bit for bit. */
 SK_API sk_status sk_spmv_host(sk_matrix A, const void* x_host, void* y_host);
 
 /* ---------------------------------------------------------------- */

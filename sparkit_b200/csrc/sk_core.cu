@@ -260,6 +260,7 @@ void destroy_handle(sk_matrix A) {
   if (A->stream) cudaStreamSynchronize(A->stream);
   for (void* p : A->allocations) cudaFree(p);
   if (A->io) cudaFree(A->io);
+  if (A->pipe) destroy_host_pipe(A->pipe);
   if (A->ws) cudaFree(A->ws);
   if (A->ws2) cudaFree(A->ws2);
   if (A->stream) cudaStreamDestroy(A->stream);

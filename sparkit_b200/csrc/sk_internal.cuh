@@ -121,6 +121,12 @@ struct Bsr {
   i64 sell_blocks = 0;
 };
 
+// Plan of the pipelined host-buffer product (sk_spmv_host), built on the
+// first call: row chunks, the prefix of x each chunk reads, and the copy
+// streams and events.
+struct HostPipe;
+void destroy_host_pipe(HostPipe* p);
+
 }  // namespace sk
 
 struct sk_matrix_s {
@@ -137,6 +143,7 @@ struct sk_matrix_s {
   std::vector<void*> allocations;
   sk::i64 device_bytes = 0;
   void* io = nullptr;  // x and y buffers of the host-pointer calls
+  sk::HostPipe* pipe = nullptr;  // chunk plan of sk_spmv_host
   // Grow-only workspace of the solver calls on this handle.
   void* ws = nullptr;
   size_t ws_bytes = 0;
