@@ -182,6 +182,22 @@ SK_API sk_status sk_matrix_info(sk_matrix A, int64_t info[8]);
  * used by the mixed-precision solver and the FP32 SpMV. */
 SK_API sk_status sk_matrix_add_f32_values(sk_matrix A);
 
+/* Adds a diagonal copy of a CSR handle whose entries lie on at most 16
+ * diagonals c - r (a stencil in natural order) with every row's columns in
+ * ascending order: the values of each 32-row slice stored diagonal by
+ * diagonal, and a mask of the entries each row stores.  The later products
+ * on the handle (sk_spmv, sk_spmv_host, the solvers' steps, the per-step
+ * FP32 inner solve of the mixed solver) read it instead of the CSR arrays:
+ * no column indices and no gathered x, and each row summed over its stored
+ * entries in its CSR order, so the results keep their bits.  The persistent
+ * FP32 inner solve keeps reading the SELL-32 copy.
+ * No reference counterpart: a device layout of Compressed_row_matrix
+ * (Compressed_row_matrix.hpp:20-132), as the SELL-32 copy is.  *built is 1
+ * when the handle has the copy, 0 when its pattern does not qualify (more
+ * than 16 diagonals, planes more than half empty, or a row whose columns
+ * do not ascend); the handle is unchanged then. */
+SK_API sk_status sk_matrix_add_diagonals(sk_matrix A, int* built);
+
 /* ---------------------------------------------------------------- */
 /* SpMV: y = A x                                                     */
 /* ---------------------------------------------------------------- */

@@ -382,7 +382,9 @@ using namespace sk;
 i64 sk_matrix_s::spmv_bytes() const {
   const i64 V = dtype == SK_F64 ? 8 : 4;
   switch (format) {
-    case SK_CSR: return V * nnz + 4 * nnz + 4 * (nrow + 1) + V * ncol + V * nrow;
+    case SK_CSR:
+      if (csr.dia_n) return (V * csr.dia_n + 2) * nrow + V * ncol + V * nrow;  // planes, mask, x, y
+      return V * nnz + 4 * nnz + 4 * (nrow + 1) + V * ncol + V * nrow;
     case SK_ELL: return (V + 4) * nnz + V * ncol + V * nrow;
     case SK_JAD: return (V + 4) * nnz + 4 * (jad.njd + 1) + 4 * nrow + V * ncol + V * nrow;
     case SK_BSR:
@@ -673,7 +675,8 @@ sk_status sk_matrix_info(sk_matrix A, int64_t info[8]) {
 sk_status sk_matrix_add_f32_values(sk_matrix A) {
   SK_CHECK(A, SK_INVALID_ARG, "null handle");
   SK_CHECK(A->format == SK_CSR, SK_NOT_SUPPORTED, "FP32 value copy is for CSR handles");
-  if (A->dtype == SK_F32 || A->csr.vals32) return SK_OK;
+  if (A->dtype == SK_F32) return SK_OK;
+  if (A->csr.vals32) return build_dia_f32(A);  // planes added after the copy
   void* p = nullptr;
   sk_status st = dev_alloc(A, &p, (A->nnz + 8) * 4);
   if (st != SK_OK) return st;
@@ -692,7 +695,7 @@ sk_status sk_matrix_add_f32_values(sk_matrix A) {
     A->csr.sell_vals32 = static_cast<float*>(q);
   }
   SK_CUDA(cudaStreamSynchronize(A->stream));
-  return SK_OK;
+  return build_dia_f32(A);
 }
 
 }  // extern "C"

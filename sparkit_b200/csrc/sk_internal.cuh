@@ -23,6 +23,7 @@ constexpr int kRowsMax = 256;    // CSR: rows per CTA (one per thread)
 constexpr int kBsrTileVals = 4096;  // BSR: block values staged per CTA
 constexpr int kMaxRed = 4;       // fused reductions carried per kernel
 constexpr int kSellMaxRow = 64;  // CSR rows up to this length use SELL-32
+constexpr int kDiaMax = 16;      // diagonals of the diagonal copy of a CSR handle
 
 // ------------------------------------------------------------------
 // Status plumbing
@@ -77,6 +78,19 @@ struct Csr {
   int* sell_off = nullptr;             // nslices + 1 entry offsets
   unsigned char* sell_len = nullptr;   // entries per row
   i64 sell_entries = 0;                // padded size
+  // Diagonal copy (sk_matrix_add_diagonals) of a handle whose entries lie
+  // on at most kDiaMax diagonals c - r = off[d] and whose rows hold their
+  // columns in ascending order, slice-major like the SELL-32 copy: A(r, r +
+  // off[d]) at ((r / 32) * dia_n + d) * 32 + r % 32, so that the values a
+  // warp reads for its 32 rows are dia_n consecutive 32-value segments.
+  // Bit d of mask[r] says whether row r stores that entry.  The product
+  // sums a row's stored entries in ascending column order, the CSR order.
+  int dia_n = 0;
+  int dia_off[kDiaMax] = {};
+  i64 dia_len = 0;  // values in the copy: ceil(nrow / 32) * 32 * dia_n
+  void* dia_vals = nullptr;
+  float* dia_vals32 = nullptr;
+  unsigned short* dia_mask = nullptr;
 };
 
 // ELLPACK: slot-major (column-major) copy of the reference's row-major
@@ -189,7 +203,7 @@ namespace sk {
 
 // The FP32 value copy in the layout the product kernel reads.
 inline const float* f32_values(const sk_matrix_s* A) {
-  return A->csr.sell ? A->csr.sell_vals32 : A->csr.vals32;
+  return A->csr.dia_n ? A->csr.dia_vals32 : A->csr.sell ? A->csr.sell_vals32 : A->csr.vals32;
 }
 
 cudaStream_t pick_stream(sk_matrix A, sk_stream s);
@@ -274,6 +288,9 @@ sk_status upload_vector(sk_matrix A, const std::vector<V>& h, V** dev, cudaStrea
 // The product's tables of a CSR handle whose row_ptr / col_ind / vals are
 // already on the device, from the host copy of its row pointers.
 sk_status csr_finish(sk_matrix A, const int64_t* row_ptr, cudaStream_t st);
+
+// FP32 planes of the diagonal copy of an FP64 handle (no-op without one).
+sk_status build_dia_f32(sk_matrix A);
 
 // BSR block-row partition of the product kernel (host row pointers) and
 // the sliced copy of 2x2 / 3x3 handles.

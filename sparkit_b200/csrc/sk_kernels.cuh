@@ -343,6 +343,72 @@ sell_spmv_kernel(int nrow, const int* __restrict__ off, const unsigned char* __r
 }
 
 // ------------------------------------------------------------------
+// CSR through its diagonal copy: one thread per row.  Diagonal d of a
+// warp's 32 rows is one contiguous 32-value segment of the slice-major copy
+// (a slice's segments are adjacent), and x[i + off[d]] is contiguous too,
+// so neither the matrix stream nor the reads of x are gathers, and no
+// column index is read.  The loads do not wait for the row's mask: a diagonal the row does
+// not store reads a zero plane entry and a clamped x, and the mask leaves
+// both out of the sum.  A row sums its stored entries in ascending column
+// order from 0: the order of its CSR row, so the bits of sparse_blas.hpp:
+// 25-28.  Rows r0 .. r1 - 1; y indexed by the absolute row.
+// ------------------------------------------------------------------
+struct DiaArgs {
+  int n;  // diagonals
+  int r0, r1;
+  int ncol;
+  const unsigned short* mask;
+  int off[kDiaMax];
+};
+
+inline DiaArgs dia_args(const sk_matrix_s* A, i64 r0, i64 r1) {
+  DiaArgs g{};
+  g.n = A->csr.dia_n;
+  g.r0 = static_cast<int>(r0);
+  g.r1 = static_cast<int>(r1);
+  g.ncol = static_cast<int>(A->ncol);
+  g.mask = A->csr.dia_mask;
+  for (int d = 0; d < kDiaMax; ++d) g.off[d] = A->csr.dia_off[d];
+  return g;
+}
+
+template <typename T, class Epi, int MINB>
+__global__ void __launch_bounds__(kThreads, MINB)
+dia_spmv_kernel(DiaArgs g, const T* __restrict__ va, const T* __restrict__ x, Epi epi, RedWs ws,
+                const Scalars* sc) {
+  constexpr int NR = Epi::kNR;
+  if (solve_done(sc)) return;
+  double red[NR > 0 ? NR : 1];
+#pragma unroll
+  for (int j = 0; j < (NR > 0 ? NR : 1); ++j) red[j] = 0.0;
+  for (int i = g.r0 + blockIdx.x * kThreads + threadIdx.x; i < g.r1; i += gridDim.x * kThreads) {
+    const unsigned m = __ldcs(g.mask + i);
+    const T* vs = va + static_cast<long long>(i >> 5) * (32 * g.n) + (i & 31);
+    // groups of G diagonals: the loads of a group are issued together
+    constexpr int G = sizeof(T) == 8 ? 2 : 4;
+    T sum = T(0);
+#pragma unroll
+    for (int d0 = 0; d0 < kDiaMax; d0 += G) {
+      if (d0 >= g.n) break;
+      T v[G], xv[G];
+#pragma unroll
+      for (int j = 0; j < G; ++j)
+        if (d0 + j < g.n) {
+          v[j] = __ldcs(vs + 32 * (d0 + j));
+          xv[j] = __ldg(x + min(max(i + g.off[d0 + j], 0), g.ncol - 1));
+        }
+#pragma unroll
+      for (int j = 0; j < G; ++j)
+        if (d0 + j < g.n && ((m >> (d0 + j)) & 1u)) sum = add(sum, mul(v[j], xv[j]));
+    }
+    epi(i, sum, red);
+  }
+  if constexpr (NR > 0) {
+    grid_reduce<NR>(red, ws, [&](const double* t) { epi.finalize(t); });
+  }
+}
+
+// ------------------------------------------------------------------
 // ELLPACK (slot-major): one thread per row, sequential over its slots,
 // stopping at the row's length (the reference stops at the first -1).
 // ------------------------------------------------------------------
@@ -548,7 +614,7 @@ bsr_sell_kernel(int nrow, int ncol, int nbr, int nbr_trunc, const int* __restric
 // Grid size of the SpMV launch for a handle (for sizing RedWs).
 inline int spmv_grid(const sk_matrix_s* A) {
   switch (A->format) {
-    case SK_CSR: return A->csr.sell ? ceil_div(A->nrow, kThreads) : A->csr.nparts;
+    case SK_CSR: return A->csr.sell || A->csr.dia_n ? ceil_div(A->nrow, kThreads) : A->csr.nparts;
     case SK_BSR: return A->bsr.sell ? ceil_div(A->bsr.nbr, kThreads) : A->bsr.nparts;
     default: return ceil_div(A->nrow, kThreads);
   }
@@ -566,6 +632,9 @@ struct SpmvTune {
   static constexpr int kSellU = sizeof(T) == 8 ? 4 : 8;
   static constexpr bool kSellPred = sizeof(T) != 8;
   static constexpr int kSellMinB = sizeof(T) == 8 ? kMinB : 5;
+  // the diagonal kernel runs the SELL grid at the SELL residency, so that
+  // a fused reduction sums the same rows in the same CTAs (the same bits)
+  static constexpr int kDiaMinB = kSellMinB;
 };
 
 // Grid of a thread-per-row product over `rows` rows: one CTA per 256
@@ -588,6 +657,13 @@ void launch_spmv(const sk_matrix_s* A, const T* x, Epi const& epi, RedWs ws,
   if (A->nrow == 0) return;
   switch (A->format) {
     case SK_CSR: {
+      if (A->csr.dia_n) {
+        const T* v = vals_override ? vals_override : static_cast<const T*>(A->csr.dia_vals);
+        SK_LAUNCH((dia_spmv_kernel<T, Epi, SpmvTune<T, Epi>::kDiaMinB>),
+                  row_grid<Epi>(A, A->nrow, SpmvTune<T, Epi>::kSellMinB), kThreads, 0, st,
+                  dia_args(A, 0, A->nrow), v, x, epi, ws, sc);
+        break;
+      }
       if (A->csr.sell) {
         const T* v = vals_override ? vals_override : static_cast<const T*>(A->csr.sell_vals);
         SK_LAUNCH((sell_spmv_kernel<T, Epi, SpmvTune<T, Epi>::kSellU, SpmvTune<T, Epi>::kSellPred,

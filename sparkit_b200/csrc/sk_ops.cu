@@ -246,7 +246,11 @@ template <typename T>
 static void launch_chunk(const sk_matrix_s* A, const HostPipe& p, int c, const T* x, T* y, cudaStream_t st) {
   using Tune = SpmvTune<T, EpiStore<T>>;
   const i64 r0 = c ? p.row_end[static_cast<size_t>(c) - 1] : 0, r1 = p.row_end[static_cast<size_t>(c)];
-  if (A->csr.sell) {
+  if (A->csr.dia_n) {
+    SK_LAUNCH((dia_spmv_kernel<T, EpiStore<T>, Tune::kDiaMinB>), static_cast<int>(ceil_div(r1 - r0, kThreads)),
+              kThreads, 0, st, dia_args(A, r0, r1), static_cast<const T*>(A->csr.dia_vals), x, EpiStore<T>{y},
+              RedWs{}, nullptr);
+  } else if (A->csr.sell) {
     SK_LAUNCH((sell_spmv_kernel<T, EpiStore<T>, Tune::kSellU, Tune::kSellPred, Tune::kSellMinB>),
               static_cast<int>(ceil_div(r1 - r0, kThreads)), kThreads, 0, st, static_cast<int>(r1 - r0),
               A->csr.sell_off + r0 / 32, A->csr.sell_len + r0, A->csr.sell_col,

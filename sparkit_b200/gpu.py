@@ -157,6 +157,13 @@ class Device_matrix:
     def add_f32_values(self):
         check(lib().sk_matrix_add_f32_values(self.handle))
 
+    def add_diagonals(self):
+        """Adds the diagonal copy of a stencil-pattern CSR handle; False when
+        the pattern does not qualify (the handle is then unchanged)."""
+        built = ctypes.c_int(0)
+        check(lib().sk_matrix_add_diagonals(self.handle, ctypes.byref(built)))
+        return bool(built.value)
+
     def spmv(self, x, y, stream=None):
         """y = A x on device tensors (or raw device pointers)."""
         xs = _ptr(x) if not isinstance(x, int) else ctypes.c_void_p(x)
