@@ -190,7 +190,8 @@ SK_API sk_status sk_matrix_add_f32_values(sk_matrix A);
  * FP32 inner solve of the mixed solver) read it instead of the CSR arrays:
  * no column indices and no gathered x, and each row summed over its stored
  * entries in its CSR order, so the results keep their bits.  The persistent
- * FP32 inner solve keeps reading the SELL-32 copy.
+ * FP32 inner solve of the mixed solver reads it too, at two CTAs per SM
+ * (its dot products then sum in another order than over SELL-32).
  * No reference counterpart: a device layout of Compressed_row_matrix
  * (Compressed_row_matrix.hpp:20-132), as the SELL-32 copy is.  *built is 1
  * when the handle has the copy, 0 when its pattern does not qualify (more

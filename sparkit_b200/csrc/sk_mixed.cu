@@ -5,10 +5,12 @@
 // conjugate gradient (conjugate_gradient.hpp:122-312, Jacobi or identity
 // left preconditioner, true residual only at k = 0) in FP32, exactly as the
 // per-step path of sk_solvers.cu runs it, but without a kernel boundary per
-// step.  One CTA per SM stays resident for the whole solve; each iteration
+// step.  One CTA per SM (two over the diagonal copy) stays resident for
+// the whole solve; each iteration
 // is three phases separated by grid barriers:
 //
-//   A  q = A p (SELL-32 rows, summed in storage order) and <p, q>  -> alpha
+//   A  q = A p (SELL-32 rows, or the rows of the diagonal copy, each summed
+//      in storage order) and <p, q>                               -> alpha
 //   B  d += alpha p, r -= alpha q, <r, r> and <r, D^-1 r>          -> test, beta
 //   C  p = D^-1 r + beta p
 //
@@ -30,7 +32,8 @@
 namespace sk {
 namespace {
 
-constexpr int kPT = 512;   // threads per CTA (one CTA per SM, up to 128 registers)
+constexpr int kPT = 512;   // threads per CTA (SELL: one CTA per SM, up to 128 registers;
+                           // diagonal copy: two CTAs per SM, up to 64)
 constexpr int kPW = kPT / 32;
 constexpr int kPU = 8;     // SELL slots loaded together
 constexpr int kSlot = 4;   // doubles per CTA and reduction
@@ -50,7 +53,10 @@ struct PArgs {
   const int* off;
   const unsigned char* len;
   const int* col;
-  const float* val;
+  const float* val;  // SELL-32 values, or the FP32 values of the diagonal copy
+  int dia_n;         // diagonal copy: diagonals, row masks and offsets
+  const unsigned short* dia_mask;
+  int dia_off[kDiaMax];
   const float* inv_d;
   float* r;
   float* d;
@@ -262,8 +268,69 @@ __device__ __forceinline__ double phase_spmv(PArgs const& a, int t0, int T) {
   return pq;
 }
 
-template <bool JAC>
-__global__ void __launch_bounds__(kPT, 1) inner_cg_kernel(PArgs a) {
+// Phase A over the diagonal copy.  The values of a warp's rows for one
+// diagonal are one 32-value segment and the reads of p at row + off[d] are
+// contiguous, so no load depends on another: each thread issues the value
+// and p loads of kDiaRows rows for kDiaGroup diagonals at a time without
+// waiting for the rows' masks (a diagonal a row does not store reads a zero
+// value and a clamped p, and the mask leaves both out of the sum).  The
+// kernel runs 2 CTAs per SM here (this phase needs few registers), which
+// hides the load latency better than the deeper register pipeline of the
+// SELL phase at one CTA per SM.  Each row is summed from 0 over its stored
+// diagonals in ascending column order (its CSR order).  Returns this
+// thread's share of <p, q>.
+constexpr int kDiaRows = 2;
+constexpr int kDiaGroup = 4;
+
+__device__ __forceinline__ double phase_spmv_dia(PArgs const& a, int t0, int T) {
+  constexpr int R = kDiaRows, C = kDiaGroup;
+  double pq = 0.0;
+  const int last = a.n - 1;
+  const long long sl = 32 * a.dia_n;
+  for (int i = t0; i < a.n; i += R * T) {
+    unsigned m[R];
+    float s[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const int row = i + r * T;
+      m[r] = row < a.n ? __ldcs(a.dia_mask + row) : 0u;
+      s[r] = 0.0f;
+    }
+#pragma unroll
+    for (int d0 = 0; d0 < kDiaMax; d0 += C) {
+      if (d0 >= a.dia_n) break;
+      float v[R][C], g[R][C];
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        const int row = min(i + r * T, last);
+        const float* vs = a.val + (row >> 5) * sl + (row & 31);
+#pragma unroll
+        for (int j = 0; j < C; ++j)
+          if (d0 + j < a.dia_n) {
+            v[r][j] = __ldcs(vs + 32 * (d0 + j));
+            g[r][j] = a.p[min(max(row + a.dia_off[d0 + j], 0), last)];
+          }
+      }
+#pragma unroll
+      for (int r = 0; r < R; ++r)
+#pragma unroll
+        for (int j = 0; j < C; ++j)
+          if (d0 + j < a.dia_n && ((m[r] >> (d0 + j)) & 1u)) s[r] = add(s[r], mul(v[r][j], g[r][j]));
+    }
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const int row = i + r * T;
+      if (row < a.n) {
+        a.q[row] = s[r];
+        pq += static_cast<double>(mul(a.p[row], s[r]));
+      }
+    }
+  }
+  return pq;
+}
+
+template <bool JAC, bool DIA>
+__global__ void __launch_bounds__(kPT, DIA ? 2 : 1) inner_cg_kernel(PArgs a) {
   const int n = a.n;
   const int T = gridDim.x * kPT;
   const int t0 = blockIdx.x * kPT + threadIdx.x;
@@ -298,7 +365,9 @@ __global__ void __launch_bounds__(kPT, 1) inner_cg_kernel(PArgs a) {
   if (bnorm == 0.0f) conv = 1;
   while (!conv && it < a.max_iters) {
     // A: compute_step_size (:233-239)
-    double pq[1] = {phase_spmv(a, t0, T)};
+    double pq[1];
+    if constexpr (DIA) pq[0] = phase_spmv_dia(a, t0, T);
+    else pq[0] = phase_spmv(a, t0, T);
     if (!grid_allreduce<1>(pq, a, 1, epoch)) return;
     const float alpha = rz / static_cast<float>(pq[0]);
     // B: compute_new_solution, compute_new_residual, is_converged
@@ -376,9 +445,15 @@ __global__ void __launch_bounds__(kPT, 1) inner_cg_kernel(PArgs a) {
   }
 }
 
-const void* pick_kernel(bool jac) {
-  return jac ? reinterpret_cast<const void*>(&inner_cg_kernel<true>)
-             : reinterpret_cast<const void*>(&inner_cg_kernel<false>);
+// The handle's diagonal copy when it has FP32 values, else its SELL copy.
+bool use_dia(sk_matrix A) { return A->csr.dia_n > 0 && A->csr.dia_vals32; }
+
+const void* pick_kernel(bool jac, bool dia) {
+  if (dia)
+    return jac ? reinterpret_cast<const void*>(&inner_cg_kernel<true, true>)
+               : reinterpret_cast<const void*>(&inner_cg_kernel<false, true>);
+  return jac ? reinterpret_cast<const void*>(&inner_cg_kernel<true, false>)
+             : reinterpret_cast<const void*>(&inner_cg_kernel<false, false>);
 }
 
 // CTAs of the cooperative grid (0: the kernel does not fit).
@@ -394,26 +469,29 @@ int coop_grid(sk_matrix A, const void* k) {
 }  // namespace
 
 bool inner_persistent_ok(sk_matrix A) {
-  if (!A || A->format != SK_CSR || !A->csr.sell || !A->csr.sell_vals32 || A->nrow <= 0) return false;
+  if (!A || A->format != SK_CSR || A->nrow <= 0) return false;
+  if (!use_dia(A) && !(A->csr.sell && A->csr.sell_vals32)) return false;
   if (A->nrow > INT_MAX / 4) return false;
   int coop = 0;
   if (cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, A->device) != cudaSuccess || !coop) return false;
-  return coop_grid(A, pick_kernel(true)) > 0 && coop_grid(A, pick_kernel(false)) > 0;
+  return coop_grid(A, pick_kernel(true, use_dia(A))) > 0 && coop_grid(A, pick_kernel(false, use_dia(A))) > 0;
 }
 
 size_t inner_persistent_scratch(sk_matrix A) {
-  return sizeof(SyncWords) + static_cast<size_t>(2) * 2 * A->sm_count * kSlot * sizeof(double) + 256;
+  return sizeof(SyncWords) + static_cast<size_t>(2) * kPT * kSlot * sizeof(double) + 256;
 }
 
 sk_status inner_cg_persistent(sk_matrix A, const float* inv_d, float* r, float* d, float* p, float* q,
                               void* scratch, double tol, long long max_iters, cudaStream_t st,
                               InnerResult* out) {
   *out = InnerResult{};
-  SK_CHECK(inner_persistent_ok(A), SK_NOT_SUPPORTED, "persistent inner solve needs a SELL CSR handle with FP32 values");
-  const void* k = pick_kernel(inv_d != nullptr);
+  SK_CHECK(inner_persistent_ok(A), SK_NOT_SUPPORTED,
+           "persistent inner solve needs a CSR handle with FP32 SELL values or an FP32 diagonal copy");
+  const bool dia = use_dia(A);
+  const void* k = pick_kernel(inv_d != nullptr, dia);
   int grid = coop_grid(A, k);
   SK_CHECK(grid > 0, SK_NOT_SUPPORTED, "persistent inner solve does not fit on the device");
-  grid = std::min(std::min(grid, 2 * A->sm_count), kPT);  // a CTA sums the grid's slots one per thread
+  grid = std::min(grid, kPT);  // a CTA sums the grid's slots one per thread  // a CTA sums the grid's slots one per thread
   const int need = ceil_div(A->nrow, kPT);
   if (grid > need) grid = need;
   SyncWords* sync = static_cast<SyncWords*>(scratch);
@@ -421,10 +499,17 @@ sk_status inner_cg_persistent(sk_matrix A, const float* inv_d, float* r, float* 
   SK_CUDA(cudaMemsetAsync(sync, 0, sizeof(SyncWords), st));
   PArgs a{};
   a.n = static_cast<int>(A->nrow);
-  a.off = A->csr.sell_off;
-  a.len = A->csr.sell_len;
-  a.col = A->csr.sell_col;
-  a.val = A->csr.sell_vals32;
+  if (dia) {
+    a.val = A->csr.dia_vals32;
+    a.dia_n = A->csr.dia_n;
+    a.dia_mask = A->csr.dia_mask;
+    for (int d = 0; d < kDiaMax; ++d) a.dia_off[d] = A->csr.dia_off[d];
+  } else {
+    a.off = A->csr.sell_off;
+    a.len = A->csr.sell_len;
+    a.col = A->csr.sell_col;
+    a.val = A->csr.sell_vals32;
+  }
   a.inv_d = inv_d;
   a.r = r;
   a.d = d;
