@@ -54,6 +54,8 @@ def parse():
                    help="run 20 FP64 and 20 FP32 CG iterations on the GRF diffusion matrix (for ncu launch lists)")
     p.add_argument("--profile-learned", action="store_true",
                    help="apply the (untrained) learned preconditioner on 512^2 four times, for ncu")
+    p.add_argument("--profile-mixed-diagonals", action="store_true",
+                   help="the --profile-mixed run on a handle with its diagonal copy")
     p.add_argument("--profile-mixed", action="store_true",
                    help="one mixed solve with 100 persistent FP32 inner iterations on the 128^3 GRF problem, for ncu")
     p.add_argument("--no-convert", action="store_true")
@@ -901,16 +903,18 @@ def profile_learned(grid=512, applies=4):
     return 0
 
 
-def profile_mixed(grid, inner=100):
+def profile_mixed(grid, inner=100, diagonals=False):
     """One outer step of the mixed solver on the GRF diffusion problem with
     `inner` persistent FP32 inner iterations, twice (warm-up, then the
-    captured one)."""
+    captured one); with `diagonals`, on a handle carrying its diagonal copy."""
     import torch
 
     from sparkit_b200 import gpu, matgen
     torch.cuda.set_device(0)
     G = matgen.diffusion_3d_grf(grid, sigma=2.0, corr_len=8.0, seed=0)
     Gd = gpu.Device_matrix(G)
+    if diagonals:
+        assert Gd.add_diagonals()
     Gd.add_f32_values()
     b = torch.from_numpy(matgen.uniform_vector(G.shape()[0], seed=0)).cuda()
     for _ in range(2):
@@ -956,6 +960,8 @@ def main():
         return profile_learned()
     if args.profile_mixed:
         return profile_mixed(args.grid)
+    if args.profile_mixed_diagonals:
+        return profile_mixed(args.grid, diagonals=True)
     import torch
     world, rank, local = dist_setup()
     if world > 1:
