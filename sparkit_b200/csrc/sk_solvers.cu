@@ -15,6 +15,7 @@
 #include <map>
 #include <vector>
 
+#include "sk_arnoldi.cuh"
 #include "sk_learned.cuh"
 #include "sk_vec.cuh"
 #include "sk_mixed.cuh"
@@ -1007,7 +1008,10 @@ static sk_status fgmres_solve(sk_matrix A, sk_precond M, const T* b, T* x,
   std::vector<char*> vv;
   char* extra = nullptr;
   const i64 hist_cap = cfg->collect_residuals ? cfg->max_iterations : 0;
-  sk_status s = carve_common(A, st, 0, 0, static_cast<size_t>(nvecs) * ldv * sizeof(T) + small_bytes + 512,
+  // the Arnoldi step's barrier words and reduction slots (2 x grid <= 2 x 512)
+  const size_t arn_bytes = 256 + 2 * 512 * sizeof(double);
+  sk_status s = carve_common(A, st, 0, 0,
+                             static_cast<size_t>(nvecs) * ldv * sizeof(T) + small_bytes + arn_bytes + 1024,
                              hist_cap, &c, &vv, &extra);
   if (s != SK_OK) return s;
   T* V = reinterpret_cast<T*>(extra);
@@ -1022,6 +1026,15 @@ static sk_status fgmres_solve(sk_matrix A, sk_precond M, const T* b, T* x,
   sm.y = sm.g + (m + 2);
   sm.zero = sm.y + (m + 2);
   if (general_left) gl.tmp = V + ((m + 1) + (alias_z ? 0 : m)) * ldv;  // after V and Z
+  // Modified Gram-Schmidt of each Arnoldi step as one cooperative launch
+  // when w fits on chip (sk_arnoldi.cu), else one launch per basis vector.
+  ArnoldiPlan aplan;
+  const bool arnoldi_fused = arnoldi_plan<T>(A, n, &aplan);
+  auto* arn_sync = reinterpret_cast<ArnoldiSync*>(
+      (reinterpret_cast<uintptr_t>(smallp) + small_bytes + 255) & ~uintptr_t(255));
+  double* arn_slots = reinterpret_cast<double*>(reinterpret_cast<char*>(arn_sync) + 256);
+  sk_status arn_status = SK_OK;
+  if (arnoldi_fused) SK_CUDA(cudaMemsetAsync(arn_sync, 0, sizeof(ArnoldiSync), st));
   *out = sk_summary{};
   double bnorm = 0;
   if ((s = norm_b<T>(b, n, c, st, &bnorm)) != SK_OK) return s;
@@ -1063,12 +1076,18 @@ static sk_status fgmres_solve(sk_matrix A, sk_precond M, const T* b, T* x,
       } else {
         launch_spmv<T>(A, Zj, EpiFgW<T>{Vj1, V, sm.H + j * um1, gl.linv}, c.ws, c.sc, q);
       }
-      for (int i = 0; i <= j; ++i) {
-        const T* vnext = i < j ? V + (i + 1) * ldv : nullptr;
-        launch_vec(n, OpFgMgs<T>{Vj1, V + i * ldv, vnext, sm.H + i + j * um1, sm.H + (i + 1) + j * um1, T(0)},
-                   c.ws, c.sc, q);
+      if (arnoldi_fused) {
+        const sk_status as = arnoldi_launch<T>(
+            aplan, ArnoldiArgs<T>{n, Vj1, V, ldv, j, sm.H + j * um1, gl.divide, c.sc, arn_sync, arn_slots, 0}, q);
+        if (as != SK_OK && arn_status == SK_OK) arn_status = as;
+      } else {
+        for (int i = 0; i <= j; ++i) {
+          const T* vnext = i < j ? V + (i + 1) * ldv : nullptr;
+          launch_vec(n, OpFgMgs<T>{Vj1, V + i * ldv, vnext, sm.H + i + j * um1, sm.H + (i + 1) + j * um1, T(0)},
+                     c.ws, c.sc, q);
+        }
+        launch_vec(n, OpFgScale<T>{Vj1, sm.H + (j + 1) + j * um1, T(0), gl.divide}, c.ws, c.sc, q);
       }
-      launch_vec(n, OpFgScale<T>{Vj1, sm.H + (j + 1) + j * um1, T(0), gl.divide}, c.ws, c.sc, q);
       g_launches.fetch_add(1, std::memory_order_relaxed);
       scalar_kernel<<<1, 1, 0, q>>>(FgGivens<T>{c.sc, c.hist, sm, j, m});
     }
@@ -1133,13 +1152,21 @@ static sk_status fgmres_solve(sk_matrix A, sk_precond M, const T* b, T* x,
       enqueue_cycle(gs, m_eff, M);
     }
     cudaError_t le = cudaGetLastError();
-    if (le != cudaSuccess) {
+    if (le != cudaSuccess || arn_status != SK_OK) {
       drop_graphs();
-      return cuda_fail(le, "FGMRES cycle");
+      return le != cudaSuccess ? cuda_fail(le, "FGMRES cycle") : arn_status;
     }
     if ((s = read_scalars(c.sc, &h, gs)) != SK_OK) {
       drop_graphs();
       return s;
+    }
+    if (arnoldi_fused) {
+      int err = 0;
+      SK_CUDA(cudaMemcpy(&err, &arn_sync->err, sizeof(int), cudaMemcpyDeviceToHost));
+      if (err) {
+        drop_graphs();
+        return fail(SK_TIMEOUT, "FGMRES Arnoldi step: a grid barrier wait ran out");
+      }
     }
     ++cycle;
     if (fallback && M != fallback && !h.converged && h.rnorm > stall_ratio * h.beta_cycle) {
