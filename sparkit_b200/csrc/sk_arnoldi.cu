@@ -113,7 +113,6 @@ __global__ void __launch_bounds__(kAT, 1) arnoldi_mgs_kernel(ArnoldiArgs<T> a) {
   const i64 r0 = static_cast<i64>(blockIdx.x) * a.rows_per_cta;
   const i64 r1 = a.n < r0 + a.rows_per_cta ? a.n : r0 + a.rows_per_cta;
   const int cnt = r1 > r0 ? static_cast<int>(r1 - r0) : 0;
-#pragma unroll 8
   for (int k = threadIdx.x; k < cnt; k += kAT) wt[k] = a.w[r0 + k];
   __syncthreads();
   unsigned epoch = 0;
@@ -124,9 +123,6 @@ __global__ void __launch_bounds__(kAT, 1) arnoldi_mgs_kernel(ArnoldiArgs<T> a) {
     const T* vi = a.V + static_cast<i64>(i) * a.ldv + r0;
     const T* vn = i < a.j ? a.V + static_cast<i64>(i + 1) * a.ldv + r0 : nullptr;
     double red = 0.0;
-    // unrolled so that a thread's loads of several rows are in flight
-    // together; the terms still enter red in row order
-#pragma unroll 8
     for (int k = threadIdx.x; k < cnt; k += kAT) {
       const T wk = sub(wt[k], mul(h, vi[k]));
       wt[k] = wk;
