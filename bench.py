@@ -54,6 +54,8 @@ def parse():
                    help="run 20 FP64 and 20 FP32 CG iterations on the GRF diffusion matrix (for ncu launch lists)")
     p.add_argument("--profile-learned", action="store_true",
                    help="apply the (untrained) learned preconditioner on 512^2 four times, for ncu")
+    p.add_argument("--profile-gmres", action="store_true",
+                   help="40 iterations of GMRES(30) on the 1024^2 convection-diffusion problem (for ncu)")
     p.add_argument("--profile-mixed-diagonals", action="store_true",
                    help="the --profile-mixed run on a handle with its diagonal copy")
     p.add_argument("--profile-mixed", action="store_true",
@@ -925,6 +927,23 @@ def profile_mixed(grid, inner=100, diagonals=False):
     return 0
 
 
+def profile_gmres(grid=1024, iters=40):
+    """A short Jacobi-left GMRES(30) on the grid^2 upwind convection-diffusion
+    problem (`iters` iterations, too few for the cycle to be captured as a
+    CUDA graph), for a capture of the Arnoldi step's kernel."""
+    import torch
+
+    from sparkit_b200 import gpu, matgen
+    torch.cuda.set_device(0)
+    A = matgen.convection_diffusion_2d(grid, grid, 1.0, 0.9, 0.5)
+    n = A.shape()[0]
+    Ad = gpu.Device_matrix(A)
+    b = matgen.uniform_vector(n, seed=2)
+    s = gpu.gmres(b, np.zeros(n), gpu.Gmres_config(1e-10, 30, iters), gpu.spmv(Ad), left=gpu.jacobi(Ad))
+    assert s.computed_iterations == iters
+    return 0
+
+
 def profile_solvers(grid):
     """A short plain FP64 Jacobi-CG (20 iterations) and a short mixed solve
     (one outer step of 20 FP32 iterations) for per-kernel launch lists."""
@@ -962,6 +981,8 @@ def main():
         return profile_mixed(args.grid)
     if args.profile_mixed_diagonals:
         return profile_mixed(args.grid, diagonals=True)
+    if args.profile_gmres:
+        return profile_gmres()
     import torch
     world, rank, local = dist_setup()
     if world > 1:
