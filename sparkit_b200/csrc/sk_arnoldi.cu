@@ -20,7 +20,7 @@
 namespace sk {
 namespace {
 
-constexpr int kAT = 512;  // threads per CTA (one CTA per SM)
+constexpr int kAT = 512;  // threads per CTA (two CTAs per SM where w fits)
 constexpr int kAW = kAT / 32;
 constexpr unsigned long long kArnWaitNs = 2000000000ull;  // 2 s per barrier wait
 
@@ -106,7 +106,7 @@ __device__ bool arn_allreduce(double& v, double* slots, int set, ArnoldiSync* s,
 }
 
 template <typename T>
-__global__ void __launch_bounds__(kAT, 1) arnoldi_mgs_kernel(ArnoldiArgs<T> a) {
+__global__ void __launch_bounds__(kAT, 2) arnoldi_mgs_kernel(ArnoldiArgs<T> a) {
   extern __shared__ __align__(16) unsigned char arn_smem[];
   T* wt = reinterpret_cast<T*>(arn_smem);
   if (solve_done(a.sc)) return;  // the same flag for every CTA
@@ -151,24 +151,29 @@ int arnoldi_grid(const sk_matrix_s* A, i64 n, size_t* smem_out, i64* rows_out) {
   if (cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, A->device) != cudaSuccess || !coop) return 0;
   int optin = 0;
   if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, A->device) != cudaSuccess) return 0;
-  int grid = std::min<i64>(A->sm_count, (n + kAT - 1) / kAT);
-  const i64 rows = (n + grid - 1) / grid;
-  const size_t smem = static_cast<size_t>(rows) * sizeof(T);
-  if (smem + 2048 > static_cast<size_t>(optin)) return 0;  // w does not fit on chip
-  if (cudaFuncSetAttribute(arnoldi_mgs_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           static_cast<int>(smem)) != cudaSuccess) {
-    cudaGetLastError();
-    return 0;
+  // two CTAs per SM when both fit (twice the warps and half the rows per
+  // thread to hide the loads of each basis vector), else one
+  for (int per : {2, 1}) {
+    const int grid = static_cast<int>(std::min<i64>(static_cast<i64>(per) * A->sm_count, (n + kAT - 1) / kAT));
+    const i64 rows = (n + grid - 1) / grid;
+    const size_t smem = static_cast<size_t>(rows) * sizeof(T);
+    if (smem + 2048 > static_cast<size_t>(optin) || grid > kAT) continue;  // w does not fit on chip
+    if (cudaFuncSetAttribute(arnoldi_mgs_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             static_cast<int>(smem)) != cudaSuccess) {
+      cudaGetLastError();
+      continue;
+    }
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, arnoldi_mgs_kernel<T>, kAT, smem) != cudaSuccess) {
+      cudaGetLastError();
+      continue;
+    }
+    if (per_sm < 1 || grid > per_sm * A->sm_count) continue;
+    *smem_out = smem;
+    *rows_out = rows;
+    return grid;
   }
-  int per_sm = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, arnoldi_mgs_kernel<T>, kAT, smem) != cudaSuccess) {
-    cudaGetLastError();
-    return 0;
-  }
-  if (per_sm < 1 || grid > per_sm * A->sm_count || grid > kAT) return 0;
-  *smem_out = smem;
-  *rows_out = rows;
-  return grid;
+  return 0;
 }
 
 }  // namespace
