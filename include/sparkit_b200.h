@@ -70,6 +70,17 @@ SK_API sk_status sk_device_count(int* count);
 /* Count of this library's kernel launches since load (for accounting). */
 SK_API sk_status sk_launch_count(int64_t* count);
 
+/* No reference counterpart: a setting for tests of the timeout path.  The
+ * persistent kernels (the mixed solver's inner CG, the GMRES / FGMRES
+ * Arnoldi step) wait at grid barriers, and every wait is bounded in time:
+ * when it runs out the kernel returns and the call reports SK_TIMEOUT.
+ * limit_ns sets that bound for launches made after this call (0 restores
+ * the default of 2 s; at most 10 s).  unmeetable != 0 makes every barrier
+ * of those launches wait for one arrival more than the grid makes, so that
+ * the first wait runs out on an ordinary, correct solve.  Process-wide;
+ * sk_debug_set_wait(0, 0) restores the defaults. */
+SK_API sk_status sk_debug_set_wait(uint64_t limit_ns, int32_t unmeetable);
+
 /* Device memory helpers, so that a C/C++ caller needs no CUDA headers. */
 SK_API sk_status sk_device_alloc(void** dev, size_t bytes);
 SK_API sk_status sk_device_free(void* dev);
@@ -343,15 +354,16 @@ SK_API sk_status sk_precond_destroy(sk_precond M);
 /* No reference counterpart: an addition of this library.  The Chebyshev
  * apply z = p(A) r of sk_precond_apply, for callers that cannot allocate
  * device memory when they apply the preconditioner (a callback inside
- * another solver's loop with its memory reserved up front, or a stream being
- * captured into a CUDA graph).  It takes the parameters of
+ * another solver library's loop, where that library reserved all device
+ * memory up front).  It takes the parameters of
  * sk_chebyshev_create directly and keeps its two work vectors in a static
  * device array instead of allocating them: A is a square CSR handle of at
  * most 1,048,576 rows (larger ones fail with SK_INVALID_ARG), degree is at
  * most 64, and every GPU that runs it holds that 16 MiB array until the
  * process exits.  Calls share the array, so calls that overlap on the GPU
- * race; serialize them.  The first call on a device looks the array up and
- * should come before any stream capture.  Results are identical to
+ * race; serialize them.  Every call looks the array's device address up;
+ * the first call on a device may load the module to do so and should come
+ * before any stream capture.  Results are identical to
  * sk_precond_apply with a preconditioner from sk_chebyshev_create. */
 SK_API sk_status sk_chebyshev_apply_noalloc(sk_matrix A, double lambda_min,
                                             double lambda_max, int64_t degree,

@@ -22,7 +22,6 @@ namespace {
 
 constexpr int kAT = 512;  // threads per CTA (two CTAs per SM where w fits)
 constexpr int kAW = kAT / 32;
-constexpr unsigned long long kArnWaitNs = 2000000000ull;  // 2 s per barrier wait
 
 __device__ __forceinline__ unsigned long long arn_ld_acquire(const unsigned long long* p) {
   unsigned long long v;
@@ -37,15 +36,16 @@ __device__ __forceinline__ unsigned long long arn_now_ns() {
 }
 
 // Barrier number `epoch` (from 1) of this launch: passed when the arrival
-// counter reaches epoch * gridDim.x.  False when a wait ran out here or in
-// another CTA (the error word is set); the caller then returns.
-__device__ bool arn_barrier(ArnoldiSync* s, unsigned& epoch) {
+// counter reaches epoch * gridDim.x (+ bias, which only the timeout tests
+// set).  False when a wait ran out here or in another CTA (the error word
+// is set); the caller then returns.
+__device__ bool arn_barrier(ArnoldiSync* s, unsigned& epoch, unsigned long long wait_ns, unsigned bias) {
   __shared__ int s_ok;
   __syncthreads();
   if (threadIdx.x == 0) {
     int ok = 1;
     epoch += 1;
-    const unsigned long long target = static_cast<unsigned long long>(epoch) * gridDim.x;
+    const unsigned long long target = static_cast<unsigned long long>(epoch) * gridDim.x + bias;
     asm volatile("fence.acq_rel.gpu;\n\tred.relaxed.gpu.global.add.u64 [%0], 1;" ::"l"(&s->arrived) : "memory");
     unsigned long long t0 = 0;
     for (unsigned spins = 0; arn_ld_acquire(&s->arrived) < target; ++spins) {
@@ -57,7 +57,7 @@ __device__ bool arn_barrier(ArnoldiSync* s, unsigned& epoch) {
         const unsigned long long t = arn_now_ns();
         if (t0 == 0) {
           t0 = t;
-        } else if (t - t0 > kArnWaitNs) {
+        } else if (t - t0 > wait_ns) {
           atomicExch(&s->err, 1);
           ok = 0;
           break;
@@ -79,7 +79,8 @@ __device__ __forceinline__ double arn_warp_sum(double v) {
 // The grid-wide sum of v, the same bits in every thread of every CTA: a
 // block tree, one slot per CTA, a barrier, then every CTA sums the slots in
 // CTA order with the same tree.  Consecutive sums alternate slot sets.
-__device__ bool arn_allreduce(double& v, double* slots, int set, ArnoldiSync* s, unsigned& epoch) {
+__device__ bool arn_allreduce(double& v, double* slots, int set, ArnoldiSync* s, unsigned& epoch,
+                              unsigned long long wait_ns, unsigned bias) {
   __shared__ double s_part[kAW];
   __shared__ double s_tot;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -91,7 +92,7 @@ __device__ bool arn_allreduce(double& v, double* slots, int set, ArnoldiSync* s,
     double t = arn_warp_sum(lane < kAW ? s_part[lane] : 0.0);
     if (lane == 0) slot[blockIdx.x] = t;
   }
-  if (!arn_barrier(s, epoch)) return false;
+  if (!arn_barrier(s, epoch, wait_ns, bias)) return false;
   double t = threadIdx.x < gridDim.x ? __ldcg(slot + threadIdx.x) : 0.0;
   t = arn_warp_sum(t);
   if (lane == 0) s_part[warp] = t;
@@ -128,7 +129,7 @@ __global__ void __launch_bounds__(kAT, 2) arnoldi_mgs_kernel(ArnoldiArgs<T> a) {
       wt[k] = wk;
       red += static_cast<double>(mul(vn ? vn[k] : wk, wk));
     }
-    if (!arn_allreduce(red, a.slots, i & 1, a.sync, epoch)) return;
+    if (!arn_allreduce(red, a.slots, i & 1, a.sync, epoch, a.wait_ns, a.bias)) return;
     const T d = static_cast<T>(red);
     const T hn = vn ? d : sqrt(d);
     hd = static_cast<double>(hn);
@@ -158,8 +159,11 @@ int arnoldi_grid(const sk_matrix_s* A, i64 n, size_t* smem_out, i64* rows_out) {
     const i64 rows = (n + grid - 1) / grid;
     const size_t smem = static_cast<size_t>(rows) * sizeof(T);
     if (smem + 2048 > static_cast<size_t>(optin) || grid > kAT) continue;  // w does not fit on chip
+    // The attribute is process-wide: it is always set to the largest size
+    // any plan can use, so a plan made on another thread never lowers it
+    // below this plan's size between this call and the launch.
     if (cudaFuncSetAttribute(arnoldi_mgs_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             static_cast<int>(smem)) != cudaSuccess) {
+                             optin - 2048) != cudaSuccess) {
       cudaGetLastError();
       continue;
     }
@@ -188,6 +192,8 @@ bool arnoldi_plan(const sk_matrix_s* A, i64 n, ArnoldiPlan* p) {
 template <typename T>
 sk_status arnoldi_launch(const ArnoldiPlan& p, ArnoldiArgs<T> a, cudaStream_t st) {
   a.rows_per_cta = p.rows_per_cta;
+  a.wait_ns = wait_limit_ns();
+  a.bias = wait_target_bias();
   // the step's barriers count from 0; the error word stays for the solve
   SK_CUDA(cudaMemsetAsync(&a.sync->arrived, 0, sizeof(unsigned long long), st));
   cudaLaunchConfig_t cfg{};

@@ -29,7 +29,9 @@ struct ArnoldiArgs {
   const Scalars* sc;
   ArnoldiSync* sync;
   double* slots;
-  i64 rows_per_cta;  // set by arnoldi_launch
+  i64 rows_per_cta;             // set by arnoldi_launch
+  unsigned long long wait_ns;   // bound of each barrier wait, set by arnoldi_launch
+  unsigned bias;                // extra arrivals a barrier waits for (timeout tests)
 };
 
 struct ArnoldiPlan {

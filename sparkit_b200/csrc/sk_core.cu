@@ -10,6 +10,12 @@
 namespace sk {
 
 std::atomic<i64> g_launches{0};
+
+constexpr unsigned long long kDefaultWaitNs = 2000000000ull;  // 2 s per barrier wait
+static std::atomic<unsigned long long> g_wait_ns{kDefaultWaitNs};
+static std::atomic<unsigned> g_wait_bias{0};
+unsigned long long wait_limit_ns() { return g_wait_ns.load(std::memory_order_relaxed); }
+unsigned wait_target_bias() { return g_wait_bias.load(std::memory_order_relaxed); }
 static thread_local std::string t_last_error;
 
 void set_error(std::string const& msg) { t_last_error = msg; }
@@ -413,6 +419,13 @@ sk_status sk_device_count(int* count) {
 sk_status sk_launch_count(int64_t* count) {
   SK_CHECK(count, SK_INVALID_ARG, "null count");
   *count = g_launches.load();
+  return SK_OK;
+}
+
+sk_status sk_debug_set_wait(uint64_t limit_ns, int32_t unmeetable) {
+  SK_CHECK(limit_ns <= 10000000000ull, SK_INVALID_ARG, "wait limit above 10 s");
+  g_wait_ns.store(limit_ns ? limit_ns : kDefaultWaitNs);
+  g_wait_bias.store(unmeetable ? 1u : 0u);
   return SK_OK;
 }
 

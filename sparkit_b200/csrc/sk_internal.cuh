@@ -43,6 +43,12 @@ sk_status cuda_fail(cudaError_t e, char const* what);
     if (!(cond)) return ::sk::fail((st), (msg));                         \
   } while (0)
 
+// Bound of every grid-barrier wait of the persistent kernels, in ns, and the
+// extra arrivals each barrier waits for (0, or 1 when sk_debug_set_wait
+// makes the barriers unmeetable to test the timeout path).
+unsigned long long wait_limit_ns();
+unsigned wait_target_bias();
+
 // Every kernel launch of the library goes through SK_LAUNCH so that
 // sk_launch_count() can account for them.
 extern std::atomic<i64> g_launches;

@@ -37,7 +37,6 @@ constexpr int kPT = 512;   // threads per CTA (SELL: one CTA per SM, up to 128 r
 constexpr int kPW = kPT / 32;
 constexpr int kPU = 8;     // SELL slots loaded together
 constexpr int kSlot = 4;   // doubles per CTA and reduction
-constexpr unsigned long long kWaitNs = 2000000000ull;  // 2 s per barrier wait
 
 struct SyncWords {
   unsigned long long arrived;  // total arrivals, never reset during a solve
@@ -66,6 +65,8 @@ struct PArgs {
   SyncWords* sync;
   float tol;
   long long max_iters;
+  unsigned long long wait_ns;  // bound of each barrier wait
+  unsigned bias;               // extra arrivals a barrier waits for (timeout tests)
 };
 
 __device__ __forceinline__ unsigned long long ld_acquire(const unsigned long long* p) {
@@ -86,16 +87,17 @@ __device__ __forceinline__ unsigned long long global_ns() {
 }
 
 // Grid barrier on one monotonic arrival counter: barrier number e (from 1)
-// is passed when the counter reaches e * gridDim.x.  False: a wait ran out
-// (here or in another CTA) and the kernel must return.  The clock and the
-// error word are read once per 256 polls.
-__device__ bool grid_barrier(SyncWords* s, unsigned& epoch) {
+// is passed when the counter reaches e * gridDim.x (+ bias, which only the
+// timeout tests set).  False: a wait ran out (here or in another CTA) and
+// the kernel must return.  The clock and the error word are read once per
+// 256 polls.
+__device__ bool grid_barrier(SyncWords* s, unsigned& epoch, unsigned long long wait_ns, unsigned bias) {
   __shared__ int s_ok;
   __syncthreads();
   if (threadIdx.x == 0) {
     int ok = 1;
     epoch += 1;
-    const unsigned long long target = static_cast<unsigned long long>(epoch) * gridDim.x;
+    const unsigned long long target = static_cast<unsigned long long>(epoch) * gridDim.x + bias;
     arrive_release(&s->arrived);
     unsigned long long t0 = 0;
     for (unsigned spins = 0; ld_acquire(&s->arrived) < target; ++spins) {
@@ -107,7 +109,7 @@ __device__ bool grid_barrier(SyncWords* s, unsigned& epoch) {
         const unsigned long long t = global_ns();
         if (t0 == 0) {
           t0 = t;
-        } else if (t - t0 > kWaitNs) {
+        } else if (t - t0 > wait_ns) {
           atomicExch(&s->err, 1);
           ok = 0;
           break;
@@ -143,7 +145,7 @@ __device__ __forceinline__ bool grid_allreduce(double (&v)[NR], PArgs const& a, 
 #pragma unroll
       for (int j = 0; j < NR; ++j) slot[static_cast<size_t>(blockIdx.x) * kSlot + j] = t[j];
   }
-  if (!grid_barrier(a.sync, epoch)) return false;
+  if (!grid_barrier(a.sync, epoch, a.wait_ns, a.bias)) return false;
   // every thread below gridDim.x reads one CTA's slot (one round trip),
   // then a fixed tree over the CTA
   double t[NR];
@@ -435,7 +437,7 @@ __global__ void __launch_bounds__(kPT, DIA ? 2 : 1) inner_cg_kernel(PArgs a) {
     }
     if (j < n4) p4[j] = dir4(r4[j], JAC ? z4[j] : zero4, p4[j]);
     if (tail < n) a.p[tail] = dir(a.r[tail], JAC ? a.inv_d[tail] : 0.f, a.p[tail]);
-    if (!grid_barrier(a.sync, epoch)) return;
+    if (!grid_barrier(a.sync, epoch, a.wait_ns, a.bias)) return;
   }
 
   if (blockIdx.x == 0 && threadIdx.x == 0) {
@@ -491,7 +493,7 @@ sk_status inner_cg_persistent(sk_matrix A, const float* inv_d, float* r, float* 
   const void* k = pick_kernel(inv_d != nullptr, dia);
   int grid = coop_grid(A, k);
   SK_CHECK(grid > 0, SK_NOT_SUPPORTED, "persistent inner solve does not fit on the device");
-  grid = std::min(grid, kPT);  // a CTA sums the grid's slots one per thread  // a CTA sums the grid's slots one per thread
+  grid = std::min(grid, kPT);  // a CTA sums the grid's slots one per thread
   const int need = ceil_div(A->nrow, kPT);
   if (grid > need) grid = need;
   SyncWords* sync = static_cast<SyncWords*>(scratch);
@@ -519,6 +521,8 @@ sk_status inner_cg_persistent(sk_matrix A, const float* inv_d, float* r, float* 
   a.sync = sync;
   a.tol = static_cast<float>(tol);
   a.max_iters = max_iters;
+  a.wait_ns = wait_limit_ns();
+  a.bias = wait_target_bias();
   void* params[] = {&a};
   g_launches.fetch_add(1, std::memory_order_relaxed);
   SK_CUDA(cudaLaunchCooperativeKernel(k, dim3(grid), dim3(kPT), params, 0, st));

@@ -57,29 +57,12 @@ __global__ void extract_inv_diag_kernel(i64 len, const int* __restrict__ rp,
   }
 }
 
-// Chebyshev coefficients of 1/lambda on [lmin, lmax]: the discrete cosine
-// sampling of chebyshev_preconditioner.hpp:53-73, evaluated on the host in
-// the value type T with the C library's cos.
+// Chebyshev coefficients (chebyshev_preconditioner.hpp:53-73) as the
+// handle's host copy.
 template <typename T>
 static std::vector<double> cheb_coeffs(T lmin, T lmax, i64 degree) {
-  const i64 d = degree;
-  const i64 N = std::max<i64>(d + 1, 64);
-  const T pi = static_cast<T>(3.141592653589793238462643383279502884L);
-  const T center = (lmax + lmin) / T(2);
-  const T half_width = (lmax - lmin) / T(2);
-  std::vector<double> out(static_cast<size_t>(d + 1));
-  for (i64 k = 0; k <= d; ++k) {
-    T ck = T(0);
-    for (i64 j = 0; j < N; ++j) {
-      T tj = std::cos(pi * (T(j) + T(0.5)) / T(N));
-      T lj = center + half_width * tj;
-      T fj = T(1) / lj;
-      T cos_k = std::cos(pi * T(k) * (T(j) + T(0.5)) / T(N));
-      ck += fj * cos_k;
-    }
-    out[static_cast<size_t>(k)] = static_cast<double>(T(2) * ck / T(N));
-  }
-  out[0] = static_cast<double>(static_cast<T>(out[0]) * T(0.5));
+  std::vector<double> out(static_cast<size_t>(degree + 1));
+  chebyshev_coefficients<T>(lmin, lmax, degree, out.data());
   return out;
 }
 

@@ -416,8 +416,12 @@ struct EpiBiResid {
     sc->rho = sc->alpha = sc->omega = 1.0;
     if (sc->max_iters <= 0) {
       sc->done = 1;
-    } else if (static_cast<T>(sc->rho_new) == T(0)) {  // :204 (the reference spins forever)
-      sc->status = SK_BREAKDOWN;
+    } else if (static_cast<T>(sc->rho_new) == T(0)) {
+      // rho_0 = <r_0, r_0> = 0: the initial guess solves the system.  The
+      // reference returns from every step here without using budget and
+      // spins forever (:203-204); this solve ends converged with 0
+      // iterations, as FGMRES does for a zero initial residual.
+      sc->converged = 1;
       sc->done = 1;
     }
   }
@@ -472,7 +476,16 @@ struct EpiBiV {
   }
   __device__ void finalize(const double* t) const {
     sc->iters += 1;
-    sc->alpha = static_cast<double>(static_cast<T>(sc->rho_new) / static_cast<T>(t[0]));
+    const T rv = static_cast<T>(t[0]);
+    if (rv == T(0)) {
+      // <r_hat, v> = 0: the reference divides by it (:211) and runs the
+      // rest of its budget on infinities and NaNs, ending unconverged; this
+      // solve ends unconverged here with SK_BREAKDOWN.
+      sc->status = SK_BREAKDOWN;
+      sc->done = 1;
+      return;
+    }
+    sc->alpha = static_cast<double>(static_cast<T>(sc->rho_new) / rv);
   }
 };
 

@@ -13,6 +13,8 @@
 // tree, and hence the rounding, is reproducible.
 #pragma once
 
+#include <cmath>
+
 #include "sk_kernels.cuh"
 
 namespace sk {
@@ -214,25 +216,50 @@ struct OpScaleCopySkip {  // z = c * r, skipped once the solve is done
   __device__ void finalize(const double*) const {}
 };
 
-// z = p(A) r on device.  work holds 2 n-vectors.  `sc` (may be null) makes
-// every launch a no-op once a solve has finished.  vals32 selects the FP32
-// value copy of an FP64 CSR handle (mixed precision, T = float).
+// Chebyshev coefficients of 1/lambda on [lmin, lmax]: the discrete cosine
+// sampling of chebyshev_preconditioner.hpp:53-73, evaluated on the host in
+// the value type T with the C library's cos, written into out[0..degree]
+// (the caller's array: nothing is allocated).
 template <typename T>
-void chebyshev_apply_device(const sk_precond_s* M, const T* r, T* z, T* work, RedWs ws,
-                            const Scalars* sc, cudaStream_t st, const T* vals_override = nullptr) {
-  const sk_matrix_s* A = M->A;
+void chebyshev_coefficients(T lmin, T lmax, i64 degree, double* out) {
+  const i64 d = degree;
+  const i64 N = d + 1 > 64 ? d + 1 : 64;
+  const T pi = static_cast<T>(3.141592653589793238462643383279502884L);
+  const T center = (lmax + lmin) / T(2);
+  const T half_width = (lmax - lmin) / T(2);
+  for (i64 k = 0; k <= d; ++k) {
+    T ck = T(0);
+    for (i64 j = 0; j < N; ++j) {
+      T tj = std::cos(pi * (T(j) + T(0.5)) / T(N));
+      T lj = center + half_width * tj;
+      T fj = T(1) / lj;
+      T cos_k = std::cos(pi * T(k) * (T(j) + T(0.5)) / T(N));
+      ck += fj * cos_k;
+    }
+    out[k] = static_cast<double>(T(2) * ck / T(N));
+  }
+  out[0] = static_cast<double>(static_cast<T>(out[0]) * T(0.5));
+}
+
+// z = p(A) r by the Clenshaw recurrence of chebyshev_preconditioner.hpp:98-169,
+// with the coefficients co[0..d] and two n-vectors of work, w0 and w1, owned
+// by the caller.  `sc` (may be null) makes every launch a no-op once a solve
+// has finished.  vals_override selects the FP32 value copy of an FP64 CSR
+// handle (mixed precision, T = float).
+template <typename T>
+void chebyshev_clenshaw(const sk_matrix_s* A, const double* co, i64 d, T lmin, T lmax, const T* r, T* z,
+                        T* w0, T* w1, RedWs ws, const Scalars* sc, cudaStream_t st,
+                        const T* vals_override = nullptr) {
   const i64 n = A->nrow;
-  const T lmin = static_cast<T>(M->lambda_min), lmax = static_cast<T>(M->lambda_max);
   const T sum = lmax + lmin;
   const T diff = lmax - lmin;
-  const i64 d = M->degree;
-  auto c = [&](i64 k) { return static_cast<T>(M->coeffs[static_cast<size_t>(k)]); };
+  auto c = [&](i64 k) { return static_cast<T>(co[k]); };
   if (d == 0 || diff == T(0)) {
     launch_vec(n, OpScaleCopySkip<T>{c(0), r, z}, ws, sc, st);
     return;
   }
-  T* b_prev = work;
-  T* b_curr = work + n;
+  T* b_prev = w0;
+  T* b_curr = w1;
   launch_vec(n, OpChebInit<T>{c(d), r, b_curr, b_prev, nullptr}, ws, sc, st);
   for (i64 k = d - 1; k >= 1; --k) {
     launch_spmv<T>(A, b_curr, EpiChebStep<T>{c(k), sum, diff, r, b_curr, b_prev}, ws, sc, st,
@@ -243,6 +270,15 @@ void chebyshev_apply_device(const sk_precond_s* M, const T* r, T* z, T* work, Re
   }
   launch_spmv<T>(A, b_curr, EpiChebFinal<T>{c(0), sum, diff, r, b_curr, b_prev, z}, ws, sc, st,
                  vals_override);
+}
+
+// z = M^{-1} r for a Chebyshev preconditioner handle; work holds 2 n-vectors.
+template <typename T>
+void chebyshev_apply_device(const sk_precond_s* M, const T* r, T* z, T* work, RedWs ws,
+                            const Scalars* sc, cudaStream_t st, const T* vals_override = nullptr) {
+  chebyshev_clenshaw<T>(M->A, M->coeffs.data(), M->degree, static_cast<T>(M->lambda_min),
+                        static_cast<T>(M->lambda_max), r, z, work, work + M->A->nrow, ws, sc, st,
+                        vals_override);
 }
 
 }  // namespace sk

@@ -52,6 +52,37 @@ def _is_device(a):
     return not isinstance(a, np.ndarray) and hasattr(a, "data_ptr")
 
 
+def _check_vec(a, n, dtype, device, name):
+    """Raises unless `a` is a contiguous CUDA torch tensor of `n` values of
+    `dtype` on CUDA device `device` (None: any).  The C entry points that
+    take device vectors take no length, so a host array, a CPU tensor, a
+    short vector or the other precision would otherwise be read or written
+    out of bounds by the kernels; this check runs before anything is
+    launched."""
+    import torch
+    if not isinstance(a, torch.Tensor):
+        raise TypeError(f"{name} must be a CUDA torch tensor, not {type(a).__name__}")
+    want = torch.float64 if np.dtype(dtype) == np.float64 else torch.float32
+    if a.dtype != want:
+        raise TypeError(f"{name} has dtype {a.dtype}; the matrix holds {np.dtype(dtype).name} values")
+    if not a.is_contiguous():
+        raise ValueError(f"{name} must be contiguous")
+    if a.numel() != n:
+        raise ValueError(f"{name} holds {a.numel()} values; {n} are needed")
+    if not a.is_cuda:
+        raise ValueError(f"{name} is on {a.device}, not on a CUDA device")
+    if device is not None and a.device.index != device:
+        raise ValueError(f"{name} is on cuda:{a.device.index}; the matrix is on cuda:{device}")
+
+
+def _current_device():
+    try:
+        import torch
+        return torch.cuda.current_device() if torch.cuda.is_available() else None
+    except Exception:
+        return None
+
+
 CUDA_STREAM_LEGACY = 1  # cudaStreamLegacy
 
 
@@ -100,6 +131,7 @@ class Device_matrix:
         self.dtype = dt
         self._shape = (n, m)
         self._block = (A.block_rows(), A.block_cols()) if isinstance(A, Block_sparse_row_matrix) else None
+        self.device = _current_device()
 
     @classmethod
     def _wrap(cls, h, dtype, shape, block=None):
@@ -108,6 +140,7 @@ class Device_matrix:
         self.dtype = np.dtype(dtype)
         self._shape = tuple(shape)
         self._block = block
+        self.device = _current_device()
         return self
 
     def shape(self):
@@ -165,13 +198,22 @@ class Device_matrix:
         return bool(built.value)
 
     def spmv(self, x, y, stream=None):
-        """y = A x on device tensors (or raw device pointers)."""
+        """y = A x on device tensors (or raw device pointers, which the
+        caller vouches for)."""
+        n, m = self._shape
+        if not isinstance(x, int):
+            _check_vec(x, m, self.dtype, self.device, "x")
+        if not isinstance(y, int):
+            _check_vec(y, n, self.dtype, self.device, "y")
         xs = _ptr(x) if not isinstance(x, int) else ctypes.c_void_p(x)
         ys = _ptr(y) if not isinstance(y, int) else ctypes.c_void_p(y)
         st = stream if stream is not None else _stream_of(x)
         check(lib().sk_spmv(self.handle, xs, ys, st))
 
     def spmv_f32(self, x, y, stream=None):
+        n, m = self._shape
+        _check_vec(x, m, np.float32, self.device, "x")
+        _check_vec(y, n, np.float32, self.device, "y")
         st = stream if stream is not None else _stream_of(x)
         check(lib().sk_spmv_f32(self.handle, _ptr(x), _ptr(y), st))
 
@@ -259,6 +301,8 @@ class _Precond:
 
     def apply(self, r, z, stream=None):
         """z = M^{-1} r on device tensors."""
+        _check_vec(r, self.n, self.A.dtype, self.A.device, "r")
+        _check_vec(z, self.n, self.A.dtype, self.A.device, "z")
         st = stream if stream is not None else _stream_of(r)
         check(lib().sk_precond_apply(self.handle, self.n, _ptr(r), _ptr(z), st))
 
@@ -365,13 +409,24 @@ def estimate_eigenvalue_bounds(Ad, num_iter=30):
     return lo.value, hi.value
 
 
+def debug_set_wait(limit_ns=0, unmeetable=False):
+    """sk_debug_set_wait: the time bound of the persistent kernels'
+    grid-barrier waits (0 restores 2 s) and, for tests of the timeout path,
+    barriers that wait for one arrival more than the grid makes."""
+    check(lib().sk_debug_set_wait(int(limit_ns), int(bool(unmeetable))))
+
+
 def chebyshev_apply_noalloc(Ad, lambda_min, lambda_max, degree, r, z, stream=None):
     """z = p(A) r like chebyshev_preconditioner(Ad, ...).apply(r, z), for
     callers that cannot allocate device memory at apply time: no handle is
     created and the work vectors live in the library's static device array
     (square CSR, at most 1,048,576 rows, degree <= 64; overlapping calls on
     the GPU race; the first call on a device should precede any stream
-    capture)."""
+    capture).  r and z must be contiguous CUDA tensors of n values of the
+    matrix's value type on its device; anything else raises before a launch."""
+    n = Ad.shape()[0]
+    _check_vec(r, n, Ad.dtype, Ad.device, "r")
+    _check_vec(z, n, Ad.dtype, Ad.device, "z")
     st = stream if stream is not None else _stream_of(r)
     check(lib().sk_chebyshev_apply_noalloc(Ad.handle, float(lambda_min), float(lambda_max), int(degree),
                                            _ptr(r), _ptr(z), st))
@@ -425,12 +480,18 @@ def _run(fn_dev, fn_host, b, x, Ad, cfg_struct, max_hist, collect):
     s = _lib.Summary()
     hist = np.zeros(max(int(max_hist), 1) + 4, dtype=np.float64) if collect else None
     if _is_device(b):
+        n = Ad.shape()[0]
+        _check_vec(b, n, Ad.dtype, Ad.device, "b")
+        _check_vec(x, n, Ad.dtype, Ad.device, "x")
         st = _stream_of(b)
         check(fn_dev(_ptr(b), _ptr(x), ctypes.byref(cfg_struct), ctypes.byref(s), _ptr(hist), st))
     else:
         if not (isinstance(x, np.ndarray) and x.flags.c_contiguous and x.dtype == Ad.dtype):
             raise TypeError("x must be a contiguous numpy array of the matrix's value type")
         bb = np.ascontiguousarray(b, dtype=Ad.dtype)
+        n = Ad.shape()[0]
+        if bb.shape != (n,) or x.shape != (n,):
+            raise ValueError(f"b and x must hold {n} values (got {bb.shape} and {x.shape})")
         check(fn_host(_ptr(bb), _ptr(x), ctypes.byref(cfg_struct), ctypes.byref(s), _ptr(hist)))
     out = Summary(s.residual_norm, s.computed_iterations, bool(s.converged), [], s.status)
     if collect:
@@ -575,6 +636,9 @@ def mixed_cg(b, x, cfg, op, jacobi_inner=True):
                          0 if cfg.persistent else 1)
     s = _lib.MixedSummary()
     hist = np.zeros(cfg.max_outer + 2) if cfg.collect_residuals else None
+    n = Ad.shape()[0]
+    _check_vec(b, n, np.float64, Ad.device, "b")
+    _check_vec(x, n, np.float64, Ad.device, "x")
     check(lib().sk_mixed_cg_solve(Ad.handle, int(jacobi_inner), _ptr(b), _ptr(x), ctypes.byref(c), ctypes.byref(s),
                                   _ptr(hist), _stream_of(b)))
     out = Mixed_summary(s.residual_norm, s.outer_iterations, s.inner_iterations, bool(s.converged), s.status,

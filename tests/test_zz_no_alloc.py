@@ -2,9 +2,9 @@
 through the C ABI, against the regular handle-based apply.
 
 It serves callers that cannot allocate device memory when they apply the
-preconditioner (a callback inside another solver's loop, or a stream under
-graph capture), so its work vectors live in a static device array shared by
-all calls.  Two calls in a row must each give exactly the regular apply's
+preconditioner (a callback inside another solver library's loop, where that
+library reserved all device memory up front), so its work vectors live in a
+static device array shared by all calls.  Two calls in a row must each give exactly the regular apply's
 result, so the second call cannot be affected by what the first one left in
 the shared array.  This file is collected last, and passes alone in a fresh
 process as well as after the other tests."""
