@@ -97,6 +97,25 @@ struct Csr {
   void* dia_vals = nullptr;
   float* dia_vals32 = nullptr;
   unsigned short* dia_mask = nullptr;
+  // Symmetrically scaled FP32 copies for the Jacobi inner solve of the
+  // mixed solver (sk_mixed.cu): S = D^-1/2 A D^-1/2 without its unit
+  // diagonal, in the SELL-32 layout (sym_off, sym_len, sym_col, sym_val) or
+  // as diagonal planes without the main one (sym_dn planes at sym_doff,
+  // values sym_dval, row masks sym_dmask, laid out like the diagonal copy).
+  // sym_isq = 1 / sqrt(a_ii) (FP64), sym_diag = a_ii (FP32).  State: 0 not
+  // built, 1 built, -1 not possible (a diagonal entry absent or not
+  // positive, or no SELL-32 / diagonal copy to derive it from).
+  int sym_sell_state = 0, sym_dia_state = 0, sym_diag_state = 0;
+  int* sym_off = nullptr;
+  unsigned char* sym_len = nullptr;
+  int* sym_col = nullptr;
+  float* sym_val = nullptr;
+  int sym_dn = 0;
+  int sym_doff[kDiaMax] = {};
+  float* sym_dval = nullptr;
+  unsigned short* sym_dmask = nullptr;
+  double* sym_isq = nullptr;
+  float* sym_diag = nullptr;
 };
 
 // ELLPACK: slot-major (column-major) copy of the reference's row-major

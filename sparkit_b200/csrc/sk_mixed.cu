@@ -3,28 +3,39 @@
 //
 // No reference counterpart as a whole: the iteration is the reference's
 // conjugate gradient (conjugate_gradient.hpp:122-312, Jacobi or identity
-// left preconditioner, true residual only at k = 0) in FP32, exactly as the
-// per-step path of sk_solvers.cu runs it, but without a kernel boundary per
-// step.  One CTA per SM (two over the diagonal copy) stays resident for
-// the whole solve; each iteration
-// is three phases separated by grid barriers:
+// left preconditioner, true residual only at k = 0) in FP32, without a
+// kernel boundary per step.  One CTA per SM (two over the diagonal copy)
+// stays resident for the whole solve.
 //
-//   A  q = A p (SELL-32 rows, or the rows of the diagonal copy, each summed
-//      in storage order) and <p, q>                               -> alpha
-//   B  d += alpha p, r -= alpha q, <r, r> and <r, D^-1 r>          -> test, beta
-//   C  p = D^-1 r + beta p
+// The Jacobi inner solve runs on the symmetrically scaled matrix
+// S = D^-1/2 A D^-1/2 (D = diag(A)), whose diagonal is 1 and is not stored:
+// CG on S y = D^-1/2 r0 with d = D^-1/2 y takes, in exact arithmetic, the
+// same steps as Jacobi-preconditioned CG on A d = r0 (<r_S, r_S> is
+// <r, D^-1 r>), but reads no inverse diagonal and streams one entry per row
+// less.  The unpreconditioned inner solve runs on A itself.  Either way the
+// preconditioned residual is the residual, so each iteration is two phases
+// separated by grid-wide reductions:
 //
-// The dot products are reduced deterministically: each CTA publishes its
-// partial in a slot before the barrier, and after it every CTA sums all the
-// slots in the same fixed order, so every CTA holds the same scalars and
-// takes the same convergence decision.  Barrier waits are bounded in time;
-// a wait that runs out sets an error word that makes every other CTA leave
-// at its next wait, and the host reports SK_TIMEOUT.
+//   S  w = M r for this CTA's rows (M = S or A); p = r + beta p and
+//      q = w + beta q, which equals M p by linearity, so no second product
+//      is needed; <p, q>                                          -> alpha
+//   U  d += alpha p, r -= alpha q, <r, r> and the unscaled ||r||^2
+//      (the sum of a_ii r_i^2 on S)                               -> test, beta
 //
-// The vectors (r, d, p, q and the inverse diagonal, 5 x 4 B per row) stay
-// in L2 (a persisting window set by the caller) while the matrix streams
-// through it with evict-first loads.
+// The convergence test is the reference's ||r|| / ||r0|| < tol on the
+// residual of A d = r0 (conjugate_gradient.hpp:264-276).  The dot products
+// are reduced deterministically: each CTA publishes its partial in a slot
+// before the barrier, and after it every CTA sums all the slots in the same
+// fixed order, so every CTA holds the same scalars and takes the same
+// decision.  Barrier waits are bounded in time; a wait that runs out sets
+// an error word that makes every other CTA leave at its next wait, and the
+// host reports SK_TIMEOUT.
+//
+// The vectors (r, d, p, q and the diagonal, 5 x 4 B per row) stay in L2 (a
+// persisting window set by the caller) while the matrix streams through it
+// with evict-first loads.
 #include <climits>
+#include <vector>
 
 #include "sk_kernels.cuh"
 #include "sk_mixed.cuh"
@@ -49,14 +60,14 @@ struct SyncWords {
 
 struct PArgs {
   int n;
-  const int* off;
+  const int* off;  // SELL-32 form
   const unsigned char* len;
   const int* col;
-  const float* val;  // SELL-32 values, or the FP32 values of the diagonal copy
-  int dia_n;         // diagonal copy: diagonals, row masks and offsets
+  const float* val;  // SELL-32 values, or the diagonal planes
+  int dia_n;         // diagonal form: planes, row masks and offsets
   const unsigned short* dia_mask;
   int dia_off[kDiaMax];
-  const float* inv_d;
+  const float* wdiag;  // a_ii of A when the matrix is the scaled S, else null
   float* r;
   float* d;
   float* p;
@@ -192,18 +203,30 @@ __device__ __forceinline__ void row_fetch(PArgs const& a, int len, int base, int
     }
 }
 
-// Phase A: q = A p over this thread's rows t0, t0 + T, ... with each row
-// summed from 0 in storage order (sparse_blas.hpp:25-28, the order of the
-// per-step FP32 product).  Three rows are in flight per thread: the slots
-// of row k+2 stream from HBM while the gathers of row k+1 return and row k
-// is summed, so neither the matrix stream nor the gathers wait on each
-// other.  Returns this thread's share of <p, q>.
-__device__ __forceinline__ double phase_spmv(PArgs const& a, int t0, int T) {
+// The direction update of one row from its product w = (M r)_i: p = r +
+// beta p, q = w + beta q (p = r, q = w at the first step); returns p q.
+__device__ __forceinline__ double row_direction(PArgs const& a, int i, float ri, float w, float pi, float qi,
+                                                float beta, bool first) {
+  const float pn = first ? ri : add(ri, mul(beta, pi));
+  const float qn = first ? w : add(w, mul(beta, qi));
+  a.p[i] = pn;
+  a.q[i] = qn;
+  return static_cast<double>(mul(pn, qn));
+}
+
+// Phase S over SELL rows: each row's product summed from r_i (UNIT: the
+// unit diagonal of S) or from 0, then its stored entries in storage order.
+// Three rows are in flight per thread: the slots of row k+2 stream from
+// HBM while the gathers of row k+1 return and row k is summed, so neither
+// the matrix stream nor the gathers wait on each other.  Returns this
+// thread's share of <p, q>.
+template <bool UNIT>
+__device__ __forceinline__ double phase_s_sell(PArgs const& a, int t0, int T, float beta, bool first) {
   double pq = 0.0;
   // row a: summed this step; row b: slots arrived, gathers issued this
   // step; row c: slots issued this step
   int ia = t0, la, basea, lb, bb, lc, bc;
-  float va[kPU], ga[kPU], pa = 0.0f;
+  float va[kPU], ga[kPU], ra = 0.0f, pa = 0.0f, qa = 0.0f;
   int cb[kPU];
   float vb[kPU];
   row_meta(a, ia, la, basea);
@@ -211,9 +234,15 @@ __device__ __forceinline__ double phase_spmv(PArgs const& a, int t0, int T) {
 #pragma unroll
   for (int j = 0; j < kPU; ++j) {
     va[j] = vb[j];
-    ga[j] = (j < la) ? a.p[cb[j]] : 0.0f;
+    ga[j] = (j < la) ? a.r[cb[j]] : 0.0f;
   }
-  if (ia < a.n) pa = a.p[ia];
+  if (ia < a.n) {
+    ra = a.r[ia];
+    if (!first) {
+      pa = a.p[ia];
+      qa = a.q[ia];
+    }
+  }
   row_meta(a, ia + T, lb, bb);
   row_fetch(a, lb, bb, 0, cb, vb);
   row_meta(a, ia + 2 * T, lc, bc);
@@ -225,15 +254,22 @@ __device__ __forceinline__ double phase_spmv(PArgs const& a, int t0, int T) {
     row_fetch(a, lc, bc, 0, cc, vc);
     int ld, bd;
     row_meta(a, ia + 3 * T, ld, bd);
-    // gathers of row b
+    // gathers and own values of row b
     float gb[kPU];
 #pragma unroll
     for (int j = 0; j < kPU; ++j)
-      if (j < lb) gb[j] = a.p[cb[j]];
+      if (j < lb) gb[j] = a.r[cb[j]];
     const int ib = ia + T;
-    const float pb = ib < a.n ? a.p[ib] : 0.0f;
+    float rb = 0.0f, pb = 0.0f, qb = 0.0f;
+    if (ib < a.n) {
+      rb = a.r[ib];
+      if (!first) {
+        pb = a.p[ib];
+        qb = a.q[ib];
+      }
+    }
     // sum of row a
-    float sum = 0.0f;
+    float sum = UNIT ? ra : 0.0f;
 #pragma unroll
     for (int j = 0; j < kPU; ++j)
       if (j < la) sum = add(sum, mul(va[j], ga[j]));
@@ -243,18 +279,19 @@ __device__ __forceinline__ double phase_spmv(PArgs const& a, int t0, int T) {
       row_fetch(a, la, basea, k, c, v);
 #pragma unroll
       for (int j = 0; j < kPU; ++j)
-        if (k + j < la) g[j] = a.p[c[j]];
+        if (k + j < la) g[j] = a.r[c[j]];
 #pragma unroll
       for (int j = 0; j < kPU; ++j)
         if (k + j < la) sum = add(sum, mul(v[j], g[j]));
     }
-    a.q[ia] = sum;
-    pq += static_cast<double>(mul(pa, sum));
+    pq += row_direction(a, ia, ra, sum, pa, qa, beta, first);
     // rotate a <- b <- c <- d
     ia = ib;
     la = lb;
     basea = bb;
+    ra = rb;
     pa = pb;
+    qa = qb;
     lb = lc;
     bb = bc;
     lc = ld;
@@ -270,33 +307,38 @@ __device__ __forceinline__ double phase_spmv(PArgs const& a, int t0, int T) {
   return pq;
 }
 
-// Phase A over the diagonal copy.  The values of a warp's rows for one
-// diagonal are one 32-value segment and the reads of p at row + off[d] are
+// Phase S over diagonal planes.  The values of a warp's rows for one
+// diagonal are one 32-value segment and the reads of r at row + off[d] are
 // contiguous, so no load depends on another: each thread issues the value
-// and p loads of kDiaRows rows for kDiaGroup diagonals at a time without
+// and r loads of kDiaRows rows for kDiaGroup diagonals at a time without
 // waiting for the rows' masks (a diagonal a row does not store reads a zero
-// value and a clamped p, and the mask leaves both out of the sum).  The
+// value and a clamped r, and the mask leaves both out of the sum).  The
 // kernel runs 2 CTAs per SM here (this phase needs few registers), which
-// hides the load latency better than the deeper register pipeline of the
-// SELL phase at one CTA per SM.  Each row is summed from 0 over its stored
-// diagonals in ascending column order (its CSR order).  Returns this
-// thread's share of <p, q>.
+// hides the load latency better than a deeper register pipeline at one CTA
+// per SM.  Each row is summed from r_i (UNIT) or 0 over its stored
+// diagonals in ascending column order.  Returns this thread's share of
+// <p, q>.
 constexpr int kDiaRows = 2;
 constexpr int kDiaGroup = 4;
 
-__device__ __forceinline__ double phase_spmv_dia(PArgs const& a, int t0, int T) {
+template <bool UNIT>
+__device__ __forceinline__ double phase_s_dia(PArgs const& a, int t0, int T, float beta, bool first) {
   constexpr int R = kDiaRows, C = kDiaGroup;
   double pq = 0.0;
   const int last = a.n - 1;
   const long long sl = 32 * a.dia_n;
   for (int i = t0; i < a.n; i += R * T) {
     unsigned m[R];
-    float s[R];
+    float s[R], ro[R], po[R], qo[R];
 #pragma unroll
     for (int r = 0; r < R; ++r) {
       const int row = i + r * T;
-      m[r] = row < a.n ? __ldcs(a.dia_mask + row) : 0u;
-      s[r] = 0.0f;
+      const bool in = row < a.n;
+      m[r] = in ? __ldcs(a.dia_mask + row) : 0u;
+      ro[r] = in ? a.r[row] : 0.0f;
+      po[r] = in && !first ? a.p[row] : 0.0f;
+      qo[r] = in && !first ? a.q[row] : 0.0f;
+      s[r] = UNIT ? ro[r] : 0.0f;
     }
 #pragma unroll
     for (int d0 = 0; d0 < kDiaMax; d0 += C) {
@@ -310,7 +352,7 @@ __device__ __forceinline__ double phase_spmv_dia(PArgs const& a, int t0, int T) 
         for (int j = 0; j < C; ++j)
           if (d0 + j < a.dia_n) {
             v[r][j] = __ldcs(vs + 32 * (d0 + j));
-            g[r][j] = a.p[min(max(row + a.dia_off[d0 + j], 0), last)];
+            g[r][j] = a.r[min(max(row + a.dia_off[d0 + j], 0), last)];
           }
       }
 #pragma unroll
@@ -322,80 +364,79 @@ __device__ __forceinline__ double phase_spmv_dia(PArgs const& a, int t0, int T) 
 #pragma unroll
     for (int r = 0; r < R; ++r) {
       const int row = i + r * T;
-      if (row < a.n) {
-        a.q[row] = s[r];
-        pq += static_cast<double>(mul(a.p[row], s[r]));
-      }
+      if (row < a.n) pq += row_direction(a, row, ro[r], s[r], po[r], qo[r], beta, first);
     }
   }
   return pq;
 }
 
-template <bool JAC, bool DIA>
+template <bool DIA, bool UNIT>
 __global__ void __launch_bounds__(kPT, DIA ? 2 : 1) inner_cg_kernel(PArgs a) {
   const int n = a.n;
   const int T = gridDim.x * kPT;
   const int t0 = blockIdx.x * kPT + threadIdx.x;
-  // element-wise phases: four rows per 16-byte access, two accesses per
-  // thread and step, rows 4 * n4 .. n - 1 by the first threads
+  // phase U: four rows per 16-byte access, two accesses per thread and
+  // step, rows 4 * n4 .. n - 1 by the first threads
   const int n4 = n >> 2;
   const int tail = 4 * n4 + t0;
   const float4* q4 = reinterpret_cast<const float4*>(a.q);
-  const float4* z4 = reinterpret_cast<const float4*>(a.inv_d);
-  float4* p4 = reinterpret_cast<float4*>(a.p);
+  const float4* p4 = reinterpret_cast<const float4*>(a.p);
+  const float4* w4 = reinterpret_cast<const float4*>(a.wdiag);
   float4* d4 = reinterpret_cast<float4*>(a.d);
   float4* r4 = reinterpret_cast<float4*>(a.r);
-  const float4 zero4 = make_float4(0.f, 0.f, 0.f, 0.f);
+  const float4 one4 = make_float4(1.f, 1.f, 1.f, 1.f);
   unsigned epoch = 0;
-  // k = 0 (reorthogonalize, :217-230, with d = 0 so r = r0): z = M r,
-  // p = z, rz = <r, z>; and ||r0|| (the solve's ||b||, :194).
+  // k = 0 (reorthogonalize, :217-230, with d = 0 so r = r0): <r, r> and the
+  // unscaled ||r0||^2 (the solve's ||b||, :194)
   double v0[2] = {0.0, 0.0};
   for (int i = t0; i < n; i += T) {
     const float ri = a.r[i];
-    const float zi = JAC ? mul(a.inv_d[i], ri) : ri;
     a.d[i] = 0.0f;
-    a.p[i] = zi;
-    v0[0] += static_cast<double>(mul(ri, zi));
-    v0[1] += static_cast<double>(mul(ri, ri));
+    const float rr = mul(ri, ri);
+    v0[0] += static_cast<double>(rr);
+    v0[1] += static_cast<double>(UNIT ? mul(a.wdiag[i], rr) : rr);
   }
   if (!grid_allreduce<2>(v0, a, 0, epoch)) return;
   const float bnorm = sqrtf(static_cast<float>(v0[1]));
-  float rz = static_cast<float>(v0[0]);
+  float rho = static_cast<float>(v0[0]);
+  float beta = 0.0f;
   long long it = 0;
   int conv = 0;
   float rn = bnorm;
   if (bnorm == 0.0f) conv = 1;
   while (!conv && it < a.max_iters) {
-    // A: compute_step_size (:233-239)
+    // S: the product, the direction update and compute_step_size (:233-239)
+    const bool first = it == 0;
     double pq[1];
-    if constexpr (DIA) pq[0] = phase_spmv_dia(a, t0, T);
-    else pq[0] = phase_spmv(a, t0, T);
+    if constexpr (DIA) pq[0] = phase_s_dia<UNIT>(a, t0, T, beta, first);
+    else pq[0] = phase_s_sell<UNIT>(a, t0, T, beta, first);
     if (!grid_allreduce<1>(pq, a, 1, epoch)) return;
-    const float alpha = rz / static_cast<float>(pq[0]);
-    // B: compute_new_solution, compute_new_residual, is_converged
-    // (:242-276) and the new <r, z> (:279-284)
+    const float alpha = rho / static_cast<float>(pq[0]);
+    // U: compute_new_solution, compute_new_residual, is_converged
+    // (:242-276) and the next <r, z> (:279-284)
     double rr[2] = {0.0, 0.0};
-    auto upd = [&](float pi, float qi, float di, float ro, float zi, float& dn, float& rnew) {
+    auto upd = [&](float pi, float qi, float di, float ro, float wi, float& dn, float& rnew) {
       dn = add(mul(alpha, pi), di);
       rnew = sub(ro, mul(alpha, qi));
-      rr[0] += static_cast<double>(mul(rnew, rnew));
-      if (JAC) rr[1] += static_cast<double>(mul(rnew, mul(zi, rnew)));
+      const float r2 = mul(rnew, rnew);
+      rr[0] += static_cast<double>(r2);
+      if (UNIT) rr[1] += static_cast<double>(mul(wi, r2));
     };
-    auto upd4 = [&](float4 pv, float4 qv, float4 dv, float4 rv, float4 zv, float4& dn, float4& rw) {
-      upd(pv.x, qv.x, dv.x, rv.x, zv.x, dn.x, rw.x);
-      upd(pv.y, qv.y, dv.y, rv.y, zv.y, dn.y, rw.y);
-      upd(pv.z, qv.z, dv.z, rv.z, zv.z, dn.z, rw.z);
-      upd(pv.w, qv.w, dv.w, rv.w, zv.w, dn.w, rw.w);
+    auto upd4 = [&](float4 pv, float4 qv, float4 dv, float4 rv, float4 wv, float4& dn, float4& rw) {
+      upd(pv.x, qv.x, dv.x, rv.x, wv.x, dn.x, rw.x);
+      upd(pv.y, qv.y, dv.y, rv.y, wv.y, dn.y, rw.y);
+      upd(pv.z, qv.z, dv.z, rv.z, wv.z, dn.z, rw.z);
+      upd(pv.w, qv.w, dv.w, rv.w, wv.w, dn.w, rw.w);
     };
     int j = t0;
     for (; j + T < n4; j += 2 * T) {
       const int j1 = j + T;
       const float4 pv0 = p4[j], qv0 = q4[j], dv0 = d4[j], rv0 = r4[j];
       const float4 pv1 = p4[j1], qv1 = q4[j1], dv1 = d4[j1], rv1 = r4[j1];
-      const float4 zv0 = JAC ? z4[j] : zero4, zv1 = JAC ? z4[j1] : zero4;
+      const float4 wv0 = UNIT ? w4[j] : one4, wv1 = UNIT ? w4[j1] : one4;
       float4 dn0, rw0, dn1, rw1;
-      upd4(pv0, qv0, dv0, rv0, zv0, dn0, rw0);
-      upd4(pv1, qv1, dv1, rv1, zv1, dn1, rw1);
+      upd4(pv0, qv0, dv0, rv0, wv0, dn0, rw0);
+      upd4(pv1, qv1, dv1, rv1, wv1, dn1, rw1);
       d4[j] = dn0;
       r4[j] = rw0;
       d4[j1] = dn1;
@@ -403,41 +444,24 @@ __global__ void __launch_bounds__(kPT, DIA ? 2 : 1) inner_cg_kernel(PArgs a) {
     }
     if (j < n4) {
       float4 dn, rw;
-      upd4(p4[j], q4[j], d4[j], r4[j], JAC ? z4[j] : zero4, dn, rw);
+      upd4(p4[j], q4[j], d4[j], r4[j], UNIT ? w4[j] : one4, dn, rw);
       d4[j] = dn;
       r4[j] = rw;
     }
     if (tail < n) {
       float dn, rw;
-      upd(a.p[tail], a.q[tail], a.d[tail], a.r[tail], JAC ? a.inv_d[tail] : 0.f, dn, rw);
+      upd(a.p[tail], a.q[tail], a.d[tail], a.r[tail], UNIT ? a.wdiag[tail] : 1.f, dn, rw);
       a.d[tail] = dn;
       a.r[tail] = rw;
     }
     if (!grid_allreduce<2>(rr, a, 0, epoch)) return;
     ++it;
-    rn = sqrtf(static_cast<float>(rr[0]));
+    rn = sqrtf(static_cast<float>(UNIT ? rr[1] : rr[0]));
     conv = rn / bnorm < a.tol ? 1 : 0;
     if (conv || it >= a.max_iters) break;
-    const float rz_new = static_cast<float>(JAC ? rr[1] : rr[0]);
-    const float beta = rz_new / rz;
-    rz = rz_new;
-    // C: update_direction (:285-290)
-    auto dir = [&](float ri, float zi, float pi) { return add(JAC ? mul(zi, ri) : ri, mul(beta, pi)); };
-    auto dir4 = [&](float4 rv, float4 zv, float4 pv) {
-      return make_float4(dir(rv.x, zv.x, pv.x), dir(rv.y, zv.y, pv.y), dir(rv.z, zv.z, pv.z),
-                         dir(rv.w, zv.w, pv.w));
-    };
-    j = t0;
-    for (; j + T < n4; j += 2 * T) {
-      const int j1 = j + T;
-      const float4 rv0 = r4[j], pv0 = p4[j], rv1 = r4[j1], pv1 = p4[j1];
-      const float4 zv0 = JAC ? z4[j] : zero4, zv1 = JAC ? z4[j1] : zero4;
-      p4[j] = dir4(rv0, zv0, pv0);
-      p4[j1] = dir4(rv1, zv1, pv1);
-    }
-    if (j < n4) p4[j] = dir4(r4[j], JAC ? z4[j] : zero4, p4[j]);
-    if (tail < n) a.p[tail] = dir(a.r[tail], JAC ? a.inv_d[tail] : 0.f, a.p[tail]);
-    if (!grid_barrier(a.sync, epoch, a.wait_ns, a.bias)) return;
+    const float rho_new = static_cast<float>(rr[0]);
+    beta = rho_new / rho;  // update_direction (:285-290), applied in the next phase S
+    rho = rho_new;
   }
 
   if (blockIdx.x == 0 && threadIdx.x == 0) {
@@ -447,15 +471,12 @@ __global__ void __launch_bounds__(kPT, DIA ? 2 : 1) inner_cg_kernel(PArgs a) {
   }
 }
 
-// The handle's diagonal copy when it has FP32 values, else its SELL copy.
-bool use_dia(sk_matrix A) { return A->csr.dia_n > 0 && A->csr.dia_vals32; }
-
-const void* pick_kernel(bool jac, bool dia) {
+const void* pick_kernel(bool dia, bool unit) {
   if (dia)
-    return jac ? reinterpret_cast<const void*>(&inner_cg_kernel<true, true>)
-               : reinterpret_cast<const void*>(&inner_cg_kernel<false, true>);
-  return jac ? reinterpret_cast<const void*>(&inner_cg_kernel<true, false>)
-             : reinterpret_cast<const void*>(&inner_cg_kernel<false, false>);
+    return unit ? reinterpret_cast<const void*>(&inner_cg_kernel<true, true>)
+                : reinterpret_cast<const void*>(&inner_cg_kernel<true, false>);
+  return unit ? reinterpret_cast<const void*>(&inner_cg_kernel<false, true>)
+              : reinterpret_cast<const void*>(&inner_cg_kernel<false, false>);
 }
 
 // CTAs of the cooperative grid (0: the kernel does not fit).
@@ -468,7 +489,218 @@ int coop_grid(sk_matrix A, const void* k) {
   return per_sm * A->sm_count;
 }
 
+// ------------------------------------------------------------------
+// The scaled copies of S = D^-1/2 A D^-1/2, built from the FP64 CSR arrays
+// on the first Jacobi inner solve that needs them.
+// ------------------------------------------------------------------
+
+// isq_i = 1 / sqrt(a_ii) and a_ii as float; counts the rows whose diagonal
+// entry is absent or not positive (S is then not formed).
+__global__ void sym_diag_kernel(i64 n, const int* __restrict__ rp, const int* __restrict__ ci,
+                                const double* __restrict__ v, double* __restrict__ isq,
+                                float* __restrict__ dg, unsigned long long* bad) {
+  for (i64 i = blockIdx.x * static_cast<i64>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<i64>(gridDim.x) * blockDim.x) {
+    double a = 0.0;
+    for (int k = rp[i]; k < rp[i + 1]; ++k)
+      if (ci[k] == i) a = v[k];
+    if (!(a > 0.0)) {
+      atomicAdd(bad, 1ull);
+      a = 1.0;
+    }
+    isq[i] = __ddiv_rn(1.0, __dsqrt_rn(a));
+    dg[i] = static_cast<float>(a);
+  }
+}
+
+__device__ __forceinline__ float sym_value(double a, double isq_i, double isq_j) {
+  return static_cast<float>(__dmul_rn(__dmul_rn(a, isq_i), isq_j));
+}
+
+// Off-diagonal entries of each row, and the largest count of each 32-row
+// slice (one warp per slice; the grid covers whole slices).
+__global__ void sym_sell_count_kernel(i64 n, const int* __restrict__ rp, const int* __restrict__ ci,
+                                      int* __restrict__ slice_w) {
+  const i64 i = blockIdx.x * static_cast<i64>(blockDim.x) + threadIdx.x;
+  int cnt = 0;
+  if (i < n) {
+    cnt = rp[i + 1] - rp[i];
+    for (int k = rp[i]; k < rp[i + 1]; ++k)
+      if (ci[k] == i) --cnt;
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) cnt = max(cnt, __shfl_xor_sync(0xffffffffu, cnt, o));
+  if ((threadIdx.x & 31) == 0 && i < n) slice_w[i >> 5] = cnt;
+}
+
+__global__ void sym_sell_fill_kernel(i64 n, const int* __restrict__ rp, const int* __restrict__ ci,
+                                     const double* __restrict__ v, const double* __restrict__ isq,
+                                     const int* __restrict__ off, int* __restrict__ col,
+                                     float* __restrict__ val, unsigned char* __restrict__ len) {
+  for (i64 i = blockIdx.x * static_cast<i64>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<i64>(gridDim.x) * blockDim.x) {
+    const i64 base = off[i >> 5] + (i & 31);
+    const double si = isq[i];
+    int k = 0;
+    for (int e = rp[i]; e < rp[i + 1]; ++e) {
+      const int c = ci[e];
+      if (c == i) continue;
+      col[base + 32 * k] = c;
+      val[base + 32 * k] = sym_value(v[e], si, isq[c]);
+      ++k;
+    }
+    len[i] = static_cast<unsigned char>(k);
+  }
+}
+
+struct SymOffsets {
+  int n;
+  int off[kDiaMax];
+};
+
+__global__ void sym_dia_fill_kernel(i64 n, const int* __restrict__ rp, const int* __restrict__ ci,
+                                    const double* __restrict__ v, const double* __restrict__ isq, SymOffsets o,
+                                    float* __restrict__ planes, unsigned short* __restrict__ mask) {
+  for (i64 r = blockIdx.x * static_cast<i64>(blockDim.x) + threadIdx.x; r < n;
+       r += static_cast<i64>(gridDim.x) * blockDim.x) {
+    unsigned m = 0;
+    const double sr = isq[r];
+    for (int k = rp[r]; k < rp[r + 1]; ++k) {
+      const int c = ci[k];
+      if (c == r) continue;
+      const int off = c - static_cast<int>(r);
+      int d = 0;
+      while (d + 1 < o.n && o.off[d] != off) ++d;  // every off-diagonal offset is in the set
+      planes[((r >> 5) * o.n + d) * 32 + (r & 31)] = sym_value(v[k], sr, isq[c]);
+      m |= 1u << d;
+    }
+    mask[r] = static_cast<unsigned short>(m);
+  }
+}
+
+sk_status sym_prepare_diag(sk_matrix A, cudaStream_t st) {
+  auto& C = A->csr;
+  if (C.sym_diag_state) return SK_OK;
+  const i64 n = A->nrow;
+  void *isq = nullptr, *dg = nullptr, *bad = nullptr;
+  sk_status s;
+  if ((s = dev_alloc(A, &isq, (n + 64) * 8)) != SK_OK) return s;
+  if ((s = dev_alloc(A, &dg, (n + 64) * 4)) != SK_OK) return s;
+  if ((s = dev_alloc(A, &bad, 8)) != SK_OK) return s;
+  SK_CUDA(cudaMemsetAsync(bad, 0, 8, st));
+  SK_LAUNCH(sym_diag_kernel, grid_for(n), kThreads, 0, st, n, C.row_ptr, C.col_ind,
+            static_cast<const double*>(C.vals), static_cast<double*>(isq), static_cast<float*>(dg),
+            static_cast<unsigned long long*>(bad));
+  unsigned long long nb = 0;
+  SK_CUDA(cudaMemcpyAsync(&nb, bad, 8, cudaMemcpyDeviceToHost, st));
+  SK_CUDA(cudaStreamSynchronize(st));
+  C.sym_isq = static_cast<double*>(isq);
+  C.sym_diag = static_cast<float*>(dg);
+  C.sym_diag_state = nb ? -1 : 1;
+  return SK_OK;
+}
+
+sk_status sym_prepare_sell(sk_matrix A, cudaStream_t st) {
+  auto& C = A->csr;
+  const i64 n = A->nrow;
+  const i64 nslices = (n + 31) / 32;
+  void* wdev = nullptr;
+  sk_status s;
+  SK_CUDA(cudaMalloc(&wdev, (nslices + 1) * sizeof(int)));
+  SK_LAUNCH(sym_sell_count_kernel, ceil_div(nslices * 32, kThreads), kThreads, 0, st, n, C.row_ptr, C.col_ind,
+            static_cast<int*>(wdev));
+  std::vector<int> w(static_cast<size_t>(nslices));
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaMemcpyAsync(w.data(), wdev, nslices * sizeof(int), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  cudaFree(wdev);
+  if (e != cudaSuccess) return cuda_fail(e, "scaled SELL row counts");
+  std::vector<int> off(static_cast<size_t>(nslices) + 1, 0);
+  i64 total = 0;
+  for (i64 k = 0; k < nslices; ++k) {
+    if (w[static_cast<size_t>(k)] > 255) {
+      C.sym_sell_state = -1;
+      return SK_OK;
+    }
+    off[static_cast<size_t>(k)] = static_cast<int>(total);
+    total += 32 * static_cast<i64>(w[static_cast<size_t>(k)]);
+    if (total > (i64(1) << 31) - 64) {
+      C.sym_sell_state = -1;
+      return SK_OK;
+    }
+  }
+  off[static_cast<size_t>(nslices)] = static_cast<int>(total);
+  void *col = nullptr, *val = nullptr, *len = nullptr;
+  if ((s = dev_alloc(A, &col, (total + 64) * 4)) != SK_OK) return s;
+  if ((s = dev_alloc(A, &val, (total + 64) * 4)) != SK_OK) return s;
+  if ((s = dev_alloc(A, &len, n + 64)) != SK_OK) return s;
+  SK_CUDA(cudaMemsetAsync(col, 0, (total + 64) * 4, st));
+  SK_CUDA(cudaMemsetAsync(val, 0, (total + 64) * 4, st));
+  if ((s = upload_vector(A, off, &C.sym_off, st)) != SK_OK) return s;
+  SK_LAUNCH(sym_sell_fill_kernel, grid_for(n), kThreads, 0, st, n, C.row_ptr, C.col_ind,
+            static_cast<const double*>(C.vals), C.sym_isq, C.sym_off, static_cast<int*>(col),
+            static_cast<float*>(val), static_cast<unsigned char*>(len));
+  SK_CUDA(cudaGetLastError());
+  SK_CUDA(cudaStreamSynchronize(st));
+  C.sym_col = static_cast<int*>(col);
+  C.sym_val = static_cast<float*>(val);
+  C.sym_len = static_cast<unsigned char*>(len);
+  C.sym_sell_state = 1;
+  return SK_OK;
+}
+
+sk_status sym_prepare_dia(sk_matrix A, cudaStream_t st) {
+  auto& C = A->csr;
+  const i64 n = A->nrow;
+  SymOffsets o{};
+  for (int k = 0; k < C.dia_n; ++k)
+    if (C.dia_off[k] != 0) o.off[o.n++] = C.dia_off[k];
+  if (o.n == 0) {
+    C.sym_dia_state = -1;
+    return SK_OK;
+  }
+  const i64 len = (n + 31) / 32 * 32 * o.n;
+  void *planes = nullptr, *mask = nullptr;
+  sk_status s;
+  if ((s = dev_alloc(A, &planes, len * 4 + 64)) != SK_OK) return s;
+  if ((s = dev_alloc(A, &mask, (n + 64) * 2)) != SK_OK) return s;
+  SK_CUDA(cudaMemsetAsync(planes, 0, len * 4 + 64, st));
+  SK_LAUNCH(sym_dia_fill_kernel, grid_for(n), kThreads, 0, st, n, C.row_ptr, C.col_ind,
+            static_cast<const double*>(C.vals), C.sym_isq, o, static_cast<float*>(planes),
+            static_cast<unsigned short*>(mask));
+  SK_CUDA(cudaGetLastError());
+  SK_CUDA(cudaStreamSynchronize(st));
+  C.sym_dval = static_cast<float*>(planes);
+  C.sym_dmask = static_cast<unsigned short*>(mask);
+  C.sym_dn = o.n;
+  for (int k = 0; k < o.n; ++k) C.sym_doff[k] = o.off[k];
+  C.sym_dia_state = 1;
+  return SK_OK;
+}
+
+// The diagonal copy when the handle has one with FP32 values, else SELL.
+bool use_dia(sk_matrix A) { return A->csr.dia_n > 0 && A->csr.dia_vals32; }
+
 }  // namespace
+
+sk_status inner_sym_prepare(sk_matrix A, cudaStream_t st, bool* ok) {
+  *ok = false;
+  if (!A || A->format != SK_CSR || A->dtype != SK_F64 || A->nrow <= 0) return SK_OK;
+  const bool dia = use_dia(A);
+  if (!dia && !A->csr.sell) return SK_OK;
+  sk_status s = sym_prepare_diag(A, st);
+  if (s != SK_OK || A->csr.sym_diag_state < 0) return s;
+  if (dia) {
+    if (!A->csr.sym_dia_state && (s = sym_prepare_dia(A, st)) != SK_OK) return s;
+    *ok = A->csr.sym_dia_state > 0;
+  } else {
+    if (!A->csr.sym_sell_state && (s = sym_prepare_sell(A, st)) != SK_OK) return s;
+    *ok = A->csr.sym_sell_state > 0;
+  }
+  return SK_OK;
+}
+
+const double* inner_sym_isq(sk_matrix A) { return A->csr.sym_isq; }
 
 bool inner_persistent_ok(sk_matrix A) {
   if (!A || A->format != SK_CSR || A->nrow <= 0) return false;
@@ -476,21 +708,26 @@ bool inner_persistent_ok(sk_matrix A) {
   if (A->nrow > INT_MAX / 4) return false;
   int coop = 0;
   if (cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, A->device) != cudaSuccess || !coop) return false;
-  return coop_grid(A, pick_kernel(true, use_dia(A))) > 0 && coop_grid(A, pick_kernel(false, use_dia(A))) > 0;
+  const bool dia = use_dia(A);
+  return coop_grid(A, pick_kernel(dia, true)) > 0 && coop_grid(A, pick_kernel(dia, false)) > 0;
 }
 
 size_t inner_persistent_scratch(sk_matrix A) {
   return sizeof(SyncWords) + static_cast<size_t>(2) * kPT * kSlot * sizeof(double) + 256;
 }
 
-sk_status inner_cg_persistent(sk_matrix A, const float* inv_d, float* r, float* d, float* p, float* q,
-                              void* scratch, double tol, long long max_iters, cudaStream_t st,
-                              InnerResult* out) {
+sk_status inner_cg_persistent(sk_matrix A, bool scaled, float* r, float* d, float* p, float* q, void* scratch,
+                              double tol, long long max_iters, cudaStream_t st, InnerResult* out) {
   *out = InnerResult{};
   SK_CHECK(inner_persistent_ok(A), SK_NOT_SUPPORTED,
            "persistent inner solve needs a CSR handle with FP32 SELL values or an FP32 diagonal copy");
   const bool dia = use_dia(A);
-  const void* k = pick_kernel(inv_d != nullptr, dia);
+  const auto& C = A->csr;
+  SK_CHECK(!scaled || C.sym_diag_state > 0, SK_NOT_SUPPORTED,
+           "scaled inner solve: D^-1/2 A D^-1/2 is not formed (a diagonal entry is absent or not positive)");
+  SK_CHECK(!scaled || (dia ? C.sym_dia_state > 0 : C.sym_sell_state > 0), SK_NOT_SUPPORTED,
+           "scaled inner solve: the scaled copy is not built");
+  const void* k = pick_kernel(dia, scaled);
   int grid = coop_grid(A, k);
   SK_CHECK(grid > 0, SK_NOT_SUPPORTED, "persistent inner solve does not fit on the device");
   grid = std::min(grid, kPT);  // a CTA sums the grid's slots one per thread
@@ -501,18 +738,28 @@ sk_status inner_cg_persistent(sk_matrix A, const float* inv_d, float* r, float* 
   SK_CUDA(cudaMemsetAsync(sync, 0, sizeof(SyncWords), st));
   PArgs a{};
   a.n = static_cast<int>(A->nrow);
-  if (dia) {
-    a.val = A->csr.dia_vals32;
-    a.dia_n = A->csr.dia_n;
-    a.dia_mask = A->csr.dia_mask;
-    for (int d = 0; d < kDiaMax; ++d) a.dia_off[d] = A->csr.dia_off[d];
+  if (dia && scaled) {
+    a.val = C.sym_dval;
+    a.dia_n = C.sym_dn;
+    a.dia_mask = C.sym_dmask;
+    for (int j = 0; j < kDiaMax; ++j) a.dia_off[j] = C.sym_doff[j];
+  } else if (dia) {
+    a.val = C.dia_vals32;
+    a.dia_n = C.dia_n;
+    a.dia_mask = C.dia_mask;
+    for (int j = 0; j < kDiaMax; ++j) a.dia_off[j] = C.dia_off[j];
+  } else if (scaled) {
+    a.off = C.sym_off;
+    a.len = C.sym_len;
+    a.col = C.sym_col;
+    a.val = C.sym_val;
   } else {
-    a.off = A->csr.sell_off;
-    a.len = A->csr.sell_len;
-    a.col = A->csr.sell_col;
-    a.val = A->csr.sell_vals32;
+    a.off = C.sell_off;
+    a.len = C.sell_len;
+    a.col = C.sell_col;
+    a.val = C.sell_vals32;
   }
-  a.inv_d = inv_d;
+  a.wdiag = scaled ? C.sym_diag : nullptr;
   a.r = r;
   a.d = d;
   a.p = p;

@@ -13,22 +13,33 @@ struct InnerResult {
 };
 
 // Whether the handle can run the persistent inner solve: a CSR handle with
-// its SELL-32 copy and FP32 values, and a device that can co-schedule the
-// grid (cooperative launch).
+// its SELL-32 copy and FP32 values or its FP32 diagonal copy, and a device
+// that can co-schedule the grid (cooperative launch).
 bool inner_persistent_ok(sk_matrix A);
+
+// Forms, once per handle, the symmetrically scaled FP32 copy S = D^-1/2 A
+// D^-1/2 (without its unit diagonal) in the layout the persistent solve
+// reads (the diagonal copy when the handle has one, else SELL-32), and
+// 1 / sqrt(a_ii).  *ok is false when S cannot be formed (an FP32 handle, a
+// diagonal entry absent or not positive, no SELL-32 or diagonal copy).
+sk_status inner_sym_prepare(sk_matrix A, cudaStream_t st, bool* ok);
+
+// 1 / sqrt(a_ii) (FP64, n values) after inner_sym_prepare succeeded.
+const double* inner_sym_isq(sk_matrix A);
 
 // Scratch of the persistent solve: the grid-barrier words and the
 // per-CTA reduction slots.
 size_t inner_persistent_scratch(sk_matrix A);
 
-// Solves A d = r0 from d = 0 with Jacobi (inv_d != null) or unpreconditioned
-// CG in FP32, the reference iteration (conjugate_gradient.hpp:122-312 with
-// restart_iterations = max_iters: the true residual only at k = 0), until
-// ||r|| / ||r0|| < tol on the recursive residual or max_iters.  r holds r0 on
-// entry and the final residual on exit; p and q are work vectors of n
-// floats; scratch holds inner_persistent_scratch(A) bytes.  Synchronous.
-sk_status inner_cg_persistent(sk_matrix A, const float* inv_d, float* r, float* d, float* p, float* q,
-                              void* scratch, double tol, long long max_iters, cudaStream_t st,
-                              InnerResult* out);
+// CG in FP32 until ||r|| / ||r0|| < tol on the recursive residual of
+// A d = r0 or max_iters (conjugate_gradient.hpp:122-312 with
+// restart_iterations = max_iters: the true residual only at k = 0).
+// scaled: the Jacobi-preconditioned solve, run as CG on S y = r (r holds
+// D^-1/2 r0 on entry, d receives y; the caller scales both); otherwise
+// unpreconditioned CG on A.  r holds the final residual on exit; p and q
+// are work vectors of n floats (16-byte aligned); scratch holds
+// inner_persistent_scratch(A) bytes.  Synchronous.
+sk_status inner_cg_persistent(sk_matrix A, bool scaled, float* r, float* d, float* p, float* q, void* scratch,
+                              double tol, long long max_iters, cudaStream_t st, InnerResult* out);
 
 }  // namespace sk

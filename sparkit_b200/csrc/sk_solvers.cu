@@ -1844,6 +1844,47 @@ struct OpScaleDown {
   __device__ void finalize(const double*) const {}
 };
 
+// The scaled inner right-hand side of the Jacobi inner solve on
+// S = D^-1/2 A D^-1/2: r32 = D^-1/2 r / ||r||, and the inner guess 0.
+struct OpScaleDownSym {
+  static constexpr int kNR = 0;
+  const double* r;
+  const double* isq;
+  float* r32;
+  float* d32;
+  double inv;
+  __device__ bool prepare(const Scalars* s) {
+    inv = 1.0 / s->rnorm;
+    return true;
+  }
+  struct In { double r, s; };
+  __device__ In load(i64 i) const { return {r[i], isq[i]}; }
+  __device__ void apply(i64 i, In const& q, double*) const {
+    r32[i] = static_cast<float>(q.r * q.s * inv);
+    d32[i] = 0.0f;
+  }
+  __device__ void finalize(const double*) const {}
+};
+
+// x += ||r|| D^-1/2 y (the scaled inner solution y back in A's variables)
+struct OpRefineSym {
+  static constexpr int kNR = 0;
+  double* x;
+  const float* d32;
+  const double* isq;
+  double scale;
+  __device__ bool prepare(const Scalars* s) {
+    scale = s->rnorm;
+    return true;
+  }
+  struct In { double x, s; float d; };
+  __device__ In load(i64 i) const { return {x[i], isq[i], d32[i]}; }
+  __device__ void apply(i64 i, In const& q, double*) const {
+    x[i] = q.x + scale * (q.s * static_cast<double>(q.d));
+  }
+  __device__ void finalize(const double*) const {}
+};
+
 // x += ||r|| d
 struct OpRefine {
   static constexpr int kNR = 0;
@@ -1898,7 +1939,16 @@ static sk_status mixed_cg_solve(sk_matrix A, bool jacobi, const double* b, doubl
   //   [ r32 | r64 | outer scalars, counters, reduction slots ]
   // The inner solve runs as one persistent launch (sk_mixed.cu) when the
   // handle allows it, else as one kernel per CG step (cg_solve<float>).
-  const bool persistent = cfg->inner_kernel == 0 && inner_persistent_ok(A);
+  bool persistent = cfg->inner_kernel == 0 && inner_persistent_ok(A);
+  if (persistent && jacobi) {
+    // the persistent Jacobi inner solve runs on S = D^-1/2 A D^-1/2 (formed
+    // once per handle); without it, the per-step inner solve is used
+    bool sym_ok = false;
+    sk_status s0 = inner_sym_prepare(A, st, &sym_ok);
+    if (s0 != SK_OK) return s0;
+    persistent = sym_ok;
+  }
+  const double* isq = persistent && jacobi ? inner_sym_isq(A) : nullptr;
   out->inner_kernel = persistent ? 0 : 1;
   const int cap = spmv_grid(A);
   // persistent form: p, q and the inner residual in the first three
@@ -1988,7 +2038,10 @@ static sk_status mixed_cg_solve(sk_matrix A, bool jacobi, const double* b, doubl
         break;
       }
       if (outer >= cfg->max_outer) break;
-      launch_vec(n, OpScaleDown{r, persistent ? rv : r32, d32, 0.0}, ws, so, st);
+      if (isq)
+        launch_vec(n, OpScaleDownSym{r, isq, rv, d32, 0.0}, ws, so, st);
+      else
+        launch_vec(n, OpScaleDown{r, persistent ? rv : r32, d32, 0.0}, ws, so, st);
       // The last step needs only the remaining factor tol ||b|| / ||r||: its
       // inner tolerance is tightened to half of that when that is below the
       // configured one (floor 1e-7, about what FP32 CG can resolve), so that
@@ -2002,8 +2055,8 @@ static sk_status mixed_cg_solve(sk_matrix A, bool jacobi, const double* b, doubl
       L2Window win(cfg->l2_window ? st : nullptr, inner_base, resident_bytes);
       if (persistent) {
         InnerResult ir;
-        status = inner_cg_persistent(A, jacobi ? inv32 : nullptr, rv, d32, pv, qv, pscratch, icfg.tolerance,
-                                     icfg.max_iterations, st, &ir);
+        status = inner_cg_persistent(A, jacobi, rv, d32, pv, qv, pscratch, icfg.tolerance, icfg.max_iterations, st,
+                                     &ir);
         is.computed_iterations = ir.iterations;
         is.converged = ir.converged;
       } else {
@@ -2015,7 +2068,10 @@ static sk_status mixed_cg_solve(sk_matrix A, bool jacobi, const double* b, doubl
       if (status != SK_OK) break;
       out->inner_iterations += is.computed_iterations;
       t_outer = clk::now();
-      launch_vec(n, OpRefine{x, d32, 0.0}, ws, so, st);
+      if (isq)
+        launch_vec(n, OpRefineSym{x, d32, isq, 0.0}, ws, so, st);
+      else
+        launch_vec(n, OpRefine{x, d32, 0.0}, ws, so, st);
       out->outer_ms += ms_since(t_outer);
     }
   }

@@ -1,0 +1,265 @@
+// The C++ drop-in (include/sparkit_b200.hpp) next to the sparkit reference:
+// the reference's own matrix classes, config structs and solvers, and the
+// same unqualified calls given device operator objects.
+//
+//   dropin_test nodevice   on a machine without a GPU: the overloads compile
+//                          and construction reports SK_NO_DEVICE
+//   dropin_test gpu        on a B200: products bit-exact with the
+//                          reference's multiply in all four formats; the
+//                          configuration-1 Jacobi-CG (256 x 256 Dirichlet
+//                          Laplacian, tolerance 1e-10) against the
+//                          reference's conjugate_gradient with the same
+//                          CGConfig; BiCGSTAB and FGMRES(30) against the
+//                          reference's on 48 x 48 convection-diffusion;
+//                          the zero-diagonal error; FP32 values.
+// Prints one line per check and exits non-zero on the first failure.
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <random>
+#include <span>
+#include <string>
+#include <vector>
+
+#include <sparkit/data/chebyshev_preconditioner.hpp>
+#include <sparkit/data/conversions.hpp>
+#include <sparkit/data/jacobi.hpp>
+#include <sparkit/data/matgen.hpp>
+#include <sparkit/data/sparse_blas.hpp>
+#include <sparkit/data/spmv.hpp>
+
+#include "sparkit_b200.hpp"
+
+using namespace sparkit::data::detail;
+
+namespace {
+
+int failures = 0;
+
+void expect(bool ok, std::string const& what) {
+  std::printf("%s %s\n", ok ? "ok  " : "FAIL", what.c_str());
+  if (!ok) {
+    ++failures;
+    std::fflush(stdout);
+    std::exit(1);
+  }
+}
+
+// The configuration-1 matrix: 5-point Dirichlet Laplacian on an m x m grid
+// (4 on the diagonal, -1 to in-grid neighbours).
+template <typename T>
+Compressed_row_matrix<T> dirichlet_2d(size_type m) {
+  std::vector<Entry<T>> e;
+  for (size_type r = 0; r < m; ++r)
+    for (size_type c = 0; c < m; ++c) {
+      const auto i = r * m + c;
+      if (r > 0) e.push_back({Index{i, i - m}, T(-1)});
+      if (c > 0) e.push_back({Index{i, i - 1}, T(-1)});
+      e.push_back({Index{i, i}, T(4)});
+      if (c + 1 < m) e.push_back({Index{i, i + 1}, T(-1)});
+      if (r + 1 < m) e.push_back({Index{i, i + m}, T(-1)});
+    }
+  return make_matrix<T>(Shape{m * m, m * m}, e);
+}
+
+template <typename T>
+std::vector<T> uniform(std::size_t n, unsigned seed) {
+  std::mt19937_64 g(seed);
+  std::uniform_real_distribution<double> u(-1.0, 1.0);
+  std::vector<T> v(n);
+  for (auto& x : v) x = static_cast<T>(u(g));
+  return v;
+}
+
+bool iters_close(long long a, long long b) { return std::llabs(a - b) <= std::max(2LL, (b * 2 + 99) / 100); }
+
+template <typename T>
+double rel_residual(Compressed_row_matrix<T> const& A, std::vector<T> const& b, std::vector<T> const& x) {
+  auto ax = multiply(A, std::span<T const>{x});
+  double num = 0, den = 0;
+  for (std::size_t i = 0; i < b.size(); ++i) {
+    num += (double(b[i]) - double(ax[i])) * (double(b[i]) - double(ax[i]));
+    den += double(b[i]) * double(b[i]);
+  }
+  return std::sqrt(num / den);
+}
+
+template <typename M, typename T>
+void check_product(char const* name, M const& host, std::vector<T> const& x, std::vector<T> const& ref) {
+  sk::gpu::Device_matrix<T> Ad(host);
+  auto y = multiply(Ad, std::span<T const>{x});
+  expect(y == ref, std::string("multiply bit-exact: ") + name);
+}
+
+void run_gpu() {
+  // ---- products in the four formats against the reference's multiply
+  {
+    auto A = dirichlet_2d<double>(40);
+    auto x = uniform<double>(1600, 7);
+    auto y = multiply(A, std::span<double const>{x});
+    check_product("CSR", A, x, y);
+    check_product("ELL", to_ellpack(A), x, multiply(to_ellpack(A), std::span<double const>{x}));
+    check_product("JAD", to_jagged_diagonal(A), x, multiply(to_jagged_diagonal(A), std::span<double const>{x}));
+    check_product("BSR 2x2", to_block_sparse_row(A, 2, 2), x,
+                  multiply(to_block_sparse_row(A, 2, 2), std::span<double const>{x}));
+  }
+  // ---- configuration 1: Jacobi-CG, 256 x 256, tolerance 1e-10
+  {
+    const size_type m = 256, n = m * m;
+    auto A = dirichlet_2d<double>(m);
+    auto xs = uniform<double>(n, 0);
+    auto b = multiply(A, std::span<double const>{xs});
+    CGConfig<double> cfg{.tolerance = 1e-10, .restart_iterations = 100000, .max_iterations = 100000};
+    // the reference, as its tests call it
+    auto inv_d = jacobi(A);
+    auto apply_A = [&A](auto first, auto last, auto out) {
+      auto r = multiply(A, std::span<double const>{first, last});
+      std::copy(r.begin(), r.end(), out);
+    };
+    auto apply_J = [&inv_d](auto first, auto last, auto out) { jacobi_apply(inv_d, first, last, out); };
+    auto ident = [](auto first, auto last, auto out) { std::copy(first, last, out); };
+    std::vector<double> x_ref(n, 0.0);
+    auto s_ref = conjugate_gradient(b.begin(), b.end(), x_ref.begin(), x_ref.end(), cfg, apply_A, apply_J, ident);
+    // the drop-in: the same call with device objects
+    sk::gpu::Device_matrix<double> Ad(A);
+    std::vector<double> x(n, 0.0);
+    auto s = conjugate_gradient(b.begin(), b.end(), x.begin(), x.end(), cfg, sk::gpu::spmv(Ad), sk::gpu::jacobi(Ad),
+                                sk::gpu::identity);
+    std::printf("     config 1: device %lld iterations, reference %lld\n", (long long)s.computed_iterations,
+                (long long)s_ref.computed_iterations);
+    static_assert(std::is_same_v<decltype(s), CGSummary<double>>);
+    expect(s.converged && s_ref.converged, "config 1 converged");
+    expect(iters_close(s.computed_iterations, s_ref.computed_iterations), "config 1 iterations within 2%");
+    expect(rel_residual(A, b, x) < 1e-9, "config 1 true residual");
+    double dx = 0, nx = 0;
+    for (size_type i = 0; i < n; ++i) {
+      dx = std::max(dx, std::abs(x[i] - x_ref[i]));
+      nx = std::max(nx, std::abs(x_ref[i]));
+    }
+    expect(dx <= 1e-7 * nx, "config 1 solution agrees with the reference's");
+    // residual history as in the reference
+    CGConfig<double> hcfg{.tolerance = 1e-10, .restart_iterations = 100000, .max_iterations = 40,
+                          .collect_residuals = true};
+    std::vector<double> xh(n, 0.0), xh_ref(n, 0.0);
+    auto h = conjugate_gradient(b.begin(), b.end(), xh.begin(), xh.end(), hcfg, sk::gpu::spmv(Ad),
+                                sk::gpu::jacobi(Ad), sk::gpu::identity);
+    auto h_ref = conjugate_gradient(b.begin(), b.end(), xh_ref.begin(), xh_ref.end(), hcfg, apply_A, apply_J, ident);
+    bool same = h.iteration_residuals.size() == h_ref.iteration_residuals.size();
+    for (std::size_t k = 0; same && k < h.iteration_residuals.size(); ++k)
+      same = std::abs(h.iteration_residuals[k] - h_ref.iteration_residuals[k]) <=
+             1e-10 * std::abs(h_ref.iteration_residuals[k]);
+    expect(same && !h.converged && h.computed_iterations == 40, "CG residual history follows the reference's");
+  }
+  // ---- BiCGSTAB and FGMRES(30) on 48 x 48 upwind convection-diffusion
+  {
+    auto A = convection_diffusion_2d<double>(48, 48, 1.0, 0.9, 0.5);
+    const std::size_t n = 48 * 48;
+    auto xs = uniform<double>(n, 2);
+    auto b = multiply(A, std::span<double const>{xs});
+    auto inv_d = jacobi(A);
+    auto apply_A = [&A](auto first, auto last, auto out) {
+      auto r = multiply(A, std::span<double const>{first, last});
+      std::copy(r.begin(), r.end(), out);
+    };
+    auto apply_J = [&inv_d](auto first, auto last, auto out) { jacobi_apply(inv_d, first, last, out); };
+    auto ident = [](auto first, auto last, auto out) { std::copy(first, last, out); };
+    sk::gpu::Device_matrix<double> Ad(A);
+    {
+      Bicgstab_config<double> cfg{.tolerance = 1e-10, .max_iterations = 3000};
+      std::vector<double> x(n, 0.0), x_ref(n, 0.0);
+      auto s_ref = bicgstab(b.begin(), b.end(), x_ref.begin(), x_ref.end(), cfg, apply_A, apply_J, ident);
+      auto s = bicgstab(b.begin(), b.end(), x.begin(), x.end(), cfg, sk::gpu::spmv(Ad), sk::gpu::jacobi(Ad),
+                        sk::gpu::identity);
+      static_assert(std::is_same_v<decltype(s), Bicgstab_summary<double>>);
+      std::printf("     BiCGSTAB: device %lld, reference %lld\n", (long long)s.computed_iterations,
+                  (long long)s_ref.computed_iterations);
+      expect(s.converged == s_ref.converged && s.converged, "BiCGSTAB converged");
+      expect(iters_close(s.computed_iterations, s_ref.computed_iterations), "BiCGSTAB iterations within 2%");
+      expect(rel_residual(A, b, x) < 1e-9, "BiCGSTAB true residual");
+    }
+    {
+      Fgmres_config<double> cfg{.tolerance = 1e-10, .restart_dimension = 30, .max_iterations = 3000};
+      std::vector<double> x(n, 0.0), x_ref(n, 0.0);
+      auto s_ref = fgmres(b.begin(), b.end(), x_ref.begin(), x_ref.end(), cfg, apply_A, apply_J);
+      auto s = fgmres(b.begin(), b.end(), x.begin(), x.end(), cfg, sk::gpu::spmv(Ad), sk::gpu::jacobi(Ad));
+      static_assert(std::is_same_v<decltype(s), Fgmres_summary<double>>);
+      std::printf("     FGMRES(30): device %lld, reference %lld\n", (long long)s.computed_iterations,
+                  (long long)s_ref.computed_iterations);
+      expect(s.converged && s_ref.converged, "FGMRES converged");
+      expect(iters_close(s.computed_iterations, s_ref.computed_iterations), "FGMRES iterations within 2%");
+      expect(rel_residual(A, b, x) < 1e-9, "FGMRES true residual");
+    }
+    {
+      // Chebyshev with the reference's coefficients, through the device apply
+      auto T4 = tridiagonal_matrix<double>(64, -1.0, 4.0, -1.0);
+      auto bt = uniform<double>(64, 3);
+      auto prec = chebyshev_preconditioner(T4, 2.0, 6.0, 5);
+      auto apply_T = [&T4](auto first, auto last, auto out) {
+        auto r = multiply(T4, std::span<double const>{first, last});
+        std::copy(r.begin(), r.end(), out);
+      };
+      auto apply_C = [&prec](auto first, auto last, auto out) { chebyshev_preconditioner_apply(prec, first, last, out); };
+      CGConfig<double> cfg{.tolerance = 1e-12, .restart_iterations = 50, .max_iterations = 100};
+      std::vector<double> x(64, 0.0), x_ref(64, 0.0);
+      auto s_ref = conjugate_gradient(bt.begin(), bt.end(), x_ref.begin(), x_ref.end(), cfg, apply_T, apply_C, ident);
+      sk::gpu::Device_matrix<double> Td(T4);
+      auto s = conjugate_gradient(bt.begin(), bt.end(), x.begin(), x.end(), cfg, sk::gpu::spmv(Td),
+                                  sk::gpu::chebyshev(Td, 2.0, 6.0, 5), sk::gpu::identity);
+      expect(s.converged && s_ref.converged && iters_close(s.computed_iterations, s_ref.computed_iterations),
+             "Chebyshev-preconditioned CG against the reference's");
+    }
+  }
+  // ---- jacobi on a zero diagonal throws as jacobi.hpp:31 does
+  {
+    auto Z = make_matrix<double>(Shape{2, 2}, {Entry<double>{Index{0, 1}, 1.0}, Entry<double>{Index{1, 1}, 2.0}});
+    sk::gpu::Device_matrix<double> Zd(Z);
+    bool threw = false;
+    try {
+      (void)sk::gpu::jacobi(Zd);
+    } catch (std::invalid_argument const& e) {
+      threw = std::string(e.what()) == "jacobi: zero diagonal entry";
+    }
+    expect(threw, "zero diagonal throws std::invalid_argument");
+  }
+  // ---- FP32 values
+  {
+    auto A = dirichlet_2d<float>(64);
+    auto xs = uniform<float>(4096, 5);
+    auto b = multiply(A, std::span<float const>{xs});
+    sk::gpu::Device_matrix<float> Ad(A);
+    auto y = multiply(Ad, std::span<float const>{xs});
+    expect(y == b, "FP32 multiply bit-exact");
+    std::vector<float> x(4096, 0.0f);
+    CGConfig<float> cfg{.tolerance = 1e-5f, .restart_iterations = 10000, .max_iterations = 10000};
+    auto s = conjugate_gradient(b.begin(), b.end(), x.begin(), x.end(), cfg, sk::gpu::spmv(Ad), sk::gpu::jacobi(Ad),
+                                sk::gpu::identity);
+    expect(s.converged && rel_residual(A, b, x) < 1e-4, "FP32 Jacobi-CG converged");
+  }
+}
+
+void run_nodevice() {
+  auto A = dirichlet_2d<double>(4);
+  bool no_device = false;
+  try {
+    sk::gpu::Device_matrix<double> Ad(A);
+  } catch (sk::gpu::error const& e) {
+    no_device = e.status() == SK_NO_DEVICE;
+  }
+  expect(no_device, "construction without a GPU reports SK_NO_DEVICE");
+}
+
+}  // namespace
+
+int main(int argc, char** argv) {
+  const std::string mode = argc > 1 ? argv[1] : "";
+  if (mode == "gpu") {
+    run_gpu();
+  } else if (mode == "nodevice") {
+    run_nodevice();
+  } else {
+    std::fprintf(stderr, "usage: dropin_test gpu|nodevice\n");
+    return 2;
+  }
+  std::printf("dropin_test %s: all checks passed\n", mode.c_str());
+  return failures ? 1 : 0;
+}
