@@ -33,6 +33,73 @@ inline int prec_kind(const sk_precond_s* M) {
 }
 
 // ------------------------------------------------------------------
+// Step chunks as CUDA graphs.  Once a solve has run its first chunks
+// directly, each later chunk of `len` steps (the same launches with the
+// same arguments every time: the kernels read their scalars from device
+// memory and turn into no-ops once the solve is done) is captured once and
+// then replayed, one graph launch per chunk instead of one host launch per
+// kernel.  Preconditioners whose apply does host work (the learned network,
+// the two-level form) keep the direct launches.
+// ------------------------------------------------------------------
+struct StepGraph {
+  cudaGraphExec_t exec = nullptr;
+  i64 len = 0;
+  i64 launches = 0;
+  StepGraph() = default;
+  StepGraph(StepGraph const&) = delete;
+  StepGraph& operator=(StepGraph const&) = delete;
+  ~StepGraph() {
+    if (exec) cudaGraphExecDestroy(exec);
+  }
+  // Enqueues `n_steps` steps on gs through the graph (captured on first use
+  // or when the chunk length changes); enqueue(n) issues n steps on gs.
+  template <class F>
+  sk_status replay(cudaStream_t gs, i64 n_steps, F const& enqueue) {
+    if (!exec || len != n_steps) {
+      if (exec) cudaGraphExecDestroy(exec);
+      exec = nullptr;
+      const i64 before = g_launches.load();
+      cudaGraph_t g = nullptr;
+      cudaError_t e = cudaStreamBeginCapture(gs, cudaStreamCaptureModeThreadLocal);
+      if (e == cudaSuccess) {
+        enqueue(n_steps);
+        e = cudaStreamEndCapture(gs, &g);
+      }
+      if (e == cudaSuccess) e = cudaGraphInstantiate(&exec, g, 0);
+      if (g) cudaGraphDestroy(g);
+      if (e != cudaSuccess) {
+        exec = nullptr;
+        return cuda_fail(e, "solver step capture");
+      }
+      launches = g_launches.load() - before;
+      g_launches.fetch_sub(launches);  // counted at each replay instead
+      len = n_steps;
+    }
+    g_launches.fetch_add(launches);
+    SK_CUDA(cudaGraphLaunch(exec, gs));
+    return SK_OK;
+  }
+};
+
+// Whether a preconditioner's apply is device launches only (none, Jacobi,
+// Chebyshev), so that its steps can be captured.
+inline bool capturable(const sk_precond_s* M) { return !M || M->kind == 1 || M->kind == 2; }
+
+// The stream a solve with captured chunks runs on: the caller's, unless it
+// is a default stream (the legacy stream cannot be captured), in which case
+// the caller's stream is drained and the handle's own stream is used.  The
+// solve's last host read synchronizes that stream, so the caller sees the
+// results in order.
+static sk_status solve_stream(sk_matrix A, cudaStream_t st, cudaStream_t* gs) {
+  *gs = st;
+  if (st == nullptr || st == cudaStreamLegacy || st == cudaStreamPerThread) {
+    SK_CUDA(cudaStreamSynchronize(st));
+    *gs = A->stream;
+  }
+  return SK_OK;
+}
+
+// ------------------------------------------------------------------
 // Workspace carved out of the handle's grow-only buffer.
 // ------------------------------------------------------------------
 struct Carver {
@@ -372,11 +439,11 @@ static sk_status cg_solve(sk_matrix A, sk_precond L, sk_precond R, const T* b, T
   h.hist_on = cfg->collect_residuals ? 1 : 0;
   if ((s = put_scalars(c.sc, h, st)) != SK_OK) return s;
   const int lk = prec_kind(L);
-  i64 k = 0, chunk = 8;
-  while (k < cfg->max_iterations) {
-    const i64 todo = std::min(chunk, cfg->max_iterations - k);
-    for (i64 j = 0; j < todo; ++j, ++k) {
-      const bool reorth = (k % cfg->restart_iterations) == 0;
+  const bool graphs = capturable(L) && capturable(R);
+  if (graphs && (s = solve_stream(A, st, &st)) != SK_OK) return s;
+  auto steps = [&](i64 k0, i64 cnt) {
+    for (i64 j = 0; j < cnt; ++j) {
+      const bool reorth = ((k0 + j) % cfg->restart_iterations) == 0;
       if (lk == PK_IDENTITY)
         cg_iteration<T, PK_IDENTITY>(A, L, R, reorth, b, x, r, z, p, hatp, q, c, st, vals);
       else if (lk == PK_JACOBI)
@@ -384,10 +451,25 @@ static sk_status cg_solve(sk_matrix A, sk_precond L, sk_precond R, const T* b, T
       else
         cg_iteration<T, PK_OTHER>(A, L, R, reorth, b, x, r, z, p, hatp, q, c, st, vals);
     }
+  };
+  StepGraph sg;
+  constexpr i64 kMaxChunk = 64;
+  i64 k = 0, chunk = 8;
+  while (k < cfg->max_iterations) {
+    const i64 todo = std::min(chunk, cfg->max_iterations - k);
+    // a chunk without a true-residual step (k % restart_iterations == 0)
+    // repeats the same launches and is replayed from its graph
+    const i64 next_reorth = (k + cfg->restart_iterations - 1) / cfg->restart_iterations * cfg->restart_iterations;
+    if (graphs && todo == kMaxChunk && next_reorth >= k + todo) {
+      if ((s = sg.replay(st, todo, [&](i64 cnt) { steps(k, cnt); })) != SK_OK) return s;
+    } else {
+      steps(k, todo);
+    }
+    k += todo;
     SK_CUDA(cudaGetLastError());
     if ((s = read_scalars(c.sc, &h, st)) != SK_OK) return s;
     if (h.done) break;
-    chunk = std::min<i64>(chunk * 2, 64);
+    chunk = std::min<i64>(chunk * 2, kMaxChunk);
   }
   return finish_summary(c, st, out, history_host);
 }
@@ -707,9 +789,10 @@ static sk_status bicgstab_solve(sk_matrix A, sk_precond L, sk_precond R, const T
   SK_CUDA(cudaMemsetAsync(v, 0, n * sizeof(T), st));
   launch_spmv<T>(A, x, EpiBiResid<T>{b, r, r_hat, c.sc}, c.ws, nullptr, st);
   const int lk = prec_kind(L), rk = prec_kind(R);
-  i64 steps = 0, chunk = 4;
-  while (steps < std::max<i64>(cfg->max_iterations, 1)) {
-    for (i64 j = 0; j < chunk; ++j, ++steps) {
+  const bool graphs = capturable(L) && capturable(R);
+  if (graphs && (s = solve_stream(A, st, &st)) != SK_OK) return s;
+  auto steps_of = [&](i64 cnt) {
+    for (i64 j = 0; j < cnt; ++j) {
 #define SK_BI_STEP(LKV, RKV)                                                                  \
   bicgstab_step<T, LKV, RKV>(A, L, R, x, r, r_hat, p, v, sv, t, p_hat, s_hat, tmp, c, st)
       if (lk == PK_IDENTITY && rk == PK_IDENTITY) SK_BI_STEP(PK_IDENTITY, PK_IDENTITY);
@@ -719,10 +802,21 @@ static sk_status bicgstab_solve(sk_matrix A, sk_precond L, sk_precond R, const T
       else SK_BI_STEP(PK_OTHER, PK_OTHER);
 #undef SK_BI_STEP
     }
+  };
+  StepGraph sg;
+  constexpr i64 kMaxChunk = 32;
+  i64 steps = 0, chunk = 4;
+  while (steps < std::max<i64>(cfg->max_iterations, 1)) {
+    if (graphs && chunk == kMaxChunk) {
+      if ((s = sg.replay(st, chunk, steps_of)) != SK_OK) return s;
+    } else {
+      steps_of(chunk);
+    }
+    steps += chunk;
     SK_CUDA(cudaGetLastError());
     if ((s = read_scalars(c.sc, &h, st)) != SK_OK) return s;
     if (h.done && !h.half) break;
-    chunk = std::min<i64>(chunk * 2, 32);
+    chunk = std::min<i64>(chunk * 2, kMaxChunk);
   }
   return finish_summary(c, st, out, history_host);
 }
@@ -1429,9 +1523,10 @@ static sk_status cgs_solve(sk_matrix A, sk_precond L, sk_precond R, const T* b, 
   if ((s = put_scalars(c.sc, h, st)) != SK_OK) return s;
   launch_spmv<T>(A, x, EpiCgsInit<T>{b, r, r_hat, p, u, c.sc}, c.ws, nullptr, st);
   const LRPair<T> lr(L, R);
-  i64 steps = 0, chunk = 4;
-  while (!h.done) {
-    for (i64 j = 0; j < chunk; ++j, ++steps) {  // cgs_step (:212-232)
+  const bool graphs = capturable(L) && capturable(R);
+  if (graphs && (s = solve_stream(A, st, &st)) != SK_OK) return s;
+  auto steps_of = [&](i64 cnt) {
+    for (i64 j = 0; j < cnt; ++j) {  // cgs_step (:212-232)
       apply_lr<T>(lr, n, p, tmp, p_hat, c, st);
       launch_spmv<T>(A, p_hat, EpiCgsQhat<T>{q_hat, r_hat, c.sc}, c.ws, c.sc, st);
       launch_vec(n, OpCgsQ<T>{u, q_hat, q, u_hat, p_hat, x, lr.invl, lr.invr, lr.fused, T(0)}, c.ws, c.sc, st);
@@ -1442,9 +1537,19 @@ static sk_status cgs_solve(sk_matrix A, sk_precond L, sk_precond R, const T* b, 
       launch_spmv<T>(A, p_hat, EpiCgsR<T>{r, r_hat, c.sc, c.hist}, c.ws, c.sc, st);
       launch_vec(n, OpCgsDir<T>{r, q, u, p, T(0)}, c.ws, c.sc, st);
     }
+  };
+  StepGraph sg;
+  constexpr i64 kMaxChunk = 32;
+  i64 chunk = 4;
+  while (!h.done) {
+    if (graphs && chunk == kMaxChunk) {
+      if ((s = sg.replay(st, chunk, steps_of)) != SK_OK) return s;
+    } else {
+      steps_of(chunk);
+    }
     SK_CUDA(cudaGetLastError());
     if ((s = read_scalars(c.sc, &h, st)) != SK_OK) return s;
-    chunk = std::min<i64>(chunk * 2, 32);
+    chunk = std::min<i64>(chunk * 2, kMaxChunk);
   }
   return finish_summary(c, st, out, history_host);
 }
@@ -1732,9 +1837,10 @@ static sk_status minres_solve(sk_matrix A, sk_precond L, sk_precond R, const T* 
   SK_CUDA(cudaGetLastError());
   if ((s = read_scalars(c.sc, &h, st)) != SK_OK) return s;
   if (!h.done && cfg->max_iterations <= 0) h.done = 1;
-  i64 chunk = 4;
-  while (!h.done) {
-    for (i64 j = 0; j < chunk; ++j) {  // minres_step (:225-234)
+  const bool graphs = capturable(L) && capturable(R);
+  if (graphs && (s = solve_stream(A, st, &st)) != SK_OK) return s;
+  auto steps_of = [&](i64 cnt) {
+    for (i64 j = 0; j < cnt; ++j) {  // minres_step (:225-234)
       launch_spmv<T>(A, z, EpiMinW<T>{w, z, ms}, c.ws, c.sc, st);
       launch_vec(n, OpMinLanczos<T>{w, v, vp, lr.invl, lr.invr, lr.fused, c.sc, ms, c.hist, T(0), T(0)}, c.ws,
                  c.sc, st);
@@ -1744,9 +1850,19 @@ static sk_status minres_solve(sk_matrix A, sk_precond L, sk_precond R, const T* 
       }
       launch_vec(n, OpMinUpdate<T>{d, dp, x, z, v, vp, w, ms, T(0), T(0), T(0), T(0), T(0), 0}, c.ws, nullptr, st);
     }
+  };
+  StepGraph sg;
+  constexpr i64 kMaxChunk = 32;
+  i64 chunk = 4;
+  while (!h.done) {
+    if (graphs && chunk == kMaxChunk) {
+      if ((s = sg.replay(st, chunk, steps_of)) != SK_OK) return s;
+    } else {
+      steps_of(chunk);
+    }
     SK_CUDA(cudaGetLastError());
     if ((s = read_scalars(c.sc, &h, st)) != SK_OK) return s;
-    chunk = std::min<i64>(chunk * 2, 32);
+    chunk = std::min<i64>(chunk * 2, kMaxChunk);
   }
   return finish_summary(c, st, out, history_host);
 }
