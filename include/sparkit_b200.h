@@ -70,6 +70,23 @@ SK_API sk_status sk_device_count(int* count);
 /* Count of this library's kernel launches since load (for accounting). */
 SK_API sk_status sk_launch_count(int64_t* count);
 
+/* Summation order of the solvers' dot products and norms (process-wide,
+ * read at the start of each solve).  SK_SUM_TREE (the default) sums each
+ * one in a fixed, deterministic tree over the grid: repeatable bit for bit,
+ * and fast.  SK_SUM_SEQUENTIAL sums the terms one after another in element
+ * order, in the value type, as std::inner_product does in every solver of
+ * the reference (conjugate_gradient.hpp:194-282, bicgstab.hpp:328-335,
+ * fgmres.hpp:266,400, cgs.hpp:313-320, minres.hpp:170-259,
+ * gmres.hpp:165-272); with the products and
+ * element-wise updates already in the reference's arithmetic order, a
+ * solve then reproduces the reference's iterates.  It is for validation:
+ * one warp adds each sum's n terms in turn, which costs n dependent
+ * additions per dot product.  The mixed-precision, batched and Lanczos
+ * paths keep the tree order. */
+enum { SK_SUM_TREE = 0, SK_SUM_SEQUENTIAL = 1 };
+SK_API sk_status sk_set_summation_order(int32_t order);
+SK_API sk_status sk_get_summation_order(int32_t* order);
+
 /* No reference counterpart: a setting for tests of the timeout path.  The
  * persistent kernels (the mixed solver's inner CG, the GMRES / FGMRES
  * Arnoldi step) wait at grid barriers, and every wait is bounded in time:

@@ -235,8 +235,24 @@ static void SKO_FN(sko_apply_prec_)(const sko_precond* M, const sko_operator* A,
  * instead taken in 256-element sequential chunks whose partial sums are then
  * added in order -- a different association of the same products, used only
  * to measure how sensitive a solver's iteration count is to the summation
- * order (the GPU sums in a fixed tree). */
+ * order (the GPU sums in a fixed tree by default).  Order 2 sums from the
+ * last element down; order 3 sums the rounded products accurately
+ * (double-double) and rounds once. */
 static SKO_T SKO_FN(sko_dot_)(const SKO_T* a, const SKO_T* b, int64_t n) {
+  if (sko_dot_order == 3) {
+    /* the same rounded products summed in double-double (two-sum of each
+     * addition, Knuth; accurate to about 2^-104 of the sum's magnitude) and
+     * rounded once: the accurately summed dot product */
+    double hi = 0.0, lo = 0.0;
+    for (int64_t i = 0; i < n; ++i) {
+      const double p = (double)(a[i] * b[i]);
+      const double s = hi + p;
+      const double bp = s - hi;
+      lo += (hi - (s - bp)) + (p - bp);
+      hi = s;
+    }
+    return (SKO_T)(hi + lo);
+  }
   if (sko_dot_order == 2) {
     SKO_T s = 0;
     for (int64_t i = n; i > 0; --i) s += a[i - 1] * b[i - 1];

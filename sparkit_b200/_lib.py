@@ -104,6 +104,8 @@ SIGNATURES = [
     ("sk_device_count", [ctypes.POINTER(ctypes.c_int)]),
     ("sk_launch_count", [P_i64]),
     ("sk_debug_set_wait", [ctypes.c_uint64, ctypes.c_int32]),
+    ("sk_set_summation_order", [ctypes.c_int32]),
+    ("sk_get_summation_order", [ctypes.POINTER(ctypes.c_int32)]),
     ("sk_device_alloc", [ctypes.POINTER(c_vp), ctypes.c_size_t]),
     ("sk_device_free", [c_vp]),
     ("sk_memcpy_h2d", [c_vp, c_vp, ctypes.c_size_t, c_vp]),

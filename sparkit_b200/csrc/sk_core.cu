@@ -14,6 +14,8 @@ std::atomic<i64> g_launches{0};
 constexpr unsigned long long kDefaultWaitNs = 2000000000ull;  // 2 s per barrier wait
 static std::atomic<unsigned long long> g_wait_ns{kDefaultWaitNs};
 static std::atomic<unsigned> g_wait_bias{0};
+static std::atomic<int> g_sum_order{0};
+bool summation_sequential() { return g_sum_order.load(std::memory_order_relaxed) != 0; }
 unsigned long long wait_limit_ns() { return g_wait_ns.load(std::memory_order_relaxed); }
 unsigned wait_target_bias() { return g_wait_bias.load(std::memory_order_relaxed); }
 static thread_local std::string t_last_error;
@@ -419,6 +421,18 @@ sk_status sk_device_count(int* count) {
 sk_status sk_launch_count(int64_t* count) {
   SK_CHECK(count, SK_INVALID_ARG, "null count");
   *count = g_launches.load();
+  return SK_OK;
+}
+
+sk_status sk_set_summation_order(int32_t order) {
+  SK_CHECK(order == SK_SUM_TREE || order == SK_SUM_SEQUENTIAL, SK_INVALID_ARG, "unknown summation order");
+  g_sum_order.store(order);
+  return SK_OK;
+}
+
+sk_status sk_get_summation_order(int32_t* order) {
+  SK_CHECK(order, SK_INVALID_ARG, "null pointer");
+  *order = g_sum_order.load();
   return SK_OK;
 }
 

@@ -237,11 +237,24 @@ sk_status dev_alloc(sk_matrix A, void** p, size_t bytes);
 // Grid-wide deterministic reduction workspace: one slot of kMaxRed doubles
 // per CTA plus an arrival counter.  The last CTA to arrive sums the slots in
 // CTA order, so the result does not depend on scheduling.
+//
+// In the sequential summation order (sk_set_summation_order), `seq` holds
+// each element's terms instead (term j of element i at seq[j * seq_ld + i],
+// i < seq_n), and the last CTA sums them in element order, one warp per
+// reduction, in the value type (seq_f32: float), as std::inner_product does.
 struct RedWs {
   double* partials = nullptr;
   unsigned* counter = nullptr;
   int capacity = 0;  // CTAs
+  double* seq = nullptr;
+  i64 seq_ld = 0;
+  i64 seq_n = 0;
+  int seq_f32 = 0;
 };
+
+// Whether the solvers sum their dot products in the reference's sequential
+// order (sk_set_summation_order); read once at the start of each solve.
+bool summation_sequential();
 
 // Solver scalars resident on the device for a whole solve.  Written only
 // by the finalize step of a fused kernel (one thread of the last CTA) or by

@@ -76,9 +76,38 @@ __device__ __forceinline__ void block_reduce(double (&v)[NR]) {
 
 // Sums v over the whole grid; the last CTA to arrive calls fin(total) on
 // thread 0.  Deterministic: CTA partials are summed in CTA order.
+// The sequential order: warp j sums term j of elements 0 .. n-1 in element
+// order (s = s + t_i from s = 0, in the value type), each lane holding the
+// same running sum; the 32 terms of the next group are loaded while the
+// current group is added.  Result in t[j] of every lane of warp j.
+template <int NR>
+__device__ __forceinline__ void sequential_sums(RedWs const& ws, double (&t)[NR]) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (warp >= NR) return;
+  const double* src = ws.seq + static_cast<size_t>(warp) * ws.seq_ld;
+  const i64 n = ws.seq_n;
+  double s64 = 0.0;
+  float s32 = 0.0f;
+  double nxt = lane < n ? __ldcg(src + lane) : 0.0;
+  for (i64 i0 = 0; i0 < n; i0 += 32) {
+    const double cur = nxt;
+    nxt = i0 + 32 + lane < n ? __ldcg(src + i0 + 32 + lane) : 0.0;
+    const int cnt = n - i0 < 32 ? static_cast<int>(n - i0) : 32;
+    if (ws.seq_f32) {
+      for (int k = 0; k < cnt; ++k) s32 = __fadd_rn(s32, static_cast<float>(__shfl_sync(0xffffffffu, cur, k)));
+    } else {
+      for (int k = 0; k < cnt; ++k) s64 = __dadd_rn(s64, __shfl_sync(0xffffffffu, cur, k));
+    }
+  }
+#pragma unroll
+  for (int j = 0; j < NR; ++j)
+    if (j == warp) t[j] = ws.seq_f32 ? static_cast<double>(s32) : s64;
+}
+
 template <int NR, class Fin>
 __device__ __forceinline__ void grid_reduce(double (&v)[NR], RedWs ws, Fin const& fin) {
   __shared__ bool am_last;
+  __shared__ double seq_tot[NR];
   block_reduce<NR>(v);
   if (threadIdx.x == 0) {
 #pragma unroll
@@ -93,6 +122,19 @@ __device__ __forceinline__ void grid_reduce(double (&v)[NR], RedWs ws, Fin const
   double t[NR];
 #pragma unroll
   for (int j = 0; j < NR; ++j) t[j] = 0.0;
+  if (ws.seq) {
+    sequential_sums<NR>(ws, t);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (warp < NR && lane == 0) seq_tot[warp] = t[warp];
+    __syncthreads();
+    if (threadIdx.x == 0) {
+#pragma unroll
+      for (int j = 0; j < NR; ++j) t[j] = seq_tot[j];
+      fin(t);
+      *ws.counter = 0u;
+    }
+    return;
+  }
   // 4 partials per thread in flight at a time: the loads are independent,
   // only their (fixed-order) sum is sequential
   unsigned b = threadIdx.x;
@@ -120,6 +162,25 @@ __device__ __forceinline__ void grid_reduce(double (&v)[NR], RedWs ws, Fin const
 
 __device__ __forceinline__ bool solve_done(const Scalars* sc) {
   return sc != nullptr && *reinterpret_cast<const volatile int*>(&sc->done) != 0;
+}
+
+// Hands element i's contribution to a fused reduction: accumulated into
+// red (the tree order), or, in the sequential order, stored as element i's
+// terms for the last CTA to sum in element order.
+template <int NR, class F>
+__device__ __forceinline__ void reduce_terms(RedWs const& ws, i64 i, double* red, F const& f) {
+  if constexpr (NR > 0) {
+    if (ws.seq) {
+      double e[NR];
+#pragma unroll
+      for (int j = 0; j < NR; ++j) e[j] = 0.0;
+      f(e);
+#pragma unroll
+      for (int j = 0; j < NR; ++j) ws.seq[static_cast<size_t>(j) * ws.seq_ld + i] = e[j];
+      return;
+    }
+  }
+  f(red);
 }
 
 // ------------------------------------------------------------------
@@ -195,7 +256,7 @@ csr_spmv_kernel(const int* __restrict__ rp, const int* __restrict__ ci,
       part_sum = add(part_sum, mul(__ldcs(va + k), __ldg(x + __ldcs(ci + k))));
     acc[0] = static_cast<double>(part_sum);
     block_reduce<1>(acc);
-    if (tid == 0) epi(r0, static_cast<T>(acc[0]), red);
+    if (tid == 0) reduce_terms<NR>(ws, r0, red, [&](double* rr) { epi(r0, static_cast<T>(acc[0]), rr); });
   } else {
     // Thread tid owns entries s + tid + 256 j (j < 8).  Row 0 of the tile
     // starts at s and row nr ends at e, so only rows 1..nr-1 need rp.
@@ -233,7 +294,7 @@ csr_spmv_kernel(const int* __restrict__ rp, const int* __restrict__ ci,
         const int a = srp[tid], b = srp[tid + 1];
         T sum = T(0);
         for (int k = a; k < b; ++k) sum = add(sum, sprod[k]);
-        epi(r0 + tid, sum, red);
+        reduce_terms<NR>(ws, r0 + tid, red, [&](double* rr) { epi(r0 + tid, sum, rr); });
       }
     } else {
       // L lanes per row (a power of two chosen at upload from the tile's
@@ -250,7 +311,7 @@ csr_spmv_kernel(const int* __restrict__ rp, const int* __restrict__ ci,
         }
         for (int off = L >> 1; off > 0; off >>= 1)
           sum = add(sum, __shfl_xor_sync(0xffffffffu, sum, off));
-        if (row < nr && lane == 0) epi(r0 + row, sum, red);
+        if (row < nr && lane == 0) reduce_terms<NR>(ws, r0 + row, red, [&](double* rr) { epi(r0 + row, sum, rr); });
       }
     }
   }
@@ -335,7 +396,7 @@ sell_spmv_kernel(int nrow, const int* __restrict__ off, const unsigned char* __r
       c = __ldcs(cp + 32 * k);
       v = __ldcs(vp + 32 * k);
     });
-    epi(i, sum, red);
+    reduce_terms<NR>(ws, i, red, [&](double* rr) { epi(i, sum, rr); });
   }
   if constexpr (NR > 0) {
     grid_reduce<NR>(red, ws, [&](const double* t) { epi.finalize(t); });
@@ -401,7 +462,7 @@ dia_spmv_kernel(DiaArgs g, const T* __restrict__ va, const T* __restrict__ x, Ep
       for (int j = 0; j < G; ++j)
         if (d0 + j < g.n && ((m >> (d0 + j)) & 1u)) sum = add(sum, mul(v[j], xv[j]));
     }
-    epi(i, sum, red);
+    reduce_terms<NR>(ws, i, red, [&](double* rr) { epi(i, sum, rr); });
   }
   if constexpr (NR > 0) {
     grid_reduce<NR>(red, ws, [&](const double* t) { epi.finalize(t); });
@@ -429,7 +490,7 @@ ell_spmv_kernel(int nrow, long long ld, const int* __restrict__ col, const T* __
       c = __ldcs(cp + k * ld);
       v = __ldcs(vp + k * ld);
     });
-    epi(i, sum, red);
+    reduce_terms<NR>(ws, i, red, [&](double* rr) { epi(i, sum, rr); });
   }
   if constexpr (NR > 0) {
     grid_reduce<NR>(red, ws, [&](const double* t) { epi.finalize(t); });
@@ -457,7 +518,7 @@ jad_spmv_kernel(int nrow, const int* __restrict__ perm, const int* __restrict__ 
       c = __ldcs(col + idx);
       v = __ldcs(va + idx);
     });
-    epi(perm[i], sum, red);
+    reduce_terms<NR>(ws, perm[i], red, [&](double* rr) { epi(perm[i], sum, rr); });
   }
   if constexpr (NR > 0) {
     grid_reduce<NR>(red, ws, [&](const double* t) { epi.finalize(t); });
@@ -547,7 +608,7 @@ bsr_spmv_kernel(int nrow, int ncol, int br_rt, int bc_rt, int nbr_trunc,
   if (active) {
     const int I = I0 + my_I;
     const int row = I * br + my_r;
-    if (row < nrow) epi(row, I < nbr_trunc ? acc : T(0), red);
+    if (row < nrow) reduce_terms<NR>(ws, row, red, [&](double* rr) { epi(row, I < nbr_trunc ? acc : T(0), rr); });
   }
   if constexpr (NR > 0) {
     grid_reduce<NR>(red, ws, [&](const double* t) { epi.finalize(t); });
@@ -603,7 +664,7 @@ bsr_sell_kernel(int nrow, int ncol, int nbr, int nbr_trunc, const int* __restric
 #pragma unroll
     for (int r = 0; r < BR; ++r) {
       const int row = I * BR + r;
-      if (row < nrow) epi(row, acc[r], red);
+      if (row < nrow) reduce_terms<NR>(ws, row, red, [&](double* rr) { epi(row, acc[r], rr); });
     }
   }
   if constexpr (NR > 0) {

@@ -142,14 +142,20 @@ static size_t common_bytes(sk_matrix A, i64 nvec, size_t vb, size_t extra, i64 h
          static_cast<size_t>(hist_cap + 8) * 8 + static_cast<size_t>(nvec) * (vb + 256) + extra + 1024;
 }
 
+// Terms of the sequential summation order: kMaxRed per row.
+static size_t seq_bytes(sk_matrix A) { return static_cast<size_t>(kMaxRed) * (A->nrow + 8) * 8 + 256; }
+
 // Carves from `base` when given (the caller sized it with common_bytes),
 // else from the handle's grow-only workspace.
 static sk_status carve_common(sk_matrix A, cudaStream_t st, i64 nvec, size_t vb, size_t extra,
                               i64 hist_cap, SolveCommon* c, std::vector<char*>* vecs,
                               char** extra_ptr, char* base = nullptr) {
   const int cap = std::max(spmv_grid(A), vec_grid(A->nrow));
+  // the sequential order applies to the solves that use the handle's own
+  // workspace (the reference's solvers), not to a caller-sized region
+  const bool seq = !base && summation_sequential();
   if (!base) {
-    sk_status s = ensure_ws(A, common_bytes(A, nvec, vb, extra, hist_cap));
+    sk_status s = ensure_ws(A, common_bytes(A, nvec, vb, extra, hist_cap) + (seq ? seq_bytes(A) : 0));
     if (s != SK_OK) return s;
     base = static_cast<char*>(A->ws);
   }
@@ -161,6 +167,12 @@ static sk_status carve_common(sk_matrix A, cudaStream_t st, i64 nvec, size_t vb,
   c->hist = cv.take<double>(static_cast<size_t>(hist_cap + 8) * 8);
   for (i64 k = 0; k < nvec; ++k) vecs->push_back(cv.take<char>(vb));
   if (extra_ptr) *extra_ptr = cv.take<char>(extra);
+  if (seq) {
+    c->ws.seq = cv.take<double>(seq_bytes(A));
+    c->ws.seq_ld = A->nrow + 8;
+    c->ws.seq_n = A->nrow;
+    c->ws.seq_f32 = A->dtype == SK_F32 ? 1 : 0;
+  }
   c->used = cv.off;
   SK_CUDA(cudaMemsetAsync(c->sc, 0, sizeof(Scalars), st));
   SK_CUDA(cudaMemsetAsync(c->ws.counter, 0, sizeof(unsigned) * 4, st));
@@ -1136,7 +1148,7 @@ static sk_status fgmres_solve(sk_matrix A, sk_precond M, const T* b, T* x,
   // Modified Gram-Schmidt of each Arnoldi step as one cooperative launch
   // when w fits on chip (sk_arnoldi.cu), else one launch per basis vector.
   ArnoldiPlan aplan;
-  const bool arnoldi_fused = arnoldi_plan<T>(A, n, &aplan);
+  const bool arnoldi_fused = !c.ws.seq && arnoldi_plan<T>(A, n, &aplan);
   auto* arn_sync = reinterpret_cast<ArnoldiSync*>(
       (reinterpret_cast<uintptr_t>(smallp) + small_bytes + 255) & ~uintptr_t(255));
   double* arn_slots = reinterpret_cast<double*>(reinterpret_cast<char*>(arn_sync) + 256);

@@ -62,7 +62,7 @@ __global__ void __launch_bounds__(kThreads, 4) vec_kernel(i64 n, Op op, RedWs ws
 #pragma unroll
     for (int u = 0; u < U; ++u) {
       const i64 i = i0 + 32 * u;
-      if (i < n) op.apply(i, in[u], red);
+      if (i < n) reduce_terms<NR>(ws, i, red, [&](double* rr) { op.apply(i, in[u], rr); });
     }
   }
   if constexpr (NR > 0) {

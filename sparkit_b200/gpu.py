@@ -409,6 +409,21 @@ def estimate_eigenvalue_bounds(Ad, num_iter=30):
     return lo.value, hi.value
 
 
+SUM_TREE, SUM_SEQUENTIAL = 0, 1
+
+
+def set_summation_order(order):
+    """sk_set_summation_order: SUM_TREE (default, fast, deterministic) or
+    SUM_SEQUENTIAL (the reference's element-order sums, for validation)."""
+    check(lib().sk_set_summation_order(int(order)))
+
+
+def summation_order():
+    v = ctypes.c_int32()
+    check(lib().sk_get_summation_order(ctypes.byref(v)))
+    return v.value
+
+
 def debug_set_wait(limit_ns=0, unmeetable=False):
     """sk_debug_set_wait: the time bound of the persistent kernels'
     grid-barrier waits (0 restores 2 s) and, for tests of the timeout path,

@@ -1,0 +1,136 @@
+"""The solvers in the reference's summation order (sk_set_summation_order
+with SK_SUM_SEQUENTIAL): every dot product and norm is summed term after
+term in element order, in the value type, as std::inner_product does in
+the reference.  The products, the element-wise updates, the square roots
+and divisions already follow the reference's arithmetic (no fused
+multiply-adds, IEEE rounding), and the CSR product sums rows of up to 32
+entries in storage order, so a solve reproduces the reference's: the same
+iteration count, the same residual history and the same solution, bit for
+bit.
+
+In the default tree order the counts of BiCGSTAB and CGS move by several
+percent (test_gpu_solvers.py); test_oracle.py shows that the reference's
+own algorithm moves as much under any other summation order, the
+accurately rounded sum included."""
+import numpy as np
+import pytest
+
+from sparkit_b200 import gpu, matgen
+from tests.helpers import golden_problem
+
+pytestmark = pytest.mark.gpu
+
+PRECS = {"none": None, "jacobi": "jacobi", "cheb": ("chebyshev", 0.5, 9.0, 6)}
+PROBLEMS = ["grid16", "tridiag4", "convdiff", "nonsym", "lap2d_24", "upwind_20"]
+SPD = {"grid16", "tridiag4", "lap2d_24"}
+
+
+@pytest.fixture
+def sequential(gpu_lib):
+    gpu.set_summation_order(gpu.SUM_SEQUENTIAL)
+    try:
+        yield
+    finally:
+        gpu.set_summation_order(gpu.SUM_TREE)
+
+
+def make_prec(spec, Ad):
+    if spec is None:
+        return gpu.identity
+    if spec == "jacobi":
+        return gpu.jacobi(Ad)
+    _, lmin, lmax, deg = spec
+    return gpu.chebyshev_preconditioner(Ad, lmin, lmax, deg)
+
+
+def test_order_setting(gpu_lib):
+    assert gpu.summation_order() == gpu.SUM_TREE
+    with pytest.raises(Exception):
+        gpu.set_summation_order(7)
+
+
+@pytest.mark.parametrize("name", PROBLEMS)
+@pytest.mark.parametrize("pname", list(PRECS))
+def test_golden_solves_bit_identical(sequential, golden, name, pname):
+    A = golden_problem(golden, name)
+    n = A.shape()[0]
+    b = golden[f"solve/{name}/b"]
+    Ad = gpu.Device_matrix(A)
+    M = make_prec(PRECS[pname], Ad)
+    runs = {"bicgstab": lambda x: gpu.bicgstab(b, x, gpu.Bicgstab_config(1e-12, 500, True), gpu.spmv(Ad), M),
+            "fgmres": lambda x: gpu.fgmres(b, x, gpu.Fgmres_config(1e-12, 5, 500, True), gpu.spmv(Ad), M),
+            "gmres_left": lambda x: gpu.gmres(b, x, gpu.Gmres_config(1e-12, 5, 500, True), gpu.spmv(Ad), left=M),
+            "gmres_right": lambda x: gpu.gmres(b, x, gpu.Gmres_config(1e-12, 6, 500, True), gpu.spmv(Ad), right=M),
+            "cgs": lambda x: gpu.cgs(b, x, gpu.Cgs_config(1e-12, 500, True), gpu.spmv(Ad), left=M)}
+    if name in SPD:
+        runs["minres"] = lambda x: gpu.minres(b, x, gpu.Minres_config(1e-12, 500, True), gpu.spmv(Ad), left=M)
+        runs["cg_left"] = lambda x: gpu.conjugate_gradient(b, x, gpu.CGConfig(1e-12, 50, 500, True), gpu.spmv(Ad), M,
+                                                           gpu.identity)
+        runs["cg_right"] = lambda x: gpu.conjugate_gradient(b, x, gpu.CGConfig(1e-12, 7, 500, True), gpu.spmv(Ad),
+                                                            gpu.identity, M)
+    for rname, fn in runs.items():
+        key = f"solve/{name}/{pname}/{rname}"
+        x = np.zeros(n)
+        s = fn(x)
+        assert s.computed_iterations == int(golden[f"{key}/iters"]), (key, s.computed_iterations)
+        assert s.converged == bool(golden[f"{key}/converged"]), key
+        hist = golden[f"{key}/history"]
+        assert np.array_equal(np.array(s.iteration_residuals), hist), key
+        assert np.array_equal(x, golden[f"{key}/x"]), (key, np.max(np.abs(x - golden[f"{key}/x"])))
+
+
+@pytest.mark.parametrize("grid", [48, 96])
+@pytest.mark.parametrize("pname", ["none", "jacobi", "cheb"])
+def test_nonsymmetric_medium_bit_identical(sequential, oracle, grid, pname):
+    """BiCGSTAB, CGS and FGMRES(30) on the upwind convection-diffusion
+    problems whose iteration counts move most with the summation order."""
+    A = matgen.convection_diffusion_2d(grid, grid, 1.0, 0.9, 0.5)
+    n = A.shape()[0]
+    b = oracle.spmv(A, matgen.uniform_vector(n, seed=2))
+    spec = {"none": None, "jacobi": "jacobi", "cheb": ("chebyshev", 0.2, 9.5, 8)}[pname]
+    Ad = gpu.Device_matrix(A)
+    M = make_prec(spec, Ad)
+    cases = (("bicgstab", lambda x: gpu.bicgstab(b, x, gpu.Bicgstab_config(1e-10, 3000), gpu.spmv(Ad), M),
+              lambda: oracle.bicgstab(A, b, np.zeros(n), 1e-10, 3000, left=spec)),
+             ("cgs", lambda x: gpu.cgs(b, x, gpu.Cgs_config(1e-10, 3000), gpu.spmv(Ad), left=M),
+              lambda: oracle.cgs(A, b, np.zeros(n), 1e-10, 3000, left=spec)),
+             ("fgmres", lambda x: gpu.fgmres(b, x, gpu.Fgmres_config(1e-10, 30, 3000), gpu.spmv(Ad), M),
+              lambda: oracle.fgmres(A, b, np.zeros(n), 1e-10, 30, 3000, prec=spec)))
+    for name, run, ref in cases:
+        x = np.zeros(n)
+        s = run(x)
+        xr, sr = ref()
+        assert s.computed_iterations == sr["computed_iterations"], (name, s.computed_iterations,
+                                                                    sr["computed_iterations"])
+        assert s.converged == sr["converged"], name
+        assert np.array_equal(x, xr), (name, np.max(np.abs(x - xr)))
+
+
+def test_config1_cg_bit_identical(sequential, oracle):
+    """Configuration 1: Jacobi-CG on the 256 x 256 Dirichlet Laplacian to
+    1e-10, the same 724 steps and the same solution as the reference."""
+    A = matgen.laplacian_2d_dirichlet(256)
+    n = A.shape()[0]
+    b = oracle.spmv(A, matgen.uniform_vector(n, seed=0))
+    xr, sr = oracle.cg(A, b, np.zeros(n), 1e-10, 100000, 100000, left="jacobi", collect=True)
+    Ad = gpu.Device_matrix(A)
+    x = np.zeros(n)
+    s = gpu.conjugate_gradient(b, x, gpu.CGConfig(1e-10, 100000, 100000, True), gpu.spmv(Ad), gpu.jacobi(Ad))
+    assert s.computed_iterations == sr["computed_iterations"] and s.converged and sr["converged"]
+    assert np.array_equal(np.array(s.iteration_residuals), np.array(sr["iteration_residuals"]))
+    assert np.array_equal(x, xr)
+
+
+def test_fp32_solves_bit_identical(sequential, oracle):
+    """FP32 values: the sums run in float, as the reference's
+    std::inner_product<float> does."""
+    A = matgen.convection_diffusion_2d(32, 32, 1.0, 0.9, 0.5, dtype=np.float32)
+    n = A.shape()[0]
+    b = oracle.spmv(A, matgen.uniform_vector(n, seed=4, dtype=np.float32))
+    Ad = gpu.Device_matrix(A)
+    J = gpu.jacobi(Ad)
+    x = np.zeros(n, dtype=np.float32)
+    s = gpu.bicgstab(b, x, gpu.Bicgstab_config(1e-5, 2000), gpu.spmv(Ad), J)
+    xr, sr = oracle.bicgstab(A, b, np.zeros(n, dtype=np.float32), 1e-5, 2000, left="jacobi")
+    assert s.computed_iterations == sr["computed_iterations"] and s.converged == sr["converged"]
+    assert np.array_equal(x, xr)

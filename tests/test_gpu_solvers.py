@@ -28,13 +28,18 @@ def make_prec(spec, Ad):
 
 
 def iters_close(a, b, solver="cg"):
-    """+-2% (at least 1) for CG, FGMRES, GMRES and MINRES.  BiCGSTAB's and
-    CGS's counts move with the summation order of their dot products even on
-    the CPU (the reference re-run with chunked sums shifts by ~2%,
-    test_oracle.py records it), and the GPU sums in a tree, so their band is
-    +-12%; their solutions are checked through the true residual instead."""
-    frac = 0.12 if solver in ("bicgstab", "cgs") else 0.02
-    return abs(a - b) <= max(1, int(np.ceil(frac * b)))
+    """+-2% (at least 2) for CG, FGMRES, GMRES and MINRES in the default
+    tree summation order.  BiCGSTAB's and CGS's counts move with the
+    summation order of their dot products: the reference's own algorithm
+    summed in any other order, the accurately rounded sum included, needs up
+    to 9% more or fewer products on these problems (test_oracle.py), and on
+    the GPU the largest shift measured is 8% (BiCGSTAB, 48 x 48
+    convection-diffusion, no preconditioner).  Their band is therefore
+    +-10% here, with the same convergence decision and the true residual
+    checked; in the reference's sequential order (test_gpu_sequential.py)
+    every count and solution equals the reference's exactly."""
+    frac = 0.10 if solver in ("bicgstab", "cgs") else 0.02
+    return abs(a - b) <= max(2, int(np.ceil(frac * b)))
 
 
 def test_jacobi_bitwise(gpu_lib, golden, known):

@@ -349,24 +349,38 @@ def test_generators_match_reference(reference):
             assert np.array_equal(getattr(a, f)(), getattr(b, f)())
 
 
-def test_bicgstab_iteration_count_depends_on_summation_order(oracle):
-    """Evidence for the BiCGSTAB parity band of the GPU tests: the
-    reference algorithm itself, with its dot products summed in 256-entry
-    chunks instead of sequentially, needs a different number of matrix-
-    vector products on a nonsymmetric problem, while FGMRES and CG need
-    exactly the same."""
-    A = matgen.convection_diffusion_2d(48, 48, 1.0, 0.9, 0.5)
-    n = A.shape()[0]
-    b = oracle.spmv(A, matgen.uniform_vector(n, seed=2))
-    counts = {}
+def test_krylov_iteration_counts_depend_on_summation_order(oracle):
+    """Evidence for the BiCGSTAB / CGS parity band of the GPU tests in the
+    default tree order: the reference algorithm itself (bit-exact with the
+    compiled reference in the sequential order 0), with its dot products
+    summed in 256-entry chunks (order 1), from the last element down (order
+    2) or accurately, in double-double rounded once (order 3), needs a
+    different number of matrix-vector products on the upwind
+    convection-diffusion problems: BiCGSTAB and CGS move by up to about 9%,
+    even under the accurate sum, while FGMRES(30) stays within 1%.  Only the
+    reference's own sequential order reproduces its counts
+    (test_gpu_sequential.py runs the GPU solvers in that order)."""
+    shift = {"bicgstab": 0.0, "cgs": 0.0, "fgmres": 0.0}
     try:
-        for mode in (0, 1):
-            oracle.set_dot_order(mode)
-            _, s = oracle.bicgstab(A, b, np.zeros(n), 1e-10, 3000, left="jacobi")
-            _, f = oracle.fgmres(A, b, np.zeros(n), 1e-10, 30, 3000, prec="jacobi")
-            counts[mode] = (s["computed_iterations"], f["computed_iterations"])
+        for g in (48, 96):
+            A = matgen.convection_diffusion_2d(g, g, 1.0, 0.9, 0.5)
+            n = A.shape()[0]
+            b = oracle.spmv(A, matgen.uniform_vector(n, seed=2))
+            for prec in (None, "jacobi"):
+                base = None
+                for mode in (0, 1, 2, 3):
+                    oracle.set_dot_order(mode)
+                    _, s = oracle.bicgstab(A, b, np.zeros(n), 1e-10, 20000, left=prec)
+                    _, c = oracle.cgs(A, b, np.zeros(n), 1e-10, 20000, left=prec)
+                    _, f = oracle.fgmres(A, b, np.zeros(n), 1e-10, 30, 20000, prec=prec)
+                    its = {"bicgstab": s["computed_iterations"], "cgs": c["computed_iterations"],
+                           "fgmres": f["computed_iterations"]}
+                    assert s["converged"] and c["converged"] and f["converged"]
+                    if base is None:
+                        base = its
+                    for k in its:
+                        shift[k] = max(shift[k], abs(its[k] - base[k]) / base[k])
     finally:
         oracle.set_dot_order(0)
-    assert counts[0][0] != counts[1][0]          # BiCGSTAB moves
-    assert counts[0][1] == counts[1][1]          # FGMRES does not
-    assert abs(counts[0][0] - counts[1][0]) <= 0.05 * counts[0][0]
+    assert shift["bicgstab"] > 0.05 and shift["cgs"] > 0.05, shift
+    assert shift["fgmres"] <= 0.01, shift
