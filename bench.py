@@ -266,20 +266,32 @@ def sweep(stream, grid):
             Ad.close()
     del A
     B = matgen.vector_laplacian_3d_bsr(grid, seed=1)
-    Bd = gpu.Device_matrix(B)
-    xb = torch.from_numpy(matgen.uniform_vector(B.shape()[0], seed=2)).cuda()
-    yb = torch.empty_like(xb)
-    ms = time_device(lambda: Bd.spmv(xb, yb, stream=sptr), 200, 20, stream)
-    out["vec3_bsr33_f64"] = {"gbs": Bd.info()["spmv_bytes"] / ms / 1e6, "us": ms * 1e3}
-    Bd.close()
+    for tag, dt in (("f64", np.float64), ("f32", np.float32)):
+        Bd = gpu.Device_matrix(B, dtype=dt)
+        xb = torch.from_numpy(matgen.uniform_vector(B.shape()[0], seed=2, dtype=dt)).cuda()
+        yb = torch.empty_like(xb)
+        ms = time_device(lambda: Bd.spmv(xb, yb, stream=sptr), 200, 20, stream)
+        out[f"vec3_bsr33_{tag}"] = {"gbs": Bd.info()["spmv_bytes"] / ms / 1e6, "us": ms * 1e3}
+        Bd.close()
     del B
+    # matrix B: CSR, and JAD and ELL built on the device from the CSR handle
+    # (the ELL holds 2048 slots per row, 2.05e9 slots; its byte model counts
+    # the stored entries only), FP64 and FP32
     Z = matgen.zipf_random(1_000_000, s=1.5, cap=2048, seed=0)
-    Zd = gpu.Device_matrix(Z)
-    xz = torch.from_numpy(matgen.uniform_vector(Z.shape()[0], seed=3)).cuda()
-    yz = torch.empty_like(xz)
-    ms = time_device(lambda: Zd.spmv(xz, yz, stream=sptr), 200, 20, stream)
-    out["zipf_csr_f64"] = {"gbs": Zd.info()["spmv_bytes"] / ms / 1e6, "us": ms * 1e3, "nnz": Z.size(),
-                           "mean_row": Z.size() / Z.shape()[0]}
+    for tag, dt in (("f64", np.float64), ("f32", np.float32)):
+        Zd = gpu.Device_matrix(Z, dtype=dt)
+        xz = torch.from_numpy(matgen.uniform_vector(Z.shape()[0], seed=3, dtype=dt)).cuda()
+        yz = torch.empty_like(xz)
+        ms = time_device(lambda: Zd.spmv(xz, yz, stream=sptr), 200, 20, stream)
+        out[f"zipf_csr_{tag}"] = {"gbs": Zd.info()["spmv_bytes"] / ms / 1e6, "us": ms * 1e3, "nnz": Z.size(),
+                                  "mean_row": Z.size() / Z.shape()[0]}
+        for fmt, conv in (("jad", gpu.to_jagged_diagonal), ("ell", gpu.to_ellpack)):
+            H = conv(Zd)
+            ms = time_device(lambda: H.spmv(xz, yz, stream=sptr), 40, 5, stream)
+            out[f"zipf_{fmt}_{tag}"] = {"gbs": H.info()["spmv_bytes"] / ms / 1e6, "us": ms * 1e3,
+                                        "device_bytes": H.info()["device_bytes"]}
+            H.close()
+        Zd.close()
     return out
 
 

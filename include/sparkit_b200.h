@@ -532,6 +532,30 @@ SK_API sk_status sk_mixed_cg_solve(sk_matrix A, int32_t jacobi,
                                    sk_mixed_summary* out, double* history_host,
                                    sk_stream s);
 
+/* Mixed-precision FGMRES(m) (no reference counterpart as a whole; the inner
+ * solve is fgmres.hpp:96-428 in FP32): FP64 iterative refinement around an
+ * FP32 FGMRES(m) inner solve.  FP64 stays in the outer residual b - A x,
+ * the solution update and the inner Hessenberg least-squares problem
+ * (Givens rotations, back substitution); the basis vectors, the products
+ * (the handle's FP32 value copy, made on first use) and the Gram-Schmidt
+ * sums are FP32.  M: NULL, Jacobi, Chebyshev (applied in FP32) or a
+ * two-level preconditioner (applied in FP64); the learned network is
+ * refused.  b and x are FP64 device vectors of an FP64 CSR handle. */
+typedef struct {
+  double tolerance;          /* outer, on the true FP64 residual */
+  double inner_tolerance;    /* FP32 FGMRES relative tolerance on |g| */
+  int64_t restart_dimension; /* m */
+  int64_t max_outer;
+  int64_t max_inner;         /* FP32 FGMRES iterations per outer step */
+  int32_t collect_residuals; /* true residual norm per outer step */
+  int32_t adaptive_last_step;
+} sk_mixed_fgmres_config;
+
+SK_API sk_status sk_mixed_fgmres_solve(sk_matrix A, sk_precond M, const double* b_dev,
+                                       double* x_dev, const sk_mixed_fgmres_config* cfg,
+                                       sk_mixed_summary* out, double* history_host,
+                                       sk_stream s);
+
 /* ---------------------------------------------------------------- */
 /* Batched solves (no reference counterpart: the reference solves one */
 /* system per call; the comparison is a loop of the plain solver)     */

@@ -55,6 +55,12 @@ class MixedConfig(ctypes.Structure):
                 ("l2_window", c_i32), ("inner_kernel", c_i32)]
 
 
+class MixedFgmresConfig(ctypes.Structure):
+    _fields_ = [("tolerance", c_dbl), ("inner_tolerance", c_dbl), ("restart_dimension", c_i64),
+                ("max_outer", c_i64), ("max_inner", c_i64), ("collect_residuals", c_i32),
+                ("adaptive_last_step", c_i32)]
+
+
 class MixedSummary(ctypes.Structure):
     _fields_ = [("residual_norm", c_dbl), ("outer_iterations", c_i64), ("inner_iterations", c_i64),
                 ("converged", c_i32), ("status", c_i32), ("setup_ms", c_dbl), ("inner_ms", c_dbl),
@@ -162,6 +168,8 @@ SIGNATURES = [
                          c_vp, c_vp]),
     ("sk_mixed_cg_solve", [c_vp, c_i32, c_vp, c_vp, ctypes.POINTER(MixedConfig), ctypes.POINTER(MixedSummary),
                            c_vp, c_vp]),
+    ("sk_mixed_fgmres_solve", [c_vp, c_vp, c_vp, c_vp, ctypes.POINTER(MixedFgmresConfig),
+                               ctypes.POINTER(MixedSummary), c_vp, c_vp]),
     ("sk_batch_create", [ctypes.POINTER(c_vp), c_i64, c_vp, c_vp, c_vp, c_vp]),
     ("sk_batch_destroy", [c_vp]),
     ("sk_batched_cg_solve", [c_vp, c_vp, c_vp, ctypes.POINTER(BatchConfig), ctypes.POINTER(BatchResults), c_vp]),

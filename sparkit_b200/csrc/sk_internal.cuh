@@ -222,6 +222,10 @@ struct sk_precond_s {
   double* tbuf2 = nullptr;
   double* rc = nullptr;
   double* zc = nullptr;
+  // FP64 staging of an FP32 apply of a two-level preconditioner (the
+  // mixed-precision FGMRES): r widened in, z narrowed out
+  double* cvt_in = nullptr;
+  double* cvt_out = nullptr;
 };
 
 namespace sk {
@@ -232,6 +236,11 @@ inline const float* f32_values(const sk_matrix_s* A) {
 }
 
 cudaStream_t pick_stream(sk_matrix A, sk_stream s);
+
+// Makes the FP32 copies an FP32 apply of a preconditioner of an FP64 handle
+// reads (the inverse diagonal as float, the handle's FP32 values);
+// SK_NOT_SUPPORTED for a preconditioner without an FP32 apply.
+sk_status precond_prepare_f32(sk_precond_s* M, cudaStream_t st);
 sk_status dev_alloc(sk_matrix A, void** p, size_t bytes);
 
 // Grid-wide deterministic reduction workspace: one slot of kMaxRed doubles

@@ -66,22 +66,68 @@ static std::vector<double> cheb_coeffs(T lmin, T lmax, i64 degree) {
   return out;
 }
 
+// out = in converted to the other precision, skipped once a solve is done.
+template <typename From, typename To>
+struct OpConvert {
+  static constexpr int kNR = 0;
+  struct In { From v; };
+  const From* in;
+  To* out;
+  __device__ bool prepare(const Scalars* sc) { return !solve_done(sc); }
+  __device__ In load(i64 i) const { return {in[i]}; }
+  __device__ void apply(i64 i, In const& v, double*) const { out[i] = static_cast<To>(v.v); }
+  __device__ void finalize(const double*) const {}
+};
+
+// An FP32 apply of a preconditioner made on an FP64 handle (the inner
+// solve of the mixed-precision FGMRES) uses its FP32 copies: the inverse
+// diagonal rounded to float, the handle's FP32 values for the Chebyshev
+// products; a two-level preconditioner runs in FP64 between a widening and
+// a narrowing pass.
 template <typename T>
 static void precond_apply_t(const sk_precond_s* M, i64 n, const T* r, T* z, RedWs ws,
                             const Scalars* sc, cudaStream_t st) {
+  constexpr bool narrow = sizeof(T) == 4;
+  const bool from64 = M && M->dtype == SK_F64;
   if (!M) {
     launch_vec(n, OpCopy<T>{r, z}, ws, sc, st);
   } else if (M->kind == 1) {
-    launch_vec(n, OpJacobi<T>{static_cast<const T*>(M->inv_diag), r, z}, ws, sc, st);
+    const T* inv = narrow && from64 ? reinterpret_cast<const T*>(M->inv_diag32) : static_cast<const T*>(M->inv_diag);
+    launch_vec(n, OpJacobi<T>{inv, r, z}, ws, sc, st);
   } else if (M->kind == 3) {
     if constexpr (sizeof(T) == 8) {
       if (learned_apply(M, r, z, st) != SK_OK) set_error("learned preconditioner apply failed");
     }
   } else if (M->kind == 4) {
-    if constexpr (sizeof(T) == 8) twolevel_apply(M, r, z, ws, sc, st);
+    if constexpr (sizeof(T) == 8) {
+      twolevel_apply(M, r, z, ws, sc, st);
+    } else {
+      launch_vec(n, OpConvert<float, double>{r, M->cvt_in}, ws, sc, st);
+      twolevel_apply(M, M->cvt_in, M->cvt_out, ws, sc, st);
+      launch_vec(n, OpConvert<double, float>{M->cvt_out, z}, ws, sc, st);
+    }
   } else {
-    chebyshev_apply_device<T>(M, r, z, static_cast<T*>(M->work), ws, sc, st);
+    const T* vals = narrow && from64 ? reinterpret_cast<const T*>(f32_values(M->A)) : nullptr;
+    chebyshev_apply_device<T>(M, r, z, static_cast<T*>(M->work), ws, sc, st, vals);
   }
+}
+
+sk_status precond_prepare_f32(sk_precond_s* M, cudaStream_t st) {
+  if (!M || M->dtype != SK_F64) return SK_OK;
+  if (M->kind == 1 && !M->inv_diag32) {
+    void* p = nullptr;
+    SK_CUDA(cudaMalloc(&p, static_cast<size_t>(M->n + 8) * 4));
+    launch_vec(M->n, OpConvert<double, float>{static_cast<const double*>(M->inv_diag), static_cast<float*>(p)},
+               RedWs{}, nullptr, st);
+    SK_CUDA(cudaGetLastError());
+    SK_CUDA(cudaStreamSynchronize(st));
+    M->inv_diag32 = static_cast<float*>(p);
+  } else if (M->kind == 2 && !f32_values(M->A)) {
+    return sk_matrix_add_f32_values(M->A);
+  } else if (M->kind == 3) {
+    return fail(SK_NOT_SUPPORTED, "the learned preconditioner has no FP32 apply (use it as a two-level smoother)");
+  }
+  return SK_OK;
 }
 
 void precond_apply_dispatch(const sk_precond_s* M, sk_dtype dt, i64 n, const void* r, void* z,

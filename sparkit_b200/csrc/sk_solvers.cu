@@ -27,6 +27,11 @@ void precond_apply_dispatch(const sk_precond_s* M, sk_dtype dt, i64 n, const voi
 
 enum { PK_IDENTITY = 0, PK_JACOBI = 1, PK_OTHER = 2 };
 
+// The dtype of a solve's vectors (an FP64 handle runs FP32 vectors in the
+// mixed-precision solvers).
+template <typename T>
+constexpr sk_dtype kVecType = sizeof(T) == 8 ? SK_F64 : SK_F32;
+
 inline int prec_kind(const sk_precond_s* M) {
   if (!M) return PK_IDENTITY;
   return M->kind == 1 ? PK_JACOBI : PK_OTHER;
@@ -1109,7 +1114,8 @@ template <typename T>
 static sk_status fgmres_solve(sk_matrix A, sk_precond M, const T* b, T* x,
                               const sk_fgmres_config* cfg, sk_summary* out, double* history_host,
                               cudaStream_t st, sk_precond fallback = nullptr, double stall_ratio = 0.0,
-                              int64_t* switched_at = nullptr, sk_precond left = nullptr, bool gmres = false) {
+                              int64_t* switched_at = nullptr, sk_precond left = nullptr, bool gmres = false,
+                              const T* vals = nullptr, bool hess64 = false) {
   const i64 n = A->nrow;
   const int m = static_cast<int>(cfg->restart_dimension);
   SK_CHECK(m >= 1 && m <= 4096, SK_INVALID_ARG, "restart_dimension must be in [1, 4096]");
@@ -1176,24 +1182,24 @@ static sk_status fgmres_solve(sk_matrix A, sk_precond M, const T* b, T* x,
   // cycle, and a converged solve turns the remaining kernels into no-ops.
   auto enqueue_cycle = [&](cudaStream_t q, int m_eff, sk_precond P) {
     if (general_left) {  // r0 = b - A x; v0 = M_L r0; beta = ||v0|| (:214-224)
-      launch_spmv<T>(A, x, EpiGmResid<T>{b, gl.tmp}, c.ws, nullptr, q);
-      precond_apply_dispatch(gl.L, A->dtype, n, gl.tmp, V, c.ws, nullptr, q);
+      launch_spmv<T>(A, x, EpiGmResid<T>{b, gl.tmp}, c.ws, nullptr, q, vals);
+      precond_apply_dispatch(gl.L, kVecType<T>, n, gl.tmp, V, c.ws, nullptr, q);
       launch_vec(n, OpGmInitNorm<T>{V, c.sc, sm, m, gl.divide}, c.ws, nullptr, q);
     } else {
-      launch_spmv<T>(A, x, EpiFgInit<T>{b, V, c.sc, sm, m, gl.linv, gl.divide}, c.ws, nullptr, q);
+      launch_spmv<T>(A, x, EpiFgInit<T>{b, V, c.sc, sm, m, gl.linv, gl.divide}, c.ws, nullptr, q, vals);
     }
     launch_vec(n, OpFgScale<T>{V, nullptr, T(0), gl.divide}, c.ws, c.sc, q);
     for (int j = 0; j < m_eff; ++j) {
       T* Vj = V + j * ldv;
       T* Vj1 = V + (j + 1) * ldv;
       T* Zj = Z + j * ldv;
-      if (!alias_z) precond_apply_dispatch(P, A->dtype, n, Vj, Zj, c.ws, c.sc, q);
+      if (!alias_z) precond_apply_dispatch(P, kVecType<T>, n, Vj, Zj, c.ws, c.sc, q);
       if (general_left) {  // v_{j+1} = M_L A z_j, then h_0j = <v_0, v_{j+1}>
-        launch_spmv<T>(A, Zj, EpiStore<T>{gl.tmp}, c.ws, c.sc, q);
-        precond_apply_dispatch(gl.L, A->dtype, n, gl.tmp, Vj1, c.ws, c.sc, q);
+        launch_spmv<T>(A, Zj, EpiStore<T>{gl.tmp}, c.ws, c.sc, q, vals);
+        precond_apply_dispatch(gl.L, kVecType<T>, n, gl.tmp, Vj1, c.ws, c.sc, q);
         launch_vec(n, OpFgMgs<T>{Vj1, V, V, sm.zero, sm.H + j * um1, T(0)}, c.ws, c.sc, q);
       } else {
-        launch_spmv<T>(A, Zj, EpiFgW<T>{Vj1, V, sm.H + j * um1, gl.linv}, c.ws, c.sc, q);
+        launch_spmv<T>(A, Zj, EpiFgW<T>{Vj1, V, sm.H + j * um1, gl.linv}, c.ws, c.sc, q, vals);
       }
       if (arnoldi_fused) {
         const sk_status as = arnoldi_launch<T>(
@@ -1208,10 +1214,16 @@ static sk_status fgmres_solve(sk_matrix A, sk_precond M, const T* b, T* x,
         launch_vec(n, OpFgScale<T>{Vj1, sm.H + (j + 1) + j * um1, T(0), gl.divide}, c.ws, c.sc, q);
       }
       g_launches.fetch_add(1, std::memory_order_relaxed);
-      scalar_kernel<<<1, 1, 0, q>>>(FgGivens<T>{c.sc, c.hist, sm, j, m});
+      if (hess64)  // the least-squares problem in FP64 around FP32 vectors
+        scalar_kernel<<<1, 1, 0, q>>>(FgGivens<double>{c.sc, c.hist, sm, j, m});
+      else
+        scalar_kernel<<<1, 1, 0, q>>>(FgGivens<T>{c.sc, c.hist, sm, j, m});
     }
     g_launches.fetch_add(1, std::memory_order_relaxed);
-    scalar_kernel<<<1, 1, 0, q>>>(FgBackSub<T>{c.sc, sm, m});
+    if (hess64)
+      scalar_kernel<<<1, 1, 0, q>>>(FgBackSub<double>{c.sc, sm, m});
+    else
+      scalar_kernel<<<1, 1, 0, q>>>(FgBackSub<T>{c.sc, sm, m});
     launch_vec(n, OpFgUpdateX<T>{x, Z, ldv, sm.y, 0}, c.ws, c.sc, q);
   };
   // Solves expected to run several cycles replay each cycle as a CUDA graph
@@ -2207,6 +2219,106 @@ static sk_status mixed_cg_solve(sk_matrix A, bool jacobi, const double* b, doubl
   return status;
 }
 
+// Mixed-precision FGMRES(m): FP64 iterative refinement around an FP32
+// FGMRES(m) inner solve.  FP64 stays in the outer residual r = b - A x
+// (EpiResid64), the solution update x += ||r|| d (OpRefine) and the inner
+// solve's Hessenberg least-squares problem (Givens rotations and back
+// substitution, FgGivens<double> / FgBackSub<double>); the inner basis
+// vectors, the products (the handle's FP32 values) and the Gram-Schmidt
+// sums run in FP32 (fgmres.hpp:96-428 in FP32 otherwise).  M is applied in
+// FP32 (Jacobi, Chebyshev) or, for a two-level preconditioner, in FP64
+// between a widening and a narrowing pass.
+static sk_status mixed_fgmres_solve(sk_matrix A, sk_precond M, const double* b, double* x,
+                                    const sk_mixed_fgmres_config* cfg, sk_mixed_summary* out, double* history,
+                                    cudaStream_t st) {
+  const i64 n = A->nrow;
+  *out = sk_mixed_summary{};
+  out->inner_kernel = 1;
+  using clk = std::chrono::steady_clock;
+  auto ms_since = [](clk::time_point t0) {
+    return std::chrono::duration<double, std::milli>(clk::now() - t0).count();
+  };
+  const auto t_setup = clk::now();
+  sk_status s = SK_OK;
+  if (!f32_values(A) && (s = sk_matrix_add_f32_values(A)) != SK_OK) return s;
+  if ((s = precond_prepare_f32(M, st)) != SK_OK) return s;
+  // the outer vectors in the second workspace (shared with the mixed CG,
+  // whose FP32 Jacobi there is rebuilt on its next call)
+  const int cap = spmv_grid(A);
+  const size_t need = 4096 + static_cast<size_t>(n + 64) * (8 + 4 + 4) + 4096 +
+                      static_cast<size_t>(std::max(cap, vec_grid(n))) * kMaxRed * 8 + 2048;
+  if (A->ws2_bytes < need) {
+    if (A->ws2) {
+      cudaStreamSynchronize(st);
+      cudaFree(A->ws2);
+      A->ws2 = nullptr;
+    }
+    SK_CUDA(cudaMalloc(&A->ws2, need));
+    A->ws2_bytes = need;
+  }
+  A->mixed_jacobi_ready = false;
+  Carver cv{static_cast<char*>(A->ws2)};
+  double* r = cv.take<double>(static_cast<size_t>(n + 8) * 8);
+  float* r32 = cv.take<float>(static_cast<size_t>(n + 8) * 4);
+  float* d32 = cv.take<float>(static_cast<size_t>(n + 8) * 4);
+  Scalars* so = cv.take<Scalars>(sizeof(Scalars));
+  unsigned* cnt = cv.take<unsigned>(16);
+  double* partials = cv.take<double>(static_cast<size_t>(std::max(cap, vec_grid(n))) * kMaxRed * 8);
+  SK_CUDA(cudaMemsetAsync(so, 0, sizeof(Scalars), st));
+  SK_CUDA(cudaMemsetAsync(cnt, 0, 16, st));
+  RedWs ws{partials, cnt, std::max(cap, vec_grid(n))};
+  double bnorm = 0;
+  {
+    launch_vec(n, OpNormB<double>{b, so}, ws, nullptr, st);
+    Scalars h;
+    if ((s = read_scalars(so, &h, st)) != SK_OK) return s;
+    bnorm = h.bnorm;
+  }
+  out->setup_ms = ms_since(t_setup);
+  if (bnorm == 0.0) {
+    SK_CUDA(cudaMemsetAsync(x, 0, n * 8, st));
+    SK_CUDA(cudaStreamSynchronize(st));
+    out->converged = 1;
+    return SK_OK;
+  }
+  sk_fgmres_config icfg{cfg->inner_tolerance, cfg->restart_dimension, cfg->max_inner, 0};
+  for (i64 outer = 0;; ++outer) {
+    auto t_outer = clk::now();
+    launch_spmv<double>(A, x, EpiResid64{b, r, so}, ws, nullptr, st);
+    Scalars h;
+    s = read_scalars(so, &h, st);
+    out->outer_ms += ms_since(t_outer);
+    if (s != SK_OK) break;
+    out->residual_norm = h.rnorm;
+    if (history && cfg->collect_residuals) history[outer] = h.rnorm;
+    out->outer_iterations = outer;
+    if (h.rnorm / bnorm < cfg->tolerance) {
+      out->converged = 1;
+      break;
+    }
+    if (outer >= cfg->max_outer) break;
+    launch_vec(n, OpScaleDown{r, r32, d32, 0.0}, ws, so, st);
+    // the last step needs only the remaining factor tol ||b|| / ||r||
+    // (floor 1e-6, about what FP32 FGMRES resolves)
+    const double needed = cfg->tolerance * bnorm / h.rnorm;
+    icfg.tolerance = cfg->inner_tolerance;
+    if (cfg->adaptive_last_step && 0.5 * needed < cfg->inner_tolerance)
+      icfg.tolerance = std::max(0.5 * needed, 1e-6);
+    sk_summary is{};
+    auto t_inner = clk::now();
+    s = fgmres_solve<float>(A, M, r32, d32, &icfg, &is, nullptr, st, nullptr, 0.0, nullptr, nullptr, false,
+                            f32_values(A), true);
+    out->inner_ms += ms_since(t_inner);
+    if (s != SK_OK) break;
+    out->inner_iterations += is.computed_iterations;
+    t_outer = clk::now();
+    launch_vec(n, OpRefine{x, d32, 0.0}, ws, so, st);
+    out->outer_ms += ms_since(t_outer);
+  }
+  SK_CUDA(cudaStreamSynchronize(st));
+  return s;
+}
+
 }  // namespace sk
 
 using namespace sk;
@@ -2425,4 +2537,21 @@ extern "C" sk_status sk_mixed_cg_solve(sk_matrix A, int32_t jacobi, const double
   // a created stream), ordered after the caller's stream.
   SK_CUDA(cudaStreamSynchronize(static_cast<cudaStream_t>(s)));
   return mixed_cg_solve(A, jacobi != 0, b_dev, x_dev, cfg, out, history_host, A->stream);
+}
+
+extern "C" sk_status sk_mixed_fgmres_solve(sk_matrix A, sk_precond M, const double* b_dev, double* x_dev,
+                                           const sk_mixed_fgmres_config* cfg, sk_mixed_summary* out,
+                                           double* history_host, sk_stream s) {
+  sk_status st = check_solver_args(A, M, nullptr, b_dev, x_dev);
+  if (st != SK_OK) return st;
+  SK_CHECK(cfg && out, SK_INVALID_ARG, "null config or summary");
+  SK_CHECK(A->dtype == SK_F64 && A->format == SK_CSR, SK_INVALID_ARG,
+           "the mixed-precision solver needs an FP64 CSR handle");
+  SK_CHECK(cfg->max_outer >= 0 && cfg->max_inner > 0, SK_INVALID_ARG, "bad iteration limits");
+  SK_CHECK(cfg->restart_dimension >= 1 && cfg->restart_dimension <= 4096, SK_INVALID_ARG,
+           "restart_dimension must be in [1, 4096]");
+  SK_CHECK(!M || M->kind != 3, SK_NOT_SUPPORTED,
+           "the learned preconditioner has no FP32 apply (use it as a two-level smoother)");
+  SK_CUDA(cudaStreamSynchronize(static_cast<cudaStream_t>(s)));
+  return mixed_fgmres_solve(A, M, b_dev, x_dev, cfg, out, history_host, A->stream);
 }

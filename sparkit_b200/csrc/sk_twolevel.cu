@@ -181,7 +181,7 @@ void twolevel_apply(const sk_precond_s* M, const double* r, double* z, RedWs ws,
 }
 
 void twolevel_release(sk_precond_s* M) {
-  for (double** p : {&M->coarse_inv, &M->tbuf, &M->tbuf2, &M->rc, &M->zc}) {
+  for (double** p : {&M->coarse_inv, &M->tbuf, &M->tbuf2, &M->rc, &M->zc, &M->cvt_in, &M->cvt_out}) {
     if (*p) cudaFree(*p);
     *p = nullptr;
   }
@@ -251,6 +251,8 @@ sk_status sk_twolevel_create(sk_precond* out, sk_matrix A, sk_precond smoother, 
   if (e == cudaSuccess) e = cudaMalloc(&M->tbuf2, static_cast<size_t>(n + 8) * 8);
   if (e == cudaSuccess) e = cudaMalloc(&M->rc, static_cast<size_t>(nc + 8) * 8);
   if (e == cudaSuccess) e = cudaMalloc(&M->zc, static_cast<size_t>(nc + 8) * 8);
+  if (e == cudaSuccess) e = cudaMalloc(&M->cvt_in, static_cast<size_t>(n + 8) * 8);
+  if (e == cudaSuccess) e = cudaMalloc(&M->cvt_out, static_cast<size_t>(n + 8) * 8);
   if (e == cudaSuccess)
     e = cudaMemcpy(M->coarse_inv, inv.data(), static_cast<size_t>(nc * nc) * 8, cudaMemcpyHostToDevice);
   if (e != cudaSuccess) {

@@ -663,6 +663,40 @@ def mixed_cg(b, x, cfg, op, jacobi_inner=True):
     return out
 
 
+@dataclass
+class Mixed_fgmres_config:
+    """FP32-inner FGMRES(m) / FP64-outer iterative refinement
+    (sk_mixed_fgmres_solve)."""
+    tolerance: float = 1e-10
+    inner_tolerance: float = 1e-4
+    restart_dimension: int = 30
+    max_outer: int = 50
+    max_inner: int = 3000
+    collect_residuals: bool = False
+    adaptive_last_step: bool = True
+
+
+def mixed_fgmres(b, x, cfg, op, preconditioner=identity):
+    """Solves A x = b to cfg.tolerance on the true FP64 residual with FP32
+    FGMRES(m) inner solves whose Hessenberg least-squares problem runs in
+    FP64.  b and x are FP64 CUDA tensors (x holds the initial guess)."""
+    Ad = _op_matrix(op)
+    n = Ad.shape()[0]
+    _check_vec(b, n, np.float64, Ad.device, "b")
+    _check_vec(x, n, np.float64, Ad.device, "x")
+    c = _lib.MixedFgmresConfig(cfg.tolerance, cfg.inner_tolerance, cfg.restart_dimension, cfg.max_outer,
+                               cfg.max_inner, int(cfg.collect_residuals), int(cfg.adaptive_last_step))
+    s = _lib.MixedSummary()
+    hist = np.zeros(cfg.max_outer + 2) if cfg.collect_residuals else None
+    check(lib().sk_mixed_fgmres_solve(Ad.handle, _handle(preconditioner), _ptr(b), _ptr(x), ctypes.byref(c),
+                                      ctypes.byref(s), _ptr(hist), _stream_of(b)))
+    out = Mixed_summary(s.residual_norm, s.outer_iterations, s.inner_iterations, bool(s.converged), s.status,
+                        [], s.setup_ms, s.inner_ms, s.outer_ms, False)
+    if hist is not None:
+        out.residual_history = hist[: s.outer_iterations + 1].tolist()
+    return out
+
+
 # ------------------------------------------------------------------
 # Learned variable preconditioner of FGMRES (no reference counterpart:
 # fgmres.hpp:452-470 takes any callable as its variable preconditioner)

@@ -132,3 +132,63 @@ def test_persistent_inner_repeatable(gpu_lib):
         torch.cuda.synchronize()
         xs.append(xd.cpu().numpy())
     assert np.array_equal(xs[0], xs[1])
+
+
+def _true_rel(oracle, A, b, xd):
+    return np.linalg.norm(b - oracle.spmv(A, xd.cpu().numpy())) / np.linalg.norm(b)
+
+
+@pytest.mark.parametrize("pname", ["jacobi", "cheb"])
+def test_mixed_fgmres_reaches_fp64_tolerance(gpu_lib, oracle, pname):
+    """FP32 FGMRES(30) inside FP64 refinement on a nonsymmetric upwind
+    convection-diffusion problem: the true FP64 residual reaches 1e-10, and
+    the FP32 inner work stays comparable to the plain FP64 solve's."""
+    import torch
+    A = matgen.convection_diffusion_2d(64, 64, 1.0, 0.9, 0.5)
+    n = A.shape()[0]
+    b = matgen.uniform_vector(n, seed=3)
+    Ad = gpu.Device_matrix(A)
+    M = gpu.jacobi(Ad) if pname == "jacobi" else gpu.chebyshev_preconditioner(Ad, 0.2, 9.5, 8)
+    bd = torch.from_numpy(b).cuda()
+    xd = torch.zeros_like(bd)
+    s = gpu.mixed_fgmres(bd, xd, gpu.Mixed_fgmres_config(1e-10, 1e-4, 30, 20, 5000, True), gpu.spmv(Ad), M)
+    torch.cuda.synchronize()
+    rel = _true_rel(oracle, A, b, xd)
+    assert s.converged and rel < 1e-10, (s, rel)
+    assert abs(s.residual_norm / np.linalg.norm(b) - rel) < 1e-12
+    assert all(a > c for a, c in zip(s.residual_history, s.residual_history[1:]))
+    x = np.zeros(n)
+    sp = gpu.fgmres(b, x, gpu.Fgmres_config(1e-10, 30, 20000), gpu.spmv(Ad), M)
+    assert sp.converged and s.inner_iterations <= 1.5 * sp.computed_iterations, (s.inner_iterations,
+                                                                                  sp.computed_iterations)
+
+
+def test_mixed_fgmres_two_level(gpu_lib, oracle):
+    """Configuration 4's operator at 128 x 128 (GRF diffusion, upwind
+    convection, cell Peclet 1-100) with the two-level Jacobi preconditioner
+    applied in FP64 between FP32 inner vectors: 1e-10 on the true residual."""
+    import torch
+    A, _ = matgen.convdiff_2d_grf(128, seed=777)
+    n = A.shape()[0]
+    b = np.random.default_rng(3).uniform(-1, 1, n)
+    Ad = gpu.Device_matrix(A)
+    M = gpu.twolevel(Ad, gpu.jacobi(Ad), 128, 128, 2)
+    bd = torch.from_numpy(b).cuda()
+    xd = torch.zeros_like(bd)
+    s = gpu.mixed_fgmres(bd, xd, gpu.Mixed_fgmres_config(1e-10, 1e-4, 30, 30, 5000), gpu.spmv(Ad), M)
+    torch.cuda.synchronize()
+    rel = _true_rel(oracle, A, b, xd)
+    assert s.converged and rel < 1e-10, (s, rel)
+
+
+def test_mixed_fgmres_refuses_the_network(gpu_lib):
+    import torch
+    from sparkit_b200 import _lib
+    A, _ = matgen.convdiff_2d_grf(32, seed=1)
+    Ad = gpu.Device_matrix(A)
+    net = gpu.Net(seed=0)
+    L = gpu.learned_preconditioner(Ad, net, 32, 32)
+    bd = torch.ones(A.shape()[0], dtype=torch.float64, device="cuda")
+    with pytest.raises(_lib.SkError) as e:
+        gpu.mixed_fgmres(bd, torch.zeros_like(bd), gpu.Mixed_fgmres_config(), gpu.spmv(Ad), L)
+    assert e.value.status == 9
