@@ -319,6 +319,38 @@ static sk_status build_sell(sk_matrix A, const int64_t* rp, cudaStream_t st_) {
   return SK_OK;
 }
 
+// The split product's row lists (long rows by decreasing length, ties in
+// row order; short rows in row order) for a CSR handle without SELL-32
+// whose rows longer than kHybLong hold at least half of the entries.  The
+// long rows' share of the wave follows their share of the work, a short
+// row's entry counting twice (its loads are not coalesced).
+static sk_status build_hybrid(sk_matrix A, const int64_t* rp, cudaStream_t st_) {
+  const i64 n = A->nrow;
+  if (n == 0 || A->nnz == 0) return SK_OK;
+  std::vector<int> shorts, longs;
+  i64 long_nnz = 0;
+  for (i64 i = 0; i < n; ++i) {
+    const i64 len = rp[i + 1] - rp[i];
+    if (len > kHybLong) {
+      longs.push_back(static_cast<int>(i));
+      long_nnz += len;
+    } else {
+      shorts.push_back(static_cast<int>(i));
+    }
+  }
+  if (2 * long_nnz < A->nnz) return SK_OK;
+  std::stable_sort(longs.begin(), longs.end(), [&](int a, int b) { return rp[a + 1] - rp[a] > rp[b + 1] - rp[b]; });
+  sk_status st;
+  if (!shorts.empty() && (st = upload_vector(A, shorts, &A->csr.hyb_short, st_)) != SK_OK) return st;
+  if ((st = upload_vector(A, longs, &A->csr.hyb_long, st_)) != SK_OK) return st;
+  A->csr.hyb_nshort = static_cast<int>(shorts.size());
+  A->csr.hyb_nlong = static_cast<int>(longs.size());
+  const double short_work = 2.0 * static_cast<double>(A->nnz - long_nnz);
+  A->csr.hyb_long_frac = static_cast<double>(long_nnz) / (static_cast<double>(long_nnz) + short_work);
+  A->csr.hyb = true;
+  return SK_OK;
+}
+
 // Adds the sliced copy of a 2x2 or 3x3 BSR handle when every block row has
 // at most kSellMaxRow blocks and the padding stays within a quarter.
 sk_status build_bsr_sell(sk_matrix A, const int64_t* rp, cudaStream_t st_) {
@@ -380,7 +412,8 @@ sk_status csr_finish(sk_matrix A, const int64_t* row_ptr, cudaStream_t st_) {
     tiles[b] = make_int2(part[b], static_cast<int>(row_ptr[part[b]]));
   if ((st = upload_vector(A, tiles, &A->csr.tiles, st_)) != SK_OK) return st;
   if ((st = upload_vector(A, lanes, &A->csr.lanes, st_)) != SK_OK) return st;
-  return build_sell(A, row_ptr, st_);
+  if ((st = build_sell(A, row_ptr, st_)) != SK_OK) return st;
+  return A->csr.sell ? SK_OK : build_hybrid(A, row_ptr, st_);
 }
 
 }  // namespace sk

@@ -24,6 +24,7 @@ constexpr int kBsrTileVals = 4096;  // BSR: block values staged per CTA
 constexpr int kMaxRed = 4;       // fused reductions carried per kernel
 constexpr int kSellMaxRow = 64;  // CSR rows up to this length use SELL-32
 constexpr int kDiaMax = 16;      // diagonals of the diagonal copy of a CSR handle
+constexpr int kHybLong = 32;     // rows longer than this take a warp in the split product
 
 // ------------------------------------------------------------------
 // Status plumbing
@@ -84,6 +85,16 @@ struct Csr {
   int* sell_off = nullptr;             // nslices + 1 entry offsets
   unsigned char* sell_len = nullptr;   // entries per row
   i64 sell_entries = 0;                // padded size
+  // Split product for skewed rows (when SELL-32 is refused and rows longer
+  // than kHybLong entries hold most of the entries): the long rows, by
+  // decreasing length, one warp each; the short rows, in row order, one
+  // thread each.  A share hyb_long_frac of the kernel's one wave of CTAs
+  // takes the long rows.
+  bool hyb = false;
+  int* hyb_short = nullptr;
+  int* hyb_long = nullptr;
+  int hyb_nshort = 0, hyb_nlong = 0;
+  double hyb_long_frac = 0.0;
   // Diagonal copy (sk_matrix_add_diagonals) of a handle whose entries lie
   // on at most kDiaMax diagonals c - r = off[d] and whose rows hold their
   // columns in ascending order, slice-major like the SELL-32 copy: A(r, r +

@@ -404,6 +404,70 @@ sell_spmv_kernel(int nrow, const int* __restrict__ off, const unsigned char* __r
 }
 
 // ------------------------------------------------------------------
+// CSR split by row length, for skewed matrices (a few rows hold most of
+// the entries).  One wave of CTAs: the last long_ctas CTAs take the long
+// rows (more than kHybLong entries, by decreasing length, round robin over
+// their warps), one warp per row: each lane sums the entries k = lane,
+// lane + 32, ... into four independent partial sums (four loads of the
+// contiguous row segment and four gathers of x in flight per lane), which
+// a fixed shuffle tree then adds.  The other CTAs take the short rows in
+// row order, one thread per row, each summed in storage order from 0 (the
+// bits of sparse_blas.hpp:25-28).  No shared memory, so the L1 serves the
+// random gathers of x only.
+// ------------------------------------------------------------------
+template <typename T, class Epi, int MINB>
+__global__ void __launch_bounds__(kThreads, MINB)
+hyb_spmv_kernel(const int* __restrict__ rp, const int* __restrict__ ci, const T* __restrict__ va,
+                const T* __restrict__ x, const int* __restrict__ short_rows, int nshort,
+                const int* __restrict__ long_rows, int nlong, int long_ctas, Epi epi, RedWs ws,
+                const Scalars* sc) {
+  constexpr int NR = Epi::kNR;
+  if (solve_done(sc)) return;
+  double red[NR > 0 ? NR : 1];
+#pragma unroll
+  for (int j = 0; j < (NR > 0 ? NR : 1); ++j) red[j] = 0.0;
+  const int short_ctas = static_cast<int>(gridDim.x) - long_ctas;
+  if (static_cast<int>(blockIdx.x) >= short_ctas) {
+    constexpr int W = kThreads / 32;
+    const int lane = threadIdx.x & 31;
+    const int nw = long_ctas * W;
+    for (int w = (static_cast<int>(blockIdx.x) - short_ctas) * W + (threadIdx.x >> 5); w < nlong; w += nw) {
+      const int row = __ldg(long_rows + w);
+      const int b = __ldg(rp + row), e = __ldg(rp + row + 1);
+      T a0 = T(0), a1 = T(0), a2 = T(0), a3 = T(0);
+      int k = b + lane;
+      for (; k + 96 < e; k += 128) {
+        const int c0 = __ldcs(ci + k), c1 = __ldcs(ci + k + 32), c2 = __ldcs(ci + k + 64), c3 = __ldcs(ci + k + 96);
+        const T v0 = __ldcs(va + k), v1 = __ldcs(va + k + 32), v2 = __ldcs(va + k + 64), v3 = __ldcs(va + k + 96);
+        const T x0 = __ldg(x + c0), x1 = __ldg(x + c1), x2 = __ldg(x + c2), x3 = __ldg(x + c3);
+        a0 = add(a0, mul(v0, x0));
+        a1 = add(a1, mul(v1, x1));
+        a2 = add(a2, mul(v2, x2));
+        a3 = add(a3, mul(v3, x3));
+      }
+      for (; k < e; k += 32) a0 = add(a0, mul(__ldcs(va + k), __ldg(x + __ldcs(ci + k))));
+      T sum = add(add(a0, a1), add(a2, a3));
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) sum = add(sum, __shfl_xor_sync(0xffffffffu, sum, o));
+      if (lane == 0) reduce_terms<NR>(ws, row, red, [&](double* rr) { epi(row, sum, rr); });
+    }
+  } else {
+    for (int t = blockIdx.x * kThreads + threadIdx.x; t < nshort; t += short_ctas * kThreads) {
+      const int row = __ldg(short_rows + t);
+      const int b = __ldg(rp + row), n = __ldg(rp + row + 1) - b;
+      const T sum = row_dot<T, 4, true>(n, x, [&](int k, int& c, T& v) {
+        c = __ldcs(ci + b + k);
+        v = __ldcs(va + b + k);
+      });
+      reduce_terms<NR>(ws, row, red, [&](double* rr) { epi(row, sum, rr); });
+    }
+  }
+  if constexpr (NR > 0) {
+    grid_reduce<NR>(red, ws, [&](const double* t) { epi.finalize(t); });
+  }
+}
+
+// ------------------------------------------------------------------
 // CSR through its diagonal copy: one thread per row.  Diagonal d of a
 // warp's 32 rows is one contiguous 32-value segment of the slice-major copy
 // (a slice's segments are adjacent), and x[i + off[d]] is contiguous too,
@@ -735,6 +799,16 @@ void launch_spmv(const sk_matrix_s* A, const T* x, Epi const& epi, RedWs ws,
         break;
       }
       const T* v = vals_override ? vals_override : static_cast<const T*>(A->csr.vals);
+      if (A->csr.hyb) {
+        constexpr int MB = 6;  // 40 registers: four loads and gathers in flight per lane without spills
+        const int grid = A->sm_count * MB;
+        const int nl = A->csr.hyb_nlong, ns = A->csr.hyb_nshort;
+        int lc = static_cast<int>(grid * A->csr.hyb_long_frac + 0.5);
+        lc = nl == 0 ? 0 : ns == 0 ? grid : (lc < 1 ? 1 : lc > grid - 1 ? grid - 1 : lc);
+        SK_LAUNCH((hyb_spmv_kernel<T, Epi, MB>), grid, kThreads, 0, st, A->csr.row_ptr, A->csr.col_ind, v, x,
+                  A->csr.hyb_short, ns, A->csr.hyb_long, nl, lc, epi, ws, sc);
+        break;
+      }
       SK_LAUNCH((csr_spmv_kernel<T, Epi>), A->csr.nparts, kThreads, 0, st,
                 A->csr.row_ptr, A->csr.col_ind, v, x, A->csr.tiles, A->csr.lanes, epi,
                 ws, sc);

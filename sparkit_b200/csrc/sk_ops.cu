@@ -205,7 +205,9 @@ static sk_status plan_host_pipe(sk_matrix A) {
   const size_t V = vbytes(A->dtype);
   const i64 n = A->nrow;
   int want = static_cast<int>(std::min<i64>(kPipeMaxChunks, (n * static_cast<i64>(V)) / kPipeChunkBytes));
-  if (A->format != SK_CSR || A->nnz == 0 || A->ncol == 0 || want < 2) {
+  // (the split product of skewed rows reads x everywhere from its first
+  // rows on, so it runs whole)
+  if (A->format != SK_CSR || A->nnz == 0 || A->ncol == 0 || want < 2 || A->csr.hyb) {
     p->chunks = 1;
     A->pipe = guard.release();
     return SK_OK;
