@@ -400,6 +400,7 @@ SK_API sk_status sk_batch_destroy(sk_batch B) {
 
 SK_API sk_status sk_batched_cg_solve(sk_batch B, const double* b_dev, double* x_dev, const sk_batch_config* cfg,
                                      sk_batch_results* res, sk_stream s) {
+  Range range_("sk batched_cg");
   SK_CHECK(B && cfg && res && b_dev && x_dev, SK_INVALID_ARG, "null argument");
   SK_CHECK(res->inner_iterations && res->outer_iterations && res->relative_residual && res->converged,
            SK_INVALID_ARG, "result arrays must be device arrays of nsys entries");

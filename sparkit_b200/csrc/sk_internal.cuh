@@ -13,6 +13,8 @@
 
 #include "../../include/sparkit_b200.h"
 
+#include <nvtx3/nvToolsExt.h>
+
 namespace sk {
 
 using i64 = std::int64_t;
@@ -43,6 +45,15 @@ sk_status cuda_fail(cudaError_t e, char const* what);
   do {                                                                   \
     if (!(cond)) return ::sk::fail((st), (msg));                         \
   } while (0)
+
+// A named NVTX range (solver phases in a profiler's timeline); NVTX is
+// header-only and costs nothing unless a tool is attached.
+struct Range {
+  explicit Range(const char* name) { nvtxRangePushA(name); }
+  ~Range() { nvtxRangePop(); }
+  Range(Range const&) = delete;
+  Range& operator=(Range const&) = delete;
+};
 
 // Bound of every grid-barrier wait of the persistent kernels, in ns, and the
 // extra arrivals each barrier waits for (0, or 1 when sk_debug_set_wait

@@ -432,6 +432,7 @@ template <typename T>
 static sk_status cg_solve(sk_matrix A, sk_precond L, sk_precond R, const T* b, T* x,
                           const sk_cg_config* cfg, sk_summary* out, double* history_host,
                           cudaStream_t st, const T* vals = nullptr, char* ws_base = nullptr) {
+  Range range_("sk conjugate_gradient");
   const i64 n = A->nrow;
   const size_t vb = static_cast<size_t>(n + 8) * sizeof(T);
   SolveCommon c;
@@ -778,6 +779,7 @@ template <typename T>
 static sk_status bicgstab_solve(sk_matrix A, sk_precond L, sk_precond R, const T* b, T* x,
                                 const sk_bicgstab_config* cfg, sk_summary* out,
                                 double* history_host, cudaStream_t st) {
+  Range range_("sk bicgstab");
   const i64 n = A->nrow;
   const size_t vb = static_cast<size_t>(n + 8) * sizeof(T);
   SolveCommon c;
@@ -1116,6 +1118,7 @@ static sk_status fgmres_solve(sk_matrix A, sk_precond M, const T* b, T* x,
                               cudaStream_t st, sk_precond fallback = nullptr, double stall_ratio = 0.0,
                               int64_t* switched_at = nullptr, sk_precond left = nullptr, bool gmres = false,
                               const T* vals = nullptr, bool hess64 = false) {
+  Range range_("sk fgmres");
   const i64 n = A->nrow;
   const int m = static_cast<int>(cfg->restart_dimension);
   SK_CHECK(m >= 1 && m <= 4096, SK_INVALID_ARG, "restart_dimension must be in [1, 4096]");
@@ -1520,6 +1523,7 @@ struct OpCgsDir {
 template <typename T>
 static sk_status cgs_solve(sk_matrix A, sk_precond L, sk_precond R, const T* b, T* x, const sk_cgs_config* cfg,
                            sk_summary* out, double* history_host, cudaStream_t st) {
+  Range range_("sk cgs");
   const i64 n = A->nrow;
   const size_t vb = static_cast<size_t>(n + 8) * sizeof(T);
   SolveCommon c;
@@ -1823,6 +1827,7 @@ template <typename T>
 static sk_status minres_solve(sk_matrix A, sk_precond L, sk_precond R, const T* b, T* x,
                               const sk_minres_config* cfg, sk_summary* out, double* history_host,
                               cudaStream_t st) {
+  Range range_("sk minres");
   const i64 n = A->nrow;
   const size_t vb = static_cast<size_t>(n + 8) * sizeof(T);
   SolveCommon c;
@@ -2062,6 +2067,7 @@ __global__ void inv_diag32_kernel(i64 n, const int* __restrict__ rp, const int* 
 static sk_status mixed_cg_solve(sk_matrix A, bool jacobi, const double* b, double* x,
                                 const sk_mixed_config* cfg, sk_mixed_summary* out, double* history,
                                 cudaStream_t st) {
+  Range range_("sk mixed_cg");
   const i64 n = A->nrow;
   *out = sk_mixed_summary{};
   using clk = std::chrono::steady_clock;
@@ -2192,6 +2198,7 @@ static sk_status mixed_cg_solve(sk_matrix A, bool jacobi, const double* b, doubl
         icfg.tolerance = std::max(0.5 * needed, 1e-7);
       sk_summary is{};
       auto t_inner = clk::now();
+      Range inner_range("sk mixed_cg inner FP32 solve");
       L2Window win(cfg->l2_window ? st : nullptr, inner_base, resident_bytes);
       if (persistent) {
         InnerResult ir;
@@ -2231,6 +2238,7 @@ static sk_status mixed_cg_solve(sk_matrix A, bool jacobi, const double* b, doubl
 static sk_status mixed_fgmres_solve(sk_matrix A, sk_precond M, const double* b, double* x,
                                     const sk_mixed_fgmres_config* cfg, sk_mixed_summary* out, double* history,
                                     cudaStream_t st) {
+  Range range_("sk mixed_fgmres");
   const i64 n = A->nrow;
   *out = sk_mixed_summary{};
   out->inner_kernel = 1;
@@ -2306,6 +2314,7 @@ static sk_status mixed_fgmres_solve(sk_matrix A, sk_precond M, const double* b, 
       icfg.tolerance = std::max(0.5 * needed, 1e-6);
     sk_summary is{};
     auto t_inner = clk::now();
+    Range inner_range("sk mixed_fgmres inner FP32 solve");
     s = fgmres_solve<float>(A, M, r32, d32, &icfg, &is, nullptr, st, nullptr, 0.0, nullptr, nullptr, false,
                             f32_values(A), true);
     out->inner_ms += ms_since(t_inner);
