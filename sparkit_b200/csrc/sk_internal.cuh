@@ -239,7 +239,7 @@ struct sk_precond_s {
   sk_precond_s* smoother = nullptr;
   sk::i64 agg = 0, coarse_n = 0;
   int post = 0, coarse_first = 0;
-  double* coarse_inv = nullptr;
+  float* coarse_inv = nullptr;  // FP32, row-major nc x nc
   double* tbuf = nullptr;
   double* tbuf2 = nullptr;
   double* rc = nullptr;

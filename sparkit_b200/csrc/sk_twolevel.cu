@@ -23,7 +23,11 @@
 // banded LU without pivoting (Ac is an M-matrix when A is: Galerkin
 // aggregation keeps the signs and the diagonal dominance of the upwind
 // convection-diffusion operators) and inverted column by column.  The
-// inverse (nc x nc FP64, nc <= 4096) is applied as one deterministic GEMV.
+// inverse (nc x nc, nc <= 4096, stored in FP32) is applied as one
+// deterministic GEMV with FP64 products and sums.  Solving with the banded
+// factors instead would read 4 MB rather than 64 MiB, but each of its nc
+// rows waits on the previous ones (a chain of nc dependent steps on one
+// SM), where the GEMV spreads the rows over every SM.
 // Every reduction runs in a fixed order, so applies are repeatable bit for
 // bit, and the apply launches kernels only (it can be captured).
 #include <algorithm>
@@ -64,17 +68,30 @@ __global__ void __launch_bounds__(kThreads) restrict_kernel(int nx, int agg, int
 }
 
 // zc = Ainv rc: one warp per coarse row, lane-strided partial sums and a
-// shuffle tree.
-__global__ void __launch_bounds__(kThreads) coarse_gemv_kernel(int nc, const double* __restrict__ ainv,
+// shuffle tree.  The inverse is stored in FP32 (64 MiB at nc = 4096: half
+// the bytes of the FP64 inverse, and within the L2) and every product is
+// formed and summed in FP64; the float rounding of the inverse (relative
+// 6e-8 per entry) perturbs the coarse correction of a preconditioner only.
+// Each lane reads four consecutive floats (16 bytes) per step.
+__global__ void __launch_bounds__(kThreads) coarse_gemv_kernel(int nc, const float* __restrict__ ainv,
                                                                const double* __restrict__ rc,
                                                                double* __restrict__ zc, const Scalars* sc) {
   if (solve_done(sc)) return;
   const int I = blockIdx.x * (kThreads / 32) + (threadIdx.x >> 5);
   const int lane = threadIdx.x & 31;
   if (I >= nc) return;
-  const double* row = ainv + static_cast<i64>(I) * nc;
+  const float* row = ainv + static_cast<i64>(I) * nc;
   double s[1] = {0.0};
-  for (int j = lane; j < nc; j += 32) s[0] += row[j] * rc[j];
+  int j = 4 * lane;
+  if ((nc & 3) == 0) {
+    for (; j < nc; j += 128) {
+      const float4 a = __ldg(reinterpret_cast<const float4*>(row + j));
+      s[0] += static_cast<double>(a.x) * rc[j] + static_cast<double>(a.y) * rc[j + 1] +
+              static_cast<double>(a.z) * rc[j + 2] + static_cast<double>(a.w) * rc[j + 3];
+    }
+  } else {
+    for (j = lane; j < nc; j += 32) s[0] += static_cast<double>(row[j]) * rc[j];
+  }
   warp_reduce<1>(s);
   if (lane == 0) zc[I] = s[0];
 }
@@ -156,8 +173,8 @@ void twolevel_apply(const sk_precond_s* M, const double* r, double* z, RedWs ws,
   const sk_precond_s* S = M->smoother;
   auto coarse = [&](const double* t, int set) {  // z (+)= P Ac^-1 P^T t
     SK_LAUNCH(restrict_kernel, nc, kThreads, 0, st, nx, agg, mcx, t, M->rc, sc);
-    SK_LAUNCH(coarse_gemv_kernel, ceil_div(nc, kThreads / 32), kThreads, 0, st, nc, M->coarse_inv, M->rc, M->zc,
-              sc);
+    SK_LAUNCH(coarse_gemv_kernel, ceil_div(nc, kThreads / 32), kThreads, 0, st, nc,
+              M->coarse_inv, M->rc, M->zc, sc);
     SK_LAUNCH(prolong_kernel, ew_blocks(n), kThreads, 0, st, n, nx, agg, mcx, M->zc, nullptr, set, z, sc);
   };
   auto smooth_add = [&]() {  // z += S(r - A z)
@@ -181,7 +198,9 @@ void twolevel_apply(const sk_precond_s* M, const double* r, double* z, RedWs ws,
 }
 
 void twolevel_release(sk_precond_s* M) {
-  for (double** p : {&M->coarse_inv, &M->tbuf, &M->tbuf2, &M->rc, &M->zc, &M->cvt_in, &M->cvt_out}) {
+  if (M->coarse_inv) cudaFree(M->coarse_inv);
+  M->coarse_inv = nullptr;
+  for (double** p : {&M->tbuf, &M->tbuf2, &M->rc, &M->zc, &M->cvt_in, &M->cvt_out}) {
     if (*p) cudaFree(*p);
     *p = nullptr;
   }
@@ -246,7 +265,8 @@ sk_status sk_twolevel_create(sk_precond* out, sk_matrix A, sk_precond smoother, 
   M->coarse_n = nc;
   M->post = (flags & SK_TWOLEVEL_POST_SMOOTH) ? 1 : 0;
   M->coarse_first = (flags & SK_TWOLEVEL_COARSE_FIRST) ? 1 : 0;
-  cudaError_t e = cudaMalloc(&M->coarse_inv, static_cast<size_t>(nc * nc) * 8);
+  std::vector<float> inv32(inv.begin(), inv.end());
+  cudaError_t e = cudaMalloc(&M->coarse_inv, static_cast<size_t>(nc * nc) * 4 + 64);
   if (e == cudaSuccess) e = cudaMalloc(&M->tbuf, static_cast<size_t>(n + 8) * 8);
   if (e == cudaSuccess) e = cudaMalloc(&M->tbuf2, static_cast<size_t>(n + 8) * 8);
   if (e == cudaSuccess) e = cudaMalloc(&M->rc, static_cast<size_t>(nc + 8) * 8);
@@ -254,7 +274,7 @@ sk_status sk_twolevel_create(sk_precond* out, sk_matrix A, sk_precond smoother, 
   if (e == cudaSuccess) e = cudaMalloc(&M->cvt_in, static_cast<size_t>(n + 8) * 8);
   if (e == cudaSuccess) e = cudaMalloc(&M->cvt_out, static_cast<size_t>(n + 8) * 8);
   if (e == cudaSuccess)
-    e = cudaMemcpy(M->coarse_inv, inv.data(), static_cast<size_t>(nc * nc) * 8, cudaMemcpyHostToDevice);
+    e = cudaMemcpy(M->coarse_inv, inv32.data(), static_cast<size_t>(nc * nc) * 4, cudaMemcpyHostToDevice);
   if (e != cudaSuccess) {
     twolevel_release(M);
     delete M;

@@ -24,7 +24,8 @@ def _dense_parts(A, nx, ny, agg):
 def test_twolevel_apply_matches_numpy(gpu_lib, post):
     """Jacobi smoother: z = D^-1 r; z += P Ac^-1 P^T (r - A z)
     [; z += D^-1 (r - A z)], against the same steps in NumPy (the coarse
-    inverse from LAPACK there, a banded LU here)."""
+    inverse from LAPACK in FP64 there; a banded LU here, its inverse stored
+    in FP32 and applied with FP64 products: within 1e-6)."""
     import torch
     from tests.test_gpu_learned import rect_convdiff
     nx, ny, agg = 64, 48, 8
@@ -44,7 +45,8 @@ def test_twolevel_apply_matches_numpy(gpu_lib, post):
     if post:
         z = z + (r - M @ z) / d
     got = zd.cpu().numpy()
-    assert np.linalg.norm(got - z) / np.linalg.norm(z) < 1e-10
+    # the coarse inverse is stored in FP32 (products and sums in FP64)
+    assert np.linalg.norm(got - z) / np.linalg.norm(z) < 1e-6
     # repeatable bit for bit (fixed-order reductions)
     z2 = torch.zeros_like(rd)
     T.apply(rd, z2)
