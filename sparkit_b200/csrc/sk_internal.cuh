@@ -234,8 +234,8 @@ struct sk_precond_s {
   float* coef = nullptr;
   sk::i64 grid_nx = 0, grid_ny = 0;
   // two-level (kind 4): smoother (not owned), agg x agg aggregates of the
-  // grid, the dense inverse of the Galerkin coarse operator (coarse_n^2
-  // FP64, row-major) and work vectors
+  // grid, the dense inverse of the Galerkin coarse operator (coarse_n^2,
+  // stored in FP32) and FP64 work vectors
   sk_precond_s* smoother = nullptr;
   sk::i64 agg = 0, coarse_n = 0;
   int post = 0, coarse_first = 0;
