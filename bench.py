@@ -723,6 +723,32 @@ def learned_runs(train_grid=128, instances=200, cycles=100, eval_grids=(128, 512
                     "loss_last50": float(h[-50:].mean())}
     pairs.close()
 
+    def mixed_vs_plain(M, Ad, A, b, reps=3):
+        """FGMRES(30) to a 1e-10 true residual with M: plain FP64 against FP32
+        inner FGMRES(30) (FP64 Hessenberg least-squares) in FP64 refinement;
+        best wall time of the repetitions after the first."""
+        res = {}
+        bh = b.cpu().numpy()
+        for name in ("plain_fp64", "mixed_fp32_fp64"):
+            ts = []
+            for _ in range(reps):
+                xd = torch.zeros_like(b)
+                torch.cuda.synchronize()
+                t1 = time.perf_counter()
+                if name == "plain_fp64":
+                    s = gpu.fgmres(b, xd, gpu.Fgmres_config(1e-10, 30, 6000), gpu.spmv(Ad), M)
+                    its = {"iterations": s.computed_iterations}
+                else:
+                    s = gpu.mixed_fgmres(b, xd, gpu.Mixed_fgmres_config(1e-10, 1e-4, 30, 50, 6000), gpu.spmv(Ad), M)
+                    its = {"outer": s.outer_iterations, "inner_iterations": s.inner_iterations,
+                           "inner_ms": s.inner_ms, "outer_ms": s.outer_ms}
+                torch.cuda.synchronize()
+                ts.append((time.perf_counter() - t1) * 1e3)
+            rel = float(np.linalg.norm(bh - O.spmv(A, xd.cpu().numpy())) / np.linalg.norm(bh))
+            res[name] = {"ms": min(ts[1:]), "converged": bool(s.converged), "true_rel_residual": rel, **its}
+        res["speedup_mixed_vs_plain"] = res["plain_fp64"]["ms"] / res["mixed_fp32_fp64"]["ms"]
+        return res
+
     def run(M, Ad, A, b, maxit):
         xd = torch.zeros_like(b)
         torch.cuda.synchronize()
@@ -762,6 +788,7 @@ def learned_runs(train_grid=128, instances=200, cycles=100, eval_grids=(128, 512
         if big:
             agg = g // 64
             r["twolevel_jacobi"] = run(gpu.twolevel(Ad, J, g, g, agg), Ad, A, b, 3000)
+            r["fgmres_to_1e-10_fp64_vs_mixed"] = mixed_vs_plain(gpu.twolevel(Ad, J, g, g, agg), Ad, A, b)
             r["twolevel_learned"] = run(gpu.twolevel(Ad, L, g, g, agg, coarse_first=True), Ad, A, b, 3000)
             r["twolevel_aggregates"] = [agg, (g // agg) ** 2]
         plain = [r["jacobi"], r["chebyshev8"]]
