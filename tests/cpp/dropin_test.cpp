@@ -165,6 +165,10 @@ void run_gpu() {
     auto ident = [](auto first, auto last, auto out) { std::copy(first, last, out); };
     sk::gpu::Device_matrix<double> Ad(A);
     {
+      // BiCGSTAB's count moves with the summation order of its dot products
+      // (up to about 9% on this problem under any order but the
+      // reference's): the default tree order is held to 10%, and the
+      // reference's sequential order (sk_set_summation_order) to equality
       Bicgstab_config<double> cfg{.tolerance = 1e-10, .max_iterations = 3000};
       std::vector<double> x(n, 0.0), x_ref(n, 0.0);
       auto s_ref = bicgstab(b.begin(), b.end(), x_ref.begin(), x_ref.end(), cfg, apply_A, apply_J, ident);
@@ -174,8 +178,17 @@ void run_gpu() {
       std::printf("     BiCGSTAB: device %lld, reference %lld\n", (long long)s.computed_iterations,
                   (long long)s_ref.computed_iterations);
       expect(s.converged == s_ref.converged && s.converged, "BiCGSTAB converged");
-      expect(iters_close(s.computed_iterations, s_ref.computed_iterations), "BiCGSTAB iterations within 2%");
+      expect(std::llabs(static_cast<long long>(s.computed_iterations - s_ref.computed_iterations)) <=
+                 std::max(2LL, static_cast<long long>(s_ref.computed_iterations) / 10),
+             "BiCGSTAB iterations within 10% (tree order)");
       expect(rel_residual(A, b, x) < 1e-9, "BiCGSTAB true residual");
+      sk::gpu::check(sk_set_summation_order(SK_SUM_SEQUENTIAL));
+      std::vector<double> xs(n, 0.0);
+      auto ss = bicgstab(b.begin(), b.end(), xs.begin(), xs.end(), cfg, sk::gpu::spmv(Ad), sk::gpu::jacobi(Ad),
+                         sk::gpu::identity);
+      sk::gpu::check(sk_set_summation_order(SK_SUM_TREE));
+      expect(ss.computed_iterations == s_ref.computed_iterations && xs == x_ref,
+             "BiCGSTAB in the sequential order: the reference's count and solution, bit for bit");
     }
     {
       Fgmres_config<double> cfg{.tolerance = 1e-10, .restart_dimension = 30, .max_iterations = 3000};

@@ -74,9 +74,10 @@ def test_golden_solves_bit_identical(sequential, golden, name, pname):
         s = fn(x)
         assert s.computed_iterations == int(golden[f"{key}/iters"]), (key, s.computed_iterations)
         assert s.converged == bool(golden[f"{key}/converged"]), key
+        # (CGS with Chebyshev on grid16 runs into NaN in the reference too)
         hist = golden[f"{key}/history"]
-        assert np.array_equal(np.array(s.iteration_residuals), hist), key
-        assert np.array_equal(x, golden[f"{key}/x"]), (key, np.max(np.abs(x - golden[f"{key}/x"])))
+        assert np.array_equal(np.array(s.iteration_residuals), hist, equal_nan=True), key
+        assert np.array_equal(x, golden[f"{key}/x"], equal_nan=True), (key, np.max(np.abs(x - golden[f"{key}/x"])))
 
 
 @pytest.mark.parametrize("grid", [48, 96])
