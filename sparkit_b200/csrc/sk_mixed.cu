@@ -205,10 +205,11 @@ __device__ __forceinline__ void row_fetch(PArgs const& a, int len, int base, int
 
 // The direction update of one row from its product w = (M r)_i: p = r +
 // beta p, q = w + beta q (p = r, q = w at the first step); returns p q.
+template <bool FIRST>
 __device__ __forceinline__ double row_direction(PArgs const& a, int i, float ri, float w, float pi, float qi,
-                                                float beta, bool first) {
-  const float pn = first ? ri : add(ri, mul(beta, pi));
-  const float qn = first ? w : add(w, mul(beta, qi));
+                                                float beta) {
+  const float pn = FIRST ? ri : add(ri, mul(beta, pi));
+  const float qn = FIRST ? w : add(w, mul(beta, qi));
   a.p[i] = pn;
   a.q[i] = qn;
   return static_cast<double>(mul(pn, qn));
@@ -220,8 +221,8 @@ __device__ __forceinline__ double row_direction(PArgs const& a, int i, float ri,
 // HBM while the gathers of row k+1 return and row k is summed, so neither
 // the matrix stream nor the gathers wait on each other.  Returns this
 // thread's share of <p, q>.
-template <bool UNIT>
-__device__ __forceinline__ double phase_s_sell(PArgs const& a, int t0, int T, float beta, bool first) {
+template <bool UNIT, bool FIRST>
+__device__ __forceinline__ double phase_s_sell(PArgs const& a, int t0, int T, float beta) {
   double pq = 0.0;
   // row a: summed this step; row b: slots arrived, gathers issued this
   // step; row c: slots issued this step
@@ -238,7 +239,7 @@ __device__ __forceinline__ double phase_s_sell(PArgs const& a, int t0, int T, fl
   }
   if (ia < a.n) {
     ra = a.r[ia];
-    if (!first) {
+    if (!FIRST) {
       pa = a.p[ia];
       qa = a.q[ia];
     }
@@ -263,7 +264,7 @@ __device__ __forceinline__ double phase_s_sell(PArgs const& a, int t0, int T, fl
     float rb = 0.0f, pb = 0.0f, qb = 0.0f;
     if (ib < a.n) {
       rb = a.r[ib];
-      if (!first) {
+      if (!FIRST) {
         pb = a.p[ib];
         qb = a.q[ib];
       }
@@ -284,7 +285,7 @@ __device__ __forceinline__ double phase_s_sell(PArgs const& a, int t0, int T, fl
       for (int j = 0; j < kPU; ++j)
         if (k + j < la) sum = add(sum, mul(v[j], g[j]));
     }
-    pq += row_direction(a, ia, ra, sum, pa, qa, beta, first);
+    pq += row_direction<FIRST>(a, ia, ra, sum, pa, qa, beta);
     // rotate a <- b <- c <- d
     ia = ib;
     la = lb;
@@ -321,8 +322,8 @@ __device__ __forceinline__ double phase_s_sell(PArgs const& a, int t0, int T, fl
 constexpr int kDiaRows = 2;
 constexpr int kDiaGroup = 4;
 
-template <bool UNIT>
-__device__ __forceinline__ double phase_s_dia(PArgs const& a, int t0, int T, float beta, bool first) {
+template <bool UNIT, bool FIRST>
+__device__ __forceinline__ double phase_s_dia(PArgs const& a, int t0, int T, float beta) {
   constexpr int R = kDiaRows, C = kDiaGroup;
   double pq = 0.0;
   const int last = a.n - 1;
@@ -336,8 +337,8 @@ __device__ __forceinline__ double phase_s_dia(PArgs const& a, int t0, int T, flo
       const bool in = row < a.n;
       m[r] = in ? __ldcs(a.dia_mask + row) : 0u;
       ro[r] = in ? a.r[row] : 0.0f;
-      po[r] = in && !first ? a.p[row] : 0.0f;
-      qo[r] = in && !first ? a.q[row] : 0.0f;
+      po[r] = in && !FIRST ? a.p[row] : 0.0f;
+      qo[r] = in && !FIRST ? a.q[row] : 0.0f;
       s[r] = UNIT ? ro[r] : 0.0f;
     }
 #pragma unroll
@@ -364,7 +365,7 @@ __device__ __forceinline__ double phase_s_dia(PArgs const& a, int t0, int T, flo
 #pragma unroll
     for (int r = 0; r < R; ++r) {
       const int row = i + r * T;
-      if (row < a.n) pq += row_direction(a, row, ro[r], s[r], po[r], qo[r], beta, first);
+      if (row < a.n) pq += row_direction<FIRST>(a, row, ro[r], s[r], po[r], qo[r], beta);
     }
   }
   return pq;
@@ -404,64 +405,75 @@ __global__ void __launch_bounds__(kPT, DIA ? 2 : 1) inner_cg_kernel(PArgs a) {
   int conv = 0;
   float rn = bnorm;
   if (bnorm == 0.0f) conv = 1;
-  while (!conv && it < a.max_iters) {
+  // phase S of one step (the first with p = r, q = A r) and <p, q>
+  auto phase_s = [&](double (&pq)[1], bool first_step) -> bool {
+    if (first_step) {
+      if constexpr (DIA) pq[0] = phase_s_dia<UNIT, true>(a, t0, T, beta);
+      else pq[0] = phase_s_sell<UNIT, true>(a, t0, T, beta);
+    } else {
+      if constexpr (DIA) pq[0] = phase_s_dia<UNIT, false>(a, t0, T, beta);
+      else pq[0] = phase_s_sell<UNIT, false>(a, t0, T, beta);
+    }
+    return grid_allreduce<1>(pq, a, 1, epoch);
+  };
+  double pq[1] = {0.0};
+  if (!conv && a.max_iters > 0) {
     // S: the product, the direction update and compute_step_size (:233-239)
-    const bool first = it == 0;
-    double pq[1];
-    if constexpr (DIA) pq[0] = phase_s_dia<UNIT>(a, t0, T, beta, first);
-    else pq[0] = phase_s_sell<UNIT>(a, t0, T, beta, first);
-    if (!grid_allreduce<1>(pq, a, 1, epoch)) return;
-    const float alpha = rho / static_cast<float>(pq[0]);
-    // U: compute_new_solution, compute_new_residual, is_converged
-    // (:242-276) and the next <r, z> (:279-284)
-    double rr[2] = {0.0, 0.0};
-    auto upd = [&](float pi, float qi, float di, float ro, float wi, float& dn, float& rnew) {
-      dn = add(mul(alpha, pi), di);
-      rnew = sub(ro, mul(alpha, qi));
-      const float r2 = mul(rnew, rnew);
-      rr[0] += static_cast<double>(r2);
-      if (UNIT) rr[1] += static_cast<double>(mul(wi, r2));
-    };
-    auto upd4 = [&](float4 pv, float4 qv, float4 dv, float4 rv, float4 wv, float4& dn, float4& rw) {
-      upd(pv.x, qv.x, dv.x, rv.x, wv.x, dn.x, rw.x);
-      upd(pv.y, qv.y, dv.y, rv.y, wv.y, dn.y, rw.y);
-      upd(pv.z, qv.z, dv.z, rv.z, wv.z, dn.z, rw.z);
-      upd(pv.w, qv.w, dv.w, rv.w, wv.w, dn.w, rw.w);
-    };
-    int j = t0;
-    for (; j + T < n4; j += 2 * T) {
-      const int j1 = j + T;
-      const float4 pv0 = p4[j], qv0 = q4[j], dv0 = d4[j], rv0 = r4[j];
-      const float4 pv1 = p4[j1], qv1 = q4[j1], dv1 = d4[j1], rv1 = r4[j1];
-      const float4 wv0 = UNIT ? w4[j] : one4, wv1 = UNIT ? w4[j1] : one4;
-      float4 dn0, rw0, dn1, rw1;
-      upd4(pv0, qv0, dv0, rv0, wv0, dn0, rw0);
-      upd4(pv1, qv1, dv1, rv1, wv1, dn1, rw1);
-      d4[j] = dn0;
-      r4[j] = rw0;
-      d4[j1] = dn1;
-      r4[j1] = rw1;
+    if (!phase_s(pq, true)) return;
+    for (;;) {
+      const float alpha = rho / static_cast<float>(pq[0]);
+      // U: compute_new_solution, compute_new_residual, is_converged
+      // (:242-276) and the next <r, z> (:279-284)
+      double rr[2] = {0.0, 0.0};
+      auto upd = [&](float pi, float qi, float di, float ro, float wi, float& dn, float& rnew) {
+        dn = add(mul(alpha, pi), di);
+        rnew = sub(ro, mul(alpha, qi));
+        const float r2 = mul(rnew, rnew);
+        rr[0] += static_cast<double>(r2);
+        if (UNIT) rr[1] += static_cast<double>(mul(wi, r2));
+      };
+      auto upd4 = [&](float4 pv, float4 qv, float4 dv, float4 rv, float4 wv, float4& dn, float4& rw) {
+        upd(pv.x, qv.x, dv.x, rv.x, wv.x, dn.x, rw.x);
+        upd(pv.y, qv.y, dv.y, rv.y, wv.y, dn.y, rw.y);
+        upd(pv.z, qv.z, dv.z, rv.z, wv.z, dn.z, rw.z);
+        upd(pv.w, qv.w, dv.w, rv.w, wv.w, dn.w, rw.w);
+      };
+      int j = t0;
+      for (; j + T < n4; j += 2 * T) {
+        const int j1 = j + T;
+        const float4 pv0 = p4[j], qv0 = q4[j], dv0 = d4[j], rv0 = r4[j];
+        const float4 pv1 = p4[j1], qv1 = q4[j1], dv1 = d4[j1], rv1 = r4[j1];
+        const float4 wv0 = UNIT ? w4[j] : one4, wv1 = UNIT ? w4[j1] : one4;
+        float4 dn0, rw0, dn1, rw1;
+        upd4(pv0, qv0, dv0, rv0, wv0, dn0, rw0);
+        upd4(pv1, qv1, dv1, rv1, wv1, dn1, rw1);
+        d4[j] = dn0;
+        r4[j] = rw0;
+        d4[j1] = dn1;
+        r4[j1] = rw1;
+      }
+      if (j < n4) {
+        float4 dn, rw;
+        upd4(p4[j], q4[j], d4[j], r4[j], UNIT ? w4[j] : one4, dn, rw);
+        d4[j] = dn;
+        r4[j] = rw;
+      }
+      if (tail < n) {
+        float dn, rw;
+        upd(a.p[tail], a.q[tail], a.d[tail], a.r[tail], UNIT ? a.wdiag[tail] : 1.f, dn, rw);
+        a.d[tail] = dn;
+        a.r[tail] = rw;
+      }
+      if (!grid_allreduce<2>(rr, a, 0, epoch)) return;
+      ++it;
+      rn = sqrtf(static_cast<float>(UNIT ? rr[1] : rr[0]));
+      conv = rn / bnorm < a.tol ? 1 : 0;
+      if (conv || it >= a.max_iters) break;
+      const float rho_new = static_cast<float>(rr[0]);
+      beta = rho_new / rho;  // update_direction (:285-290), applied in phase S
+      rho = rho_new;
+      if (!phase_s(pq, false)) return;
     }
-    if (j < n4) {
-      float4 dn, rw;
-      upd4(p4[j], q4[j], d4[j], r4[j], UNIT ? w4[j] : one4, dn, rw);
-      d4[j] = dn;
-      r4[j] = rw;
-    }
-    if (tail < n) {
-      float dn, rw;
-      upd(a.p[tail], a.q[tail], a.d[tail], a.r[tail], UNIT ? a.wdiag[tail] : 1.f, dn, rw);
-      a.d[tail] = dn;
-      a.r[tail] = rw;
-    }
-    if (!grid_allreduce<2>(rr, a, 0, epoch)) return;
-    ++it;
-    rn = sqrtf(static_cast<float>(UNIT ? rr[1] : rr[0]));
-    conv = rn / bnorm < a.tol ? 1 : 0;
-    if (conv || it >= a.max_iters) break;
-    const float rho_new = static_cast<float>(rr[0]);
-    beta = rho_new / rho;  // update_direction (:285-290), applied in the next phase S
-    rho = rho_new;
   }
 
   if (blockIdx.x == 0 && threadIdx.x == 0) {

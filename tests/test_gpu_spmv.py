@@ -141,3 +141,52 @@ def test_index_validation(gpu_lib):
     with pytest.raises(_lib.SkError) as e:
         gpu.Device_matrix(big)
     assert e.value.status == 2
+
+
+def _poisoned_product(Ad, x):
+    """y = A x on the device into a NaN-filled output, so that a row the
+    kernel skips shows up as NaN."""
+    import torch
+    xd = torch.from_numpy(np.ascontiguousarray(x)).cuda()
+    yd = torch.full((Ad.shape()[0],), float("nan"), dtype=xd.dtype, device="cuda")
+    Ad.spmv(xd, yd)
+    torch.cuda.synchronize()
+    return yd.cpu().numpy()
+
+
+@pytest.mark.parametrize("fmt", ["csr", "ell", "jad", "bsr22", "bsr33"])
+def test_small_case_sweep_writes_every_row(gpu_lib, oracle, fmt):
+    """Small-case sweep (n = 1..64; empty rows; a single dense row; a row
+    longer than 32 among short ones) with NaN-poisoned outputs, against the
+    oracle: every row is written, with the oracle's bits where one thread
+    sums the row (every non-CSR format and CSR rows of up to 32 entries)."""
+    rng = np.random.default_rng(21)
+    cases = []
+    for n in list(range(1, 17)) + [31, 32, 33, 63, 64]:
+        lens = rng.integers(0, min(n, 6) + 1, size=n)
+        lens[rng.integers(0, n)] = 0                      # an empty row
+        cases.append((n, lens))
+    dense = np.zeros(48, dtype=np.int64)
+    dense[17] = 48                                         # one dense row
+    cases.append((48, dense))
+    mixed = rng.integers(0, 4, size=64)
+    mixed[5] = 40                                          # a row longer than 32
+    cases.append((64, mixed))
+    for n, lens in cases:
+        rp = np.concatenate([[0], np.cumsum(lens)]).astype(np.int64)
+        ci = np.concatenate([np.sort(rng.choice(n, size=int(k), replace=False)) for k in lens]).astype(np.int64) \
+            if lens.sum() else np.zeros(0, np.int64)
+        va = rng.standard_normal(int(lens.sum()))
+        A = formats.Compressed_row_matrix((n, n), rp, ci, va)
+        block = BSR_BLOCKS.get(fmt, (3, 3))
+        M = convert(A, fmt, block)
+        x = rng.uniform(-1, 1, n)
+        y = _poisoned_product(gpu.Device_matrix(M), x)
+        y_ref = oracle.spmv(M, x)
+        assert not np.isnan(y).any(), (fmt, n)
+        if fmt == "csr":
+            short = lens <= 32
+            assert np.array_equal(y[short], y_ref[short]), (fmt, n)
+            assert normwise_err(A, x, y, y_ref) <= 1e-14, (fmt, n)
+        else:
+            assert np.array_equal(y, y_ref), (fmt, n)
