@@ -67,6 +67,8 @@ def parse():
                    help="one sk_eigenvalue_bounds on the grid^3 Laplacian (for an ncu launch list)")
     p.add_argument("--profile-convert", action="store_true",
                    help="each device format conversion once (for an ncu launch list)")
+    p.add_argument("--profile-zipf", action="store_true",
+                   help="three CSR FP64 products of matrix B (1M rows, Zipf(1.5) lengths), for ncu")
     p.add_argument("--profile-formats", action="store_true",
                    help="run one product of every sweep format and precision (for ncu captures), no timing")
     return p.parse_args()
@@ -983,6 +985,23 @@ def profile_gmres(grid=1024, iters=40):
     return 0
 
 
+def profile_zipf():
+    """Three CSR FP64 products of matrix B (the split product of skewed
+    rows), for an ncu capture of one launch."""
+    import torch
+
+    from sparkit_b200 import gpu, matgen
+    torch.cuda.set_device(0)
+    Z = matgen.zipf_random(1_000_000, s=1.5, cap=2048, seed=0)
+    Zd = gpu.Device_matrix(Z)
+    xz = torch.from_numpy(matgen.uniform_vector(Z.shape()[0], seed=3)).cuda()
+    yz = torch.empty_like(xz)
+    for _ in range(3):
+        Zd.spmv(xz, yz)
+    torch.cuda.synchronize()
+    return 0
+
+
 def profile_solvers(grid):
     """A short plain FP64 Jacobi-CG (20 iterations) and a short mixed solve
     (one outer step of 20 FP32 iterations) for per-kernel launch lists."""
@@ -1008,6 +1027,8 @@ def main():
         return run_reference(args)
     if args.profile_formats:
         return profile_formats(args.grid)
+    if args.profile_zipf:
+        return profile_zipf()
     if args.profile_convert:
         return profile_convert(args.grid)
     if args.profile_eigen:
