@@ -201,9 +201,12 @@ static void csr_partition(const int64_t* rp, i64 n, std::vector<int>& part,
       lanes.push_back(32);
       continue;
     }
+    // Rows of up to 32 entries and longer rows go to separate tiles, so a
+    // short row is always summed by one lane in storage order.
+    const bool long0 = len0 > 32;
     while (r < n && r - r0 < kRowsMax) {
       i64 len = rp[r + 1] - rp[r];
-      if (nnz + len > kTileNnz) break;
+      if (nnz + len > kTileNnz || (len > 32) != long0) break;
       nnz += len;
       maxlen = std::max(maxlen, len);
       ++r;

@@ -101,6 +101,40 @@ __global__ void dia_to_float_kernel(const double* __restrict__ in, float* __rest
 
 }  // namespace
 
+sk_status dia_pattern(sk_matrix A, std::vector<int>* offsets) {
+  offsets->clear();
+  const i64 n = A->nrow;
+  if (A->format != SK_CSR || n == 0 || A->nnz == 0 || n > INT_MAX / 2) return SK_OK;
+  if (A->csr.dia_n) {
+    offsets->assign(A->csr.dia_off, A->csr.dia_off + A->csr.dia_n);
+    return SK_OK;
+  }
+  int* scratch = nullptr;
+  SK_CUDA(cudaMalloc(&scratch, (kDiaMax + 1) * sizeof(int)));
+  std::vector<int> h(kDiaMax + 1, kEmpty);
+  h[kDiaMax] = 0;
+  cudaError_t e = cudaMemcpyAsync(scratch, h.data(), h.size() * sizeof(int), cudaMemcpyHostToDevice, A->stream);
+  if (e == cudaSuccess) {
+    SK_LAUNCH(dia_scan_kernel, grid_for(n), kThreads, 0, A->stream, n, A->csr.row_ptr, A->csr.col_ind, scratch,
+              scratch + kDiaMax);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(h.data(), scratch, h.size() * sizeof(int), cudaMemcpyDeviceToHost, A->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(A->stream);
+  cudaFree(scratch);
+  if (e != cudaSuccess) return cuda_fail(e, "diagonal scan");
+  if (h[kDiaMax] != 0) return SK_OK;  // unsorted rows or too many diagonals
+  std::vector<int> offs;
+  for (int k = 0; k < kDiaMax; ++k)
+    if (h[k] != kEmpty) offs.push_back(h[k]);
+  std::sort(offs.begin(), offs.end());
+  const i64 nd = static_cast<i64>(offs.size());
+  if (nd == 0 || nd * n > 2 * A->nnz) return SK_OK;  // planes more than half empty
+  *offsets = offs;
+  return SK_OK;
+}
+
 sk_status build_dia_f32(sk_matrix A) {
   if (!A->csr.dia_n || A->csr.dia_vals32 || A->dtype != SK_F64) return SK_OK;
   const i64 len = A->csr.dia_len;
@@ -130,29 +164,11 @@ sk_status sk_matrix_add_diagonals(sk_matrix A, int* built) {
     return SK_OK;
   }
   const i64 n = A->nrow;
-  if (n == 0 || A->nnz == 0 || n > INT_MAX / 2) return SK_OK;
-  int* scratch = nullptr;
-  SK_CUDA(cudaMalloc(&scratch, (kDiaMax + 1) * sizeof(int)));
-  std::vector<int> h(kDiaMax + 1, kEmpty);
-  h[kDiaMax] = 0;
-  cudaError_t e = cudaMemcpyAsync(scratch, h.data(), h.size() * sizeof(int), cudaMemcpyHostToDevice, A->stream);
-  if (e == cudaSuccess) {
-    SK_LAUNCH(dia_scan_kernel, grid_for(n), kThreads, 0, A->stream, n, A->csr.row_ptr, A->csr.col_ind, scratch,
-              scratch + kDiaMax);
-    e = cudaGetLastError();
-  }
-  if (e == cudaSuccess)
-    e = cudaMemcpyAsync(h.data(), scratch, h.size() * sizeof(int), cudaMemcpyDeviceToHost, A->stream);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(A->stream);
-  cudaFree(scratch);
-  if (e != cudaSuccess) return cuda_fail(e, "diagonal scan");
-  if (h[kDiaMax] != 0) return SK_OK;  // unsorted rows or too many diagonals
   std::vector<int> offs;
-  for (int k = 0; k < kDiaMax; ++k)
-    if (h[k] != kEmpty) offs.push_back(h[k]);
-  std::sort(offs.begin(), offs.end());
+  sk_status st0 = dia_pattern(A, &offs);
+  if (st0 != SK_OK) return st0;
+  if (offs.empty()) return SK_OK;  // not a pattern of few diagonals
   const i64 nd = static_cast<i64>(offs.size());
-  if (nd == 0 || nd * n > 2 * A->nnz) return SK_OK;  // planes more than half empty
   // slice-major: the nd segments of a 32-row slice are adjacent, so that a
   // warp's loads of one row group stay within one page (separate planes
   // put each of a row's nd loads on its own page)

@@ -360,6 +360,10 @@ sk_status csr_finish(sk_matrix A, const int64_t* row_ptr, cudaStream_t st);
 
 // FP32 planes of the diagonal copy of an FP64 handle (no-op without one).
 sk_status build_dia_f32(sk_matrix A);
+// The sorted diagonal offsets c - r of a CSR handle whose pattern fits the
+// diagonal copy (at most kDiaMax diagonals, columns ascending in every row,
+// planes at most half empty); empty when it does not.
+sk_status dia_pattern(sk_matrix A, std::vector<int>* offsets);
 
 // BSR block-row partition of the product kernel (host row pointers) and
 // the sliced copy of 2x2 / 3x3 handles.

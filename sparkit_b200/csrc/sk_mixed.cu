@@ -642,6 +642,10 @@ sk_status sym_prepare_sell(sk_matrix A, cudaStream_t st) {
     }
   }
   off[static_cast<size_t>(nslices)] = static_cast<int>(total);
+  if (total > A->nnz + A->nnz / 4 + 64) {  // skewed rows: more than a quarter of padding
+    C.sym_sell_state = -1;
+    return SK_OK;
+  }
   void *col = nullptr, *val = nullptr, *len = nullptr;
   if ((s = dev_alloc(A, &col, (total + 64) * 4)) != SK_OK) return s;
   if ((s = dev_alloc(A, &val, (total + 64) * 4)) != SK_OK) return s;
@@ -661,12 +665,17 @@ sk_status sym_prepare_sell(sk_matrix A, cudaStream_t st) {
   return SK_OK;
 }
 
+// The scaled diagonal planes of the pattern's off-diagonal offsets (the
+// handle's own diagonal copy need not exist).
 sk_status sym_prepare_dia(sk_matrix A, cudaStream_t st) {
   auto& C = A->csr;
   const i64 n = A->nrow;
+  std::vector<int> offs;
+  sk_status s0 = dia_pattern(A, &offs);
+  if (s0 != SK_OK) return s0;
   SymOffsets o{};
-  for (int k = 0; k < C.dia_n; ++k)
-    if (C.dia_off[k] != 0) o.off[o.n++] = C.dia_off[k];
+  for (int k : offs)
+    if (k != 0) o.off[o.n++] = k;
   if (o.n == 0) {
     C.sym_dia_state = -1;
     return SK_OK;
@@ -690,38 +699,39 @@ sk_status sym_prepare_dia(sk_matrix A, cudaStream_t st) {
   return SK_OK;
 }
 
-// The diagonal copy when the handle has one with FP32 values, else SELL.
-bool use_dia(sk_matrix A) { return A->csr.dia_n > 0 && A->csr.dia_vals32; }
+// The layout the persistent solve reads: for the unscaled solve the
+// handle's diagonal copy when it has FP32 planes, else its SELL-32 copy;
+// for the scaled solve the scaled planes when the pattern has them, else
+// the scaled SELL-32 copy.
+bool use_dia(sk_matrix A, bool scaled) {
+  return scaled ? A->csr.sym_dia_state > 0 : A->csr.dia_n > 0 && A->csr.dia_vals32;
+}
 
 }  // namespace
 
 sk_status inner_sym_prepare(sk_matrix A, cudaStream_t st, bool* ok) {
   *ok = false;
   if (!A || A->format != SK_CSR || A->dtype != SK_F64 || A->nrow <= 0) return SK_OK;
-  const bool dia = use_dia(A);
-  if (!dia && !A->csr.sell) return SK_OK;
   sk_status s = sym_prepare_diag(A, st);
   if (s != SK_OK || A->csr.sym_diag_state < 0) return s;
-  if (dia) {
-    if (!A->csr.sym_dia_state && (s = sym_prepare_dia(A, st)) != SK_OK) return s;
-    *ok = A->csr.sym_dia_state > 0;
-  } else {
-    if (!A->csr.sym_sell_state && (s = sym_prepare_sell(A, st)) != SK_OK) return s;
-    *ok = A->csr.sym_sell_state > 0;
-  }
+  if (!A->csr.sym_dia_state && (s = sym_prepare_dia(A, st)) != SK_OK) return s;
+  if (A->csr.sym_dia_state < 0 && !A->csr.sym_sell_state && (s = sym_prepare_sell(A, st)) != SK_OK) return s;
+  *ok = A->csr.sym_dia_state > 0 || A->csr.sym_sell_state > 0;
   return SK_OK;
 }
 
 const double* inner_sym_isq(sk_matrix A) { return A->csr.sym_isq; }
 
-bool inner_persistent_ok(sk_matrix A) {
+bool inner_persistent_ok(sk_matrix A, bool scaled) {
   if (!A || A->format != SK_CSR || A->nrow <= 0) return false;
-  if (!use_dia(A) && !(A->csr.sell && A->csr.sell_vals32)) return false;
+  const auto& C = A->csr;
+  if (scaled ? !(C.sym_diag_state > 0 && (C.sym_dia_state > 0 || C.sym_sell_state > 0))
+             : !(use_dia(A, false) || (C.sell && C.sell_vals32)))
+    return false;
   if (A->nrow > INT_MAX / 4) return false;
   int coop = 0;
   if (cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, A->device) != cudaSuccess || !coop) return false;
-  const bool dia = use_dia(A);
-  return coop_grid(A, pick_kernel(dia, true)) > 0 && coop_grid(A, pick_kernel(dia, false)) > 0;
+  return coop_grid(A, pick_kernel(use_dia(A, scaled), scaled)) > 0;
 }
 
 size_t inner_persistent_scratch(sk_matrix A) {
@@ -731,14 +741,13 @@ size_t inner_persistent_scratch(sk_matrix A) {
 sk_status inner_cg_persistent(sk_matrix A, bool scaled, float* r, float* d, float* p, float* q, void* scratch,
                               double tol, long long max_iters, cudaStream_t st, InnerResult* out) {
   *out = InnerResult{};
-  SK_CHECK(inner_persistent_ok(A), SK_NOT_SUPPORTED,
-           "persistent inner solve needs a CSR handle with FP32 SELL values or an FP32 diagonal copy");
-  const bool dia = use_dia(A);
   const auto& C = A->csr;
   SK_CHECK(!scaled || C.sym_diag_state > 0, SK_NOT_SUPPORTED,
            "scaled inner solve: D^-1/2 A D^-1/2 is not formed (a diagonal entry is absent or not positive)");
-  SK_CHECK(!scaled || (dia ? C.sym_dia_state > 0 : C.sym_sell_state > 0), SK_NOT_SUPPORTED,
-           "scaled inner solve: the scaled copy is not built");
+  SK_CHECK(inner_persistent_ok(A, scaled), SK_NOT_SUPPORTED,
+           scaled ? "persistent scaled inner solve: the scaled copy is not built"
+                  : "persistent inner solve needs a CSR handle with FP32 SELL values or an FP32 diagonal copy");
+  const bool dia = use_dia(A, scaled);
   const void* k = pick_kernel(dia, scaled);
   int grid = coop_grid(A, k);
   SK_CHECK(grid > 0, SK_NOT_SUPPORTED, "persistent inner solve does not fit on the device");

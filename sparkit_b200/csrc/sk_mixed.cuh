@@ -12,16 +12,19 @@ struct InnerResult {
   double rnorm = 0;  // FP32 recursive residual norm at exit
 };
 
-// Whether the handle can run the persistent inner solve: a CSR handle with
-// its SELL-32 copy and FP32 values or its FP32 diagonal copy, and a device
-// that can co-schedule the grid (cooperative launch).
-bool inner_persistent_ok(sk_matrix A);
+// Whether the handle can run the persistent inner solve on a device that
+// can co-schedule the grid (cooperative launch).  Unscaled: a CSR handle
+// with its SELL-32 copy and FP32 values or its FP32 diagonal copy.
+// Scaled: after inner_sym_prepare succeeded.
+bool inner_persistent_ok(sk_matrix A, bool scaled);
 
 // Forms, once per handle, the symmetrically scaled FP32 copy S = D^-1/2 A
-// D^-1/2 (without its unit diagonal) in the layout the persistent solve
-// reads (the diagonal copy when the handle has one, else SELL-32), and
-// 1 / sqrt(a_ii).  *ok is false when S cannot be formed (an FP32 handle, a
-// diagonal entry absent or not positive, no SELL-32 or diagonal copy).
+// D^-1/2 (without its unit diagonal) and 1 / sqrt(a_ii).  S is stored as
+// diagonal planes when the pattern has at most 16 diagonals whose planes
+// are at most half empty (whether or not the handle keeps its own diagonal
+// copy), else as SELL-32 (rows of at most 255 off-diagonal entries, at
+// most a quarter of padding).  *ok is false when S cannot be formed (an
+// FP32 handle, a diagonal entry absent or not positive, neither layout).
 sk_status inner_sym_prepare(sk_matrix A, cudaStream_t st, bool* ok);
 
 // 1 / sqrt(a_ii) (FP64, n values) after inner_sym_prepare succeeded.

@@ -2085,14 +2085,16 @@ static sk_status mixed_cg_solve(sk_matrix A, bool jacobi, const double* b, doubl
   //   [ r32 | r64 | outer scalars, counters, reduction slots ]
   // The inner solve runs as one persistent launch (sk_mixed.cu) when the
   // handle allows it, else as one kernel per CG step (cg_solve<float>).
-  bool persistent = cfg->inner_kernel == 0 && inner_persistent_ok(A);
-  if (persistent && jacobi) {
+  bool persistent = false;
+  if (cfg->inner_kernel == 0 && jacobi) {
     // the persistent Jacobi inner solve runs on S = D^-1/2 A D^-1/2 (formed
     // once per handle); without it, the per-step inner solve is used
     bool sym_ok = false;
     sk_status s0 = inner_sym_prepare(A, st, &sym_ok);
     if (s0 != SK_OK) return s0;
-    persistent = sym_ok;
+    persistent = sym_ok && inner_persistent_ok(A, true);
+  } else if (cfg->inner_kernel == 0) {
+    persistent = inner_persistent_ok(A, false);
   }
   const double* isq = persistent && jacobi ? inner_sym_isq(A) : nullptr;
   out->inner_kernel = persistent ? 0 : 1;

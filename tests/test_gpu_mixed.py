@@ -72,9 +72,12 @@ def _far_coupled_laplacian(m, shift, eps=0.05, extra=0):
 @pytest.mark.parametrize("jacobi", [True, False])
 def test_persistent_inner_matches_per_step(gpu_lib, oracle, jacobi):
     """The persistent inner solve (one cooperative launch per outer step)
-    runs the per-step iteration; only the dot products' summation order
-    differs, so the FP32 iteration counts agree within 2% and both reach
-    the FP64 tolerance on the true residual."""
+    forms A p by the recurrence q = A r + beta q, one grid reduction fewer
+    per step than the per-step kernels.  With the symmetric Jacobi scaling
+    the FP32 counts agree within 2%; on the unscaled problem (coefficient
+    contrast e^(+-4 sigma)) the FP32 rounding of the two recurrences over
+    about 25 000 steps moves the count by up to a fifth.  Both reach the
+    FP64 tolerance on the true residual."""
     import torch
     A = matgen.diffusion_3d_grf(32, sigma=2.0, corr_len=4.0, seed=2)
     n = A.shape()[0]
@@ -92,8 +95,9 @@ def test_persistent_inner_matches_per_step(gpu_lib, oracle, jacobi):
         assert s.persistent == persistent
         res[persistent] = s
     a, p = res[False].inner_iterations, res[True].inner_iterations
-    assert abs(a - p) <= max(2, 0.02 * a), (a, p)
-    assert res[False].outer_iterations == res[True].outer_iterations
+    band = 0.02 if jacobi else 0.2
+    assert abs(a - p) <= max(2, band * a), (a, p)
+    assert abs(res[False].outer_iterations - res[True].outer_iterations) <= (0 if jacobi else 1)
 
 
 def test_persistent_inner_long_rows(gpu_lib, oracle):
@@ -148,7 +152,9 @@ def test_mixed_fgmres_reaches_fp64_tolerance(gpu_lib, oracle, pname):
     n = A.shape()[0]
     b = oracle.spmv(A, matgen.uniform_vector(n, seed=2))
     Ad = gpu.Device_matrix(A)
-    M = gpu.jacobi(Ad) if pname == "jacobi" else gpu.chebyshev_preconditioner(Ad, 0.2, 9.5, 8)
+    # (bounds 0.5..12, degree 4: the reference's FGMRES(30) converges in 60
+    # steps with them; with 0.2..9.5 it does not converge at all)
+    M = gpu.jacobi(Ad) if pname == "jacobi" else gpu.chebyshev_preconditioner(Ad, 0.5, 12.0, 4)
     bd = torch.from_numpy(b).cuda()
     xd = torch.zeros_like(bd)
     s = gpu.mixed_fgmres(bd, xd, gpu.Mixed_fgmres_config(1e-10, 1e-3, 30, 20, 3000, True), gpu.spmv(Ad), M)
