@@ -69,6 +69,8 @@ def parse():
                    help="each device format conversion once (for an ncu launch list)")
     p.add_argument("--profile-zipf", action="store_true",
                    help="three CSR FP64 products of matrix B (1M rows, Zipf(1.5) lengths), for ncu")
+    p.add_argument("--profile-zipf-panels", action="store_true",
+                   help="the --profile-zipf products on the handle's column-panel copy")
     p.add_argument("--profile-formats", action="store_true",
                    help="run one product of every sweep format and precision (for ncu captures), no timing")
     return p.parse_args()
@@ -263,8 +265,10 @@ def sweep(stream, grid):
             ms = time_device(lambda: Ad.spmv(xd, yd, stream=sptr), 300, 20, stream)
             # spmv_bytes is the byte model of the layout the product reads
             # (for the diagonal copy: its values and row masks, x and y)
-            out[f"lap3d_{fmt}_{tag}"] = {"gbs": Ad.info()["spmv_bytes"] / ms / 1e6, "us": ms * 1e3,
-                                         "bytes": Ad.info()["spmv_bytes"]}
+            info = Ad.info()
+            out[f"lap3d_{fmt}_{tag}"] = {"gbs": info["spmv_bytes"] / ms / 1e6, "us": ms * 1e3,
+                                         "bytes": info["spmv_bytes"], "layout": Ad.layout(),
+                                         "device_bytes": info["device_bytes"]}
             Ad.close()
     del A
     B = matgen.vector_laplacian_3d_bsr(grid, seed=1)
@@ -281,12 +285,29 @@ def sweep(stream, grid):
     # the stored entries only), FP64 and FP32
     Z = matgen.zipf_random(1_000_000, s=1.5, cap=2048, seed=0)
     for tag, dt in (("f64", np.float64), ("f32", np.float32)):
+        t0 = time.perf_counter()
         Zd = gpu.Device_matrix(Z, dtype=dt)
+        upload_s = time.perf_counter() - t0
         xz = torch.from_numpy(matgen.uniform_vector(Z.shape()[0], seed=3, dtype=dt)).cuda()
         yz = torch.empty_like(xz)
         ms = time_device(lambda: Zd.spmv(xz, yz, stream=sptr), 200, 20, stream)
-        out[f"zipf_csr_{tag}"] = {"gbs": Zd.info()["spmv_bytes"] / ms / 1e6, "us": ms * 1e3, "nnz": Z.size(),
-                                  "mean_row": Z.size() / Z.shape()[0]}
+        info = Zd.info()
+        csr_bytes = (8 if dt == np.float64 else 4) * Z.size() + 4 * Z.size() + 4 * (Z.shape()[0] + 1)
+        out[f"zipf_csr_{tag}"] = {"gbs": info["spmv_bytes"] / ms / 1e6, "us": ms * 1e3, "nnz": Z.size(),
+                                  "mean_row": Z.size() / Z.shape()[0], "layout": Zd.layout(),
+                                  "upload_s": upload_s, "device_bytes": info["device_bytes"],
+                                  "device_bytes_over_csr": info["device_bytes"] / csr_bytes}
+        # the opt-in column-panel copy: every row summed in the reference's
+        # order (bit-identical products), at its own speed
+        t0 = time.perf_counter()
+        built = Zd.add_panels()
+        panel_s = time.perf_counter() - t0
+        if built:
+            ms = time_device(lambda: Zd.spmv(xz, yz, stream=sptr), 200, 20, stream)
+            info = Zd.info()
+            out[f"zipf_csr_panels_{tag}"] = {"gbs": info["spmv_bytes"] / ms / 1e6, "us": ms * 1e3,
+                                             "layout": Zd.layout(), "build_s": panel_s,
+                                             "device_bytes": info["device_bytes"]}
         for fmt, conv in (("jad", gpu.to_jagged_diagonal), ("ell", gpu.to_ellpack)):
             H = conv(Zd)
             ms = time_device(lambda: H.spmv(xz, yz, stream=sptr), 40, 5, stream)
@@ -985,15 +1006,18 @@ def profile_gmres(grid=1024, iters=40):
     return 0
 
 
-def profile_zipf():
+def profile_zipf(panels=False):
     """Three CSR FP64 products of matrix B (the split product of skewed
-    rows), for an ncu capture of one launch."""
+    rows, or with `panels` the column-panel copy), for an ncu capture of one
+    launch."""
     import torch
 
     from sparkit_b200 import gpu, matgen
     torch.cuda.set_device(0)
     Z = matgen.zipf_random(1_000_000, s=1.5, cap=2048, seed=0)
     Zd = gpu.Device_matrix(Z)
+    if panels:
+        assert Zd.add_panels()
     xz = torch.from_numpy(matgen.uniform_vector(Z.shape()[0], seed=3)).cuda()
     yz = torch.empty_like(xz)
     for _ in range(3):
@@ -1027,8 +1051,8 @@ def main():
         return run_reference(args)
     if args.profile_formats:
         return profile_formats(args.grid)
-    if args.profile_zipf:
-        return profile_zipf()
+    if args.profile_zipf or args.profile_zipf_panels:
+        return profile_zipf(panels=args.profile_zipf_panels)
     if args.profile_convert:
         return profile_convert(args.grid)
     if args.profile_eigen:

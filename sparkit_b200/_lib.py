@@ -134,8 +134,10 @@ SIGNATURES = [
     ("sk_matrix_market_write", [c_vp, ctypes.c_char_p, c_i32, c_i32]),
     ("sk_matrix_destroy", [c_vp]),
     ("sk_matrix_info", [c_vp, P_i64]),
+    ("sk_matrix_layout", [c_vp, ctypes.POINTER(ctypes.c_int32)]),
     ("sk_matrix_add_f32_values", [c_vp]),
     ("sk_matrix_add_diagonals", [c_vp, ctypes.POINTER(ctypes.c_int)]),
+    ("sk_matrix_add_panels", [c_vp, ctypes.POINTER(ctypes.c_int)]),
     ("sk_spmv", [c_vp, c_vp, c_vp, c_vp]),
     ("sk_spmv_f32", [c_vp, c_vp, c_vp, c_vp]),
     ("sk_spmv_host", [c_vp, c_vp, c_vp]),

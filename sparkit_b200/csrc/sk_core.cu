@@ -735,6 +735,22 @@ sk_status sk_matrix_info(sk_matrix A, int64_t info[8]) {
   return SK_OK;
 }
 
+sk_status sk_matrix_layout(sk_matrix A, int32_t* layout) {
+  SK_CHECK(A && layout, SK_INVALID_ARG, "null handle or layout");
+  *layout = SK_LAYOUT_NATIVE;
+  if (A->format == SK_CSR) {
+    const auto& C = A->csr;
+    *layout = C.dia_n ? SK_LAYOUT_DIAGONALS
+              : C.sell ? SK_LAYOUT_SELL
+              : C.panel ? SK_LAYOUT_PANELS
+              : C.hyb ? SK_LAYOUT_SPLIT
+                      : SK_LAYOUT_NATIVE;
+  } else if (A->format == SK_BSR && A->bsr.sell) {
+    *layout = SK_LAYOUT_SELL;
+  }
+  return SK_OK;
+}
+
 sk_status sk_matrix_add_f32_values(sk_matrix A) {
   SK_CHECK(A, SK_INVALID_ARG, "null handle");
   SK_CHECK(A->format == SK_CSR, SK_NOT_SUPPORTED, "FP32 value copy is for CSR handles");

@@ -26,6 +26,10 @@ constexpr int kBsrTileVals = 4096;  // BSR: block values staged per CTA
 constexpr int kMaxRed = 4;       // fused reductions carried per kernel
 constexpr int kSellMaxRow = 64;  // CSR rows up to this length use SELL-32
 constexpr int kDiaMax = 16;      // diagonals of the diagonal copy of a CSR handle
+constexpr int kPanelSmem = 220 * 1024;  // dynamic shared memory of a column-panel CTA (at most)
+constexpr int kPanelStages = 3;           // chunk stages in flight per column-panel CTA
+constexpr int kPanelChunkEntries = 1536;  // entries per chunk (a multiple of 8)
+constexpr int kPanelChunkSlices = 48;     // slices (or slice pieces) per chunk
 constexpr int kHybLong = 32;     // rows longer than this take a warp in the split product
 
 // ------------------------------------------------------------------
@@ -106,6 +110,39 @@ struct Csr {
   int* hyb_long = nullptr;
   int hyb_nshort = 0, hyb_nlong = 0;
   double hyb_long_frac = 0.0;
+  // Column-panel copy (sk_matrix_add_panels, sk_panel.cu): every row summed
+  // in the reference's order whatever its length.  The rows are cut into pn_blocks
+  // row blocks of about equal entries, one CTA each; the columns into
+  // pn_panels panels of pn_width columns.  A CTA walks the panels in
+  // order, holding panel k of x in shared memory (double-buffered) and a
+  // running sum per row of its block, so that a row's entries are still
+  // added one after another in ascending column order from 0 (the bits of
+  // sparse_blas.hpp:25-28) while every gather of x reads shared memory.
+  // The entries of block b in panel k form segments (one per row that has
+  // entries there), sorted by decreasing length and packed 32 to a slice,
+  // a lane each.  Slot j of a slice holds entry j of the lanes whose
+  // segment is longer than j (lanes 0 .. c_j - 1), right after slot j - 1,
+  // without padding.  A panel's slices are cut into chunks of at most
+  // kPanelChunkEntries entries and kPanelChunkSlices slices (at least one
+  // chunk per panel, possibly empty); a slice with more entries than that
+  // is cut by slots into pieces that go to successive chunks.  A chunk is copied whole into a shared-memory stage by
+  // the bulk-copy engine: its values and 16-bit column offsets (from a
+  // multiple of 8 entries) and its table (pn_meta: the pieces' entry
+  // offsets, padded to 4 words, then 32 segment words per piece, local row
+  // | length << 16, 0 for none).  pn_chunk[c] = {first entry, entries
+  // rounded up to 8, first meta word, meta words}; pn_chunk_kn[c] = panel
+  // | pieces << 16.
+  bool panel = false;
+  int pn_blocks = 0, pn_panels = 0, pn_width = 0, pn_smem = 0, pn_stage_bytes = 0;
+  int* pn_row0 = nullptr;        // pn_blocks + 1 first rows
+  int* pn_chunk_ptr = nullptr;   // pn_blocks + 1 first chunks
+  int4* pn_chunk = nullptr;
+  int* pn_chunk_kn = nullptr;
+  unsigned* pn_meta = nullptr;
+  unsigned short* pn_col = nullptr;
+  void* pn_vals = nullptr;
+  int* pn_err = nullptr;         // set by a stage wait that ran out
+  i64 pn_entries = 0;            // stored entries, chunk starts rounded up to 8
   // Diagonal copy (sk_matrix_add_diagonals) of a handle whose entries lie
   // on at most kDiaMax diagonals c - r = off[d] and whose rows hold their
   // columns in ascending order, slice-major like the SELL-32 copy: A(r, r +
@@ -360,6 +397,9 @@ sk_status csr_finish(sk_matrix A, const int64_t* row_ptr, cudaStream_t st);
 
 // FP32 planes of the diagonal copy of an FP64 handle (no-op without one).
 sk_status build_dia_f32(sk_matrix A);
+// The column-panel copy of a CSR handle (host row pointers); a no-op when
+// the handle does not qualify (sk_matrix_add_panels).
+sk_status build_panel(sk_matrix A, const int64_t* rp, cudaStream_t st);
 // The sorted diagonal offsets c - r of a CSR handle whose pattern fits the
 // diagonal copy (at most kDiaMax diagonals, columns ascending in every row,
 // planes at most half empty); empty when it does not.

@@ -56,10 +56,10 @@ __device__ __forceinline__ void warp_reduce(double (&v)[NR]) {
     for (int j = 0; j < NR; ++j) v[j] += __shfl_xor_sync(0xffffffffu, v[j], off);
 }
 
-// Result valid in thread 0.  Requires blockDim.x == kThreads.
+// Result valid in thread 0.  Any whole number of warps up to 1024 threads.
 template <int NR>
 __device__ __forceinline__ void block_reduce(double (&v)[NR]) {
-  __shared__ double red_smem[kThreads / 32][NR > 0 ? NR : 1];
+  __shared__ double red_smem[32][NR > 0 ? NR : 1];
   warp_reduce<NR>(v);
   int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   __syncthreads();
@@ -69,7 +69,7 @@ __device__ __forceinline__ void block_reduce(double (&v)[NR]) {
   __syncthreads();
   if (warp == 0) {
 #pragma unroll
-    for (int j = 0; j < NR; ++j) v[j] = lane < kThreads / 32 ? red_smem[lane][j] : 0.0;
+    for (int j = 0; j < NR; ++j) v[j] = lane < static_cast<int>(blockDim.x >> 5) ? red_smem[lane][j] : 0.0;
     warp_reduce<NR>(v);
   }
 }
@@ -468,6 +468,244 @@ hyb_spmv_kernel(const int* __restrict__ rp, const int* __restrict__ ci, const T*
 }
 
 // ------------------------------------------------------------------
+// CSR through its column-panel copy (sk_panel.cu): CTA b owns rows
+// row0[b] .. row0[b+1]-1 with a running sum each in shared memory, and
+// walks the column panels in order, panel k of x in one half of a double
+// buffer (cp.async) while panel k + 1 fills the other.  The matrix stream
+// arrives in chunks (a panel's entries for this block, cut to fit a
+// stage): thread 0 keeps kPanelStages chunks in flight, each moved by
+// three bulk copies (values, column offsets, slice table) that complete
+// on the stage's mbarrier, so the warps read nothing but shared memory.  A
+// warp takes a slice (or a piece of one) of up to 32 row segments
+// (lengths non-increasing over the lanes); each lane adds its entries to
+// its row's sum one after another.  Slot j
+// of a piece holds the entries j of lanes 0 .. c_j - 1 (c_j from a
+// ballot), stored after slot j - 1.  A row has at most one segment per
+// panel (the later pieces of a slice in later chunks), and the CTA
+// synchronizes between chunks, so no two lanes touch the same sum at once
+// and every row is summed in ascending column order.  Stage waits are bounded in time; a wait that
+// runs out sets *err and the CTA skips the remaining work.
+// ------------------------------------------------------------------
+constexpr int kPanelThreads = 1024;
+
+struct PanelArgs {
+  const int* row0;
+  const int* chunk_ptr;
+  const int4* chunk;
+  const int* chunk_kn;
+  const unsigned* meta;
+  const unsigned short* col;
+  int panels, width, ncol, run_bytes, stage_bytes;
+  int x16;  // x is 16-byte aligned
+  int* err;
+  unsigned long long wait_ns;
+};
+
+inline PanelArgs panel_args(const sk_matrix_s* A, const void* x) {
+  const auto& C = A->csr;
+  PanelArgs g{};
+  g.row0 = C.pn_row0;
+  g.chunk_ptr = C.pn_chunk_ptr;
+  g.chunk = C.pn_chunk;
+  g.chunk_kn = C.pn_chunk_kn;
+  g.meta = C.pn_meta;
+  g.col = C.pn_col;
+  g.panels = C.pn_panels;
+  g.width = C.pn_width;
+  g.ncol = static_cast<int>(A->ncol);
+  g.stage_bytes = C.pn_stage_bytes;
+  g.run_bytes = C.pn_smem - 2 * C.pn_width * static_cast<int>(A->dtype == SK_F64 ? 8 : 4) -
+                kPanelStages * C.pn_stage_bytes;
+  g.x16 = (reinterpret_cast<uintptr_t>(x) & 15) == 0;
+  g.err = C.pn_err;
+  g.wait_ns = wait_limit_ns();
+  return g;
+}
+
+template <typename T>
+__device__ __forceinline__ void panel_stage(T* dst, const T* __restrict__ x, int c0, int cnt, bool x16) {
+  constexpr int E = 16 / static_cast<int>(sizeof(T));
+  int done = 0;
+  if (x16) {
+    const int n16 = cnt / E;
+    for (int i = threadIdx.x; i < n16; i += blockDim.x) cp_async16(dst + i * E, x + c0 + i * E);
+    done = n16 * E;
+  }
+  for (int i = done + threadIdx.x; i < cnt; i += blockDim.x) cp_async_elem(dst + i, x + c0 + i);
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+
+__device__ __forceinline__ unsigned pn_smem_addr(const void* p) {
+  return static_cast<unsigned>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void pn_bulk(void* dst, const void* src, unsigned bytes, unsigned long long* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+                   pn_smem_addr(dst)),
+               "l"(src), "r"(bytes), "r"(pn_smem_addr(bar))
+               : "memory");
+}
+__device__ __forceinline__ void pn_l2_prefetch(const void* p, unsigned bytes) {
+  if (bytes) asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;\n" ::"l"(p), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool pn_try_wait(unsigned long long* bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(pn_smem_addr(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Bounded wait for a stage: false once wait_ns have passed.
+__device__ __forceinline__ bool pn_wait(unsigned long long* bar, unsigned parity, unsigned long long wait_ns) {
+  unsigned long long t0 = 0;
+  for (unsigned it = 0;; ++it) {
+    if (pn_try_wait(bar, parity)) return true;
+    if ((it & 255u) == 255u) {
+      unsigned long long t;
+      asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+      if (t0 == 0) {
+        t0 = t;
+      } else if (t - t0 > wait_ns) {
+        return false;
+      }
+    }
+  }
+}
+
+template <typename T, class Epi>
+__global__ void __launch_bounds__(kPanelThreads, 1)
+panel_spmv_kernel(PanelArgs g, const T* __restrict__ va, const T* __restrict__ x, Epi epi, RedWs ws,
+                  const Scalars* sc) {
+  constexpr int NR = Epi::kNR;
+  constexpr int SC = kPanelChunkEntries;
+  constexpr unsigned V = sizeof(T);
+  if (solve_done(sc)) return;
+  extern __shared__ __align__(16) unsigned char panel_smem[];
+  __shared__ __align__(8) unsigned long long bars[kPanelStages];
+  __shared__ int s_fail;
+  T* run = reinterpret_cast<T*>(panel_smem);
+  T* xs = reinterpret_cast<T*>(panel_smem + g.run_bytes);
+  unsigned char* stages = panel_smem + g.run_bytes + 2 * g.width * V;
+  double red[NR > 0 ? NR : 1];
+#pragma unroll
+  for (int j = 0; j < (NR > 0 ? NR : 1); ++j) red[j] = 0.0;
+  const int b = blockIdx.x, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int nwarps = blockDim.x >> 5;
+  const int r0 = __ldg(g.row0 + b), nr = __ldg(g.row0 + b + 1) - r0;
+  const int c0 = __ldg(g.chunk_ptr + b), nch = __ldg(g.chunk_ptr + b + 1) - c0;
+  for (int i = threadIdx.x; i < nr; i += blockDim.x) run[i] = T(0);
+  if (threadIdx.x == 0) {
+    s_fail = 0;
+    for (int j = 0; j < kPanelStages; ++j)
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(pn_smem_addr(&bars[j])));
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  // chunk i into stage i % kPanelStages (thread 0)
+  auto issue = [&](int i) {
+    const int4 ch = __ldg(g.chunk + c0 + i);
+    unsigned long long* bar = &bars[i % kPanelStages];
+    unsigned char* st = stages + (i % kPanelStages) * g.stage_bytes;
+    const unsigned bytes = static_cast<unsigned>(ch.y) * (V + 2u) + static_cast<unsigned>(ch.w) * 4u;
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(pn_smem_addr(bar)), "r"(bytes)
+                 : "memory");
+    if (ch.y) {
+      pn_bulk(st, va + ch.x, static_cast<unsigned>(ch.y) * V, bar);
+      pn_bulk(st + SC * V, g.col + ch.x, static_cast<unsigned>(ch.y) * 2u, bar);
+    }
+    if (ch.w) pn_bulk(st + SC * (V + 2u), g.meta + ch.z, static_cast<unsigned>(ch.w) * 4u, bar);
+    if (i + kPanelStages < nch) {  // the chunk after the stages in flight: into L2
+      const int4 cn = __ldg(g.chunk + c0 + i + kPanelStages);
+      pn_l2_prefetch(va + cn.x, static_cast<unsigned>(cn.y) * V);
+      pn_l2_prefetch(g.col + cn.x, static_cast<unsigned>(cn.y) * 2u);
+    }
+  };
+  if (threadIdx.x == 0)
+    for (int i = 0; i < nch && i < kPanelStages; ++i) issue(i);
+  panel_stage(xs, x, 0, min(g.width, g.ncol), g.x16 != 0);
+  if (g.panels > 1) panel_stage(xs + g.width, x, g.width, min(g.width, g.ncol - g.width), g.x16 != 0);
+  bool ok = true;
+  int kprev = -1;
+  for (int i = 0; i < nch; ++i) {
+    const int kn = __ldg(g.chunk_kn + c0 + i);
+    const int k = kn & 0xffff, ns = kn >> 16;
+    if (k != kprev) {
+      if (k + 1 < g.panels) {
+        asm volatile("cp.async.wait_group 1;\n" ::: "memory");
+      } else {
+        asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+      }
+      __syncthreads();  // panel k of x visible; the sums of panel k - 1 written
+      kprev = k;
+    }
+    if (ok && !pn_wait(&bars[i % kPanelStages], (i / kPanelStages) & 1, g.wait_ns)) {
+      ok = false;
+      atomicExch(g.err, 1);
+    }
+    if (ok) {
+      const unsigned char* st = stages + (i % kPanelStages) * g.stage_bytes;
+      const T* sv = reinterpret_cast<const T*>(st);
+      const unsigned short* scl = reinterpret_cast<const unsigned short*>(st + SC * V);
+      const unsigned* rel = reinterpret_cast<const unsigned*>(st + SC * (V + 2u));
+      const unsigned* segw = rel + ((ns + 3) & ~3);
+      const T* xp = xs + (k & 1) * g.width;
+      for (int t = warp; t < ns; t += nwarps) {
+        const unsigned w = segw[t * 32 + lane];
+        const int len = static_cast<int>(w >> 16), row = static_cast<int>(w & 0xffffu);
+        const int base = static_cast<int>(rel[t]);
+        const int maxlen = __shfl_sync(0xffffffffu, len, 0);  // lane 0 holds the longest segment
+        T acc = len > 0 ? run[row] : T(0);
+        int off = 0;
+        for (int j = 0; j < maxlen; j += 4) {
+          unsigned short c[4];
+          T v[4];
+#pragma unroll
+          for (int u = 0; u < 4; ++u) {
+            const unsigned m = __ballot_sync(0xffffffffu, len > j + u);
+            if (len > j + u) {
+              const int e = base + off + lane;
+              c[u] = scl[e];
+              v[u] = sv[e];
+            }
+            off += __popc(m);
+          }
+#pragma unroll
+          for (int u = 0; u < 4; ++u)
+            if (len > j + u) acc = add(acc, mul(v[u], xp[c[u]]));
+        }
+        if (len > 0) run[row] = acc;
+      }
+    }
+    __syncthreads();  // stage i is free; after a panel's last chunk, its x buffer too
+    if (threadIdx.x == 0 && i + kPanelStages < nch) issue(i + kPanelStages);
+    const bool last = i + 1 == nch || (__ldg(g.chunk_kn + c0 + i + 1) & 0xffff) != k;
+    if (last && k + 2 < g.panels) {
+      const int c2 = (k + 2) * g.width;
+      panel_stage(xs + (k & 1) * g.width, x, c2, min(g.width, g.ncol - c2), g.x16 != 0);
+    }
+  }
+  asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+  if (!ok) s_fail = 1;
+  __syncthreads();
+  if (s_fail) {
+    // copies still in flight land before the CTA leaves (bounded)
+    if (threadIdx.x == 0)
+      for (int i = nch - kPanelStages < 0 ? 0 : nch - kPanelStages; i < nch; ++i)
+        pn_wait(&bars[i % kPanelStages], (i / kPanelStages) & 1, g.wait_ns);
+    __syncthreads();
+    return;
+  }
+  for (int i = threadIdx.x; i < nr; i += blockDim.x)
+    reduce_terms<NR>(ws, r0 + i, red, [&](double* rr) { epi(r0 + i, run[i], rr); });
+  if constexpr (NR > 0) {
+    grid_reduce<NR>(red, ws, [&](const double* t) { epi.finalize(t); });
+  }
+}
+
+// ------------------------------------------------------------------
 // CSR through its diagonal copy: one thread per row.  Diagonal d of a
 // warp's 32 rows is one contiguous 32-value segment of the slice-major copy
 // (a slice's segments are adjacent), and x[i + off[d]] is contiguous too,
@@ -739,7 +977,9 @@ bsr_sell_kernel(int nrow, int ncol, int nbr, int nbr_trunc, const int* __restric
 // Grid size of the SpMV launch for a handle (for sizing RedWs).
 inline int spmv_grid(const sk_matrix_s* A) {
   switch (A->format) {
-    case SK_CSR: return A->csr.sell || A->csr.dia_n ? ceil_div(A->nrow, kThreads) : A->csr.nparts;
+    case SK_CSR:
+      return A->csr.sell || A->csr.dia_n ? ceil_div(A->nrow, kThreads)
+                                         : (A->csr.nparts > A->csr.pn_blocks ? A->csr.nparts : A->csr.pn_blocks);
     case SK_BSR: return A->bsr.sell ? ceil_div(A->bsr.nbr, kThreads) : A->bsr.nparts;
     default: return ceil_div(A->nrow, kThreads);
   }
@@ -796,6 +1036,19 @@ void launch_spmv(const sk_matrix_s* A, const T* x, Epi const& epi, RedWs ws,
                   row_grid<Epi>(A, A->nrow, SpmvTune<T, Epi>::kSellMinB), kThreads, 0, st,
                   static_cast<int>(A->nrow), A->csr.sell_off, A->csr.sell_len, A->csr.sell_col, v, x,
                   epi, ws, sc);
+        break;
+      }
+      if (A->csr.panel && !vals_override) {
+        static const bool attr_set = [] {
+          return cudaFuncSetAttribute(panel_spmv_kernel<T, Epi>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      kPanelSmem) == cudaSuccess;
+        }();
+        if (!attr_set) {
+          set_error("panel product: shared-memory attribute refused");
+          break;
+        }
+        SK_LAUNCH((panel_spmv_kernel<T, Epi>), A->csr.pn_blocks, kPanelThreads, A->csr.pn_smem, st,
+                  panel_args(A, x), static_cast<const T*>(A->csr.pn_vals), x, epi, ws, sc);
         break;
       }
       const T* v = vals_override ? vals_override : static_cast<const T*>(A->csr.vals);

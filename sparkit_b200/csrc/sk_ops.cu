@@ -207,7 +207,7 @@ static sk_status plan_host_pipe(sk_matrix A) {
   int want = static_cast<int>(std::min<i64>(kPipeMaxChunks, (n * static_cast<i64>(V)) / kPipeChunkBytes));
   // (the split product of skewed rows reads x everywhere from its first
   // rows on, so it runs whole)
-  if (A->format != SK_CSR || A->nnz == 0 || A->ncol == 0 || want < 2 || A->csr.hyb) {
+  if (A->format != SK_CSR || A->nnz == 0 || A->ncol == 0 || want < 2 || A->csr.hyb || A->csr.panel) {
     p->chunks = 1;
     A->pipe = guard.release();
     return SK_OK;

@@ -180,6 +180,15 @@ class Device_matrix:
         keys = ("format", "dtype", "nrow", "ncol", "nnz", "width", "device_bytes", "spmv_bytes")
         return dict(zip(keys, list(arr)))
 
+    LAYOUTS = ("native", "sell", "diagonals", "split", "panels")
+
+    def layout(self):
+        """The device layout the product runs on (sk_matrix_layout): one of
+        LAYOUTS."""
+        v = ctypes.c_int32(0)
+        check(lib().sk_matrix_layout(self.handle, ctypes.byref(v)))
+        return self.LAYOUTS[v.value]
+
     def build_ms(self):
         """Device time of the kernels that built this handle on the device
         (sk_matrix_build_ms); 0.0 for a handle uploaded from the host."""
@@ -189,6 +198,15 @@ class Device_matrix:
 
     def add_f32_values(self):
         check(lib().sk_matrix_add_f32_values(self.handle))
+
+    def add_panels(self):
+        """Adds the column-panel copy of a CSR handle whose rows are too long
+        for SELL-32, so that every product sums each row in the reference's
+        order (sk_matrix_add_panels); False when the handle does not qualify
+        (the handle is then unchanged)."""
+        built = ctypes.c_int(0)
+        check(lib().sk_matrix_add_panels(self.handle, ctypes.byref(built)))
+        return bool(built.value)
 
     def add_diagonals(self):
         """Adds the diagonal copy of a stencil-pattern CSR handle; False when

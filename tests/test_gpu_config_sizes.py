@@ -86,10 +86,16 @@ def test_config4_plain_fgmres_512sq_history(gpu_lib, oracle):
 
 
 def test_config2_matrix_b_full_csr_product(gpu_lib, oracle):
+    """The full matrix B (1M rows, Zipf(1.5) lengths up to 2048, 68.9M
+    entries).  The default split product sums rows of up to 32 entries in
+    the reference's order (bit for bit) and longer rows in a fixed tree
+    (normwise 1e-14); with the column-panel copy every row is summed in the
+    reference's order and the product equals the oracle's bit for bit."""
     Z = matgen.zipf_random(1_000_000, s=1.5, cap=2048, seed=0)
     n = Z.shape()[0]
     x = matgen.uniform_vector(n, seed=1)
     Zd = gpu.Device_matrix(Z)
+    assert Zd.layout() == "split"
     y = gpu.multiply(Zd, x)
     yr = oracle.spmv(Z, x)
     rows = np.repeat(np.arange(n), np.diff(np.asarray(Z.row_ptr())))
@@ -97,9 +103,10 @@ def test_config2_matrix_b_full_csr_product(gpu_lib, oracle):
     np.add.at(scale, rows, np.abs(np.asarray(Z.values())) * np.abs(x[np.asarray(Z.col_ind())]))
     err = np.max(np.abs(y - yr)) / np.max(scale)
     assert err <= 1e-14, err
-    # rows of at most 32 entries are summed in the reference's order
     short = np.diff(np.asarray(Z.row_ptr())) <= 32
     assert np.array_equal(y[short], yr[short])
+    assert Zd.add_panels() and Zd.layout() == "panels"
+    assert np.array_equal(gpu.multiply(Zd, x), yr)
 
 
 def test_config5_batch_with_64k_systems(gpu_lib, oracle):

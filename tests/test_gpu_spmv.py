@@ -190,3 +190,43 @@ def test_small_case_sweep_writes_every_row(gpu_lib, oracle, fmt):
             assert normwise_err(A, x, y, y_ref) <= 1e-14, (fmt, n)
         else:
             assert np.array_equal(y, y_ref), (fmt, n)
+
+
+@pytest.mark.parametrize("dtype,n", [(np.float64, 300_000), (np.float32, 600_000)])
+def test_panel_product_bit_identical(gpu_lib, oracle, dtype, n):
+    """The column-panel copy (sk_matrix_add_panels) of a large skewed matrix
+    (Zipf(1.5) row lengths up to 2048, uniform columns over an x of 2.4 MB)
+    sums every row in ascending column order from 0, panel after panel: the
+    oracle's bits for rows of every length.  x once 16-byte aligned (16-byte staging
+    copies) and once at an 8- or 4-byte offset (element copies)."""
+    import torch
+    Z = matgen.zipf_random(n, s=1.5, cap=2048, seed=5, dtype=dtype)
+    Zd = gpu.Device_matrix(Z)
+    assert Zd.layout() == "split"
+    assert Zd.add_panels() and Zd.layout() == "panels"
+    x = matgen.uniform_vector(n, seed=6, dtype=dtype)
+    yr = oracle.spmv(Z, x)
+    tdt = torch.float64 if dtype == np.float64 else torch.float32
+    for shift in (0, 1):
+        buf = torch.empty(n + 1, dtype=tdt, device="cuda")
+        xd = buf[shift:shift + n]
+        xd.copy_(torch.from_numpy(x))
+        yd = torch.full((n,), float("nan"), dtype=tdt, device="cuda")
+        Zd.spmv(xd, yd)
+        torch.cuda.synchronize()
+        assert np.array_equal(yd.cpu().numpy(), yr), shift
+
+
+def test_panel_copy_only_where_the_order_is_not_kept(gpu_lib, oracle):
+    """A SELL-32 handle already sums each row in storage order, so the panel
+    copy is refused; a small skewed handle takes it and then matches the
+    oracle bit for bit (one panel, a handful of row blocks)."""
+    A = matgen.laplacian_2d_dirichlet(64)
+    Ad = gpu.Device_matrix(A)
+    assert Ad.layout() == "sell" and not Ad.add_panels() and Ad.layout() == "sell"
+    Z = matgen.zipf_random(20_000, s=1.5, cap=2048, seed=1)
+    Zd = gpu.Device_matrix(Z)
+    assert Zd.layout() in ("split", "native")
+    assert Zd.add_panels() and Zd.layout() == "panels"
+    x = matgen.uniform_vector(Z.shape()[0], seed=2)
+    assert np.array_equal(gpu.multiply(Zd, x), oracle.spmv(Z, x))
