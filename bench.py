@@ -1028,7 +1028,8 @@ def profile_zipf(panels=False):
 
 def profile_solvers(grid):
     """A short plain FP64 Jacobi-CG (20 iterations) and a short mixed solve
-    (one outer step of 20 FP32 iterations) for per-kernel launch lists."""
+    (one outer step of 20 FP32 iterations with one kernel per step, the
+    FP32 counterpart of the FP64 kernels) for per-kernel launch lists."""
     import torch
 
     from sparkit_b200 import gpu, matgen
@@ -1040,7 +1041,7 @@ def profile_solvers(grid):
     xd = torch.zeros_like(bd)
     gpu.conjugate_gradient(bd, xd, gpu.CGConfig(1e-10, 10 ** 6, 20), gpu.spmv(Gd), gpu.jacobi(Gd))
     xd.zero_()
-    gpu.mixed_cg(bd, xd, gpu.Mixed_config(1e-10, 1e-5, 1, 20), gpu.spmv(Gd))
+    gpu.mixed_cg(bd, xd, gpu.Mixed_config(1e-10, 1e-5, 1, 20, persistent=False), gpu.spmv(Gd))
     torch.cuda.synchronize()
     return 0
 
