@@ -715,9 +715,10 @@ def learned_runs(train_grid=128, instances=200, cycles=100, eval_grids=(128, 512
     Peclet log-uniform in [1, 100]); the network is trained on the GPU by
     the library's own kernels.  Then FGMRES(30) to a 1e-8 relative residual
     on held-out instances: single-level Jacobi, Chebyshev(8) (bounds from a
-    power iteration) and the learned preconditioner; at 512^2 also the
-    two-level forms (aggregation coarse correction) with Jacobi and with the
-    network as the smoother.  Times are wall times of the solve call with
+    power iteration) and the learned preconditioner; and the two-level forms
+    (aggregation coarse correction, 8 x 8 cells per aggregate) with Jacobi
+    and with a second network, trained on coarse-corrected pairs, as the
+    smoother after the coarse correction.  Times are wall times of the solve call with
     inputs on the device; a solve that does not converge within its cap
     reports its cap time and converged = false."""
     import torch
@@ -745,6 +746,13 @@ def learned_runs(train_grid=128, instances=200, cycles=100, eval_grids=(128, 512
     out["train"] = {"steps": 2000, "batch": 8, "ms": ts.ms, "loss_first20": float(h[:20].mean()),
                     "loss_last50": float(h[-50:].mean())}
     pairs.close()
+    # The network as the smoother of the two-level form sees coarse-corrected
+    # residuals only: a second network is trained on pairs (r - A c, e - c)
+    # with c = P Ac^-1 P^T r the coarse correction (aggregates of 8 x 8
+    # cells), r and e taken after each restart cycle of FGMRES(30) runs on
+    # further 128^2 instances; held-out pairs (10 instances) give its loss.
+    net2, out["smoother_train"] = gpu.train_coarse_corrected_smoother(m, instances=200, held=10, cycles=40,
+                                                                      steps=8000)
 
     def mixed_vs_plain(M, Ad, A, b, reps=3):
         """FGMRES(30) to a 1e-10 true residual with M: plain FP64 against FP32
@@ -808,12 +816,19 @@ def learned_runs(train_grid=128, instances=200, cycles=100, eval_grids=(128, 512
              "chebyshev8": run(gpu.chebyshev_preconditioner(Ad, lmax * 1e-2, lmax, 8), Ad, A, b,
                                2500 if big else 1500),
              "learned": run(L, Ad, A, b, 3000)}
+        agg = 8  # aggregates of 8 x 8 cells: a 16^2 coarse grid at 128^2, 64^2 at 512^2
+        r["twolevel_jacobi"] = run(gpu.twolevel(Ad, J, g, g, agg), Ad, A, b, 3000)
+        L2 = gpu.learned_preconditioner(Ad, net2, g, g)
+        r["twolevel_learned_smoother"] = run(gpu.twolevel(Ad, L2, g, g, agg, coarse_first=True), Ad, A, b, 3000)
+        tj, tl = r["twolevel_jacobi"], r["twolevel_learned_smoother"]
+        if tj["converged"] and tl["converged"]:
+            r["twolevel_learned_vs_jacobi"] = {"iterations": tj["iterations"] / tl["iterations"],
+                                               "time": tj["ms"] / tl["ms"]}
+        r["twolevel_aggregates"] = [agg, (g // agg) ** 2]
         if big:
-            agg = g // 64
-            r["twolevel_jacobi"] = run(gpu.twolevel(Ad, J, g, g, agg), Ad, A, b, 3000)
             r["fgmres_to_1e-10_fp64_vs_mixed"] = mixed_vs_plain(gpu.twolevel(Ad, J, g, g, agg), Ad, A, b)
-            r["twolevel_learned"] = run(gpu.twolevel(Ad, L, g, g, agg, coarse_first=True), Ad, A, b, 3000)
-            r["twolevel_aggregates"] = [agg, (g // agg) ** 2]
+            r["twolevel_learned_single_level_network"] = run(gpu.twolevel(Ad, L, g, g, agg, coarse_first=True),
+                                                             Ad, A, b, 3000)
         plain = [r["jacobi"], r["chebyshev8"]]
         lt = r["learned"]
         if lt["converged"]:

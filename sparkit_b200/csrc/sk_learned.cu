@@ -258,7 +258,7 @@ __device__ __forceinline__ void conv_epilogue(ConvArgs const& a, int b, int y, i
   const int h2 = a.H / 2, w2 = a.W / 2;
 #pragma unroll
   for (int c = 0; c < N / 8; ++c) {
-    uint4 mv = msk ? msk[c] : make_uint4(0, 0, 0, 0);
+    uint4 mv = msk ? __ldg(msk + c) : make_uint4(0, 0, 0, 0);
     const bf16* mb = reinterpret_cast<const bf16*>(&mv);
     uint4 o;
     bf16* ob = reinterpret_cast<bf16*>(&o);
@@ -266,7 +266,7 @@ __device__ __forceinline__ void conv_epilogue(ConvArgs const& a, int b, int y, i
 #pragma unroll
     for (int j = 0; j < 8; ++j) {
       float t = v[c * 8 + j];
-      if (a.bias) t += a.bias[c * 8 + j];
+      if (a.bias) t += __ldg(a.bias + c * 8 + j);
       if (a.relu) t = fmaxf(t, 0.0f);
       if (msk && !(__bfloat162float(mb[j]) > 0.0f)) t = 0.0f;
       ob[j] = __float2bfloat16_rn(t);
@@ -287,11 +287,19 @@ __device__ __forceinline__ void conv_epilogue(ConvArgs const& a, int b, int y, i
             pack8(q);
     }
     if (a.up_out && valid) {
+      // the four skip vectors are loaded before any store, so that their
+      // latencies overlap (the stores could alias them otherwise)
+      uint4 skv[4];
+#pragma unroll
+      for (int d = 0; d < 4; ++d) {
+        const i64 fp = (static_cast<i64>(b) * 2 * a.H + 2 * y + (d >> 1)) * (2 * a.W) + 2 * x + (d & 1);
+        skv[d] = __ldg(reinterpret_cast<const uint4*>(a.up_skip) + fp * (N / 8) + c);
+      }
 #pragma unroll
       for (int d = 0; d < 4; ++d) {
         const i64 fp = (static_cast<i64>(b) * 2 * a.H + 2 * y + (d >> 1)) * (2 * a.W) + 2 * x + (d & 1);
         float sk[8], u[8];
-        unpack8(reinterpret_cast<const uint4*>(a.up_skip)[fp * (N / 8) + c], sk);
+        unpack8(skv[d], sk);
 #pragma unroll
         for (int j = 0; j < 8; ++j) u[j] = r[j] + sk[j];
         reinterpret_cast<uint4*>(a.up_out)[fp * (N / 8) + c] = pack8(u);
@@ -689,12 +697,16 @@ __global__ void __launch_bounds__(kThreads) scale_kernel(SampleSrc src, double* 
     last = atomicAdd(counter + b, 1u) == gridDim.x - 1;
   }
   __syncthreads();
-  if (last && threadIdx.x == 0) {
+  if (last) {  // the last CTA sums the partials with all its threads (a fixed tree)
     __threadfence();
-    double t = 0.0;
-    for (int k = 0; k < static_cast<int>(gridDim.x); ++k) t += __ldcg(partial + b * kRedBlocks + k);
-    s[b] = sqrt(t / static_cast<double>(src.P));
-    counter[b] = 0u;
+    double t[1] = {0.0};
+    for (int k = threadIdx.x; k < static_cast<int>(gridDim.x); k += blockDim.x)
+      t[0] += __ldcg(partial + b * kRedBlocks + k);
+    block_reduce<1>(t);
+    if (threadIdx.x == 0) {
+      s[b] = sqrt(t[0] / static_cast<double>(src.P));
+      counter[b] = 0u;
+    }
   }
 }
 

@@ -817,6 +817,69 @@ class Pairs:
             pass
 
 
+def train_coarse_corrected_smoother(m, instances=200, held=10, cycles=40, steps=8000, agg=8, seed=1):
+    """A network for the smoother of the two-level form (twolevel(...,
+    coarse_first=True)), which only sees coarse-corrected residuals.  Pairs:
+    on `instances` + `held` seeded m^2 convection-diffusion instances
+    (matgen.convdiff_2d_grf), FGMRES(30) restart cycles from x = 0 (Jacobi,
+    or on every third instance the coarse correction alone), after each
+    cycle r = b - A x and e = x* - x moved past the coarse correction
+    c = P Ac^-1 P^T r (aggregates of agg x agg cells): (r - A c, e - c).
+    Returns the trained Net and a summary with the held-out loss (the last
+    `held` instances' pairs) before and after training."""
+    import time
+
+    import numpy as np
+    import torch
+
+    from . import matgen
+    pairs = Pairs(m, m, (instances + held) * cycles, instances + held)
+    t0 = time.perf_counter()
+    held_idx = []
+    for k in range(instances + held):
+        Am = matgen.convdiff_2d_grf(m, seed=100 + k)[0]
+        Amd = Device_matrix(Am)
+        inst = pairs.add_instance(Amd)
+        xs = np.random.default_rng(k).uniform(-1, 1, m * m) if k % 2 == 0 else \
+            matgen.gaussian_random_field((m, m), 1.0, m / 16, seed=k).ravel()
+        xsd = torch.from_numpy(xs).cuda()
+        b = torch.empty_like(xsd)
+        Amd.spmv(xsd, b)
+        J = jacobi(Amd)
+        C = twolevel(Amd, None, m, m, agg)
+        x = torch.zeros_like(b)
+        r = torch.empty_like(b)
+        z = torch.empty_like(b)
+        az = torch.empty_like(b)
+        for _ in range(cycles):
+            fgmres(b, x, Fgmres_config(1e-14, 30, 30), spmv(Amd), C if k % 3 == 0 else J)
+            Amd.spmv(x, r)
+            r = b - r
+            C.apply(r, z)
+            Amd.spmv(z, az)
+            if k >= instances:
+                held_idx.append(len(pairs))
+            pairs.add(inst, (r - az).contiguous(), (xsd - x - z).contiguous())
+        Amd.close()
+    torch.cuda.synchronize()
+    harvest_s = time.perf_counter() - t0
+    net = Net(seed=seed)
+    idx = np.array(held_idx, dtype=np.int32)
+
+    def held_loss():
+        return float(np.mean([net.loss_grad(pairs, idx[i:i + 8], mu=1.0)[0] for i in range(0, len(idx), 8)]))
+
+    before = held_loss()
+    ts = net.train(pairs, Train_config(steps=steps, batch=8, lr=2e-3, mu=1.0, seed=3))
+    h = np.array(ts.loss_history)
+    info = {"pairs": len(pairs), "held_out_pairs": len(held_idx), "grid": m, "aggregates": agg,
+            "harvest_s": harvest_s, "steps": steps, "batch": 8, "train_ms": ts.ms,
+            "loss_first20": float(h[:20].mean()), "loss_last50": float(h[-50:].mean()),
+            "held_out_loss_before": before, "held_out_loss_after": held_loss()}
+    pairs.close()
+    return net, info
+
+
 @dataclass
 class Train_config:
     steps: int = 1000
