@@ -234,75 +234,84 @@ struct ConvArgs {
   int* err;
 };
 
-// Thread = output pixel (x, y) of sample b with its N accumulators v.  All
-// threads of the CTA call it (the 2x2 pooling exchanges values between the
+// Thread = output pixel (x, y) of sample b with its N accumulators v (the
+// bias already added).  All threads of the CTA call it (the 2x2 pooling exchanges values between the
 // lanes of a warp: x + 1 is lane + 1, y + 1 is lane + 8).
 template <int N>
 __device__ __forceinline__ void conv_epilogue(ConvArgs const& a, int b, int y, int x, const float* v) {
   const bool valid = y < a.H && x < a.W;
   const i64 p = (static_cast<i64>(b) * a.H + y) * a.W + x;
   if (a.out_kind == OUT_F32) {
-    if (valid) a.outf[p] = v[0] + (a.bias ? a.bias[0] : 0.0f);
+    if (valid) a.outf[p] = v[0];
     return;
   }
   if (a.out_kind == OUT_Z64) {
-    if (valid) {
-      const float yv = v[0] + (a.bias ? a.bias[0] : 0.0f);
-      a.outz[p] = a.scale[b] * static_cast<double>(yv);
-    }
+    if (valid) a.outz[p] = a.scale[b] * static_cast<double>(v[0]);
     return;
   }
-  uint4* dst = reinterpret_cast<uint4*>(a.out + p * N);
-  const uint4* msk = (a.mask && valid) ? reinterpret_cast<const uint4*>(a.mask + p * N) : nullptr;
+  uint4* __restrict__ dst = reinterpret_cast<uint4*>(a.out + p * N);
+  const uint4* __restrict__ msk = (a.mask && valid) ? reinterpret_cast<const uint4*>(a.mask + p * N) : nullptr;
   const bool pool_writer = valid && ((x & 1) == 0) && ((y & 1) == 0);
   const int h2 = a.H / 2, w2 = a.W / 2;
+  // the reads of the epilogue (mask, the skip vectors of the four upsampled
+  // pixels) are issued before the stores of their group of channels, up to
+  // 32 channels at a time, so that their latencies overlap instead of
+  // following the stores one by one
+  const bool up = a.up_out && valid;
+  const uint4* __restrict__ skip = reinterpret_cast<const uint4*>(a.up_skip);
+  constexpr int G = N / 8 < 4 ? N / 8 : 4;
 #pragma unroll
-  for (int c = 0; c < N / 8; ++c) {
-    uint4 mv = msk ? __ldg(msk + c) : make_uint4(0, 0, 0, 0);
-    const bf16* mb = reinterpret_cast<const bf16*>(&mv);
-    uint4 o;
-    bf16* ob = reinterpret_cast<bf16*>(&o);
-    float r[8];
+  for (int cb = 0; cb < N / 8; cb += G) {
+    uint4 skv[G][4];
+    uint4 mvv[G];
 #pragma unroll
-    for (int j = 0; j < 8; ++j) {
-      float t = v[c * 8 + j];
-      if (a.bias) t += __ldg(a.bias + c * 8 + j);
-      if (a.relu) t = fmaxf(t, 0.0f);
-      if (msk && !(__bfloat162float(mb[j]) > 0.0f)) t = 0.0f;
-      ob[j] = __float2bfloat16_rn(t);
-      r[j] = __bfloat162float(ob[j]);
+    for (int g = 0; g < G; ++g) {
+      mvv[g] = msk ? __ldg(msk + cb + g) : make_uint4(0, 0, 0, 0);
+#pragma unroll
+      for (int d = 0; d < 4; ++d) {
+        const i64 fp = (static_cast<i64>(b) * 2 * a.H + 2 * y + (d >> 1)) * (2 * a.W) + 2 * x + (d & 1);
+        skv[g][d] = up ? __ldg(skip + fp * (N / 8) + cb + g) : make_uint4(0, 0, 0, 0);
+      }
     }
-    if (valid) dst[c] = o;
-    if (a.pool_out) {
-      float q[8];
+#pragma unroll
+    for (int g = 0; g < G; ++g) {
+      const int c = cb + g;
+      const bf16* mb = reinterpret_cast<const bf16*>(&mvv[g]);
+      uint4 o;
+      bf16* ob = reinterpret_cast<bf16*>(&o);
+      float r[8];
 #pragma unroll
       for (int j = 0; j < 8; ++j) {
-        const float r01 = __shfl_down_sync(0xffffffffu, r[j], 1);
-        const float r10 = __shfl_down_sync(0xffffffffu, r[j], 8);
-        const float r11 = __shfl_down_sync(0xffffffffu, r[j], 9);
-        q[j] = 0.25f * ((r[j] + r01) + (r10 + r11));
+        float t = v[c * 8 + j];
+        if (a.relu) t = fmaxf(t, 0.0f);
+        if (msk && !(__bfloat162float(mb[j]) > 0.0f)) t = 0.0f;
+        ob[j] = __float2bfloat16_rn(t);
+        r[j] = __bfloat162float(ob[j]);
       }
-      if (pool_writer)
-        reinterpret_cast<uint4*>(a.pool_out)[((static_cast<i64>(b) * h2 + y / 2) * w2 + x / 2) * (N / 8) + c] =
-            pack8(q);
-    }
-    if (a.up_out && valid) {
-      // the four skip vectors are loaded before any store, so that their
-      // latencies overlap (the stores could alias them otherwise)
-      uint4 skv[4];
+      if (valid) dst[c] = o;
+      if (a.pool_out) {
+        float q[8];
 #pragma unroll
-      for (int d = 0; d < 4; ++d) {
-        const i64 fp = (static_cast<i64>(b) * 2 * a.H + 2 * y + (d >> 1)) * (2 * a.W) + 2 * x + (d & 1);
-        skv[d] = __ldg(reinterpret_cast<const uint4*>(a.up_skip) + fp * (N / 8) + c);
+        for (int j = 0; j < 8; ++j) {
+          const float r01 = __shfl_down_sync(0xffffffffu, r[j], 1);
+          const float r10 = __shfl_down_sync(0xffffffffu, r[j], 8);
+          const float r11 = __shfl_down_sync(0xffffffffu, r[j], 9);
+          q[j] = 0.25f * ((r[j] + r01) + (r10 + r11));
+        }
+        if (pool_writer)
+          reinterpret_cast<uint4*>(a.pool_out)[((static_cast<i64>(b) * h2 + y / 2) * w2 + x / 2) * (N / 8) + c] =
+              pack8(q);
       }
+      if (up) {
 #pragma unroll
-      for (int d = 0; d < 4; ++d) {
-        const i64 fp = (static_cast<i64>(b) * 2 * a.H + 2 * y + (d >> 1)) * (2 * a.W) + 2 * x + (d & 1);
-        float sk[8], u[8];
-        unpack8(skv[d], sk);
+        for (int d = 0; d < 4; ++d) {
+          const i64 fp = (static_cast<i64>(b) * 2 * a.H + 2 * y + (d >> 1)) * (2 * a.W) + 2 * x + (d & 1);
+          float sk[8], u[8];
+          unpack8(skv[g][d], sk);
 #pragma unroll
-        for (int j = 0; j < 8; ++j) u[j] = r[j] + sk[j];
-        reinterpret_cast<uint4*>(a.up_out)[fp * (N / 8) + c] = pack8(u);
+          for (int j = 0; j < 8; ++j) u[j] = r[j] + sk[j];
+          reinterpret_cast<uint4*>(a.up_out)[fp * (N / 8) + c] = pack8(u);
+        }
       }
     }
   }
@@ -334,11 +343,16 @@ __global__ void __launch_bounds__(kConvThreads) conv3x3_kernel(const __grid_cons
   uint64_t* bar_mma = bar_load + 1;
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bar_load + 2);
   __shared__ int ok_load;
+  __shared__ float s_bias[N];
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int x0 = blockIdx.x * kTileW, y0 = blockIdx.y * kTileH, b = blockIdx.z;
   constexpr uint32_t kCols = N < 32 ? 32 : N;
 
+  // Launched as a programmatic dependent of the previous layer: the next
+  // layer may start its set-up now; this one touches no global memory
+  // until the previous grid has completed (griddepcontrol.wait).
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
   if (tid == 0) {
     mbar_init(bar_load, 1);
     mbar_init(bar_mma, 1);
@@ -350,6 +364,9 @@ __global__ void __launch_bounds__(kConvThreads) conv3x3_kernel(const __grid_cons
     tc_fence_before();
   }
   __syncthreads();
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  // (a single-channel output has one bias value)
+  if (tid < N) s_bias[tid] = a.bias && (a.out_kind == OUT_BF16 || tid == 0) ? __ldg(a.bias + tid) : 0.0f;
   if (tid == 0) {
     mbar_expect_tx(bar_load, S::kPlanes * kPlaneBytes + S::kWBytes);
     for (int c = 0; c < S::kPlanes; ++c)
@@ -369,8 +386,8 @@ __global__ void __launch_bounds__(kConvThreads) conv3x3_kernel(const __grid_cons
     if (tid == 0 && ok) {
       constexpr uint32_t idesc = umma_idesc(128, N);
       const uint32_t pbase = smem_u32(planes), wbase = smem_u32(wsm);
-#pragma unroll 1
-      for (int s = 0; s < S::kKC / 2; ++s) {
+#pragma unroll
+      for (int s = 0; s < S::kKC / 2; ++s) {  // every tap offset a constant
         const int kc0 = 2 * s, kc1 = 2 * s + 1;
         uint32_t a0, lbo;
         if constexpr (CIN == 8) {
@@ -465,6 +482,10 @@ __global__ void __launch_bounds__(kConvThreads) conv3x3_kernel(const __grid_cons
     __syncthreads();
 #pragma unroll
     for (int n = 0; n < N; ++n) v[n] = stage[tid * LD + n];
+  }
+  if (a.bias) {
+#pragma unroll
+    for (int j = 0; j < N; ++j) v[j] += s_bias[j];
   }
   conv_epilogue<N>(a, b, y0 + (tid >> 3), x0 + (tid & 7), v);
 }
@@ -1018,9 +1039,20 @@ static sk_status launch_conv(MapCache& mc, const void* in, ConvArgs const& a, cu
   sk_status s = mc.get(in, a.B, a.H, a.W, CIN, kHaloW, kHaloH, &m);
   if (s != SK_OK) return s;
   if (!attr_once(conv3x3_kernel<CIN, N, TC>, S::kBytes)) return fail(SK_CUDA_ERROR, "cudaFuncSetAttribute");
-  dim3 grid(ceil_div(a.W, kTileW), ceil_div(a.H, kTileH), a.B);
-  SK_LAUNCH((conv3x3_kernel<CIN, N, TC>), grid, kConvThreads, S::kBytes, st, m, a);
-  SK_CUDA(cudaGetLastError());
+  // programmatic dependent launch: the set-up of this layer's CTAs (barrier
+  // init, tensor-memory allocation) overlaps the tail of the previous one
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = dim3(ceil_div(a.W, kTileW), ceil_div(a.H, kTileH), a.B);
+  cfg.blockDim = dim3(kConvThreads);
+  cfg.dynamicSmemBytes = S::kBytes;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  SK_CUDA(cudaLaunchKernelEx(&cfg, conv3x3_kernel<CIN, N, TC>, m, a));
   return SK_OK;
 }
 
