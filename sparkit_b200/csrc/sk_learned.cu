@@ -46,6 +46,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstring>
+#include <algorithm>
 #include <array>
 #include <map>
 #include <mutex>
@@ -317,6 +318,36 @@ __device__ __forceinline__ void conv_epilogue(ConvArgs const& a, int b, int y, i
   }
 }
 
+// The implicit GEMM of one 16 x 8 tile: 9 * CIN / 16 tcgen05.mma into the
+// accumulator at tmem, from the staged planes at pbase (K-major, one
+// [18][10][8] BF16 plane per 8 input channels) and the packed weights at
+// wbase.  Issued by one thread.
+template <int CIN, int N>
+__device__ __forceinline__ void conv_issue_mma(uint32_t pbase, uint32_t wbase, uint32_t tmem) {
+  constexpr uint32_t idesc = umma_idesc(128, N);
+  constexpr int KC = (9 * CIN / 8 + 1) & ~1;
+#pragma unroll
+  for (int s = 0; s < KC / 2; ++s) {  // every tap offset a constant
+    const int kc0 = 2 * s, kc1 = 2 * s + 1;
+    uint32_t a0, lbo;
+    if constexpr (CIN == 8) {
+      // the two K halves are taps kc0 and kc1 of the single plane
+      const int t0 = kc0, t1 = kc1 < 9 ? kc1 : kc0;
+      const uint32_t o0 = ((t0 / 3) * kHaloW + t0 % 3) * 16, o1 = ((t1 / 3) * kHaloW + t1 % 3) * 16;
+      a0 = pbase + o0;
+      lbo = o1 - o0;
+    } else {
+      constexpr int P = CIN / 8;
+      const int t = kc0 / P, c = kc0 % P;  // kc1 is plane c + 1 of the same tap
+      a0 = pbase + c * kPlaneStride + ((t / 3) * kHaloW + t % 3) * 16;
+      lbo = kPlaneStride;
+    }
+    const uint64_t ad = umma_desc(a0, lbo, kHaloW * 16);
+    const uint64_t bd = umma_desc(wbase + kc0 * (N / 8) * 128, (N / 8) * 128, 128);
+    umma_bf16(tmem, ad, bd, idesc, s > 0 ? 1u : 0u);
+  }
+}
+
 // Shared memory of one conv CTA.
 template <int CIN, int N, bool TC>
 struct ConvSmem {
@@ -349,10 +380,12 @@ __global__ void __launch_bounds__(kConvThreads) conv3x3_kernel(const __grid_cons
   const int x0 = blockIdx.x * kTileW, y0 = blockIdx.y * kTileH, b = blockIdx.z;
   constexpr uint32_t kCols = N < 32 ? 32 : N;
 
-  // Launched as a programmatic dependent of the previous layer: the next
-  // layer may start its set-up now; this one touches no global memory
-  // until the previous grid has completed (griddepcontrol.wait).
-  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+  // Launched as a programmatic dependent of the previous layer: this CTA
+  // sets up (barriers, tensor memory), then lets the next layer launch, and
+  // touches no global memory until the previous grid has completed
+  // (griddepcontrol.wait).  The next layer can launch only once every CTA
+  // of this one holds its tensor memory, so no CTA of this layer ever waits
+  // for columns held by a CTA that waits for this layer.
   if (tid == 0) {
     mbar_init(bar_load, 1);
     mbar_init(bar_mma, 1);
@@ -364,6 +397,7 @@ __global__ void __launch_bounds__(kConvThreads) conv3x3_kernel(const __grid_cons
     tc_fence_before();
   }
   __syncthreads();
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
   asm volatile("griddepcontrol.wait;" ::: "memory");
   // (a single-channel output has one bias value)
   if (tid < N) s_bias[tid] = a.bias && (a.out_kind == OUT_BF16 || tid == 0) ? __ldg(a.bias + tid) : 0.0f;
@@ -384,28 +418,7 @@ __global__ void __launch_bounds__(kConvThreads) conv3x3_kernel(const __grid_cons
     tmem = *tmem_slot;
     bool mma_ok = ok;
     if (tid == 0 && ok) {
-      constexpr uint32_t idesc = umma_idesc(128, N);
-      const uint32_t pbase = smem_u32(planes), wbase = smem_u32(wsm);
-#pragma unroll
-      for (int s = 0; s < S::kKC / 2; ++s) {  // every tap offset a constant
-        const int kc0 = 2 * s, kc1 = 2 * s + 1;
-        uint32_t a0, lbo;
-        if constexpr (CIN == 8) {
-          // the two K halves are taps kc0 and kc1 of the single plane
-          const int t0 = kc0, t1 = kc1 < 9 ? kc1 : kc0;
-          const uint32_t o0 = ((t0 / 3) * kHaloW + t0 % 3) * 16, o1 = ((t1 / 3) * kHaloW + t1 % 3) * 16;
-          a0 = pbase + o0;
-          lbo = o1 - o0;
-        } else {
-          constexpr int P = CIN / 8;
-          const int t = kc0 / P, c = kc0 % P;  // kc1 is plane c + 1 of the same tap
-          a0 = pbase + c * kPlaneStride + ((t / 3) * kHaloW + t % 3) * 16;
-          lbo = kPlaneStride;
-        }
-        const uint64_t ad = umma_desc(a0, lbo, kHaloW * 16);
-        const uint64_t bd = umma_desc(wbase + kc0 * (N / 8) * 128, (N / 8) * 128, 128);
-        umma_bf16(tmem, ad, bd, idesc, s > 0 ? 1u : 0u);
-      }
+      conv_issue_mma<CIN, N>(smem_u32(planes), smem_u32(wsm), tmem);
       umma_commit(bar_mma);
     }
     __syncthreads();
@@ -1041,14 +1054,15 @@ static sk_status launch_conv(MapCache& mc, const void* in, ConvArgs const& a, cu
   if (!attr_once(conv3x3_kernel<CIN, N, TC>, S::kBytes)) return fail(SK_CUDA_ERROR, "cudaFuncSetAttribute");
   // programmatic dependent launch: the set-up of this layer's CTAs (barrier
   // init, tensor-memory allocation) overlaps the tail of the previous one
-  cudaLaunchConfig_t cfg{};
-  cfg.gridDim = dim3(ceil_div(a.W, kTileW), ceil_div(a.H, kTileH), a.B);
-  cfg.blockDim = dim3(kConvThreads);
-  cfg.dynamicSmemBytes = S::kBytes;
-  cfg.stream = st;
   cudaLaunchAttribute attr[1];
   attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
   attr[0].val.programmaticStreamSerializationAllowed = 1;
+  const int ntx = ceil_div(a.W, kTileW), nty = ceil_div(a.H, kTileH);
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = dim3(ntx, nty, a.B);
+  cfg.blockDim = dim3(kConvThreads);
+  cfg.dynamicSmemBytes = S::kBytes;
+  cfg.stream = st;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
   g_launches.fetch_add(1, std::memory_order_relaxed);
