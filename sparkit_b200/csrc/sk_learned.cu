@@ -238,7 +238,7 @@ struct ConvArgs {
 // Thread = output pixel (x, y) of sample b with its N accumulators v (the
 // bias already added).  All threads of the CTA call it (the 2x2 pooling exchanges values between the
 // lanes of a warp: x + 1 is lane + 1, y + 1 is lane + 8).
-template <int N>
+template <int N, bool UP>
 __device__ __forceinline__ void conv_epilogue(ConvArgs const& a, int b, int y, int x, const float* v) {
   const bool valid = y < a.H && x < a.W;
   const i64 p = (static_cast<i64>(b) * a.H + y) * a.W + x;
@@ -258,20 +258,22 @@ __device__ __forceinline__ void conv_epilogue(ConvArgs const& a, int b, int y, i
   // pixels) are issued before the stores of their group of channels, up to
   // 32 channels at a time, so that their latencies overlap instead of
   // following the stores one by one
-  const bool up = a.up_out && valid;
+  const bool up = UP && valid;
   const uint4* __restrict__ skip = reinterpret_cast<const uint4*>(a.up_skip);
   constexpr int G = N / 8 < 4 ? N / 8 : 4;
 #pragma unroll
   for (int cb = 0; cb < N / 8; cb += G) {
-    uint4 skv[G][4];
+    uint4 skv[UP ? G : 1][4];
     uint4 mvv[G];
 #pragma unroll
     for (int g = 0; g < G; ++g) {
       mvv[g] = msk ? __ldg(msk + cb + g) : make_uint4(0, 0, 0, 0);
+      if constexpr (UP) {
 #pragma unroll
-      for (int d = 0; d < 4; ++d) {
-        const i64 fp = (static_cast<i64>(b) * 2 * a.H + 2 * y + (d >> 1)) * (2 * a.W) + 2 * x + (d & 1);
-        skv[g][d] = up ? __ldg(skip + fp * (N / 8) + cb + g) : make_uint4(0, 0, 0, 0);
+        for (int d = 0; d < 4; ++d) {
+          const i64 fp = (static_cast<i64>(b) * 2 * a.H + 2 * y + (d >> 1)) * (2 * a.W) + 2 * x + (d & 1);
+          skv[g][d] = up ? __ldg(skip + fp * (N / 8) + cb + g) : make_uint4(0, 0, 0, 0);
+        }
       }
     }
 #pragma unroll
@@ -303,7 +305,8 @@ __device__ __forceinline__ void conv_epilogue(ConvArgs const& a, int b, int y, i
           reinterpret_cast<uint4*>(a.pool_out)[((static_cast<i64>(b) * h2 + y / 2) * w2 + x / 2) * (N / 8) + c] =
               pack8(q);
       }
-      if (up) {
+      if constexpr (UP) {
+        if (up) {
 #pragma unroll
         for (int d = 0; d < 4; ++d) {
           const i64 fp = (static_cast<i64>(b) * 2 * a.H + 2 * y + (d >> 1)) * (2 * a.W) + 2 * x + (d & 1);
@@ -312,6 +315,7 @@ __device__ __forceinline__ void conv_epilogue(ConvArgs const& a, int b, int y, i
 #pragma unroll
           for (int j = 0; j < 8; ++j) u[j] = r[j] + sk[j];
           reinterpret_cast<uint4*>(a.up_out)[fp * (N / 8) + c] = pack8(u);
+        }
         }
       }
     }
@@ -362,8 +366,10 @@ struct ConvSmem {
 };
 
 // TC = true: tcgen05 (product path); false: the same tile with mma.sync
-// (cross-check of the tcgen05 path in the tests).
-template <int CIN, int N, bool TC>
+// (cross-check of the tcgen05 path in the tests).  UP: the epilogue also
+// writes the upsampled sum with the skip tensor (a.up_out); the other
+// layers leave out its registers.
+template <int CIN, int N, bool TC, bool UP>
 __global__ void __launch_bounds__(kConvThreads) conv3x3_kernel(const __grid_constant__ CUtensorMap in_map,
                                                                ConvArgs a) {
   using S = ConvSmem<CIN, N, TC>;
@@ -500,7 +506,7 @@ __global__ void __launch_bounds__(kConvThreads) conv3x3_kernel(const __grid_cons
 #pragma unroll
     for (int j = 0; j < N; ++j) v[j] += s_bias[j];
   }
-  conv_epilogue<N>(a, b, y0 + (tid >> 3), x0 + (tid & 7), v);
+  conv_epilogue<N, UP>(a, b, y0 + (tid >> 3), x0 + (tid & 7), v);
 }
 
 // ------------------------------------------------------------------
@@ -1051,7 +1057,8 @@ static sk_status launch_conv(MapCache& mc, const void* in, ConvArgs const& a, cu
   CUtensorMap m;
   sk_status s = mc.get(in, a.B, a.H, a.W, CIN, kHaloW, kHaloH, &m);
   if (s != SK_OK) return s;
-  if (!attr_once(conv3x3_kernel<CIN, N, TC>, S::kBytes)) return fail(SK_CUDA_ERROR, "cudaFuncSetAttribute");
+  const auto kernel = a.up_out ? conv3x3_kernel<CIN, N, TC, true> : conv3x3_kernel<CIN, N, TC, false>;
+  if (!attr_once(kernel, S::kBytes)) return fail(SK_CUDA_ERROR, "cudaFuncSetAttribute");
   // programmatic dependent launch: the set-up of this layer's CTAs (barrier
   // init, tensor-memory allocation) overlaps the tail of the previous one
   cudaLaunchAttribute attr[1];
@@ -1066,7 +1073,7 @@ static sk_status launch_conv(MapCache& mc, const void* in, ConvArgs const& a, cu
   cfg.attrs = attr;
   cfg.numAttrs = 1;
   g_launches.fetch_add(1, std::memory_order_relaxed);
-  SK_CUDA(cudaLaunchKernelEx(&cfg, conv3x3_kernel<CIN, N, TC>, m, a));
+  SK_CUDA(cudaLaunchKernelEx(&cfg, kernel, m, a));
   return SK_OK;
 }
 
@@ -1458,13 +1465,18 @@ sk_status learned_apply(const sk_precond_s* M, const double* v, double* z, cudaS
 
 template <bool TC>
 static sk_status conv_attrs() {
-  bool ok = attr_once(conv3x3_kernel<8, 16, TC>, ConvSmem<8, 16, TC>::kBytes) &&
-            attr_once(conv3x3_kernel<16, 16, TC>, ConvSmem<16, 16, TC>::kBytes) &&
-            attr_once(conv3x3_kernel<16, 32, TC>, ConvSmem<16, 32, TC>::kBytes) &&
-            attr_once(conv3x3_kernel<32, 16, TC>, ConvSmem<32, 16, TC>::kBytes) &&
-            attr_once(conv3x3_kernel<32, 64, TC>, ConvSmem<32, 64, TC>::kBytes) &&
-            attr_once(conv3x3_kernel<64, 32, TC>, ConvSmem<64, 32, TC>::kBytes) &&
-            attr_once(conv3x3_kernel<64, 64, TC>, ConvSmem<64, 64, TC>::kBytes);
+  bool ok = true;
+  auto both = [&](auto k_plain, auto k_up, int bytes) { ok = ok && attr_once(k_plain, bytes) && attr_once(k_up, bytes); };
+#define SK_CONV_ATTR(CI, NN) \
+  both(conv3x3_kernel<CI, NN, TC, false>, conv3x3_kernel<CI, NN, TC, true>, ConvSmem<CI, NN, TC>::kBytes);
+  SK_CONV_ATTR(8, 16)
+  SK_CONV_ATTR(16, 16)
+  SK_CONV_ATTR(16, 32)
+  SK_CONV_ATTR(32, 16)
+  SK_CONV_ATTR(32, 64)
+  SK_CONV_ATTR(64, 32)
+  SK_CONV_ATTR(64, 64)
+#undef SK_CONV_ATTR
   return ok ? SK_OK : fail(SK_CUDA_ERROR, "cudaFuncSetAttribute");
 }
 
