@@ -491,6 +491,129 @@ const void* pick_kernel(bool dia, bool unit) {
               : reinterpret_cast<const void*>(&inner_cg_kernel<false, false>);
 }
 
+// ------------------------------------------------------------------
+// Plain FP64 conjugate gradient (conjugate_gradient.hpp:122-312 with a
+// Jacobi or identity left preconditioner, identity right, true residual at
+// k = 0 only) as one cooperative launch, for systems small enough that the
+// three kernels per step are bound by launch and reduction latency.  Each
+// CTA owns a contiguous block of rows; per step:
+//   1  q = A p over the CTA's rows (each row summed in storage order),
+//      <p, q>                                   -> alpha = rz / <p, q>
+//   2  x += alpha p, r -= alpha q, <r, r>, <r, D^-1 r>
+//                                               -> the test, beta, rz
+//   3  p = D^-1 r + beta p, then a grid barrier (the next product reads p)
+// with the arithmetic of the per-step kernels (OpCgUpdate, EpiCgPq,
+// OpCgDirection: the same products, sums and roundings per element); only
+// the order in which the dot products' partial sums meet differs.
+// ------------------------------------------------------------------
+struct Cg64Args {
+  PArgs g;  // n, off, len, col (SELL-32), slots, sync, wait_ns, bias
+  const double* val;
+  const double* b;
+  double* x;
+  double* r;
+  double* p;
+  double* q;
+  const double* invd;  // Jacobi: 1 / a_ii; null: identity
+  double* hist;        // residual history, or null
+  Scalars* sc;
+};
+
+__device__ __forceinline__ double sell_row64(Cg64Args const& a, int i, const double* __restrict__ v) {
+  const int len = __ldg(a.g.len + i);
+  const int base = __ldg(a.g.off + (i >> 5)) + (i & 31);
+  double sum = 0.0;
+  int k = 0;
+  for (; k + 4 <= len; k += 4) {
+    double pr[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int e = base + 32 * (k + j);
+      pr[j] = mul(__ldg(a.val + e), v[__ldg(a.g.col + e)]);
+    }
+#pragma unroll
+    for (int j = 0; j < 4; ++j) sum = add(sum, pr[j]);
+  }
+  for (; k < len; ++k) {
+    const int e = base + 32 * k;
+    sum = add(sum, mul(__ldg(a.val + e), v[__ldg(a.g.col + e)]));
+  }
+  return sum;
+}
+
+template <bool JAC>
+__global__ void __launch_bounds__(kPT, 1) cg64_kernel(Cg64Args a) {
+  unsigned epoch = 0;
+  const int n = a.g.n;
+  const int per = (((n + gridDim.x - 1) / gridDim.x) + 31) & ~31;
+  const int r0 = min(n, static_cast<int>(blockIdx.x) * per), r1 = min(n, r0 + per);
+  Scalars* sc = a.sc;
+  const double bnorm = sc->bnorm, tol = sc->tol;
+  const long long max_iters = sc->max_iters;
+  // k = 0: r = b - A x, z = D^-1 r, p = z, rz = <r, z>   (EpiCgResid)
+  double v1[1] = {0.0};
+  for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
+    const double ri = sub(a.b[i], sell_row64(a, i, a.x));
+    a.r[i] = ri;
+    const double zi = JAC ? mul(a.invd[i], ri) : ri;
+    a.p[i] = zi;
+    v1[0] += mul(ri, zi);
+  }
+  if (!grid_allreduce<1>(v1, a.g, 0, epoch)) return;
+  double rz = v1[0];
+  long long it = 0;
+  int conv = 0;
+  double rn = 0.0, alpha = 0.0, beta = 0.0;
+  int set = 1;
+  while (it < max_iters) {
+    // 1: q = A p, <p, q>                                  (EpiCgPq)
+    double pq[1] = {0.0};
+    for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
+      const double qi = sell_row64(a, i, a.p);
+      a.q[i] = qi;
+      pq[0] += mul(a.p[i], qi);
+    }
+    if (!grid_allreduce<1>(pq, a.g, set, epoch)) return;
+    set ^= 1;
+    alpha = rz / pq[0];
+    // 2: x += alpha p, r -= alpha q, <r, r>, <r, D^-1 r>  (OpCgUpdate)
+    double rr[2] = {0.0, 0.0};
+    for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
+      a.x[i] = add(mul(alpha, a.p[i]), a.x[i]);
+      const double ri = sub(a.r[i], mul(alpha, a.q[i]));
+      a.r[i] = ri;
+      rr[0] += mul(ri, ri);
+      if (JAC) rr[1] += mul(ri, mul(a.invd[i], ri));
+    }
+    if (!grid_allreduce<2>(rr, a.g, set, epoch)) return;
+    set ^= 1;
+    ++it;
+    rn = sqrt(rr[0]);
+    if (a.hist && blockIdx.x == 0 && threadIdx.x == 0) a.hist[it - 1] = rn;
+    conv = rn / bnorm < tol ? 1 : 0;
+    if (conv || it >= max_iters) break;
+    const double rz_new = JAC ? rr[1] : rr[0];
+    beta = rz_new / rz;
+    rz = rz_new;
+    // 3: p = D^-1 r + beta p                              (OpCgDirection)
+    for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
+      const double zi = JAC ? mul(a.invd[i], a.r[i]) : a.r[i];
+      a.p[i] = add(zi, mul(beta, a.p[i]));
+    }
+    if (!grid_barrier(a.g.sync, epoch, a.g.wait_ns, a.g.bias)) return;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    sc->iters = it;
+    sc->converged = conv;
+    sc->done = 1;
+    sc->rnorm = rn;
+    sc->rz = rz;
+    sc->alpha = alpha;
+    sc->beta = beta;
+    sc->hist_len = a.hist ? it : 0;
+  }
+}
+
 // CTAs of the cooperative grid (0: the kernel does not fit).
 int coop_grid(sk_matrix A, const void* k) {
   int per_sm = 0;
@@ -801,6 +924,55 @@ sk_status inner_cg_persistent(sk_matrix A, bool scaled, float* r, float* d, floa
   out->iterations = h.iterations;
   out->converged = h.converged;
   out->rnorm = h.rnorm;
+  return SK_OK;
+}
+
+bool cg64_persistent_ok(sk_matrix A) {
+  if (!A || A->format != SK_CSR || A->dtype != SK_F64 || !A->csr.sell || A->nrow <= 0) return false;
+  if (A->nrow > kCg64MaxRows || summation_sequential()) return false;
+  int coop = 0;
+  if (cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, A->device) != cudaSuccess || !coop) return false;
+  return coop_grid(A, reinterpret_cast<const void*>(&cg64_kernel<true>)) > 0 &&
+         coop_grid(A, reinterpret_cast<const void*>(&cg64_kernel<false>)) > 0;
+}
+
+sk_status cg64_persistent(sk_matrix A, const double* b, double* x, double* r, double* p, double* q,
+                          const double* invd, double* hist, Scalars* sc, void* scratch, cudaStream_t st) {
+  SK_CHECK(cg64_persistent_ok(A), SK_NOT_SUPPORTED, "persistent CG needs a small FP64 CSR handle with SELL-32");
+  const auto& C = A->csr;
+  const void* k = invd ? reinterpret_cast<const void*>(&cg64_kernel<true>)
+                       : reinterpret_cast<const void*>(&cg64_kernel<false>);
+  int grid = std::min(A->sm_count, kPT);  // one CTA per SM (cg64_persistent_ok: at least one fits)
+  const int need = ceil_div(A->nrow, 32);
+  if (grid > need) grid = need;
+  SyncWords* sync = static_cast<SyncWords*>(scratch);
+  double* slots = reinterpret_cast<double*>(static_cast<char*>(scratch) + 256);
+  SK_CUDA(cudaMemsetAsync(sync, 0, sizeof(SyncWords), st));
+  Cg64Args a{};
+  a.g.n = static_cast<int>(A->nrow);
+  a.g.off = C.sell_off;
+  a.g.len = C.sell_len;
+  a.g.col = C.sell_col;
+  a.g.slots = slots;
+  a.g.sync = sync;
+  a.g.wait_ns = wait_limit_ns();
+  a.g.bias = wait_target_bias();
+  a.val = static_cast<const double*>(C.sell_vals);
+  a.b = b;
+  a.x = x;
+  a.r = r;
+  a.p = p;
+  a.q = q;
+  a.invd = invd;
+  a.hist = hist;
+  a.sc = sc;
+  void* params[] = {&a};
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  SK_CUDA(cudaLaunchCooperativeKernel(k, dim3(grid), dim3(kPT), params, 0, st));
+  int err = 0;
+  SK_CUDA(cudaMemcpyAsync(&err, &sync->err, sizeof(int), cudaMemcpyDeviceToHost, st));
+  SK_CUDA(cudaStreamSynchronize(st));
+  if (err) return fail(SK_TIMEOUT, "persistent CG: a grid barrier wait ran out");
   return SK_OK;
 }
 

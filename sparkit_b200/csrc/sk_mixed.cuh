@@ -45,4 +45,20 @@ size_t inner_persistent_scratch(sk_matrix A);
 sk_status inner_cg_persistent(sk_matrix A, bool scaled, float* r, float* d, float* p, float* q, void* scratch,
                               double tol, long long max_iters, cudaStream_t st, InnerResult* out);
 
+// Plain FP64 CG (Jacobi or identity left preconditioner, identity right,
+// the true residual at k = 0 only) as one cooperative launch: for FP64 CSR
+// handles with SELL-32 of at most kCg64MaxRows rows, on a device that can
+// co-schedule the grid, outside the sequential summation order.
+constexpr long long kCg64MaxRows = 262144;
+bool cg64_persistent_ok(sk_matrix A);
+
+// Runs the whole solve: sc holds bnorm, tol and max_iters on entry and
+// iters, converged, done, rnorm, rz, alpha, beta and hist_len on exit; r,
+// p, q are work vectors of n values; invd is the Jacobi inverse diagonal
+// or null; hist receives one residual norm per step when not null; scratch
+// holds inner_persistent_scratch(A) bytes.  Synchronous; SK_TIMEOUT when a
+// grid barrier wait runs out.
+sk_status cg64_persistent(sk_matrix A, const double* b, double* x, double* r, double* p, double* q,
+                          const double* invd, double* hist, Scalars* sc, void* scratch, cudaStream_t st);
+
 }  // namespace sk

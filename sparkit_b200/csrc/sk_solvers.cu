@@ -13,6 +13,7 @@
 #include <chrono>
 #include <cmath>
 #include <map>
+#include <type_traits>
 #include <vector>
 
 #include "sk_arnoldi.cuh"
@@ -438,7 +439,16 @@ static sk_status cg_solve(sk_matrix A, sk_precond L, sk_precond R, const T* b, T
   SolveCommon c;
   std::vector<char*> v;
   const i64 hist_cap = cfg->collect_residuals ? cfg->max_iterations : 0;
-  sk_status s = carve_common(A, st, 5, vb, 0, hist_cap, &c, &v, nullptr, ws_base);
+  // small FP64 systems with a Jacobi or identity left preconditioner and
+  // no restart before the last step: the whole solve in one cooperative
+  // launch (sk_mixed.cu), where three kernels per step would be bound by
+  // launch and reduction latency
+  const bool cg64 = std::is_same<T, double>::value && !vals && !ws_base && !R &&
+                    (!L || L->kind == 1) && cfg->restart_iterations >= cfg->max_iterations &&
+                    cg64_persistent_ok(A);
+  const size_t pextra = cg64 ? (inner_persistent_scratch(A) + 511) & ~size_t(511) : 0;
+  char* pscratch = nullptr;
+  sk_status s = carve_common(A, st, 5, vb, pextra, hist_cap, &c, &v, cg64 ? &pscratch : nullptr, ws_base);
   if (s != SK_OK) return s;
   T *r = (T*)v[0], *z = (T*)v[1], *p = (T*)v[2], *hatp = (T*)v[3], *q = (T*)v[4];
   *out = sk_summary{};
@@ -457,6 +467,15 @@ static sk_status cg_solve(sk_matrix A, sk_precond L, sk_precond R, const T* b, T
   h.hist_on = cfg->collect_residuals ? 1 : 0;
   if ((s = put_scalars(c.sc, h, st)) != SK_OK) return s;
   const int lk = prec_kind(L);
+  if constexpr (std::is_same<T, double>::value) {
+    if (cg64) {
+      const double* invd = L ? static_cast<const double*>(L->inv_diag) : nullptr;
+      if ((s = cg64_persistent(A, b, x, r, p, q, invd, cfg->collect_residuals ? c.hist : nullptr, c.sc, pscratch,
+                               st)) != SK_OK)
+        return s;
+      return finish_summary(c, st, out, history_host);
+    }
+  }
   const bool graphs = capturable(L) && capturable(R);
   if (graphs && (s = solve_stream(A, st, &st)) != SK_OK) return s;
   auto steps = [&](i64 k0, i64 cnt) {

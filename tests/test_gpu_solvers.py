@@ -290,3 +290,24 @@ def test_device_resident_solve(gpu_lib, oracle):
     torch.cuda.synchronize()
     _, sr = oracle.cg(A, b, np.zeros(n), 1e-10, 10000, 10000, left="jacobi")
     assert s.converged and iters_close(s.computed_iterations, sr["computed_iterations"])
+
+
+def test_small_cg_runs_as_one_launch(gpu_lib, oracle):
+    """Configuration 1 (Jacobi-CG on the 256^2 Laplacian to 1e-10) runs as one
+    cooperative launch: a handful of kernels for the whole solve instead of
+    three per step, the same iteration count within 2% of the reference's
+    724 and the FP64 tolerance on the true residual; and the residual
+    history has one entry per step."""
+    A = matgen.laplacian_2d_dirichlet(256)
+    n = A.shape()[0]
+    b = oracle.spmv(A, matgen.uniform_vector(n, seed=0))
+    Ad = gpu.Device_matrix(A)
+    x = np.zeros(n)
+    before = _lib.launch_count()
+    s = gpu.conjugate_gradient(b, x, gpu.CGConfig(1e-10, 100000, 100000, True), gpu.spmv(Ad), gpu.jacobi(Ad))
+    launches = _lib.launch_count() - before
+    assert s.converged and abs(s.computed_iterations - 724) <= max(2, 0.02 * 724), s.computed_iterations
+    assert launches < 20, launches
+    assert len(s.iteration_residuals) == s.computed_iterations
+    rel = np.linalg.norm(b - oracle.spmv(A, x)) / np.linalg.norm(b)
+    assert rel < 1e-10, rel
