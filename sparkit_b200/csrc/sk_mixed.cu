@@ -496,15 +496,19 @@ const void* pick_kernel(bool dia, bool unit) {
 // Jacobi or identity left preconditioner, identity right, true residual at
 // k = 0 only) as one cooperative launch, for systems small enough that the
 // three kernels per step are bound by launch and reduction latency.  Each
-// CTA owns a contiguous block of rows; per step:
-//   1  q = A p over the CTA's rows (each row summed in storage order),
-//      <p, q>                                   -> alpha = rz / <p, q>
+// CTA owns a contiguous block of rows; per step, behind two grid-wide
+// reductions:
+//   1  p = D^-1 r + beta p for the CTA's rows into the other half of a
+//      double buffer, and q = A p with every gathered p_j recomputed the
+//      same way from r_j and the previous p_j (so no barrier is needed
+//      between the direction update and the product), <p, q>
+//                                               -> alpha = rz / <p, q>
 //   2  x += alpha p, r -= alpha q, <r, r>, <r, D^-1 r>
 //                                               -> the test, beta, rz
-//   3  p = D^-1 r + beta p, then a grid barrier (the next product reads p)
-// with the arithmetic of the per-step kernels (OpCgUpdate, EpiCgPq,
-// OpCgDirection: the same products, sums and roundings per element); only
-// the order in which the dot products' partial sums meet differs.
+// with the arithmetic of the per-step kernels (OpCgDirection, EpiCgPq,
+// OpCgUpdate: the same products, sums and roundings per element, a
+// recomputed p_j has the bits its owner stores); only the order in which
+// the dot products' partial sums meet differs.
 // ------------------------------------------------------------------
 struct Cg64Args {
   PArgs g;  // n, off, len, col (SELL-32), slots, sync, wait_ns, bias
@@ -512,14 +516,17 @@ struct Cg64Args {
   const double* b;
   double* x;
   double* r;
-  double* p;
+  double* p0;  // direction, double-buffered: step k writes p[k & 1]
+  double* p1;
   double* q;
   const double* invd;  // Jacobi: 1 / a_ii; null: identity
   double* hist;        // residual history, or null
   Scalars* sc;
 };
 
-__device__ __forceinline__ double sell_row64(Cg64Args const& a, int i, const double* __restrict__ v) {
+// (A v)_i with v_j = f(j), each row summed in storage order
+template <class F>
+__device__ __forceinline__ double sell_row64(Cg64Args const& a, int i, F const& f) {
   const int len = __ldg(a.g.len + i);
   const int base = __ldg(a.g.off + (i >> 5)) + (i & 31);
   double sum = 0.0;
@@ -529,14 +536,14 @@ __device__ __forceinline__ double sell_row64(Cg64Args const& a, int i, const dou
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
       const int e = base + 32 * (k + j);
-      pr[j] = mul(__ldg(a.val + e), v[__ldg(a.g.col + e)]);
+      pr[j] = mul(__ldg(a.val + e), f(__ldg(a.g.col + e)));
     }
 #pragma unroll
     for (int j = 0; j < 4; ++j) sum = add(sum, pr[j]);
   }
   for (; k < len; ++k) {
     const int e = base + 32 * k;
-    sum = add(sum, mul(__ldg(a.val + e), v[__ldg(a.g.col + e)]));
+    sum = add(sum, mul(__ldg(a.val + e), f(__ldg(a.g.col + e))));
   }
   return sum;
 }
@@ -550,13 +557,15 @@ __global__ void __launch_bounds__(kPT, 1) cg64_kernel(Cg64Args a) {
   Scalars* sc = a.sc;
   const double bnorm = sc->bnorm, tol = sc->tol;
   const long long max_iters = sc->max_iters;
-  // k = 0: r = b - A x, z = D^-1 r, p = z, rz = <r, z>   (EpiCgResid)
+  const double* __restrict__ invd = a.invd;
+  const double* x0 = a.x;
+  // k = 0: r = b - A x, p = z = D^-1 r, rz = <r, z>   (EpiCgResid)
   double v1[1] = {0.0};
   for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
-    const double ri = sub(a.b[i], sell_row64(a, i, a.x));
+    const double ri = sub(a.b[i], sell_row64(a, i, [&](int j) { return x0[j]; }));
     a.r[i] = ri;
-    const double zi = JAC ? mul(a.invd[i], ri) : ri;
-    a.p[i] = zi;
+    const double zi = JAC ? mul(invd[i], ri) : ri;
+    a.p0[i] = zi;
     v1[0] += mul(ri, zi);
   }
   if (!grid_allreduce<1>(v1, a.g, 0, epoch)) return;
@@ -566,12 +575,29 @@ __global__ void __launch_bounds__(kPT, 1) cg64_kernel(Cg64Args a) {
   double rn = 0.0, alpha = 0.0, beta = 0.0;
   int set = 1;
   while (it < max_iters) {
-    // 1: q = A p, <p, q>                                  (EpiCgPq)
+    // 1: p (for k > 0), q = A p, <p, q>          (OpCgDirection, EpiCgPq)
+    const double* pold = (it & 1) ? a.p0 : a.p1;  // step it - 1 wrote p[(it - 1) & 1]
+    double* pcur = (it & 1) ? a.p1 : a.p0;
+    const double* __restrict__ rr_ = a.r;
+    auto pnew = [&](int j) {
+      const double zj = JAC ? mul(invd[j], rr_[j]) : rr_[j];
+      return add(zj, mul(beta, pold[j]));
+    };
     double pq[1] = {0.0};
-    for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
-      const double qi = sell_row64(a, i, a.p);
-      a.q[i] = qi;
-      pq[0] += mul(a.p[i], qi);
+    if (it == 0) {
+      for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
+        const double qi = sell_row64(a, i, [&](int j) { return a.p0[j]; });
+        a.q[i] = qi;
+        pq[0] += mul(a.p0[i], qi);
+      }
+    } else {
+      for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
+        const double pi = pnew(i);
+        pcur[i] = pi;
+        const double qi = sell_row64(a, i, pnew);
+        a.q[i] = qi;
+        pq[0] += mul(pi, qi);
+      }
     }
     if (!grid_allreduce<1>(pq, a.g, set, epoch)) return;
     set ^= 1;
@@ -579,11 +605,11 @@ __global__ void __launch_bounds__(kPT, 1) cg64_kernel(Cg64Args a) {
     // 2: x += alpha p, r -= alpha q, <r, r>, <r, D^-1 r>  (OpCgUpdate)
     double rr[2] = {0.0, 0.0};
     for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
-      a.x[i] = add(mul(alpha, a.p[i]), a.x[i]);
+      a.x[i] = add(mul(alpha, pcur[i]), a.x[i]);
       const double ri = sub(a.r[i], mul(alpha, a.q[i]));
       a.r[i] = ri;
       rr[0] += mul(ri, ri);
-      if (JAC) rr[1] += mul(ri, mul(a.invd[i], ri));
+      if (JAC) rr[1] += mul(ri, mul(invd[i], ri));
     }
     if (!grid_allreduce<2>(rr, a.g, set, epoch)) return;
     set ^= 1;
@@ -595,12 +621,6 @@ __global__ void __launch_bounds__(kPT, 1) cg64_kernel(Cg64Args a) {
     const double rz_new = JAC ? rr[1] : rr[0];
     beta = rz_new / rz;
     rz = rz_new;
-    // 3: p = D^-1 r + beta p                              (OpCgDirection)
-    for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
-      const double zi = JAC ? mul(a.invd[i], a.r[i]) : a.r[i];
-      a.p[i] = add(zi, mul(beta, a.p[i]));
-    }
-    if (!grid_barrier(a.g.sync, epoch, a.g.wait_ns, a.g.bias)) return;
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     sc->iters = it;
@@ -936,7 +956,7 @@ bool cg64_persistent_ok(sk_matrix A) {
          coop_grid(A, reinterpret_cast<const void*>(&cg64_kernel<false>)) > 0;
 }
 
-sk_status cg64_persistent(sk_matrix A, const double* b, double* x, double* r, double* p, double* q,
+sk_status cg64_persistent(sk_matrix A, const double* b, double* x, double* r, double* p0, double* p1, double* q,
                           const double* invd, double* hist, Scalars* sc, void* scratch, cudaStream_t st) {
   SK_CHECK(cg64_persistent_ok(A), SK_NOT_SUPPORTED, "persistent CG needs a small FP64 CSR handle with SELL-32");
   const auto& C = A->csr;
@@ -961,7 +981,8 @@ sk_status cg64_persistent(sk_matrix A, const double* b, double* x, double* r, do
   a.b = b;
   a.x = x;
   a.r = r;
-  a.p = p;
+  a.p0 = p0;
+  a.p1 = p1;
   a.q = q;
   a.invd = invd;
   a.hist = hist;

@@ -54,11 +54,11 @@ bool cg64_persistent_ok(sk_matrix A);
 
 // Runs the whole solve: sc holds bnorm, tol and max_iters on entry and
 // iters, converged, done, rnorm, rz, alpha, beta and hist_len on exit; r,
-// p, q are work vectors of n values; invd is the Jacobi inverse diagonal
+// p0, p1, q are work vectors of n values; invd is the Jacobi inverse diagonal
 // or null; hist receives one residual norm per step when not null; scratch
 // holds inner_persistent_scratch(A) bytes.  Synchronous; SK_TIMEOUT when a
 // grid barrier wait runs out.
-sk_status cg64_persistent(sk_matrix A, const double* b, double* x, double* r, double* p, double* q,
+sk_status cg64_persistent(sk_matrix A, const double* b, double* x, double* r, double* p0, double* p1, double* q,
                           const double* invd, double* hist, Scalars* sc, void* scratch, cudaStream_t st);
 
 }  // namespace sk

@@ -470,8 +470,8 @@ static sk_status cg_solve(sk_matrix A, sk_precond L, sk_precond R, const T* b, T
   if constexpr (std::is_same<T, double>::value) {
     if (cg64) {
       const double* invd = L ? static_cast<const double*>(L->inv_diag) : nullptr;
-      if ((s = cg64_persistent(A, b, x, r, p, q, invd, cfg->collect_residuals ? c.hist : nullptr, c.sc, pscratch,
-                               st)) != SK_OK)
+      if ((s = cg64_persistent(A, b, x, r, p, hatp, q, invd, cfg->collect_residuals ? c.hist : nullptr, c.sc,
+                               pscratch, st)) != SK_OK)
         return s;
       return finish_summary(c, st, out, history_host);
     }
