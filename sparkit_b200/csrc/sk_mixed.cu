@@ -525,8 +525,8 @@ struct Cg64Args {
 };
 
 // (A v)_i with v_j = f(j), each row summed in storage order
-template <class F>
-__device__ __forceinline__ double sell_row64(Cg64Args const& a, int i, F const& f) {
+template <class Args, class F>
+__device__ __forceinline__ double sell_row64(Args const& a, int i, F const& f) {
   const int len = __ldg(a.g.len + i);
   const int base = __ldg(a.g.off + (i >> 5)) + (i & 31);
   double sum = 0.0;
@@ -631,6 +631,336 @@ __global__ void __launch_bounds__(kPT, 1) cg64_kernel(Cg64Args a) {
     sc->alpha = alpha;
     sc->beta = beta;
     sc->hist_len = a.hist ? it : 0;
+  }
+}
+
+// ------------------------------------------------------------------
+// Plain FP64 BiCGSTAB (bicgstab.hpp:93-361 with identity or Jacobi on
+// each side) as one cooperative launch for the same small systems.  Per
+// step, behind three grid-wide reductions:
+//   A  p = r + beta (p - omega v) and p_hat = M_R M_L p for the CTA's rows
+//      into the other half of double buffers, v = A p_hat with every
+//      gathered p_hat_j recomputed from r_j and the previous p_j, v_j;
+//      <r_hat, v>                        -> alpha, or SK_BREAKDOWN at 0
+//   B  s = r - alpha v, s_hat = M s, t = A s_hat (s_hat_j recomputed from
+//      r_j, v_j); ||s||^2, <t, t>, <t, s> -> the half-step test, omega
+//   C  x += alpha p_hat + omega s_hat, r = s - omega t; ||r||^2,
+//      <r_hat, r>                        -> the full-step test, rho
+// mirroring the per-step kernels (OpBiP, EpiBiV, OpBiS, OpBiHalfOrS,
+// EpiBiT, OpBiUpdate): the same element arithmetic, iteration counting,
+// history entries (one per half step), omega = 0 skip and breakdowns;
+// only the order in which the dot products' partial sums meet differs.
+// ------------------------------------------------------------------
+struct Bi64Args {
+  PArgs g;  // n, off, len, col (SELL-32), slots, sync, wait_ns, bias
+  const double* val;
+  const double* b;
+  double* x;
+  double* r;
+  double* r_hat;
+  double* p[2];
+  double* v[2];
+  double* p_hat;
+  double* s;
+  double* s_hat;
+  double* t;
+  const double* invl;  // Jacobi left: 1 / a_ii, or null
+  const double* invr;  // Jacobi right, or null
+  double* hist;
+  Scalars* sc;
+};
+
+__global__ void __launch_bounds__(kPT, 1) bi64_kernel(Bi64Args a) {
+  unsigned epoch = 0;
+  const int n = a.g.n;
+  const int per = (((n + gridDim.x - 1) / gridDim.x) + 31) & ~31;
+  const int r0 = min(n, static_cast<int>(blockIdx.x) * per), r1 = min(n, r0 + per);
+  Scalars* sc = a.sc;
+  const double bnorm = sc->bnorm, tol = sc->tol;
+  const long long max_iters = sc->max_iters;
+  const double* __restrict__ invl = a.invl;
+  const double* __restrict__ invr = a.invr;
+  auto hat = [&](int j, double v) {  // M_R M_L v, in that order (OpBiP, OpBiHalfOrS)
+    if (invl) v = mul(invl[j], v);
+    if (invr) v = mul(invr[j], v);
+    return v;
+  };
+  const double* x0 = a.x;
+  // compute_initial_residual, r_hat = r, rho_new = <r, r>   (EpiBiResid)
+  double v1[1] = {0.0};
+  for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
+    const double ri = sub(a.b[i], sell_row64(a, i, [&](int j) { return x0[j]; }));
+    a.r[i] = ri;
+    a.r_hat[i] = ri;
+    a.p[0][i] = 0.0;
+    a.v[0][i] = 0.0;
+    v1[0] += mul(ri, ri);
+  }
+  if (!grid_allreduce<1>(v1, a.g, 0, epoch)) return;
+  double rho_new = v1[0], rho = 1.0, alpha = 1.0, omega = 1.0;
+  long long iters = 0, hist_len = 0;
+  int converged = 0, status = 0;
+  int set = 1;
+  double last = 0.0;
+  auto record = [&](double v) {
+    if (a.hist && blockIdx.x == 0 && threadIdx.x == 0) a.hist[hist_len] = v;
+    ++hist_len;
+    last = v;
+  };
+  bool done = max_iters <= 0;
+  if (!done && rho_new == 0.0) {
+    converged = 1;
+    done = true;
+  }
+  const long long max_steps = max_iters > 1 ? max_iters : 1;
+  for (long long step = 0; !done && step < max_steps; ++step) {
+    const int cur = static_cast<int>(step & 1);
+    const double* __restrict__ pold = a.p[cur];
+    const double* __restrict__ vold = a.v[cur];
+    double* pnew = a.p[cur ^ 1];
+    double* vnew = a.v[cur ^ 1];
+    const double beta = (rho_new / rho) * (alpha / omega);
+    const double* __restrict__ rr_ = a.r;
+    auto p_of = [&](int j) { return add(rr_[j], mul(beta, sub(pold[j], mul(omega, vold[j])))); };
+    // A: p, p_hat, v = A p_hat, <r_hat, v>
+    double rv[1] = {0.0};
+    for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
+      const double pi = p_of(i);
+      pnew[i] = pi;
+      a.p_hat[i] = hat(i, pi);
+      const double vi = sell_row64(a, i, [&](int j) { return hat(j, p_of(j)); });
+      vnew[i] = vi;
+      rv[0] += mul(a.r_hat[i], vi);
+    }
+    if (!grid_allreduce<1>(rv, a.g, set, epoch)) return;
+    set ^= 1;
+    ++iters;
+    if (rv[0] == 0.0) {
+      status = SK_BREAKDOWN;
+      break;
+    }
+    alpha = rho_new / rv[0];
+    // B: s, s_hat, t = A s_hat, ||s||^2, <t, t>, <t, s>
+    const double* __restrict__ vn = vnew;
+    auto s_of = [&](int j) { return sub(rr_[j], mul(alpha, vn[j])); };
+    double st[3] = {0.0, 0.0, 0.0};
+    for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
+      const double si = s_of(i);
+      a.s[i] = si;
+      a.s_hat[i] = hat(i, si);
+      const double ti = sell_row64(a, i, [&](int j) { return hat(j, s_of(j)); });
+      a.t[i] = ti;
+      st[0] += mul(si, si);
+      st[1] += mul(ti, ti);
+      st[2] += mul(ti, si);
+    }
+    if (!grid_allreduce<3>(st, a.g, set, epoch)) return;
+    set ^= 1;
+    const double sn = sqrt(st[0]);
+    record(sn);
+    if (sn / bnorm < tol) {  // half step converged: x += alpha p_hat (OpBiHalfOrS)
+      for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) a.x[i] = add(a.x[i], mul(alpha, a.p_hat[i]));
+      converged = 1;
+      break;
+    }
+    ++iters;
+    const double tt = st[1];
+    omega = tt == 0.0 ? 0.0 : st[2] / tt;
+    const bool skip = omega == 0.0;
+    // C: x, r, ||r||^2, <r_hat, r>
+    double rr[2] = {0.0, 0.0};
+    if (!skip) {
+      for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
+        a.x[i] = add(a.x[i], add(mul(alpha, a.p_hat[i]), mul(omega, a.s_hat[i])));
+        const double ri = sub(a.s[i], mul(omega, a.t[i]));
+        a.r[i] = ri;
+        rr[0] += mul(ri, ri);
+        rr[1] += mul(a.r_hat[i], ri);
+      }
+    }
+    if (!grid_allreduce<2>(rr, a.g, set, epoch)) return;
+    set ^= 1;
+    if (!skip) {
+      rho = rho_new;
+      const double rn = sqrt(rr[0]);
+      record(rn);
+      if (rn / bnorm < tol) {
+        converged = 1;
+        break;
+      }
+      rho_new = rr[1];
+    }
+    if (iters >= max_iters) break;
+    if (rho_new == 0.0) {
+      status = SK_BREAKDOWN;
+      break;
+    }
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    sc->iters = iters;
+    sc->converged = converged;
+    sc->status = status;
+    sc->done = 1;
+    sc->rho = rho;
+    sc->rho_new = rho_new;
+    sc->alpha = alpha;
+    sc->omega = omega;
+    sc->hist_len = a.hist ? hist_len : 0;
+    sc->rnorm = last;
+    sc->half = 0;
+    sc->skip = 0;
+  }
+}
+
+// ------------------------------------------------------------------
+// Plain FP64 CGS (cgs.hpp:106-395 with identity or Jacobi on each side)
+// as one cooperative launch for the same small systems.  Per step, behind
+// two grid-wide reductions:
+//   A  the previous step's direction update (u = r + beta q,
+//      p = u + beta (q + beta p), skipped after rho_new = 0) for the
+//      CTA's rows into the other half of a double-buffered p, and
+//      q_hat = A M p with every gathered p_j recomputed from r_j, q_j and
+//      the previous p_j; <r_hat, q_hat>               -> alpha
+//   B  q = u - alpha q_hat, u_hat = M (u + q), x += alpha u_hat, and
+//      r -= alpha A u_hat with every gathered u_hat_j recomputed from u_j
+//      and q_hat_j; ||r||^2, <r_hat, r>   -> the test, rho, beta, skip
+// mirroring the per-step kernels (OpLR, EpiCgsQhat, OpCgsQ, EpiCgsR,
+// OpCgsDir): the same element arithmetic, iteration counting (two per
+// step) and history; only the order in which the dot products' partial
+// sums meet differs.
+// ------------------------------------------------------------------
+struct Cgs64Args {
+  PArgs g;  // n, off, len, col (SELL-32), slots, sync, wait_ns, bias
+  const double* val;
+  const double* b;
+  double* x;
+  double* r;
+  double* r_hat;
+  double* p[2];
+  double* u;
+  double* q;
+  double* q_hat;
+  const double* invl;  // Jacobi left: 1 / a_ii, or null
+  const double* invr;  // Jacobi right, or null
+  double* hist;
+  Scalars* sc;
+};
+
+__global__ void __launch_bounds__(kPT, 1) cgs64_kernel(Cgs64Args a) {
+  unsigned epoch = 0;
+  const int n = a.g.n;
+  const int per = (((n + gridDim.x - 1) / gridDim.x) + 31) & ~31;
+  const int r0 = min(n, static_cast<int>(blockIdx.x) * per), r1 = min(n, r0 + per);
+  Scalars* sc = a.sc;
+  const double bnorm = sc->bnorm, tol = sc->tol;
+  const long long max_iters = sc->max_iters;
+  const double* __restrict__ invl = a.invl;
+  const double* __restrict__ invr = a.invr;
+  auto hat = [&](int j, double v) {  // M_R M_L v, in that order (OpLR, OpCgsQ)
+    if (invl) v = mul(invl[j], v);
+    if (invr) v = mul(invr[j], v);
+    return v;
+  };
+  const double* x0 = a.x;
+  // compute_initial_residual: r = r_hat = p = u = b - A x, rho = <r, r>  (EpiCgsInit)
+  double v1[1] = {0.0};
+  for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
+    const double ri = sub(a.b[i], sell_row64(a, i, [&](int j) { return x0[j]; }));
+    a.r[i] = ri;
+    a.r_hat[i] = ri;
+    a.p[0][i] = ri;
+    a.u[i] = ri;
+    v1[0] += mul(ri, ri);
+  }
+  if (!grid_allreduce<1>(v1, a.g, 0, epoch)) return;
+  double rho = v1[0], alpha = 0.0, beta = 0.0, last = 0.0;
+  long long iters = 0, hist_len = 0;
+  int converged = 0, skip = 0;
+  int set = 1, cur = 0;
+  bool upd = false;  // the previous step left a direction update to apply
+  bool done = max_iters <= 0;
+  while (!done) {
+    const double* __restrict__ pold = a.p[cur];
+    double* pnew = a.p[cur ^ 1];
+    const double* __restrict__ rr_ = a.r;
+    const double* __restrict__ qq_ = a.q;
+    const bool up = upd;
+    const double bt = beta;
+    auto p_of = [&](int j) {  // OpCgsDir
+      if (!up) return pold[j];
+      const double uj = add(rr_[j], mul(bt, qq_[j]));
+      return add(uj, mul(bt, add(qq_[j], mul(bt, pold[j]))));
+    };
+    // A: direction update, q_hat = A M p, <r_hat, q_hat>
+    double rq[1] = {0.0};
+    for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
+      if (up) {
+        a.u[i] = add(rr_[i], mul(bt, qq_[i]));
+        pnew[i] = p_of(i);
+      }
+      const double qh = sell_row64(a, i, [&](int j) { return hat(j, p_of(j)); });
+      a.q_hat[i] = qh;
+      rq[0] += mul(a.r_hat[i], qh);
+    }
+    if (!grid_allreduce<1>(rq, a.g, set, epoch)) return;
+    set ^= 1;
+    if (up) cur ^= 1;
+    alpha = rho / rq[0];
+    // B: q, u_hat, x, r -= alpha A u_hat, ||r||^2, <r_hat, r>
+    const double* __restrict__ uu_ = a.u;
+    const double* __restrict__ qh_ = a.q_hat;
+    const double al = alpha;
+    auto uhat_of = [&](int j) {  // OpCgsQ
+      const double qj = sub(uu_[j], mul(al, qh_[j]));
+      return hat(j, add(uu_[j], qj));
+    };
+    double rr[2] = {0.0, 0.0};
+    for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
+      const double ui = uu_[i];
+      const double qi = sub(ui, mul(al, qh_[i]));
+      const double uh = hat(i, add(ui, qi));
+      a.x[i] = add(a.x[i], mul(al, uh));
+      const double au = sell_row64(a, i, uhat_of);
+      a.q[i] = qi;
+      const double ri = sub(rr_[i], mul(al, au));
+      a.r[i] = ri;
+      rr[0] += mul(ri, ri);
+      rr[1] += mul(a.r_hat[i], ri);
+    }
+    if (!grid_allreduce<2>(rr, a.g, set, epoch)) return;
+    set ^= 1;
+    // EpiCgsR
+    iters += 2;
+    const double rn = sqrt(rr[0]);
+    if (a.hist && blockIdx.x == 0 && threadIdx.x == 0) a.hist[hist_len] = rn;
+    ++hist_len;
+    last = rn;
+    if (rn / bnorm < tol) {
+      converged = 1;
+      break;
+    }
+    const double rho_new = rr[1];
+    if (rho_new == 0.0) {
+      skip = 1;
+      upd = false;
+    } else {
+      skip = 0;
+      beta = rho_new / rho;
+      rho = rho_new;
+      upd = true;
+    }
+    if (iters >= max_iters) done = true;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    sc->iters = iters;
+    sc->converged = converged;
+    sc->done = 1;
+    sc->rho = rho;
+    sc->alpha = alpha;
+    sc->beta = beta;
+    sc->skip = skip;
+    sc->hist_len = a.hist ? hist_len : 0;
+    sc->rnorm = last;
   }
 }
 
@@ -994,6 +1324,107 @@ sk_status cg64_persistent(sk_matrix A, const double* b, double* x, double* r, do
   SK_CUDA(cudaMemcpyAsync(&err, &sync->err, sizeof(int), cudaMemcpyDeviceToHost, st));
   SK_CUDA(cudaStreamSynchronize(st));
   if (err) return fail(SK_TIMEOUT, "persistent CG: a grid barrier wait ran out");
+  return SK_OK;
+}
+
+bool bi64_persistent_ok(sk_matrix A) {
+  if (!cg64_persistent_ok(A)) return false;
+  return coop_grid(A, reinterpret_cast<const void*>(&bi64_kernel)) > 0;
+}
+
+sk_status bi64_persistent(sk_matrix A, const double* b, double* x, double* const* vec, const double* invl,
+                          const double* invr, double* hist, Scalars* sc, void* scratch, cudaStream_t st) {
+  SK_CHECK(bi64_persistent_ok(A), SK_NOT_SUPPORTED, "persistent BiCGSTAB needs a small FP64 CSR handle with SELL-32");
+  const auto& C = A->csr;
+  int grid = std::min(A->sm_count, kPT);
+  const int need = ceil_div(A->nrow, 32);
+  if (grid > need) grid = need;
+  SyncWords* sync = static_cast<SyncWords*>(scratch);
+  double* slots = reinterpret_cast<double*>(static_cast<char*>(scratch) + 256);
+  SK_CUDA(cudaMemsetAsync(sync, 0, sizeof(SyncWords), st));
+  Bi64Args a{};
+  a.g.n = static_cast<int>(A->nrow);
+  a.g.off = C.sell_off;
+  a.g.len = C.sell_len;
+  a.g.col = C.sell_col;
+  a.g.slots = slots;
+  a.g.sync = sync;
+  a.g.wait_ns = wait_limit_ns();
+  a.g.bias = wait_target_bias();
+  a.val = static_cast<const double*>(C.sell_vals);
+  a.b = b;
+  a.x = x;
+  a.r = vec[0];
+  a.r_hat = vec[1];
+  a.p[0] = vec[2];
+  a.p[1] = vec[3];
+  a.v[0] = vec[4];
+  a.v[1] = vec[5];
+  a.p_hat = vec[6];
+  a.s = vec[7];
+  a.s_hat = vec[8];
+  a.t = vec[9];
+  a.invl = invl;
+  a.invr = invr;
+  a.hist = hist;
+  a.sc = sc;
+  void* params[] = {&a};
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  SK_CUDA(cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(&bi64_kernel), dim3(grid), dim3(kPT), params, 0,
+                                      st));
+  int err = 0;
+  SK_CUDA(cudaMemcpyAsync(&err, &sync->err, sizeof(int), cudaMemcpyDeviceToHost, st));
+  SK_CUDA(cudaStreamSynchronize(st));
+  if (err) return fail(SK_TIMEOUT, "persistent BiCGSTAB: a grid barrier wait ran out");
+  return SK_OK;
+}
+
+bool cgs64_persistent_ok(sk_matrix A) {
+  if (!cg64_persistent_ok(A)) return false;
+  return coop_grid(A, reinterpret_cast<const void*>(&cgs64_kernel)) > 0;
+}
+
+sk_status cgs64_persistent(sk_matrix A, const double* b, double* x, double* const* vec, const double* invl,
+                           const double* invr, double* hist, Scalars* sc, void* scratch, cudaStream_t st) {
+  SK_CHECK(cgs64_persistent_ok(A), SK_NOT_SUPPORTED, "persistent CGS needs a small FP64 CSR handle with SELL-32");
+  const auto& C = A->csr;
+  int grid = std::min(A->sm_count, kPT);
+  const int need = ceil_div(A->nrow, 32);
+  if (grid > need) grid = need;
+  SyncWords* sync = static_cast<SyncWords*>(scratch);
+  double* slots = reinterpret_cast<double*>(static_cast<char*>(scratch) + 256);
+  SK_CUDA(cudaMemsetAsync(sync, 0, sizeof(SyncWords), st));
+  Cgs64Args a{};
+  a.g.n = static_cast<int>(A->nrow);
+  a.g.off = C.sell_off;
+  a.g.len = C.sell_len;
+  a.g.col = C.sell_col;
+  a.g.slots = slots;
+  a.g.sync = sync;
+  a.g.wait_ns = wait_limit_ns();
+  a.g.bias = wait_target_bias();
+  a.val = static_cast<const double*>(C.sell_vals);
+  a.b = b;
+  a.x = x;
+  a.r = vec[0];
+  a.r_hat = vec[1];
+  a.p[0] = vec[2];
+  a.p[1] = vec[3];
+  a.u = vec[4];
+  a.q = vec[5];
+  a.q_hat = vec[6];
+  a.invl = invl;
+  a.invr = invr;
+  a.hist = hist;
+  a.sc = sc;
+  void* params[] = {&a};
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  SK_CUDA(cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(&cgs64_kernel), dim3(grid), dim3(kPT), params, 0,
+                                      st));
+  int err = 0;
+  SK_CUDA(cudaMemcpyAsync(&err, &sync->err, sizeof(int), cudaMemcpyDeviceToHost, st));
+  SK_CUDA(cudaStreamSynchronize(st));
+  if (err) return fail(SK_TIMEOUT, "persistent CGS: a grid barrier wait ran out");
   return SK_OK;
 }
 

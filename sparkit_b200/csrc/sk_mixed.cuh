@@ -61,4 +61,32 @@ bool cg64_persistent_ok(sk_matrix A);
 sk_status cg64_persistent(sk_matrix A, const double* b, double* x, double* r, double* p0, double* p1, double* q,
                           const double* invd, double* hist, Scalars* sc, void* scratch, cudaStream_t st);
 
+// Plain FP64 BiCGSTAB (identity or Jacobi on either side) as one
+// cooperative launch, under the same conditions as cg64_persistent_ok.
+bool bi64_persistent_ok(sk_matrix A);
+
+// Runs the whole solve: sc holds bnorm, tol and max_iters on entry and
+// iters, converged, status, done, rnorm, rho, rho_new, alpha, omega and
+// hist_len on exit; vec holds ten work vectors of n values (r, r_hat, two
+// p, two v, p_hat, s, s_hat, t); invl / invr are the Jacobi inverse
+// diagonals or null; hist receives one norm per half step when not null;
+// scratch holds inner_persistent_scratch(A) bytes.  Synchronous;
+// SK_TIMEOUT when a grid barrier wait runs out.
+sk_status bi64_persistent(sk_matrix A, const double* b, double* x, double* const* vec, const double* invl,
+                          const double* invr, double* hist, Scalars* sc, void* scratch, cudaStream_t st);
+
+// Plain FP64 CGS (identity or Jacobi on either side) as one cooperative
+// launch, under the same conditions as cg64_persistent_ok.
+bool cgs64_persistent_ok(sk_matrix A);
+
+// Runs the whole solve: sc holds bnorm, tol and max_iters on entry and
+// iters, converged, done, rnorm, rho, alpha, beta, skip and hist_len on
+// exit; vec holds seven work vectors of n values (r, r_hat, two p, u, q,
+// q_hat); invl / invr are the Jacobi inverse diagonals or null; hist
+// receives one norm per step when not null; scratch holds
+// inner_persistent_scratch(A) bytes.  Synchronous; SK_TIMEOUT when a grid
+// barrier wait runs out.
+sk_status cgs64_persistent(sk_matrix A, const double* b, double* x, double* const* vec, const double* invl,
+                           const double* invr, double* hist, Scalars* sc, void* scratch, cudaStream_t st);
+
 }  // namespace sk

@@ -804,7 +804,13 @@ static sk_status bicgstab_solve(sk_matrix A, sk_precond L, sk_precond R, const T
   SolveCommon c;
   std::vector<char*> vv;
   const i64 hist_cap = cfg->collect_residuals ? cfg->max_iterations + 2 : 0;
-  sk_status s = carve_common(A, st, 9, vb, 0, hist_cap, &c, &vv, nullptr);
+  // FP64 with identity / Jacobi sides on a small SELL handle: the whole
+  // solve in one cooperative launch (sk_mixed.cu)
+  const bool bi64 = std::is_same<T, double>::value && (!L || L->kind == 1) && (!R || R->kind == 1) &&
+                    bi64_persistent_ok(A);
+  const size_t pextra = bi64 ? (inner_persistent_scratch(A) + 511) & ~size_t(511) : 0;
+  char* pscratch = nullptr;
+  sk_status s = carve_common(A, st, bi64 ? 10 : 9, vb, pextra, hist_cap, &c, &vv, bi64 ? &pscratch : nullptr);
   if (s != SK_OK) return s;
   T *r = (T*)vv[0], *r_hat = (T*)vv[1], *p = (T*)vv[2], *v = (T*)vv[3], *sv = (T*)vv[4],
     *t = (T*)vv[5], *p_hat = (T*)vv[6], *s_hat = (T*)vv[7], *tmp = (T*)vv[8];
@@ -823,6 +829,17 @@ static sk_status bicgstab_solve(sk_matrix A, sk_precond L, sk_precond R, const T
   h.max_iters = cfg->max_iterations;
   h.hist_on = cfg->collect_residuals ? 1 : 0;
   if ((s = put_scalars(c.sc, h, st)) != SK_OK) return s;
+  if constexpr (std::is_same<T, double>::value) {
+    if (bi64) {
+      double* vec[10] = {r, r_hat, p, tmp, v, (double*)vv[9], p_hat, sv, s_hat, t};
+      const double* invl = L ? static_cast<const double*>(L->inv_diag) : nullptr;
+      const double* invr = R ? static_cast<const double*>(R->inv_diag) : nullptr;
+      if ((s = bi64_persistent(A, b, x, vec, invl, invr, cfg->collect_residuals ? c.hist : nullptr, c.sc, pscratch,
+                               st)) != SK_OK)
+        return s;
+      return finish_summary(c, st, out, history_host);
+    }
+  }
   SK_CUDA(cudaMemsetAsync(p, 0, n * sizeof(T), st));  // :173-174
   SK_CUDA(cudaMemsetAsync(v, 0, n * sizeof(T), st));
   launch_spmv<T>(A, x, EpiBiResid<T>{b, r, r_hat, c.sc}, c.ws, nullptr, st);
@@ -1548,7 +1565,13 @@ static sk_status cgs_solve(sk_matrix A, sk_precond L, sk_precond R, const T* b, 
   SolveCommon c;
   std::vector<char*> vv;
   const i64 hist_cap = cfg->collect_residuals ? cfg->max_iterations / 2 + 4 : 0;
-  sk_status s = carve_common(A, st, 9, vb, 0, hist_cap, &c, &vv, nullptr);
+  // FP64 with identity / Jacobi sides on a small SELL handle: the whole
+  // solve in one cooperative launch (sk_mixed.cu)
+  const bool c64 = std::is_same<T, double>::value && (!L || L->kind == 1) && (!R || R->kind == 1) &&
+                   cgs64_persistent_ok(A);
+  const size_t pextra = c64 ? (inner_persistent_scratch(A) + 511) & ~size_t(511) : 0;
+  char* pscratch = nullptr;
+  sk_status s = carve_common(A, st, 9, vb, pextra, hist_cap, &c, &vv, c64 ? &pscratch : nullptr);
   if (s != SK_OK) return s;
   T *r = (T*)vv[0], *r_hat = (T*)vv[1], *p = (T*)vv[2], *u = (T*)vv[3], *q = (T*)vv[4], *q_hat = (T*)vv[5],
     *u_hat = (T*)vv[6], *p_hat = (T*)vv[7], *tmp = (T*)vv[8];
@@ -1568,6 +1591,17 @@ static sk_status cgs_solve(sk_matrix A, sk_precond L, sk_precond R, const T* b, 
   h.hist_on = cfg->collect_residuals ? 1 : 0;
   h.done = cfg->max_iterations <= 0 ? 1 : 0;
   if ((s = put_scalars(c.sc, h, st)) != SK_OK) return s;
+  if constexpr (std::is_same<T, double>::value) {
+    if (c64) {
+      double* vec[7] = {r, r_hat, p, tmp, u, q, q_hat};
+      const double* invl = L ? static_cast<const double*>(L->inv_diag) : nullptr;
+      const double* invr = R ? static_cast<const double*>(R->inv_diag) : nullptr;
+      if ((s = cgs64_persistent(A, b, x, vec, invl, invr, cfg->collect_residuals ? c.hist : nullptr, c.sc, pscratch,
+                                st)) != SK_OK)
+        return s;
+      return finish_summary(c, st, out, history_host);
+    }
+  }
   launch_spmv<T>(A, x, EpiCgsInit<T>{b, r, r_hat, p, u, c.sc}, c.ws, nullptr, st);
   const LRPair<T> lr(L, R);
   const bool graphs = capturable(L) && capturable(R);
