@@ -269,6 +269,7 @@ struct sk_precond_s {
   // its grid_nx x grid_ny grid (d, w, e, s, n, 1/d; float)
   sk_net_s* net = nullptr;
   float* coef = nullptr;
+  void* xfeat = nullptr;  // BF16 [grid][8]: the fixed input channels (w, e, s, n over d)
   sk::i64 grid_nx = 0, grid_ny = 0;
   // two-level (kind 4): smoother (not owned), agg x agg aggregates of the
   // grid, the dense inverse of the Galerkin coarse operator (coarse_n^2,

@@ -232,26 +232,38 @@ struct ConvArgs {
   float* outf;          // OUT_F32: channel 0 only, [B][H][W]
   double* outz;         // OUT_Z64: z = s[b] * (float)(acc0 + bias0)
   const double* scale;  // OUT_Z64: s per sample
+  int z_add;            // OUT_Z64: z += s[b] * (float)(acc0 + bias0) instead
+  // first layer of an apply (one sample): channel 0 of the staged input
+  // planes replaced by the feature v * (1/d) / s, computed from these
+  const double* feat_v;
+  const float* feat_inv;
+  const double* feat_s;
   int* err;
 };
 
-// Thread = output pixel (x, y) of sample b with its N accumulators v (the
-// bias already added).  All threads of the CTA call it (the 2x2 pooling exchanges values between the
+// Thread = output pixel (x, y) of sample b with the NC accumulators v of
+// channels c0 .. c0 + NC - 1 of its N (the bias already added).  All
+// threads of the CTA call it (the 2x2 pooling exchanges values between the
 // lanes of a warp: x + 1 is lane + 1, y + 1 is lane + 8).
-template <int N, bool UP>
-__device__ __forceinline__ void conv_epilogue(ConvArgs const& a, int b, int y, int x, const float* v) {
+template <int N, bool UP, int NC = N>
+__device__ __forceinline__ void conv_epilogue(ConvArgs const& a, int b, int y, int x, const float* v, int c0 = 0) {
   const bool valid = y < a.H && x < a.W;
   const i64 p = (static_cast<i64>(b) * a.H + y) * a.W + x;
   if (a.out_kind == OUT_F32) {
-    if (valid) a.outf[p] = v[0];
+    if (valid && c0 == 0) a.outf[p] = v[0];
     return;
   }
   if (a.out_kind == OUT_Z64) {
-    if (valid) a.outz[p] = a.scale[b] * static_cast<double>(v[0]);
+    if (valid && c0 == 0) {
+      const double zv = a.scale[b] * static_cast<double>(v[0]);
+      a.outz[p] = a.z_add ? __dadd_rn(a.outz[p], zv) : zv;
+    }
     return;
   }
-  uint4* __restrict__ dst = reinterpret_cast<uint4*>(a.out + p * N);
-  const uint4* __restrict__ msk = (a.mask && valid) ? reinterpret_cast<const uint4*>(a.mask + p * N) : nullptr;
+  const int q0 = c0 / 8;  // first 16-byte channel group of this thread
+  uint4* __restrict__ dst = reinterpret_cast<uint4*>(a.out + p * N) + q0;
+  const uint4* __restrict__ msk =
+      (a.mask && valid) ? reinterpret_cast<const uint4*>(a.mask + p * N) + q0 : nullptr;
   const bool pool_writer = valid && ((x & 1) == 0) && ((y & 1) == 0);
   const int h2 = a.H / 2, w2 = a.W / 2;
   // the reads of the epilogue (mask, the skip vectors of the four upsampled
@@ -260,9 +272,9 @@ __device__ __forceinline__ void conv_epilogue(ConvArgs const& a, int b, int y, i
   // following the stores one by one
   const bool up = UP && valid;
   const uint4* __restrict__ skip = reinterpret_cast<const uint4*>(a.up_skip);
-  constexpr int G = N / 8 < 4 ? N / 8 : 4;
+  constexpr int G = NC / 8 < 4 ? NC / 8 : 4;
 #pragma unroll
-  for (int cb = 0; cb < N / 8; cb += G) {
+  for (int cb = 0; cb < NC / 8; cb += G) {
     uint4 skv[UP ? G : 1][4];
     uint4 mvv[G];
 #pragma unroll
@@ -272,7 +284,7 @@ __device__ __forceinline__ void conv_epilogue(ConvArgs const& a, int b, int y, i
 #pragma unroll
         for (int d = 0; d < 4; ++d) {
           const i64 fp = (static_cast<i64>(b) * 2 * a.H + 2 * y + (d >> 1)) * (2 * a.W) + 2 * x + (d & 1);
-          skv[g][d] = up ? __ldg(skip + fp * (N / 8) + cb + g) : make_uint4(0, 0, 0, 0);
+          skv[g][d] = up ? __ldg(skip + fp * (N / 8) + q0 + cb + g) : make_uint4(0, 0, 0, 0);
         }
       }
     }
@@ -302,7 +314,7 @@ __device__ __forceinline__ void conv_epilogue(ConvArgs const& a, int b, int y, i
           q[j] = 0.25f * ((r[j] + r01) + (r10 + r11));
         }
         if (pool_writer)
-          reinterpret_cast<uint4*>(a.pool_out)[((static_cast<i64>(b) * h2 + y / 2) * w2 + x / 2) * (N / 8) + c] =
+          reinterpret_cast<uint4*>(a.pool_out)[((static_cast<i64>(b) * h2 + y / 2) * w2 + x / 2) * (N / 8) + q0 + c] =
               pack8(q);
       }
       if constexpr (UP) {
@@ -314,7 +326,7 @@ __device__ __forceinline__ void conv_epilogue(ConvArgs const& a, int b, int y, i
           unpack8(skv[g][d], sk);
 #pragma unroll
           for (int j = 0; j < 8; ++j) u[j] = r[j] + sk[j];
-          reinterpret_cast<uint4*>(a.up_out)[fp * (N / 8) + c] = pack8(u);
+          reinterpret_cast<uint4*>(a.up_out)[fp * (N / 8) + q0 + c] = pack8(u);
         }
         }
       }
@@ -352,14 +364,14 @@ __device__ __forceinline__ void conv_issue_mma(uint32_t pbase, uint32_t wbase, u
   }
 }
 
-// Shared memory of one conv CTA.
-template <int CIN, int N, bool TC>
+// Shared memory of one conv CTA (TM tiles side by side along x).
+template <int CIN, int N, bool TC, int TM = 1>
 struct ConvSmem {
   static constexpr int kPlanes = CIN / 8;
   static constexpr int kKC = (9 * CIN / 8 + 1) & ~1;
   static constexpr int kWBytes = kKC * (N / 8) * 128;
   static constexpr int kIn = 0;
-  static constexpr int kW = kPlanes * kPlaneStride;
+  static constexpr int kW = TM * kPlanes * kPlaneStride;
   static constexpr int kStage = kW + kWBytes;  // mma.sync path only: [128][N + 4] floats
   static constexpr int kBar = kStage + (TC ? 0 : 128 * (N + 4) * 4);
   static constexpr int kBytes = kBar + 64;
@@ -368,11 +380,24 @@ struct ConvSmem {
 // TC = true: tcgen05 (product path); false: the same tile with mma.sync
 // (cross-check of the tcgen05 path in the tests).  UP: the epilogue also
 // writes the upsampled sum with the skip tensor (a.up_out); the other
-// layers leave out its registers.
-template <int CIN, int N, bool TC, bool UP>
-__global__ void __launch_bounds__(kConvThreads) conv3x3_kernel(const __grid_constant__ CUtensorMap in_map,
-                                                               ConvArgs a) {
-  using S = ConvSmem<CIN, N, TC>;
+// layers leave out its registers.  TM: 16 x 8 tiles per CTA side by side
+// along x (tcgen05 only), each with its own TMEM accumulator columns, so
+// that the full-resolution layers fit in one wave of resident CTAs.  CS:
+// threads per pixel (tcgen05 only); with CS = 2 the second 128 threads read
+// the upper half of the accumulator columns of the same TMEM lanes and run
+// the epilogue of those channels, which halves each thread's chain of
+// upsample-and-add loads and stores.  FEAT: the first layer of an apply
+// (8 input channels, one sample) computes channel 0 of its input, the
+// scaled vector v / d / s, into the staged planes itself; the other
+// channels come from a tensor that holds the matrix's fixed features.
+template <int CIN, int N, bool TC, bool UP, int TM = 1, int CS = 1, bool FEAT = false>
+__global__ void __launch_bounds__(kConvThreads * CS) conv3x3_kernel(const __grid_constant__ CUtensorMap in_map,
+                                                                    ConvArgs a) {
+  static_assert(TC || TM == 1, "several tiles per CTA only on the tcgen05 path");
+  static_assert(!FEAT || (CIN == 8 && TC), "fused features only for the first layer on the tcgen05 path");
+  static_assert(CS == 1 || (TC && N / CS >= 16), "channel split only on the tcgen05 path, 16 columns or more");
+  constexpr int NC = N / CS;
+  using S = ConvSmem<CIN, N, TC, TM>;
   extern __shared__ __align__(1024) unsigned char smem[];
   unsigned char* planes = smem + S::kIn;
   unsigned char* wsm = smem + S::kW;
@@ -383,8 +408,9 @@ __global__ void __launch_bounds__(kConvThreads) conv3x3_kernel(const __grid_cons
   __shared__ float s_bias[N];
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int x0 = blockIdx.x * kTileW, y0 = blockIdx.y * kTileH, b = blockIdx.z;
-  constexpr uint32_t kCols = N < 32 ? 32 : N;
+  const int px = tid & (kConvThreads - 1), cbase = (tid / kConvThreads) * NC;  // pixel, first channel
+  const int x0 = blockIdx.x * kTileW * TM, y0 = blockIdx.y * kTileH, b = blockIdx.z;
+  constexpr uint32_t kCols = TM * N < 32 ? 32 : TM * N;
 
   // Launched as a programmatic dependent of the previous layer: this CTA
   // sets up (barriers, tensor memory), then lets the next layer launch, and
@@ -408,38 +434,70 @@ __global__ void __launch_bounds__(kConvThreads) conv3x3_kernel(const __grid_cons
   // (a single-channel output has one bias value)
   if (tid < N) s_bias[tid] = a.bias && (a.out_kind == OUT_BF16 || tid == 0) ? __ldg(a.bias + tid) : 0.0f;
   if (tid == 0) {
-    mbar_expect_tx(bar_load, S::kPlanes * kPlaneBytes + S::kWBytes);
-    for (int c = 0; c < S::kPlanes; ++c)
-      tma_load_4d(planes + c * kPlaneStride, &in_map, c * 8, x0 - 1, y0 - 1, b, bar_load);
+    mbar_expect_tx(bar_load, TM * S::kPlanes * kPlaneBytes + S::kWBytes);
+    for (int t = 0; t < TM; ++t)
+      for (int c = 0; c < S::kPlanes; ++c)
+        tma_load_4d(planes + (t * S::kPlanes + c) * kPlaneStride, &in_map, c * 8, x0 + t * kTileW - 1, y0 - 1, b,
+                    bar_load);
     bulk_load(wsm, a.wpk, S::kWBytes, bar_load);
   }
   if (tid == 0) ok_load = mbar_wait(bar_load, 0, a.err, 1) ? 1 : 0;
   __syncthreads();
   const bool ok = ok_load != 0;
+  if constexpr (FEAT) {
+    // channel 0 of every halo pixel: (float)(v * (double)(1/d) / s) in BF16,
+    // zero outside the grid (the convolution's padding) or for s = 0
+    if (ok) {
+      const double sb = *a.feat_s;
+      for (int idx = tid; idx < TM * kHaloH * kHaloW; idx += blockDim.x) {
+        const int t = idx / (kHaloH * kHaloW), h = idx % (kHaloH * kHaloW);
+        const int gy = y0 - 1 + h / kHaloW, gx = x0 + t * kTileW - 1 + h % kHaloW;
+        float f = 0.0f;
+        if (gy >= 0 && gy < a.H && gx >= 0 && gx < a.W && sb > 0.0) {
+          const i64 p = static_cast<i64>(gy) * a.W + gx;
+          f = static_cast<float>(a.feat_v[p] * static_cast<double>(a.feat_inv[p]) / sb);
+        }
+        *reinterpret_cast<bf16*>(planes + t * S::kPlanes * kPlaneStride + h * 16) = __float2bfloat16_rn(f);
+      }
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // visible to the tensor cores
+    }
+    __syncthreads();
+  }
 
-  float v[N];
+  float v[NC];
   if constexpr (TC) {
     uint32_t tmem = 0;
     tc_fence_after();
     tmem = *tmem_slot;
     bool mma_ok = ok;
     if (tid == 0 && ok) {
-      conv_issue_mma<CIN, N>(smem_u32(planes), smem_u32(wsm), tmem);
+#pragma unroll
+      for (int t = 0; t < TM; ++t)
+        conv_issue_mma<CIN, N>(smem_u32(planes) + t * S::kPlanes * kPlaneStride, smem_u32(wsm), tmem + t * N);
       umma_commit(bar_mma);
     }
     __syncthreads();
     if (ok) mma_ok = mbar_wait(bar_mma, 0, a.err, 2);
     mma_ok = __syncthreads_and(mma_ok ? 1 : 0) != 0;
     tc_fence_after();
-    if (mma_ok) {
-      const uint32_t row = tmem + (static_cast<uint32_t>(warp * 32) << 16);
+    // warp w reads TMEM lanes 32 (w % 4) .. 32 (w % 4) + 31
+    const uint32_t row = tmem + (static_cast<uint32_t>((warp & 3) * 32) << 16);
+#pragma unroll 1
+    for (int t = 0; t < TM && mma_ok; ++t) {
 #pragma unroll
-      for (int c = 0; c < N / 16; ++c) {
-        float t[16];
-        tmem_ld16(row + c * 16, t);
+      for (int c = 0; c < NC / 16; ++c) {
+        float u[16];
+        tmem_ld16(row + t * N + cbase + c * 16, u);
         tmem_ld_wait();
 #pragma unroll
-        for (int j = 0; j < 16; ++j) v[c * 16 + j] = t[j];
+        for (int j = 0; j < 16; ++j) v[c * 16 + j] = u[j];
+      }
+      if (t + 1 < TM) {  // the earlier tiles' epilogues; the last one runs below
+        if (a.bias) {
+#pragma unroll
+          for (int j = 0; j < NC; ++j) v[j] += s_bias[cbase + j];
+        }
+        conv_epilogue<N, UP, NC>(a, b, y0 + (px >> 3), x0 + t * kTileW + (px & 7), v, cbase);
       }
     }
     tc_fence_before();
@@ -504,9 +562,9 @@ __global__ void __launch_bounds__(kConvThreads) conv3x3_kernel(const __grid_cons
   }
   if (a.bias) {
 #pragma unroll
-    for (int j = 0; j < N; ++j) v[j] += s_bias[j];
+    for (int j = 0; j < NC; ++j) v[j] += s_bias[cbase + j];
   }
-  conv_epilogue<N, UP>(a, b, y0 + (tid >> 3), x0 + (tid & 7), v);
+  conv_epilogue<N, UP, NC>(a, b, y0 + (px >> 3), x0 + (TM - 1) * kTileW + (px & 7), v, cbase);
 }
 
 // ------------------------------------------------------------------
@@ -766,6 +824,22 @@ __global__ void features_kernel(SampleSrc src, int B, const double* s, bf16* x) 
     for (int k = 0; k < 4; ++k) f[1 + k] = __fmul_rn(cf[(1 + k) * src.P + p], inv);
     f[5] = f[6] = f[7] = 0.0f;
     reinterpret_cast<uint4*>(x)[i] = pack8(f);
+  }
+}
+
+// x[p][0..7] (BF16) of one instance: 0, w/d, e/d, s/d, n/d, 0, 0, 0 -- the
+// features that do not depend on the vector (features_kernel's channels
+// 1-4, bit for bit); the first convolution of an apply fills channel 0.
+__global__ void fixed_features_kernel(const float* cf, i64 P, bf16* x) {
+  for (i64 p = blockIdx.x * static_cast<i64>(blockDim.x) + threadIdx.x; p < P;
+       p += static_cast<i64>(gridDim.x) * blockDim.x) {
+    const float inv = cf[5 * P + p];
+    float f[8];
+    f[0] = 0.0f;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) f[1 + k] = __fmul_rn(cf[(1 + k) * P + p], inv);
+    f[5] = f[6] = f[7] = 0.0f;
+    reinterpret_cast<uint4*>(x)[p] = pack8(f);
   }
 }
 
@@ -1051,24 +1125,51 @@ struct MapCache {
   }
 };
 
+// More tiles than this many CTAs per SM could hold at once: the layers
+// with 16 output channels take two tiles per CTA (one wave instead of two).
+constexpr int kConvWaveCtas = 8 * 148;
+
 template <int CIN, int N, bool TC>
 static sk_status launch_conv(MapCache& mc, const void* in, ConvArgs const& a, cudaStream_t st) {
-  using S = ConvSmem<CIN, N, TC>;
   CUtensorMap m;
   sk_status s = mc.get(in, a.B, a.H, a.W, CIN, kHaloW, kHaloH, &m);
   if (s != SK_OK) return s;
-  const auto kernel = a.up_out ? conv3x3_kernel<CIN, N, TC, true> : conv3x3_kernel<CIN, N, TC, false>;
-  if (!attr_once(kernel, S::kBytes)) return fail(SK_CUDA_ERROR, "cudaFuncSetAttribute");
+  const int ntiles = ceil_div(a.W, kTileW) * ceil_div(a.H, kTileH) * a.B;
+  int tm = 1, cs = 1;
+  auto kernel = a.up_out ? conv3x3_kernel<CIN, N, TC, true> : conv3x3_kernel<CIN, N, TC, false>;
+  int bytes = ConvSmem<CIN, N, TC>::kBytes;
+  if constexpr (TC && N == 16) {
+    if (!a.up_out && ntiles > kConvWaveCtas) {
+      tm = 2;
+      kernel = conv3x3_kernel<CIN, N, TC, false, 2>;
+      bytes = ConvSmem<CIN, N, TC, 2>::kBytes;
+    }
+  }
+  if constexpr (TC && N >= 32) {  // the upsample-and-add epilogue split over two threads per pixel
+    if (a.up_out) {
+      cs = 2;
+      kernel = conv3x3_kernel<CIN, N, TC, true, 1, 2>;
+    }
+  }
+  if (a.feat_v) {
+    if constexpr (TC && CIN == 8 && N == 16) {
+      SK_CHECK(a.B == 1 && !a.up_out, SK_INVALID_ARG, "fused features take one sample");
+      kernel = tm == 2 ? conv3x3_kernel<CIN, N, TC, false, 2, 1, true> : conv3x3_kernel<CIN, N, TC, false, 1, 1, true>;
+    } else {
+      return fail(SK_NOT_SUPPORTED, "fused features only in the first layer on the tcgen05 path");
+    }
+  }
+  if (!attr_once(kernel, bytes)) return fail(SK_CUDA_ERROR, "cudaFuncSetAttribute");
   // programmatic dependent launch: the set-up of this layer's CTAs (barrier
   // init, tensor-memory allocation) overlaps the tail of the previous one
   cudaLaunchAttribute attr[1];
   attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
   attr[0].val.programmaticStreamSerializationAllowed = 1;
-  const int ntx = ceil_div(a.W, kTileW), nty = ceil_div(a.H, kTileH);
+  const int ntx = ceil_div(a.W, kTileW * tm), nty = ceil_div(a.H, kTileH);
   cudaLaunchConfig_t cfg{};
   cfg.gridDim = dim3(ntx, nty, a.B);
-  cfg.blockDim = dim3(kConvThreads);
-  cfg.dynamicSmemBytes = S::kBytes;
+  cfg.blockDim = dim3(kConvThreads * cs);
+  cfg.dynamicSmemBytes = bytes;
   cfg.stream = st;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
@@ -1312,7 +1413,7 @@ static sk_status run_wgrad(sk_net N, int l, const bf16* x, const bf16* g, int H,
 // Forward pass from N->x0; the last layer writes per `last`.  Pooling and
 // the upsample-and-add of the skip connections run in the epilogues of the
 // convolutions that produce their inputs.
-static sk_status net_forward(sk_net N, ConvArgs last) {
+static sk_status net_forward(sk_net N, ConvArgs last, const bf16* xin = nullptr, const ConvArgs* feat = nullptr) {
   const int H = N->H, W = N->W, H1 = H / 2, W1 = W / 2, H2 = H / 4, W2 = W / 4, H3 = H / 8, W3 = W / 8;
   sk_status s;
   auto fwd = [&](int l, const bf16* in, int h, int w, bf16* out, bf16* pool, const bf16* skip, bf16* up) {
@@ -1323,9 +1424,14 @@ static sk_status net_forward(sk_net N, ConvArgs last) {
     a.pool_out = pool;
     a.up_skip = skip;
     a.up_out = up;
+    if (l == 0 && feat) {
+      a.feat_v = feat->feat_v;
+      a.feat_inv = feat->feat_inv;
+      a.feat_s = feat->feat_s;
+    }
     return run_conv(N, l, in, h, w, a);
   };
-  if ((s = fwd(0, N->x0, H, W, N->e0, N->p0, nullptr, nullptr)) != SK_OK) return s;
+  if ((s = fwd(0, xin ? xin : N->x0, H, W, N->e0, N->p0, nullptr, nullptr)) != SK_OK) return s;
   if ((s = fwd(1, N->p0, H1, W1, N->e1, N->p1, nullptr, nullptr)) != SK_OK) return s;
   if ((s = fwd(2, N->p1, H2, W2, N->e2, N->p2, nullptr, nullptr)) != SK_OK) return s;
   if ((s = fwd(3, N->p2, H3, W3, N->e3, nullptr, nullptr, nullptr)) != SK_OK) return s;
@@ -1445,6 +1551,20 @@ static sk_status net_step_grad(sk_net N, sk_pairs D, const int* idx_dev, int B, 
 namespace sk {
 
 sk_status learned_apply(const sk_precond_s* M, const double* v, double* z, cudaStream_t st) {
+  return learned_apply_ex(M, v, z, st, false, false);
+}
+
+double* learned_scale_slot(const sk_precond_s* M) {
+  sk_net N = M->net;
+  if (net_workspace(N, 1, static_cast<int>(M->grid_ny), static_cast<int>(M->grid_nx)) != SK_OK) return nullptr;
+  return N->s;
+}
+
+// On the tcgen05 path the first convolution computes the scaled vector
+// channel itself (the other input channels are the matrix's, fixed at
+// creation), so an apply is the scale reduction and the nine convolutions.
+sk_status learned_apply_ex(const sk_precond_s* M, const double* v, double* z, cudaStream_t st, bool add,
+                           bool scale_ready) {
   sk_net N = M->net;
   N->stream = st;
   sk_status s = net_workspace(N, 1, static_cast<int>(M->grid_ny), static_cast<int>(M->grid_nx));
@@ -1453,12 +1573,23 @@ sk_status learned_apply(const sk_precond_s* M, const double* v, double* z, cudaS
   src.v64 = v;
   src.coef = M->coef;
   src.P = M->n;
-  net_features(N, src, 1);
+  if (!scale_ready)
+    SK_LAUNCH(scale_kernel, dim3(kRedBlocks, 1), kThreads, 0, N->stream, src, N->red, N->counter, N->s);
   ConvArgs last{};
   last.out_kind = OUT_Z64;
   last.outz = z;
   last.scale = N->s;
-  s = net_forward(N, last);
+  last.z_add = add ? 1 : 0;
+  if (!N->legacy_mma && M->xfeat) {
+    ConvArgs f{};
+    f.feat_v = v;
+    f.feat_inv = M->coef + 5 * M->n;
+    f.feat_s = N->s;
+    s = net_forward(N, last, static_cast<const bf16*>(M->xfeat), &f);
+  } else {
+    SK_LAUNCH(features_kernel, ew_grid(src.P), 256, 0, N->stream, src, 1, N->s, N->x0);
+    s = net_forward(N, last);
+  }
   if (s != SK_OK && N->host_err == SK_OK) N->host_err = s;
   return s;
 }
@@ -1469,6 +1600,20 @@ static sk_status conv_attrs() {
   auto both = [&](auto k_plain, auto k_up, int bytes) { ok = ok && attr_once(k_plain, bytes) && attr_once(k_up, bytes); };
 #define SK_CONV_ATTR(CI, NN) \
   both(conv3x3_kernel<CI, NN, TC, false>, conv3x3_kernel<CI, NN, TC, true>, ConvSmem<CI, NN, TC>::kBytes);
+  if constexpr (TC) {
+    ok = ok && attr_once(conv3x3_kernel<8, 16, TC, false, 2>, ConvSmem<8, 16, TC, 2>::kBytes) &&
+         attr_once(conv3x3_kernel<16, 16, TC, false, 2>, ConvSmem<16, 16, TC, 2>::kBytes) &&
+         attr_once(conv3x3_kernel<32, 16, TC, false, 2>, ConvSmem<32, 16, TC, 2>::kBytes) &&
+         attr_once(conv3x3_kernel<8, 16, TC, false, 1, 1, true>, ConvSmem<8, 16, TC>::kBytes) &&
+         attr_once(conv3x3_kernel<8, 16, TC, false, 2, 1, true>, ConvSmem<8, 16, TC, 2>::kBytes);
+#define SK_CONV_ATTR_CS(CI, NN) \
+  ok = ok && attr_once(conv3x3_kernel<CI, NN, TC, true, 1, 2>, ConvSmem<CI, NN, TC>::kBytes);
+    SK_CONV_ATTR_CS(16, 32)
+    SK_CONV_ATTR_CS(32, 64)
+    SK_CONV_ATTR_CS(64, 32)
+    SK_CONV_ATTR_CS(64, 64)
+#undef SK_CONV_ATTR_CS
+  }
   SK_CONV_ATTR(8, 16)
   SK_CONV_ATTR(16, 16)
   SK_CONV_ATTR(16, 32)
@@ -1492,6 +1637,8 @@ sk_status learned_prepare(const sk_precond_s* M) {
 void learned_release(sk_precond_s* M) {
   if (M->coef) cudaFree(M->coef);
   M->coef = nullptr;
+  if (M->xfeat) cudaFree(M->xfeat);
+  M->xfeat = nullptr;
 }
 
 }  // namespace sk
@@ -1801,6 +1948,13 @@ sk_status sk_learned_create(sk_precond* out, sk_matrix A, sk_net net, int64_t nx
     return cuda_fail(e, "cudaMalloc (planes)");
   }
   sk_status s = grid_planes(A, nx, ny, M->coef, A->stream);
+  if (s == SK_OK && cudaMalloc(&M->xfeat, static_cast<size_t>(nx) * ny * 16) != cudaSuccess)
+    s = fail(SK_OUT_OF_MEMORY, "cudaMalloc (fixed features)");
+  if (s == SK_OK) {
+    SK_LAUNCH(fixed_features_kernel, ew_grid(M->n), 256, 0, A->stream, M->coef, M->n,
+              static_cast<bf16*>(M->xfeat));
+    if (cudaGetLastError() != cudaSuccess) s = fail(SK_CUDA_ERROR, "fixed features");
+  }
   if (s != SK_OK) {
     learned_release(M);
     delete M;

@@ -35,7 +35,9 @@
 #include <vector>
 
 #include "sk_kernels.cuh"
+#include "sk_learned.cuh"
 #include "sk_twolevel.cuh"
+#include "sk_vec.cuh"
 
 namespace sk {
 namespace {
@@ -48,6 +50,39 @@ struct EpiResidStore {
   const double* r;
   double* t;
   __device__ void operator()(int row, double az, double*) const { t[row] = __dsub_rn(r[row], az); }
+  __device__ void finalize(const double*) const {}
+};
+
+// t = r - A z and, for a learned smoother, its input scale
+// s = sqrt(mean((t / d)^2)) in the same pass (the network's scale
+// reduction, summed in this product's fixed order)
+struct EpiResidScale {
+  static constexpr int kNR = 1;
+  const double* r;
+  double* t;
+  const float* inv;  // 1 / d per cell
+  double* s_out;
+  double P;
+  __device__ void operator()(int row, double az, double* red) const {
+    const double ti = __dsub_rn(r[row], az);
+    t[row] = ti;
+    const double rt = ti * static_cast<double>(inv[row]);
+    red[0] += rt * rt;
+  }
+  __device__ void finalize(const double* tot) const { *s_out = sqrt(tot[0] / P); }
+};
+
+// z += D^-1 t: the Jacobi smoother's apply and its addition in one pass,
+// with the bits of the two (z = z + (inv_d * t))
+struct OpJacobiAdd {
+  static constexpr int kNR = 0;
+  struct In { double d, t, z; };
+  const double* inv_d;
+  const double* t;
+  double* z;
+  __device__ bool prepare(const Scalars* sc) { return !solve_done(sc); }
+  __device__ In load(i64 i) const { return {inv_d[i], t[i], z[i]}; }
+  __device__ void apply(i64 i, In const& v, double*) const { z[i] = __dadd_rn(v.z, __dmul_rn(v.d, v.t)); }
   __device__ void finalize(const double*) const {}
 };
 
@@ -178,7 +213,22 @@ void twolevel_apply(const sk_precond_s* M, const double* r, double* z, RedWs ws,
     SK_LAUNCH(prolong_kernel, ew_blocks(n), kThreads, 0, st, n, nx, agg, mcx, M->zc, nullptr, set, z, sc);
   };
   auto smooth_add = [&]() {  // z += S(r - A z)
+    if (S->kind == 3 && ws.partials && ws.capacity >= spmv_grid(A)) {
+      // learned: the scale reduction in the residual product, and the last
+      // convolution adds its output into z
+      double* sd = learned_scale_slot(S);
+      if (sd) {
+        launch_spmv<double>(A, z, EpiResidScale{r, M->tbuf, S->coef + 5 * n, sd, static_cast<double>(n)}, ws, sc,
+                            st);
+        if (learned_apply_ex(S, M->tbuf, z, st, true, true) != SK_OK) set_error("learned smoother apply failed");
+        return;
+      }
+    }
     launch_spmv<double>(A, z, EpiResidStore{r, M->tbuf}, RedWs{}, sc, st);
+    if (S->kind == 1) {
+      launch_vec(n, OpJacobiAdd{static_cast<const double*>(S->inv_diag), M->tbuf, z}, ws, sc, st);
+      return;
+    }
     precond_apply_dispatch(S, SK_F64, n, M->tbuf, M->tbuf2, ws, sc, st);
     SK_LAUNCH(prolong_kernel, ew_blocks(n), kThreads, 0, st, n, nx, agg, mcx, nullptr, M->tbuf2, 0, z, sc);
   };

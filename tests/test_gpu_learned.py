@@ -47,11 +47,13 @@ def rect_convdiff(nx, ny, seed):
     return matgen._stencil_csr(n, cand, vals, valid, np.float64)
 
 
-@pytest.mark.parametrize("nx,ny", [(64, 64), (48, 80), (256, 256), (320, 272)])
+@pytest.mark.parametrize("nx,ny", [(64, 64), (48, 80), (256, 256), (320, 272), (392, 400), (512, 512)])
 def test_planes_and_forward_match_oracle(gpu_lib, oracle, torch, nx, ny):
-    """The network's apply against the oracle's forward pass.  At 256^2 and
-    320 x 272 the full-resolution layers have more than two tiles per SM
-    and run the persistent, pipelined convolution."""
+    """The network's apply against the oracle's forward pass.  At 392 x 400
+    and 512^2 the full-resolution layers have more tiles than one wave of
+    resident CTAs and take two tiles per CTA (at 392 the last CTA of each
+    row has its second tile wholly outside the grid); every size runs the
+    first layer with the vector channel computed in the kernel."""
     A = matgen.convdiff_2d_grf(nx, seed=11)[0] if nx == ny else rect_convdiff(nx, ny, 3)
     Ad = gpu.Device_matrix(A)
     net = gpu.Net(seed=5)
