@@ -964,6 +964,179 @@ __global__ void __launch_bounds__(kPT, 1) cgs64_kernel(Cgs64Args a) {
   }
 }
 
+// ------------------------------------------------------------------
+// Plain FP64 MINRES (minres.hpp:106-418 with identity or Jacobi on each
+// side) as one cooperative launch for the same small systems.  Per step,
+// behind two grid-wide reductions:
+//   A  the previous step's update_solution and rotate_state for the CTA's
+//      rows (d, x; z = q / beta, v_prev = v, v = w / beta), and
+//      w = A z with every gathered z_j recomputed from q_j;
+//      <z, w>                                              -> alpha
+//   B  w -= alpha v + beta v_prev, q = M_R M_L w; <w, q> -> beta_new, the
+//      Givens rotation, the test and the scalars of rotate_state
+// mirroring the per-step kernels (EpiMinInit, OpMinScale, EpiMinW,
+// OpMinLanczos, min_step_finalize, OpMinUpdate): the same element and
+// scalar arithmetic, iteration counting and history; q holds what the
+// per-step form writes into v_prev before the rotation.  Only the order in
+// which the dot products' partial sums meet differs.
+// ------------------------------------------------------------------
+struct Min64Args {
+  PArgs g;  // n, off, len, col (SELL-32), slots, sync, wait_ns, bias
+  const double* val;
+  const double* b;
+  double* x;
+  double* v;
+  double* vp;
+  double* z;
+  double* w;
+  double* q;
+  double* d;
+  double* dp;
+  const double* invl;  // Jacobi left: 1 / a_ii, or null
+  const double* invr;  // Jacobi right, or null
+  double* hist;
+  Scalars* sc;
+};
+
+__global__ void __launch_bounds__(kPT, 1) min64_kernel(Min64Args a) {
+  unsigned epoch = 0;
+  const int n = a.g.n;
+  const int per = (((n + gridDim.x - 1) / gridDim.x) + 31) & ~31;
+  const int r0 = min(n, static_cast<int>(blockIdx.x) * per), r1 = min(n, r0 + per);
+  Scalars* sc = a.sc;
+  const double bnorm = sc->bnorm, tol = sc->tol;
+  const long long max_iters = sc->max_iters;
+  const double* __restrict__ invl = a.invl;
+  const double* __restrict__ invr = a.invr;
+  auto hat = [&](int j, double v) {  // M_R M_L v, in that order
+    if (invl) v = mul(invl[j], v);
+    if (invr) v = mul(invr[j], v);
+    return v;
+  };
+  const double* x0 = a.x;
+  // compute_initial_residual: v = b - A x, z = M v, beta = sqrt(<v, z>)
+  double v1[1] = {0.0};
+  for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
+    const double vi = sub(a.b[i], sell_row64(a, i, [&](int j) { return x0[j]; }));
+    const double zi = hat(i, vi);
+    a.v[i] = vi;
+    a.z[i] = zi;
+    a.vp[i] = 0.0;
+    a.d[i] = 0.0;
+    a.dp[i] = 0.0;
+    v1[0] += mul(vi, zi);
+  }
+  if (!grid_allreduce<1>(v1, a.g, 0, epoch)) return;
+  int set = 1;
+  double beta = sqrt(v1[0]);
+  double alpha = 0.0, eps = 0.0, delta = 0.0, rho = 0.0, phi = 0.0, phi_bar = beta;
+  double cs_prev = 1.0, sn_prev = 0.0, cs = 1.0, sn = 0.0, cs_new = 0.0, sn_new = 0.0, inv_bn = 0.0;
+  long long iters = 0, hist_len = 0;
+  int converged = 0;
+  double last = 0.0;
+  bool done = false;
+  if (beta == 0.0) {
+    converged = 1;
+    done = true;
+  } else {
+    inv_bn = dvd(1.0, beta);
+    for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) {  // OpMinScale
+      a.v[i] = mul(a.v[i], inv_bn);
+      a.z[i] = mul(a.z[i], inv_bn);
+    }
+    double none[1] = {0.0};  // the scaled z is gathered by the first product
+    if (!grid_allreduce<1>(none, a.g, set, epoch)) return;
+    set ^= 1;
+  }
+  if (max_iters <= 0) done = true;
+  bool pending = false, rotate = false;
+  // update_solution and rotate_state of the step just taken, for row i
+  auto update_row = [&](int i) {
+    const double dn = dvd(sub(sub(a.z[i], mul(delta, a.d[i])), mul(eps, a.dp[i])), rho);
+    a.dp[i] = a.d[i];
+    a.d[i] = dn;
+    a.x[i] = add(a.x[i], mul(phi, dn));
+    if (rotate) {
+      a.z[i] = mul(a.q[i], inv_bn);
+      a.vp[i] = a.v[i];
+      a.v[i] = mul(a.w[i], inv_bn);
+    } else {
+      a.vp[i] = a.q[i];
+    }
+  };
+  while (!done) {
+    // A: the pending update, w = A z, <z, w>
+    const bool up = pending, rot = rotate;
+    const double ib = inv_bn;
+    const double* __restrict__ qq = a.q;
+    const double* zz = a.z;
+    double zw[1] = {0.0};
+    for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
+      if (up) update_row(i);
+      const double wi = sell_row64(a, i, [&](int j) { return up && rot ? mul(qq[j], ib) : zz[j]; });
+      a.w[i] = wi;
+      zw[0] += mul(a.z[i], wi);
+    }
+    if (!grid_allreduce<1>(zw, a.g, set, epoch)) return;
+    set ^= 1;
+    pending = false;
+    alpha = zw[0];
+    // B: the Lanczos vector, q = M w, <w, q>
+    double wq[1] = {0.0};
+    for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
+      const double wi = sub(a.w[i], add(mul(alpha, a.v[i]), mul(beta, a.vp[i])));
+      const double qi = hat(i, wi);
+      a.w[i] = wi;
+      a.q[i] = qi;
+      wq[0] += mul(wi, qi);
+    }
+    if (!grid_allreduce<1>(wq, a.g, set, epoch)) return;
+    set ^= 1;
+    // min_step_finalize
+    const double beta_new = sqrt(wq[0]);
+    eps = mul(sn_prev, beta);
+    const double delta_1 = mul(cs_prev, beta);
+    const double dl = add(mul(cs, delta_1), mul(sn, alpha));
+    const double rho_bar = add(mul(-sn, delta_1), mul(cs, alpha));
+    const double rh = sqrt(add(mul(rho_bar, rho_bar), mul(beta_new, beta_new)));
+    if (rh != 0.0) {
+      cs_new = dvd(rho_bar, rh);
+      sn_new = dvd(beta_new, rh);
+      phi = mul(cs_new, phi_bar);
+      phi_bar = mul(-sn_new, phi_bar);
+      rho = rh;
+      delta = dl;
+    }
+    pending = true;
+    const double res = fabs(phi_bar);
+    if (a.hist && blockIdx.x == 0 && threadIdx.x == 0) a.hist[hist_len] = res;
+    ++hist_len;
+    last = res;
+    const bool conv = res / bnorm < tol;
+    converged = conv ? 1 : 0;
+    iters += 1;
+    rotate = !conv && beta_new != 0.0;
+    if (rotate) {
+      inv_bn = dvd(1.0, beta_new);
+      cs_prev = cs;
+      sn_prev = sn;
+      cs = cs_new;
+      sn = sn_new;
+      beta = beta_new;
+    }
+    if (conv || iters >= max_iters) done = true;
+  }
+  if (pending)
+    for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) update_row(i);
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    sc->iters = iters;
+    sc->converged = converged;
+    sc->done = 1;
+    sc->hist_len = a.hist ? hist_len : 0;
+    sc->rnorm = last;
+  }
+}
+
 // CTAs of the cooperative grid (0: the kernel does not fit).
 int coop_grid(sk_matrix A, const void* k) {
   int per_sm = 0;
@@ -1425,6 +1598,55 @@ sk_status cgs64_persistent(sk_matrix A, const double* b, double* x, double* cons
   SK_CUDA(cudaMemcpyAsync(&err, &sync->err, sizeof(int), cudaMemcpyDeviceToHost, st));
   SK_CUDA(cudaStreamSynchronize(st));
   if (err) return fail(SK_TIMEOUT, "persistent CGS: a grid barrier wait ran out");
+  return SK_OK;
+}
+
+bool min64_persistent_ok(sk_matrix A) {
+  if (!cg64_persistent_ok(A)) return false;
+  return coop_grid(A, reinterpret_cast<const void*>(&min64_kernel)) > 0;
+}
+
+sk_status min64_persistent(sk_matrix A, const double* b, double* x, double* const* vec, const double* invl,
+                           const double* invr, double* hist, Scalars* sc, void* scratch, cudaStream_t st) {
+  SK_CHECK(min64_persistent_ok(A), SK_NOT_SUPPORTED, "persistent MINRES needs a small FP64 CSR handle with SELL-32");
+  const auto& C = A->csr;
+  int grid = std::min(A->sm_count, kPT);
+  const int need = ceil_div(A->nrow, 32);
+  if (grid > need) grid = need;
+  SyncWords* sync = static_cast<SyncWords*>(scratch);
+  double* slots = reinterpret_cast<double*>(static_cast<char*>(scratch) + 256);
+  SK_CUDA(cudaMemsetAsync(sync, 0, sizeof(SyncWords), st));
+  Min64Args a{};
+  a.g.n = static_cast<int>(A->nrow);
+  a.g.off = C.sell_off;
+  a.g.len = C.sell_len;
+  a.g.col = C.sell_col;
+  a.g.slots = slots;
+  a.g.sync = sync;
+  a.g.wait_ns = wait_limit_ns();
+  a.g.bias = wait_target_bias();
+  a.val = static_cast<const double*>(C.sell_vals);
+  a.b = b;
+  a.x = x;
+  a.v = vec[0];
+  a.vp = vec[1];
+  a.z = vec[2];
+  a.w = vec[3];
+  a.q = vec[4];
+  a.d = vec[5];
+  a.dp = vec[6];
+  a.invl = invl;
+  a.invr = invr;
+  a.hist = hist;
+  a.sc = sc;
+  void* params[] = {&a};
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  SK_CUDA(cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(&min64_kernel), dim3(grid), dim3(kPT), params, 0,
+                                      st));
+  int err = 0;
+  SK_CUDA(cudaMemcpyAsync(&err, &sync->err, sizeof(int), cudaMemcpyDeviceToHost, st));
+  SK_CUDA(cudaStreamSynchronize(st));
+  if (err) return fail(SK_TIMEOUT, "persistent MINRES: a grid barrier wait ran out");
   return SK_OK;
 }
 

@@ -89,4 +89,17 @@ bool cgs64_persistent_ok(sk_matrix A);
 sk_status cgs64_persistent(sk_matrix A, const double* b, double* x, double* const* vec, const double* invl,
                            const double* invr, double* hist, Scalars* sc, void* scratch, cudaStream_t st);
 
+// Plain FP64 MINRES (identity or Jacobi on either side) as one
+// cooperative launch, under the same conditions as cg64_persistent_ok.
+bool min64_persistent_ok(sk_matrix A);
+
+// Runs the whole solve: sc holds bnorm, tol and max_iters on entry and
+// iters, converged, done, rnorm and hist_len on exit; vec holds seven work
+// vectors of n values (v, v_prev, z, w, q, d, d_prev); invl / invr are the
+// Jacobi inverse diagonals or null; hist receives one norm per step when
+// not null; scratch holds inner_persistent_scratch(A) bytes.  Synchronous;
+// SK_TIMEOUT when a grid barrier wait runs out.
+sk_status min64_persistent(sk_matrix A, const double* b, double* x, double* const* vec, const double* invl,
+                           const double* invr, double* hist, Scalars* sc, void* scratch, cudaStream_t st);
+
 }  // namespace sk

@@ -1887,7 +1887,12 @@ static sk_status minres_solve(sk_matrix A, sk_precond L, sk_precond R, const T* 
   std::vector<char*> vv;
   char* extra = nullptr;
   const i64 hist_cap = cfg->collect_residuals ? cfg->max_iterations + 2 : 0;
-  sk_status s = carve_common(A, st, 7, vb, sizeof(MinScalars) + 256, hist_cap, &c, &vv, &extra);
+  // FP64 with identity / Jacobi sides on a small SELL handle: the whole
+  // solve in one cooperative launch (sk_mixed.cu)
+  const bool m64 = std::is_same<T, double>::value && (!L || L->kind == 1) && (!R || R->kind == 1) &&
+                   min64_persistent_ok(A);
+  const size_t pextra = m64 ? (inner_persistent_scratch(A) + 511) & ~size_t(511) : 0;
+  sk_status s = carve_common(A, st, 7, vb, sizeof(MinScalars) + 512 + pextra, hist_cap, &c, &vv, &extra);
   if (s != SK_OK) return s;
   T *vp = (T*)vv[0], *v = (T*)vv[1], *z = (T*)vv[2], *w = (T*)vv[3], *tmp = (T*)vv[4], *dp = (T*)vv[5],
     *d = (T*)vv[6];
@@ -1907,6 +1912,18 @@ static sk_status minres_solve(sk_matrix A, sk_precond L, sk_precond R, const T* 
   h.max_iters = cfg->max_iterations;
   h.hist_on = cfg->collect_residuals ? 1 : 0;
   if ((s = put_scalars(c.sc, h, st)) != SK_OK) return s;
+  if constexpr (std::is_same<T, double>::value) {
+    if (m64) {
+      double* vec[7] = {v, vp, z, w, tmp, d, dp};
+      const double* invl = L ? static_cast<const double*>(L->inv_diag) : nullptr;
+      const double* invr = R ? static_cast<const double*>(R->inv_diag) : nullptr;
+      char* pscratch = extra + ((sizeof(MinScalars) + 255) & ~size_t(255)) + 256;
+      if ((s = min64_persistent(A, b, x, vec, invl, invr, cfg->collect_residuals ? c.hist : nullptr, c.sc, pscratch,
+                                st)) != SK_OK)
+        return s;
+      return finish_summary(c, st, out, history_host);
+    }
+  }
   SK_CUDA(cudaMemsetAsync(ms, 0, sizeof(MinScalars), st));
   for (T* vec : {vp, d, dp}) SK_CUDA(cudaMemsetAsync(vec, 0, n * sizeof(T), st));  // :144-158
   const LRPair<T> lr(L, R);

@@ -361,3 +361,30 @@ def test_small_bicgstab_cgs_run_as_one_launch(gpu_lib, oracle, solver, sides):
     assert s.iteration_residuals[-1] / np.linalg.norm(b) < 1e-10
     bound = 1e-8 if specs[0] else 1e-9
     assert np.linalg.norm(b - oracle.spmv(A, x)) <= bound * np.linalg.norm(b)
+
+
+@pytest.mark.parametrize("sides", [("none", "none"), ("jacobi", "none"), ("none", "jacobi"), ("jacobi", "jacobi")])
+def test_small_minres_runs_as_one_launch(gpu_lib, oracle, sides):
+    """MINRES in FP64 on a small SELL handle with identity or Jacobi on
+    either side (the 48^3 Dirichlet Laplacian to 1e-10) runs as one
+    cooperative launch: a handful of kernels for the whole solve, the
+    reference's convergence decision and iteration count within 2%, one
+    history entry per step and the true residual at the tolerance."""
+    A = matgen.laplacian_3d_dirichlet(48)
+    n = A.shape()[0]
+    b = oracle.spmv(A, matgen.uniform_vector(n, seed=2))
+    Ad = gpu.Device_matrix(A)
+    specs = [None if p == "none" else "jacobi" for p in sides]
+    ops = [gpu.identity if p is None else gpu.jacobi(Ad) for p in specs]
+    xr, sr = oracle.minres(A, b, np.zeros(n), 1e-10, 3000, left=specs[0], right=specs[1], collect=True)
+    x = np.zeros(n)
+    before = _lib.launch_count()
+    s = gpu.minres(b, x, gpu.Minres_config(1e-10, 3000, True), gpu.spmv(Ad), ops[0], ops[1])
+    launches = _lib.launch_count() - before
+    assert s.converged == sr["converged"] and s.converged
+    assert iters_close(s.computed_iterations, sr["computed_iterations"], "minres"), (
+        s.computed_iterations, sr["computed_iterations"])
+    assert launches < 20, launches
+    assert len(s.iteration_residuals) == s.computed_iterations
+    np.testing.assert_allclose(s.iteration_residuals[0], sr["iteration_residuals"][0], rtol=1e-10)
+    assert np.linalg.norm(b - oracle.spmv(A, x)) <= 1e-9 * np.linalg.norm(b)
