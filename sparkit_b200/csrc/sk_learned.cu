@@ -430,16 +430,23 @@ __global__ void __launch_bounds__(kConvThreads * CS) conv3x3_kernel(const __grid
   }
   __syncthreads();
   asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
-  asm volatile("griddepcontrol.wait;" ::: "memory");
+  // The weights and biases are written only between passes (packing after
+  // an optimizer step), before the first layer of a pass starts, and that
+  // layer starts only after every earlier kernel has completed; so they
+  // are fetched while the previous layer finishes.  The input planes are
+  // the previous layer's output: they wait for it.
   // (a single-channel output has one bias value)
   if (tid < N) s_bias[tid] = a.bias && (a.out_kind == OUT_BF16 || tid == 0) ? __ldg(a.bias + tid) : 0.0f;
   if (tid == 0) {
     mbar_expect_tx(bar_load, TM * S::kPlanes * kPlaneBytes + S::kWBytes);
+    bulk_load(wsm, a.wpk, S::kWBytes, bar_load);
+  }
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  if (tid == 0) {
     for (int t = 0; t < TM; ++t)
       for (int c = 0; c < S::kPlanes; ++c)
         tma_load_4d(planes + (t * S::kPlanes + c) * kPlaneStride, &in_map, c * 8, x0 + t * kTileW - 1, y0 - 1, b,
                     bar_load);
-    bulk_load(wsm, a.wpk, S::kWBytes, bar_load);
   }
   if (tid == 0) ok_load = mbar_wait(bar_load, 0, a.err, 1) ? 1 : 0;
   __syncthreads();
