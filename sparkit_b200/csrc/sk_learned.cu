@@ -448,23 +448,51 @@ __global__ void __launch_bounds__(kConvThreads * CS) conv3x3_kernel(const __grid
         tma_load_4d(planes + (t * S::kPlanes + c) * kPlaneStride, &in_map, c * 8, x0 + t * kTileW - 1, y0 - 1, b,
                     bar_load);
   }
+  // While the tiles arrive: FEAT loads the vector channel of its halo
+  // pixels, (float)(v * (double)(1/d) / s), zero outside the grid (the
+  // convolution's padding) or for s = 0; UP brings the skip vectors that
+  // its epilogue adds into L1.
+  constexpr int kHalo = TM * kHaloH * kHaloW;
+  constexpr int kFeatPer = FEAT ? (kHalo + kConvThreads * CS - 1) / (kConvThreads * CS) : 1;
+  float feat[kFeatPer];
+  if constexpr (FEAT) {
+    const double sb = *a.feat_s;
+#pragma unroll
+    for (int k = 0; k < kFeatPer; ++k) {
+      const int idx = tid + k * kConvThreads * CS;
+      const int t = idx / (kHaloH * kHaloW), h = idx % (kHaloH * kHaloW);
+      const int gy = y0 - 1 + h / kHaloW, gx = x0 + t * kTileW - 1 + h % kHaloW;
+      float f = 0.0f;
+      if (idx < kHalo && gy >= 0 && gy < a.H && gx >= 0 && gx < a.W && sb > 0.0) {
+        const i64 p = static_cast<i64>(gy) * a.W + gx;
+        f = static_cast<float>(a.feat_v[p] * static_cast<double>(a.feat_inv[p]) / sb);
+      }
+      feat[k] = f;
+    }
+  }
+  if constexpr (UP) {
+    const int y = y0 + (px >> 3), x = x0 + (px & 7);
+    if (a.up_skip && y < a.H && x < a.W) {
+#pragma unroll
+      for (int d = 0; d < 4; ++d) {
+        const i64 fp = (static_cast<i64>(b) * 2 * a.H + 2 * y + (d >> 1)) * (2 * a.W) + 2 * x + (d & 1);
+        asm volatile("prefetch.global.L1 [%0];" ::"l"(a.up_skip + fp * N + cbase));
+      }
+    }
+  }
   if (tid == 0) ok_load = mbar_wait(bar_load, 0, a.err, 1) ? 1 : 0;
   __syncthreads();
   const bool ok = ok_load != 0;
   if constexpr (FEAT) {
-    // channel 0 of every halo pixel: (float)(v * (double)(1/d) / s) in BF16,
-    // zero outside the grid (the convolution's padding) or for s = 0
+    // channel 0 of every halo pixel, over the tile copy's (zero) channel 0
     if (ok) {
-      const double sb = *a.feat_s;
-      for (int idx = tid; idx < TM * kHaloH * kHaloW; idx += blockDim.x) {
-        const int t = idx / (kHaloH * kHaloW), h = idx % (kHaloH * kHaloW);
-        const int gy = y0 - 1 + h / kHaloW, gx = x0 + t * kTileW - 1 + h % kHaloW;
-        float f = 0.0f;
-        if (gy >= 0 && gy < a.H && gx >= 0 && gx < a.W && sb > 0.0) {
-          const i64 p = static_cast<i64>(gy) * a.W + gx;
-          f = static_cast<float>(a.feat_v[p] * static_cast<double>(a.feat_inv[p]) / sb);
+#pragma unroll
+      for (int k = 0; k < kFeatPer; ++k) {
+        const int idx = tid + k * kConvThreads * CS;
+        if (idx < kHalo) {
+          const int t = idx / (kHaloH * kHaloW), h = idx % (kHaloH * kHaloW);
+          *reinterpret_cast<bf16*>(planes + t * S::kPlanes * kPlaneStride + h * 16) = __float2bfloat16_rn(feat[k]);
         }
-        *reinterpret_cast<bf16*>(planes + t * S::kPlanes * kPlaneStride + h * 16) = __float2bfloat16_rn(f);
       }
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // visible to the tensor cores
     }
