@@ -73,6 +73,11 @@ def parse():
                    help="the --profile-zipf products on the handle's column-panel copy")
     p.add_argument("--profile-formats", action="store_true",
                    help="run one product of every sweep format and precision (for ncu captures), no timing")
+    p.add_argument("--profile-small-solves", action="store_true",
+                   help="the one-launch FP64 solves twice each: Jacobi-CG on the 256^2 Laplacian, then Jacobi "
+                        "BiCGSTAB, CGS and MINRES (for ncu)")
+    p.add_argument("--profile-batched", action="store_true",
+                   help="the batched CG on 512 of the 4096 systems, twice (for ncu)")
     return p.parse_args()
 
 
@@ -994,6 +999,56 @@ def profile_learned(grid=512, applies=4):
     return 0
 
 
+def profile_small_solves():
+    """The one-launch FP64 solves, each twice (a warm-up, then the captured
+    one): Jacobi-CG on the 256^2 Dirichlet Laplacian (configuration 1),
+    Jacobi BiCGSTAB and CGS on the 256^2 upwind convection-diffusion
+    problem and Jacobi MINRES on the 48^3 Laplacian, all to 1e-10."""
+    import torch
+
+    from sparkit_b200 import gpu, matgen
+    torch.cuda.set_device(0)
+
+    def dev(A, seed):
+        Ad = gpu.Device_matrix(A)
+        b = torch.empty(A.shape()[0], dtype=torch.float64, device="cuda")
+        Ad.spmv(torch.from_numpy(matgen.uniform_vector(A.shape()[0], seed=seed)).cuda(), b)
+        return Ad, gpu.jacobi(Ad), b
+
+    Ad, J, b = dev(matgen.laplacian_2d_dirichlet(256), 0)
+    for _ in range(2):
+        gpu.conjugate_gradient(b, torch.zeros_like(b), gpu.CGConfig(1e-10, 100000, 100000), gpu.spmv(Ad), J)
+    Cd, JC, c = dev(matgen.convection_diffusion_2d(256, 256, 1.0, 0.9, 0.5), 2)
+    for _ in range(2):
+        gpu.bicgstab(c, torch.zeros_like(c), gpu.Bicgstab_config(1e-10, 40000), gpu.spmv(Cd), JC)
+    for _ in range(2):
+        gpu.cgs(c, torch.zeros_like(c), gpu.Cgs_config(1e-10, 40000), gpu.spmv(Cd), JC)
+    Ld, JL, l = dev(matgen.laplacian_3d_dirichlet(48), 2)
+    for _ in range(2):
+        gpu.minres(l, torch.zeros_like(l), gpu.Minres_config(1e-10, 40000), gpu.spmv(Ld), JL)
+    torch.cuda.synchronize()
+    return 0
+
+
+def profile_batched(count=512):
+    """The batched CG (lanes per row 1, 1024 threads per CTA) on the first
+    `count` systems of the configuration-5 batch, twice."""
+    import torch
+
+    from sparkit_b200 import gpu, matgen
+    torch.cuda.set_device(0)
+    offs, rp, ci, v, kinds = matgen.batched_spd_systems(4096, seed=0)
+    e = int(offs[count])
+    B = gpu.Batch(offs[:count + 1], rp[:e + 1], ci[:rp[e]], v[:rp[e]])
+    bd = torch.from_numpy(matgen.uniform_vector(int(offs[-1]), seed=1)[:e]).cuda()
+    cfg = gpu.Batch_config(lanes_per_row=1, threads_per_cta=1024)
+    for _ in range(2):
+        xd = torch.zeros_like(bd)
+        B.solve(bd, xd, cfg)
+    torch.cuda.synchronize()
+    return 0
+
+
 def profile_mixed(grid, inner=100, diagonals=False):
     """One outer step of the mixed solver on the GRF diffusion problem with
     `inner` persistent FP32 inner iterations, twice (warm-up, then the
@@ -1077,6 +1132,10 @@ def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
+    if args.profile_small_solves:
+        return profile_small_solves()
+    if args.profile_batched:
+        return profile_batched()
     if args.profile_formats:
         return profile_formats(args.grid)
     if args.profile_zipf or args.profile_zipf_panels:
