@@ -98,9 +98,36 @@ __device__ __forceinline__ void cta_sum(double (&v)[NR], double (*smem)[4]) {
 }
 
 // y_i = (A v)_i over the system's rows [r0, r0 + n); v indexed locally.
-// Row sums in FP32 (the inner method's precision).  G lanes per row.
+// Row sums in FP32 (the inner method's precision).  G lanes per row.  With
+// one lane per row the first kE entries of a row are loaded at once (their
+// columns and values, then their gathers), so that a short stencil row
+// costs three memory round trips instead of one per entry; the sum is
+// still taken entry after entry in storage order.
 template <int G, int NT, class Out>
 __device__ __forceinline__ void sys_spmv32(const BatchView& bv, int r0, int n, const float* v, Out&& out) {
+  if constexpr (G == 1) {
+    constexpr int kE = 8;
+    for (int i = threadIdx.x; i < n; i += NT) {
+      const int a = __ldg(bv.rp + r0 + i), e = __ldg(bv.rp + r0 + i + 1);
+      int c[kE];
+      float w[kE];
+#pragma unroll
+      for (int j = 0; j < kE; ++j) {
+        c[j] = a + j < e ? __ldg(bv.col + a + j) : r0;
+        w[j] = a + j < e ? __ldg(bv.val + a + j) : 0.0f;
+      }
+      float x[kE];
+#pragma unroll
+      for (int j = 0; j < kE; ++j) x[j] = v[c[j] - r0];
+      float sum = 0.0f;
+#pragma unroll
+      for (int j = 0; j < kE; ++j)
+        if (a + j < e) sum = __fadd_rn(sum, __fmul_rn(w[j], x[j]));
+      for (int k = a + kE; k < e; ++k) sum = __fadd_rn(sum, __fmul_rn(__ldg(bv.val + k), v[__ldg(bv.col + k) - r0]));
+      out(i, sum);
+    }
+    return;
+  }
   constexpr int ROWS = NT / G;
   const int lane = threadIdx.x & (G - 1);
   for (int base = 0; base < n; base += ROWS) {
@@ -117,7 +144,7 @@ __device__ __forceinline__ void sys_spmv32(const BatchView& bv, int r0, int n, c
 }
 
 template <int G, int NT>
-__global__ void __launch_bounds__(NT) batched_cg_kernel(BatchView bv, BatchArgs ar) {
+__global__ void __launch_bounds__(NT, 1024 / NT) batched_cg_kernel(BatchView bv, BatchArgs ar) {
   __shared__ double red[NT / 32][4];
   __shared__ int s_q;
   float* r = ar.ws32 + static_cast<i64>(blockIdx.x) * ar.slot32;
@@ -203,12 +230,32 @@ __global__ void __launch_bounds__(NT) batched_cg_kernel(BatchView bv, BatchArgs 
           cta_sum<NT, 1>(pq, red);
           const float alpha = rz / static_cast<float>(pq[0]);
           double s2[2] = {0.0, 0.0};
-          for (int i = tid; i < n; i += NT) {
-            d[i] = __fadd_rn(__fmul_rn(alpha, p[i]), d[i]);
-            const float ri = __fsub_rn(r[i], __fmul_rn(alpha, q[i]));
-            r[i] = ri;
-            s2[0] += static_cast<double>(__fmul_rn(ri, ri));
-            s2[1] += static_cast<double>(__fmul_rn(ri, __fmul_rn(dinv[i], ri)));
+          // four elements' operands loaded before any is written (the
+          // terms still summed in element order)
+          for (int i0 = tid; i0 < n; i0 += 4 * NT) {
+            float pv[4], dv[4], rv[4], qv[4], iv[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+              const int i = i0 + u * NT;
+              if (i < n) {
+                pv[u] = p[i];
+                dv[u] = d[i];
+                rv[u] = r[i];
+                qv[u] = q[i];
+                iv[u] = dinv[i];
+              }
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+              const int i = i0 + u * NT;
+              if (i < n) {
+                d[i] = __fadd_rn(__fmul_rn(alpha, pv[u]), dv[u]);
+                const float ri = __fsub_rn(rv[u], __fmul_rn(alpha, qv[u]));
+                r[i] = ri;
+                s2[0] += static_cast<double>(__fmul_rn(ri, ri));
+                s2[1] += static_cast<double>(__fmul_rn(ri, __fmul_rn(iv[u], ri)));
+              }
+            }
           }
           cta_sum<NT, 2>(s2, red);
           ++inner_total;
@@ -216,7 +263,23 @@ __global__ void __launch_bounds__(NT) batched_cg_kernel(BatchView bv, BatchArgs 
           const float rz_new = static_cast<float>(s2[1]);
           const float beta = rz_new / rz;
           rz = rz_new;
-          for (int i = tid; i < n; i += NT) p[i] = __fadd_rn(__fmul_rn(dinv[i], r[i]), __fmul_rn(beta, p[i]));
+          for (int i0 = tid; i0 < n; i0 += 4 * NT) {
+            float iv[4], rv[4], pv[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+              const int i = i0 + u * NT;
+              if (i < n) {
+                iv[u] = dinv[i];
+                rv[u] = r[i];
+                pv[u] = p[i];
+              }
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+              const int i = i0 + u * NT;
+              if (i < n) p[i] = __fadd_rn(__fmul_rn(iv[u], rv[u]), __fmul_rn(beta, pv[u]));
+            }
+          }
         }
         __syncthreads();
         for (int i = tid; i < n; i += NT) x[i] += rn * static_cast<double>(d[i]);
