@@ -86,20 +86,37 @@ struct OpJacobiAdd {
   __device__ void finalize(const double*) const {}
 };
 
-// rc[I] = sum of t over aggregate I, in a fixed order (thread-strided
-// partial sums, then the block tree).
-__global__ void __launch_bounds__(kThreads) restrict_kernel(int nx, int agg, int mcx, const double* __restrict__ t,
-                                                            double* __restrict__ rc, const Scalars* sc) {
+// rc[I] = sum of t over aggregate I, in the order of a 256-thread block
+// reduction (thread T adds cells T, T + 256, ... from zero; a butterfly
+// over each warp of 32 threads; a butterfly over the 8 warp sums), computed
+// by one warp per aggregate: lane l plays threads l, l + 32, ..., l + 224.
+__global__ void __launch_bounds__(kThreads) restrict_kernel(int nx, int agg, int mcx, int nc,
+                                                            const double* __restrict__ t, double* __restrict__ rc,
+                                                            const Scalars* sc) {
+  constexpr int kW = kThreads / 32;
   if (solve_done(sc)) return;
-  const int I = blockIdx.x;
+  const int I = blockIdx.x * kW + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (I >= nc) return;
   const int X0 = (I % mcx) * agg, Y0 = (I / mcx) * agg;
-  double v[1] = {0.0};
-  for (int c = threadIdx.x; c < agg * agg; c += kThreads) {
-    const int dy = c / agg, dx = c % agg;
-    v[0] += t[static_cast<i64>(Y0 + dy) * nx + X0 + dx];
+  const int cells = agg * agg;
+  double v[kW];
+#pragma unroll
+  for (int w = 0; w < kW; ++w) v[w] = 0.0;
+  for (int c0 = 0; c0 < cells; c0 += kThreads) {
+#pragma unroll
+    for (int w = 0; w < kW; ++w) {
+      const int c = c0 + 32 * w + lane;
+      if (c < cells) v[w] += t[static_cast<i64>(Y0 + c / agg) * nx + X0 + c % agg];
+    }
   }
-  block_reduce<1>(v);
-  if (threadIdx.x == 0) rc[I] = v[0];
+  warp_reduce<kW>(v);
+  double x[1] = {0.0};
+#pragma unroll
+  for (int w = 0; w < kW; ++w)
+    if (lane == w) x[0] = v[w];
+  warp_reduce<1>(x);
+  if (lane == 0) rc[I] = x[0];
 }
 
 // zc = Ainv rc: one warp per coarse row, lane-strided partial sums and a
@@ -107,7 +124,8 @@ __global__ void __launch_bounds__(kThreads) restrict_kernel(int nx, int agg, int
 // the bytes of the FP64 inverse, and within the L2) and every product is
 // formed and summed in FP64; the float rounding of the inverse (relative
 // 6e-8 per entry) perturbs the coarse correction of a preconditioner only.
-// Each lane reads four consecutive floats (16 bytes) per step.
+// Each lane reads four consecutive floats (16 bytes) per step, four steps'
+// loads in flight before their products are summed (in step order).
 __global__ void __launch_bounds__(kThreads) coarse_gemv_kernel(int nc, const float* __restrict__ ainv,
                                                                const double* __restrict__ rc,
                                                                double* __restrict__ zc, const Scalars* sc) {
@@ -119,10 +137,23 @@ __global__ void __launch_bounds__(kThreads) coarse_gemv_kernel(int nc, const flo
   double s[1] = {0.0};
   int j = 4 * lane;
   if ((nc & 3) == 0) {
-    for (; j < nc; j += 128) {
-      const float4 a = __ldg(reinterpret_cast<const float4*>(row + j));
-      s[0] += static_cast<double>(a.x) * rc[j] + static_cast<double>(a.y) * rc[j + 1] +
-              static_cast<double>(a.z) * rc[j + 2] + static_cast<double>(a.w) * rc[j + 3];
+    for (; j < nc; j += 512) {
+      float4 a[4];
+      double r[4][4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int jj = j + 128 * u;
+        if (jj < nc) {
+          a[u] = __ldg(reinterpret_cast<const float4*>(row + jj));
+#pragma unroll
+          for (int k = 0; k < 4; ++k) r[u][k] = rc[jj + k];
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+        if (j + 128 * u < nc)
+          s[0] += static_cast<double>(a[u].x) * r[u][0] + static_cast<double>(a[u].y) * r[u][1] +
+                  static_cast<double>(a[u].z) * r[u][2] + static_cast<double>(a[u].w) * r[u][3];
     }
   } else {
     for (j = lane; j < nc; j += 32) s[0] += static_cast<double>(row[j]) * rc[j];
@@ -207,7 +238,7 @@ void twolevel_apply(const sk_precond_s* M, const double* r, double* z, RedWs ws,
   const int nc = static_cast<int>(M->coarse_n);
   const sk_precond_s* S = M->smoother;
   auto coarse = [&](const double* t, int set) {  // z (+)= P Ac^-1 P^T t
-    SK_LAUNCH(restrict_kernel, nc, kThreads, 0, st, nx, agg, mcx, t, M->rc, sc);
+    SK_LAUNCH(restrict_kernel, ceil_div(nc, kThreads / 32), kThreads, 0, st, nx, agg, mcx, nc, t, M->rc, sc);
     SK_LAUNCH(coarse_gemv_kernel, ceil_div(nc, kThreads / 32), kThreads, 0, st, nc,
               M->coarse_inv, M->rc, M->zc, sc);
     SK_LAUNCH(prolong_kernel, ew_blocks(n), kThreads, 0, st, n, nx, agg, mcx, M->zc, nullptr, set, z, sc);
