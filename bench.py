@@ -78,6 +78,9 @@ def parse():
                         "BiCGSTAB, CGS and MINRES (for ncu)")
     p.add_argument("--profile-batched", action="store_true",
                    help="the batched CG on 512 of the 4096 systems, twice (for ncu)")
+    p.add_argument("--profile-c4", action="store_true",
+                   help="60 FGMRES(30) iterations with the two-level preconditioner and an untrained network "
+                        "smoother on the 512^2 problem, then 60 with two-level Jacobi (for an ncu launch list)")
     return p.parse_args()
 
 
@@ -1030,6 +1033,26 @@ def profile_small_solves():
     return 0
 
 
+def profile_c4(grid=512, iters=60):
+    """Two FGMRES(30) cycles on the configuration-4 matrix with the two-level
+    preconditioner (aggregates of 8 x 8 cells), first with a network
+    smoother (untrained weights: the kernels' work does not depend on
+    them), then with Jacobi, for a per-iteration launch list."""
+    import torch
+
+    from sparkit_b200 import gpu, matgen
+    torch.cuda.set_device(0)
+    A, _ = matgen.convdiff_2d_grf(grid, seed=777)
+    Ad = gpu.Device_matrix(A)
+    b = torch.from_numpy(np.random.default_rng(3).uniform(-1, 1, grid * grid)).cuda()
+    L = gpu.learned_preconditioner(Ad, gpu.Net(seed=1), grid, grid)
+    for M in (gpu.twolevel(Ad, L, grid, grid, 8, coarse_first=True), gpu.twolevel(Ad, gpu.jacobi(Ad), grid, grid, 8)):
+        x = torch.zeros_like(b)
+        gpu.fgmres(b, x, gpu.Fgmres_config(1e-14, 30, iters), gpu.spmv(Ad), M)
+    torch.cuda.synchronize()
+    return 0
+
+
 def profile_batched(count=512):
     """The batched CG (lanes per row 1, 1024 threads per CTA) on the first
     `count` systems of the configuration-5 batch, twice."""
@@ -1136,6 +1159,8 @@ def main():
         return profile_small_solves()
     if args.profile_batched:
         return profile_batched()
+    if args.profile_c4:
+        return profile_c4()
     if args.profile_formats:
         return profile_formats(args.grid)
     if args.profile_zipf or args.profile_zipf_panels:

@@ -120,3 +120,32 @@ def test_debug_set_wait_limits(gpu_lib):
     with pytest.raises(_lib.SkError):
         gpu.debug_set_wait(11_000_000_000, False)
     gpu.debug_set_wait(0, False)
+
+
+@pytest.mark.parametrize("solver", ["cg", "bicgstab", "cgs", "minres"])
+def test_one_launch_solver_barrier_timeout(gpu_lib, oracle, solver):
+    """The FP64 solves that run whole in one cooperative launch wait at
+    bounded grid barriers: with an unmeetable target and a 1 ms limit the
+    kernel gives up, the call reports SK_TIMEOUT, and the same handle then
+    solves normally."""
+    A = matgen.convection_diffusion_2d(48, 48, 1.0, 0.9, 0.5) if solver in ("bicgstab", "cgs") \
+        else matgen.laplacian_2d_dirichlet(48)
+    n = A.shape()[0]
+    b = oracle.spmv(A, matgen.uniform_vector(n, seed=2))
+    Ad = gpu.Device_matrix(A)
+    J = gpu.jacobi(Ad)
+    run = {"cg": lambda x: gpu.conjugate_gradient(b, x, gpu.CGConfig(1e-10, 3000, 3000), gpu.spmv(Ad), J),
+           "bicgstab": lambda x: gpu.bicgstab(b, x, gpu.Bicgstab_config(1e-10, 3000), gpu.spmv(Ad), J),
+           "cgs": lambda x: gpu.cgs(b, x, gpu.Cgs_config(1e-10, 3000), gpu.spmv(Ad), J),
+           "minres": lambda x: gpu.minres(b, x, gpu.Minres_config(1e-10, 3000), gpu.spmv(Ad), J)}[solver]
+    gpu.debug_set_wait(1_000_000, True)
+    try:
+        with pytest.raises(_lib.SkError) as e:
+            run(np.zeros(n))
+        assert e.value.status == SK_TIMEOUT and "barrier" in str(e.value)
+    finally:
+        gpu.debug_set_wait(0, False)
+    x = np.zeros(n)
+    s = run(x)
+    assert s.converged
+    assert np.linalg.norm(b - oracle.spmv(A, x)) <= 1e-8 * np.linalg.norm(b)
