@@ -38,6 +38,11 @@
 //     warps read the accumulator back with tcgen05.ld (thread = pixel) and
 //     apply bias, ReLU or the ReLU mask of the backward pass, and store
 //     16-byte vectors.
+//   * Variants: two tiles per CTA for the full-resolution 16-channel layers
+//     (one wave of resident CTAs at 512^2), two threads per pixel for the
+//     upsample-and-add epilogues, and a first layer that computes the
+//     vector's feature channel into its staged planes (the matrix's fixed
+//     channels are built once per preconditioner).
 // The weight gradient (training only) is a GEMM over pixels with
 // mma.sync.m16n8k16 on the same staged planes.
 #include <cuda.h>
