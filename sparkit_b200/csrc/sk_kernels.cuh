@@ -987,16 +987,18 @@ inline int spmv_grid(const sk_matrix_s* A) {
 
 // Row-loop variants per value type, as measured on B200 (3-D 7-point
 // Laplacian, 128^3): FP64 rows run fastest as rounds of 4 plus a serial tail
-// at 8 CTAs per SM (32 registers); FP32 SELL rows as predicated rounds of 8
-// at 6 CTAs per SM.  A fused reduction needs more registers, so those
-// kernels are bounded at 6 CTAs per SM.  Every variant sums each row in the
-// same order, so the choice never changes a result.
+// at 8 CTAs per SM (32 registers, with or without a fused reduction, no
+// spills: so a 262,144-row product with a reduction is one wave of 1024
+// CTAs, not 888 and a tail); FP32 SELL rows as predicated rounds of 8 at 5
+// CTAs per SM.  The general CSR kernel with a fused reduction needs more
+// registers and is bounded at 6 CTAs per SM.  Every variant sums each row in
+// the same order, so the choice never changes a row's result.
 template <typename T, class Epi>
 struct SpmvTune {
   static constexpr int kMinB = Epi::kNR > 0 ? 6 : 8;
   static constexpr int kSellU = sizeof(T) == 8 ? 4 : 8;
   static constexpr bool kSellPred = sizeof(T) != 8;
-  static constexpr int kSellMinB = sizeof(T) == 8 ? kMinB : 5;
+  static constexpr int kSellMinB = sizeof(T) == 8 ? 8 : 5;
   // the diagonal kernel runs the SELL grid at the SELL residency, so that
   // a fused reduction sums the same rows in the same CTAs (the same bits)
   static constexpr int kDiaMinB = kSellMinB;
