@@ -1045,6 +1045,9 @@ struct OpFgMgs {
   }
 };
 
+// Columns of up to this many rotations are rotated in thread-local arrays.
+constexpr int kFgLocal = 64;
+
 // apply_givens_rotations (:287-337), record_residual (:340-346),
 // check_convergence (:349-356), in the value type T.
 template <typename T>
@@ -1053,7 +1056,70 @@ struct FgGivens {
   double* hist;
   FgSmall sm;
   int j, m;
+  // The same steps with every operand (the column, the earlier rotations,
+  // g_j, g_j+1 and the solve's scalars) loaded in one batch, so that the
+  // single thread waits on memory once instead of once per rotation.
+  __device__ void local_path() const {
+    const int um1 = m + 1;
+    const int done = sc->done, hon = sc->hist_on;
+    const long long it = sc->iters, hl = sc->hist_len;
+    const double bnorm = sc->bnorm, tol = sc->tol;
+    double hc[kFgLocal + 2], cv[kFgLocal], sv[kFgLocal];
+    for (int i = 0; i <= j + 1; ++i) hc[i] = sm.H[i + j * um1];
+    for (int i = 0; i < j; ++i) {
+      cv[i] = sm.cs[i];
+      sv[i] = sm.sn[i];
+    }
+    const double g0 = sm.g[j], g1 = sm.g[j + 1];
+    if (done) return;
+    for (int i = 0; i < j; ++i) {
+      const T cs = static_cast<T>(cv[i]), sn = static_cast<T>(sv[i]);
+      const T hij = static_cast<T>(hc[i]), hi1 = static_cast<T>(hc[i + 1]);
+      const T temp = add(mul(cs, hij), mul(sn, hi1));
+      hc[i + 1] = static_cast<double>(add(mul(-sn, hij), mul(cs, hi1)));
+      hc[i] = static_cast<double>(temp);
+    }
+    const T a = static_cast<T>(hc[j]), bb = static_cast<T>(hc[j + 1]);
+    T cs, sn;
+    if (bb == T(0)) {
+      cs = T(1);
+      sn = T(0);
+    } else if (a == T(0)) {
+      cs = T(0);
+      sn = T(1);
+    } else {
+      const T rr = sqrt(add(mul(a, a), mul(bb, bb)));
+      cs = dvd(a, rr);
+      sn = dvd(bb, rr);
+    }
+    sm.cs[j] = static_cast<double>(cs);
+    sm.sn[j] = static_cast<double>(sn);
+    hc[j] = static_cast<double>(add(mul(cs, a), mul(sn, bb)));
+    hc[j + 1] = 0.0;
+    for (int i = 0; i <= j + 1; ++i) sm.H[i + j * um1] = hc[i];
+    const T gj = static_cast<T>(g0), gj1 = static_cast<T>(g1);
+    const T temp = add(mul(cs, gj), mul(sn, gj1));
+    const double gn = static_cast<double>(add(mul(-sn, gj), mul(cs, gj1)));
+    sm.g[j + 1] = gn;
+    sm.g[j] = static_cast<double>(temp);
+    sc->iters = it + 1;
+    sc->jfinal = j;
+    const T absres = fabs(static_cast<T>(gn));
+    sc->rnorm = static_cast<double>(absres);  // record()
+    if (hon) {
+      hist[hl] = static_cast<double>(absres);
+      sc->hist_len = hl + 1;
+    }
+    if (absres / static_cast<T>(bnorm) < static_cast<T>(tol)) {
+      sc->converged = 1;
+      sc->done = 1;
+    }
+  }
   __device__ void operator()() const {
+    if (j < kFgLocal) {
+      local_path();
+      return;
+    }
     if (sc->done) return;
     const int um1 = m + 1;
     auto H = [&](int r, int c) -> double& { return sm.H[r + c * um1]; };
